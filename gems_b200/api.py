@@ -1,0 +1,309 @@
+"""Python binding of the C-ABI (ctypes).  Method names of :class:`PhyloTree` follow the
+reference's PhyloTree (tree/phylotree.h) so callers and tests read like IQ-TREE code."""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, byref, c_double, c_int, c_longlong, c_size_t, c_uint16, c_void_p
+
+import numpy as np
+
+from . import _lib
+
+STATUS = {0: "OK", 1: "OOM", 2: "ADMISSION_REJECTED", 3: "NUMERIC_UNDERFLOW", 4: "TIMEOUT",
+          5: "BAD_ARG", 6: "CUDA", 7: "STATE", 8: "NO_DEVICE"}
+GEMS_CHILD_TIP = 0
+GEMS_CHILD_PARTIAL = 1
+PREC = {"fp64": 0, "mixed": 1}
+SCALING = {"norm": 0, "safe": 1}
+
+
+class GemsError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        msg = _lib.gems().gems_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS.get(status, status)} ({msg})")
+
+
+def _check(st: int, where: str):
+    if st != 0:
+        raise GemsError(st, where)
+
+
+class SessionDesc(ctypes.Structure):
+    _fields_ = [("ntaxa", c_int), ("nptn", c_int), ("nstates", c_int), ("ncat", c_int),
+                ("nslots", c_int), ("precision", c_int), ("scaling", c_int), ("device", c_int)]
+
+
+class Op(ctypes.Structure):
+    _fields_ = [("dst_slot", c_int), ("left_kind", c_int), ("left_id", c_int),
+                ("right_kind", c_int), ("right_id", c_int), ("pad_", c_int),
+                ("left_len", c_double), ("right_len", c_double)]
+
+
+class Branch(ctypes.Structure):
+    _fields_ = [("dad_slot", c_int), ("node_kind", c_int), ("node_id", c_int), ("pad_", c_int),
+                ("length", c_double)]
+
+
+def op_array(ops):
+    """ops: iterable of (dst, lkind, lid, rkind, rid, llen, rlen)."""
+    ops = list(ops)
+    arr = (Op * max(1, len(ops)))()
+    for i, (d, lk, li, rk, ri, ll, rl) in enumerate(ops):
+        arr[i] = Op(d, lk, li, rk, ri, 0, ll, rl)
+    return arr, len(ops)
+
+
+def branch_struct(dad_slot, node_kind, node_id, length):
+    return Branch(dad_slot, node_kind, node_id, 0, length)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(c_void_p) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Session:
+    """A device session: tips, pattern weights, model and partial slots resident in HBM."""
+
+    def __init__(self, ntaxa, nptn, nstates, ncat, nslots, precision="fp64", scaling="norm",
+                 device=0):
+        self.lib = _lib.gems()
+        self.desc = SessionDesc(ntaxa, nptn, nstates, ncat, nslots, PREC[precision],
+                                SCALING[scaling], device)
+        self.handle = c_void_p()
+        _check(self.lib.gems_session_create(byref(self.desc), byref(self.handle)),
+               "gems_session_create")
+        self.ntaxa, self.nptn, self.nstates, self.ncat = ntaxa, nptn, nstates, ncat
+        self.block = nstates * ncat
+        self.safe = scaling == "safe"
+
+    @staticmethod
+    def footprint(ntaxa, nptn, nstates, ncat, nslots, precision="fp64", scaling="norm"):
+        d = SessionDesc(ntaxa, nptn, nstates, ncat, nslots, PREC[precision], SCALING[scaling], 0)
+        out = c_size_t()
+        _check(_lib.gems().gems_session_footprint(byref(d), byref(out)), "footprint")
+        return out.value
+
+    def close(self):
+        if self.handle:
+            self.lib.gems_session_destroy(self.handle)
+            self.handle = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload_tips(self, states):
+        st = np.ascontiguousarray(states, dtype=np.uint8)
+        assert st.shape == (self.ntaxa, self.nptn)
+        _check(self.lib.gems_upload_tips(self.handle, _dptr(st)), "gems_upload_tips")
+
+    def upload_patterns(self, freq, invar=None):
+        f = _f64(freq)
+        iv = None if invar is None else _f64(invar)
+        _check(self.lib.gems_upload_patterns(self.handle, _dptr(f), _dptr(iv)),
+               "gems_upload_patterns")
+
+    def set_model(self, eval_, evec, inv_evec, rates, props):
+        arrs = [_f64(x) for x in (eval_, evec, inv_evec, rates, props)]
+        _check(self.lib.gems_set_model(self.handle, *[_dptr(a) for a in arrs]), "gems_set_model")
+
+    def set_model_from_rates(self, exch_upper, freq, rates, props):
+        arrs = [_f64(x) for x in (exch_upper, freq, rates, props)]
+        _check(self.lib.gems_set_model_from_rates(self.handle, *[_dptr(a) for a in arrs]),
+               "gems_set_model_from_rates")
+
+    def eigensystem(self):
+        n = self.nstates
+        ev, v, iv = np.zeros(n), np.zeros((n, n)), np.zeros((n, n))
+        _check(self.lib.gems_get_eigensystem(self.handle, _dptr(ev), _dptr(v), _dptr(iv)),
+               "gems_get_eigensystem")
+        return ev, v, iv
+
+    def traverse(self, ops):
+        arr, n = op_array(ops)
+        _check(self.lib.gems_traverse(self.handle, arr, n), "gems_traverse")
+
+    def branch_lnl(self, ops, br, pattern_lh=False):
+        arr, n = op_array(ops)
+        out = c_double()
+        plh = np.zeros(self.nptn) if pattern_lh else None
+        _check(self.lib.gems_branch_lnl(self.handle, arr, n, byref(br), byref(out), _dptr(plh)),
+               "gems_branch_lnl")
+        return (out.value, plh) if pattern_lh else out.value
+
+    def branch_derv(self, ops, br, compute_theta=True, df_frac=False):
+        arr, n = op_array(ops)
+        df, ddf = c_double(), c_double()
+        g = np.zeros(self.nptn) if df_frac else None
+        _check(self.lib.gems_branch_derv(self.handle, arr, n, byref(br), int(compute_theta),
+                                         byref(df), byref(ddf), _dptr(g)), "gems_branch_derv")
+        return (df.value, ddf.value, g) if df_frac else (df.value, ddf.value)
+
+    def lnl_from_buffer(self, length, pattern_lh=False):
+        out = c_double()
+        plh = np.zeros(self.nptn) if pattern_lh else None
+        _check(self.lib.gems_lnl_from_buffer(self.handle, c_double(length), byref(out),
+                                             _dptr(plh)), "gems_lnl_from_buffer")
+        return (out.value, plh) if pattern_lh else out.value
+
+    def newton_branch(self, ops, br, compute_theta, min_len, max_len, xacc, max_steps):
+        arr, n = op_array(ops)
+        opt, nev = c_double(), c_int()
+        _check(self.lib.gems_newton_branch(self.handle, arr, n, byref(br), int(compute_theta),
+                                           c_double(min_len), c_double(max_len), c_double(xacc),
+                                           max_steps, byref(opt), byref(nev)),
+               "gems_newton_branch")
+        return opt.value, nev.value
+
+    def get_partial(self, slot):
+        part = np.zeros((self.nptn, self.ncat, self.nstates))
+        per = self.ncat if self.safe else 1
+        sc = np.zeros(self.nptn * per, np.uint16)
+        _check(self.lib.gems_get_partial(self.handle, slot, _dptr(part), _dptr(sc)),
+               "gems_get_partial")
+        return part, (sc.reshape(self.nptn, per) if self.safe else sc)
+
+    def get_theta(self):
+        th = np.zeros((self.nptn, self.block))
+        sa = np.zeros(self.nptn)
+        _check(self.lib.gems_get_theta(self.handle, _dptr(th), _dptr(sa)), "gems_get_theta")
+        return th, sa
+
+    def launch_count(self):
+        n = c_longlong()
+        _check(self.lib.gems_launch_count(self.handle, byref(n)), "gems_launch_count")
+        return n.value
+
+    def stream_handle(self):
+        p = c_void_p()
+        _check(self.lib.gems_session_stream(self.handle, byref(p)), "gems_session_stream")
+        return p.value or 0
+
+    def profile(self, on=True):
+        _check(self.lib.gems_profile_enable(self.handle, int(on)), "gems_profile_enable")
+
+    def profile_read(self, kernel_id):
+        """(total_ms, launches) of kernel_id (0 traverse, 1 branch, 2 theta, 3 derv,
+        4 from-buffer, 5 newton) since the last read."""
+        ms, n = c_double(), c_longlong()
+        _check(self.lib.gems_profile_read(self.handle, kernel_id, byref(ms), byref(n)),
+               "gems_profile_read")
+        return ms.value, n.value
+
+    def sync(self):
+        _check(self.lib.gems_session_sync(self.handle), "gems_session_sync")
+
+
+class PhyloTree:
+    """PhyloTree calls of the likelihood path on a device session (C++ mirror in
+    csrc/phylotree.cpp)."""
+
+    def __init__(self, session: Session, eu, ev, lengths):
+        self.session = session
+        self.lib = session.lib
+        self.eu = np.ascontiguousarray(eu, np.int32)
+        self.ev = np.ascontiguousarray(ev, np.int32)
+        ln = _f64(lengths)
+        self.handle = c_void_p()
+        _check(self.lib.gems_tree_create(session.handle, len(self.eu), _dptr(self.eu),
+                                         _dptr(self.ev), _dptr(ln), byref(self.handle)),
+               "gems_tree_create")
+
+    @classmethod
+    def from_case(cls, tree, model, aln, precision="fp64", scaling="norm", device=0,
+                  slots="node", invar=None):
+        """Session + tree for a synthetic case (synth.Tree, synth.Model, synth.Alignment)."""
+        nint = tree.ntaxa - 2
+        nslots = nint if slots == "node" else 3 * nint
+        s = Session(tree.ntaxa, aln.npat, model.nstates, model.ncat, nslots, precision,
+                    scaling, device)
+        s.upload_tips(aln.patterns)
+        s.upload_patterns(aln.weights, invar)
+        s.set_model(model.eval, model.evec, model.inv_evec, model.rates, model.props)
+        return cls(s, tree.eu, tree.ev, tree.length)
+
+    def close(self):
+        if self.handle:
+            self.lib.gems_tree_destroy(self.handle)
+            self.handle = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference API names --
+    def setBranchLimits(self, min_len, max_len):
+        _check(self.lib.gems_tree_set_branch_limits(self.handle, c_double(min_len),
+                                                    c_double(max_len)), "set_branch_limits")
+
+    def setLength(self, u, v, x):
+        _check(self.lib.gems_tree_set_length(self.handle, u, v, c_double(x)), "set_length")
+
+    def getBranchLengths(self):
+        out = np.zeros(len(self.eu))
+        _check(self.lib.gems_tree_get_lengths(self.handle, _dptr(out)), "get_lengths")
+        return out
+
+    def clearAllPartialLH(self):
+        _check(self.lib.gems_tree_clear_all_partial_lh(self.handle), "clearAllPartialLH")
+
+    def computeLikelihood(self, pattern_lh=False):
+        out = c_double()
+        plh = np.zeros(self.session.nptn) if pattern_lh else None
+        _check(self.lib.gems_tree_compute_likelihood(self.handle, byref(out), _dptr(plh)),
+               "computeLikelihood")
+        return (out.value, plh) if pattern_lh else out.value
+
+    def computeLikelihoodBranch(self, node, dad, pattern_lh=False):
+        out = c_double()
+        plh = np.zeros(self.session.nptn) if pattern_lh else None
+        _check(self.lib.gems_tree_compute_likelihood_branch(self.handle, node, dad, byref(out),
+                                                            _dptr(plh)),
+               "computeLikelihoodBranch")
+        return (out.value, plh) if pattern_lh else out.value
+
+    def computeLikelihoodDerv(self, node, dad):
+        df, ddf = c_double(), c_double()
+        _check(self.lib.gems_tree_compute_likelihood_derv(self.handle, node, dad, byref(df),
+                                                          byref(ddf)), "computeLikelihoodDerv")
+        return df.value, ddf.value
+
+    def computeLikelihoodFromBuffer(self):
+        out = c_double()
+        _check(self.lib.gems_tree_compute_likelihood_from_buffer(self.handle, byref(out)),
+               "computeLikelihoodFromBuffer")
+        return out.value
+
+    def optimizeOneBranch(self, node1, node2, clearLH=True, maxNRStep=100):
+        _check(self.lib.gems_tree_optimize_one_branch(self.handle, node1, node2, int(clearLH),
+                                                      maxNRStep), "optimizeOneBranch")
+
+    def optimizeAllBranches(self, my_iterations=100, tolerance=0.001, maxNRStep=100):
+        out = c_double()
+        _check(self.lib.gems_tree_optimize_all_branches(self.handle, my_iterations,
+                                                        c_double(tolerance), maxNRStep,
+                                                        byref(out)), "optimizeAllBranches")
+        return out.value
+
+    def getPartial(self, node, dad):
+        s = self.session
+        part = np.zeros((s.nptn, s.ncat, s.nstates))
+        per = s.ncat if s.safe else 1
+        sc = np.zeros(s.nptn * per, np.uint16)
+        _check(self.lib.gems_tree_get_partial(self.handle, node, dad, _dptr(part), _dptr(sc)),
+               "getPartial")
+        return part, (sc.reshape(s.nptn, per) if s.safe else sc)
+
+    def stats(self):
+        ops, nev = c_longlong(), c_int()
+        _check(self.lib.gems_tree_stats(self.handle, byref(ops), byref(nev)), "stats")
+        return ops.value, nev.value

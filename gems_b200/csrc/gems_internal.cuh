@@ -1,0 +1,138 @@
+// gems_internal.cuh -- device-session state shared by the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/gems_b200.h"
+
+namespace gems {
+
+// 2^-256 underflow threshold and its log (tree/phylotree.h:61-80)
+constexpr double kScaleThr = 8.636168555094444625386e-78;
+constexpr int kScaleExp = 256;
+constexpr double kLogScaleThr = -177.4456782233459932741;
+// mixed precision (FP32 real-space partials): rescale by 2^64 below 2^-64
+constexpr float kScaleThrF = 5.421010862427522e-20f;  // 2^-64
+constexpr int kScaleExpF = 64;
+constexpr double kLogScaleThrF = -44.361419555836498;  // 64 * log(2) negated
+
+constexpr int kMaxStates = 64;
+constexpr int kMaxCat = 16;
+
+// device copy of gems_op (same layout)
+struct DevOp {
+  int dst_slot;
+  int l_kind, l_id;
+  int r_kind, r_id;
+  int pad_;
+  double l_len, r_len;
+};
+static_assert(sizeof(DevOp) == sizeof(gems_op), "op layout");
+
+// per-launch view of a session, passed by value to kernels
+struct DevCtx {
+  int P;         // padded pattern count (multiple of 32)
+  int nptn;      // real pattern count
+  int n, C, block, G;  // states, categories, C*n, lanes per pattern (pow2 >= C)
+  int unknown;   // STATE_UNKNOWN
+  int safe;
+  const uint8_t *tips;   // [ntaxa][P]
+  const double *freq;    // [P]
+  const double *invar;   // [P]
+  void *partials;        // [nslots][P][block]  (double, or float in mixed)
+  uint16_t *scale;       // [nslots][P * (safe ? C : 1)]
+  const double *inv_evec;  // [n][n]
+  const double *evec;      // [n][n]
+  const double *eval;      // [n]
+  const double *rates;     // [C]
+  const double *props;     // [C]
+  const double *tip;       // [(unknown+1)][n] eigen-space tip vectors
+  const double *tip_real;  // [(unknown+1)][n] indicator vectors (mixed path)
+  double *theta;           // [P][block]
+  double *scale_all;       // [P]
+  double *pattern_lh;      // [P]
+  double *df_frac;         // [P]
+  double *red;             // reduction partials
+  size_t slot_elems;       // P * block
+  size_t slot_scale;       // P * (safe ? C : 1)
+};
+
+struct Session {
+  gems_session_desc desc;
+  int P = 0;
+  int unknown = 0;
+  int block = 0;
+  int G = 1;
+  int nops_max = 0;
+  size_t op_stride = 0;  // doubles per op in opmats
+  cudaStream_t stream = nullptr;
+  bool model_set = false;
+  bool theta_valid = false;
+  gems_branch theta_branch{};
+  long long launches = 0;
+  // device buffers
+  uint8_t *d_tips = nullptr;
+  double *d_freq = nullptr, *d_invar = nullptr;
+  void *d_partials = nullptr;
+  uint16_t *d_scale = nullptr;
+  double *d_theta = nullptr, *d_scale_all = nullptr, *d_pattern_lh = nullptr, *d_df_frac = nullptr;
+  double *d_model = nullptr;  // eval | evec | inv_evec | rates | props | tip | tip_real
+  DevOp *d_ops = nullptr;
+  double *d_opmats = nullptr;
+  double *d_branch = nullptr;  // per-branch tables: val0,val1,val2 [block] + tip table
+  double *d_red = nullptr;     // reduction partials
+  double *d_result = nullptr;  // final scalars
+  int *d_flag = nullptr;       // device status flags (barrier timeouts)
+  unsigned int *d_bar = nullptr;  // grid barrier counters
+  // pinned host staging
+  DevOp *h_ops = nullptr;
+  double *h_result = nullptr;
+  int nred = 0;  // size of d_red in doubles
+  // kernel timing (gems_profile_*): event pairs recorded around launches
+  static constexpr int kProfKernels = 8;
+  bool prof_on = false;
+  struct ProfPair {
+    cudaEvent_t a, b;
+    int kernel;
+  };
+  std::vector<ProfPair> prof_pending;
+  std::vector<cudaEvent_t> prof_free;
+  double prof_ms[kProfKernels] = {};
+  long long prof_n[kProfKernels] = {};
+  DevCtx ctx() const;
+};
+
+// brackets a launch with timing events when profiling is on
+int prof_begin(Session *s, int kernel, cudaEvent_t *a);
+int prof_end(Session *s, int kernel, cudaEvent_t a);
+void prof_collect(Session *s);
+
+// error handling
+void set_error(const std::string &msg);
+int cuda_status(cudaError_t e, const char *what);
+
+#define GEMS_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_status(e_, #call); \
+  } while (0)
+
+// launch helpers implemented in kernels.cu
+int launch_prep_ops(Session *s, int nops);
+int launch_traverse(Session *s, int nops);
+int launch_branch_lnl(Session *s, const gems_branch *br, double *lnl);
+int launch_theta(Session *s, const gems_branch *br);
+int launch_derv(Session *s, double length, double *df, double *ddf);
+int launch_from_buffer(Session *s, double length, double *lnl);
+int launch_newton(Session *s, double length0, double min_len, double max_len, double xacc,
+                  int max_steps, double *opt_len, int *nevals);
+int launch_eigen(Session *s, const double *exch_upper, const double *freq);
+int launch_unpack_partial(Session *s, int slot, double *d_out);
+
+}  // namespace gems
+
+struct gems_session : public gems::Session {};

@@ -1,0 +1,424 @@
+// phylotree.cpp -- host C++ mirror of the PhyloTree calls on the likelihood path, driving the
+// kernel set of gems_b200.h.  The tree owns topology, branch lengths and cache flags; the
+// device session owns every buffer.  Each method names the reference member it restates
+// (paths relative to the IQ-TREE 3 source tree).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/gems_b200.h"
+
+namespace {
+
+struct Tree {
+  gems_session *s = nullptr;
+  int ntaxa = 0, nnode = 0, nedges = 0, nslots = 0;
+  bool per_branch = false;  // one slot per directed branch (no re-orientation)
+  std::vector<int> deg, adj, eu, ev;
+  std::vector<double> len;
+  // directed branch d = u*3+k: u -> adj[u*3+k]; its partial is the subtree at adj[u*3+k]
+  std::vector<char> computed;
+  std::vector<int> dslot;      // per_branch: slot of directed branch
+  std::vector<int> node_slot;  // per node: slot of internal node (LM_PER_NODE)
+  std::vector<int> owner;      // per slot: directed branch currently holding it, -1 if none
+  int cur_u = -1, cur_k = 0;
+  bool theta_computed = false;
+  double min_bl = 1e-6, max_bl = 10.0;
+  long long partial_ops = 0;
+  int newton_evals = 0;
+  std::vector<gems_op> ops;
+
+  int find(int u, int v) const {
+    for (int k = 0; k < deg[u]; k++)
+      if (adj[u * 3 + k] == v) return k;
+    return -1;
+  }
+  bool leaf(int u) const { return deg[u] == 1; }
+  int dir(int u, int v) const { return u * 3 + find(u, v); }
+
+  // slot for directed branch d (u -> v, v internal).  In LM_PER_NODE mode the node's single
+  // buffer moves to d, invalidating the branch that held it (reorientPartialLh + takeover,
+  // tree/phylotree.cpp:6011, tree/memslot.cpp:213-229).
+  int acquire(int d) {
+    const int v = adj[d];
+    int sl = per_branch ? dslot[d] : node_slot[v];
+    if (owner[sl] != d) {
+      if (owner[sl] >= 0) computed[owner[sl]] = 0;
+      owner[sl] = d;
+    }
+    return sl;
+  }
+  int slot_of(int d) const { return per_branch ? dslot[d] : node_slot[adj[d]]; }
+
+  // computeTraversalInfo (tree/phylotree.cpp:6031-6140): postorder list of stale partials
+  void collect(int dad, int node) {
+    const int d = dir(dad, node);
+    if (computed[d] || leaf(node)) return;
+    int kids[2], nk = 0;
+    for (int k = 0; k < deg[node]; k++) {
+      const int c = adj[node * 3 + k];
+      if (c == dad) continue;
+      collect(node, c);
+      kids[nk++] = c;
+    }
+    computed[d] = 1;
+    gems_op op{};
+    op.dst_slot = acquire(d);
+    auto child = [&](int c, int &kind, int &id, double &l) {
+      l = len[node * 3 + find(node, c)];
+      if (leaf(c)) {
+        kind = GEMS_CHILD_TIP;
+        id = c;
+      } else {
+        kind = GEMS_CHILD_PARTIAL;
+        id = slot_of(dir(node, c));
+      }
+    };
+    child(kids[0], op.left_kind, op.left_id, op.left_len);
+    child(kids[1], op.right_kind, op.right_id, op.right_len);
+    ops.push_back(op);
+    partial_ops++;
+  }
+
+  // the branch (node, dad) after the reference's leaf swap (phylokernelnew.h:2671-2678)
+  gems_branch branch(int &node, int &dad) {
+    if (leaf(node)) std::swap(node, dad);
+    ops.clear();
+    collect(dad, node);
+    if (!leaf(dad)) collect(node, dad);
+    gems_branch br{};
+    br.dad_slot = slot_of(dir(dad, node));
+    if (leaf(dad)) {
+      br.node_kind = GEMS_CHILD_TIP;
+      br.node_id = dad;
+    } else {
+      br.node_kind = GEMS_CHILD_PARTIAL;
+      br.node_id = slot_of(dir(node, dad));
+    }
+    br.length = len[dad * 3 + find(dad, node)];
+    return br;
+  }
+
+  void set_len(int u, int v, double x) {
+    len[u * 3 + find(u, v)] = x;
+    len[v * 3 + find(v, u)] = x;
+  }
+
+  // PhyloNode::clearReversePartialLh (tree/phylonode.cpp:22)
+  void clear_reverse(int node, int dad) {
+    for (int k = 0; k < deg[node]; k++) {
+      const int c = adj[node * 3 + k];
+      if (c == dad) continue;
+      computed[dir(c, node)] = 0;
+      clear_reverse(c, node);
+    }
+  }
+
+  // MTree::findFarthestLeaf (tree/mtree.cpp:3040)
+  int far_leaf(int node, int dad, std::vector<int> &h) const {
+    if (dad >= 0 && leaf(node)) {
+      h[node] = 0;
+      return node;
+    }
+    int res = -1;
+    h[node] = 0;
+    for (int k = 0; k < deg[node]; k++) {
+      const int c = adj[node * 3 + k];
+      if (c == dad) continue;
+      const int lf = far_leaf(c, node, h);
+      if (h[node] < h[c] + 1) {
+        h[node] = h[c] + 1;
+        res = lf;
+      }
+    }
+    return res;
+  }
+
+  // MTree::getPreOrderBranches (tree/mtree.cpp:3062)
+  void preorder(int node, int dad, const std::vector<int> &h, std::vector<int> &n1,
+                std::vector<int> &n2) const {
+    if (dad >= 0) {
+      n1.push_back(node);
+      n2.push_back(dad);
+    }
+    int nv[3], nd = deg[node];
+    for (int i = 0; i < nd; i++) nv[i] = adj[node * 3 + i];
+    for (int i = 0; i < nd; i++)
+      for (int j = i + 1; j < nd; j++)
+        if (h[nv[i]] > h[nv[j]]) std::swap(nv[i], nv[j]);
+    for (int i = 0; i < nd; i++)
+      if (nv[i] != dad) preorder(nv[i], node, h, n1, n2);
+  }
+
+  int lh_branch(int node, int dad, double *lnl, double *pattern_lh) {
+    gems_branch br = branch(node, dad);
+    return gems_branch_lnl(s, ops.data(), (int)ops.size(), &br, lnl, pattern_lh);
+  }
+
+  int derv(int node, int dad, double *df, double *ddf) {
+    int st;
+    if (!theta_computed) {
+      gems_branch br = branch(node, dad);
+      st = gems_branch_derv(s, ops.data(), (int)ops.size(), &br, 1, df, ddf, nullptr);
+      if (st == GEMS_OK) theta_computed = true;
+    } else {
+      if (leaf(node)) std::swap(node, dad);
+      gems_branch br{};
+      br.length = len[dad * 3 + find(dad, node)];
+      br.dad_slot = slot_of(dir(dad, node));
+      br.node_kind = leaf(dad) ? GEMS_CHILD_TIP : GEMS_CHILD_PARTIAL;
+      br.node_id = leaf(dad) ? dad : slot_of(dir(node, dad));
+      st = gems_branch_derv(s, nullptr, 0, &br, 0, df, ddf, nullptr);
+    }
+    return st;
+  }
+
+  int from_buffer(double *lnl) {
+    if (cur_u < 0 || !theta_computed) {
+      // computeLikelihoodFromBuffer falls back to computeLikelihoodBranch
+      const int u = cur_u < 0 ? 0 : cur_u;
+      const int v = adj[u * 3 + (cur_u < 0 ? 0 : cur_k)];
+      return lh_branch(v, u, lnl, nullptr);
+    }
+    return gems_lnl_from_buffer(s, len[cur_u * 3 + cur_k], lnl, nullptr);
+  }
+
+  // PhyloTree::optimizeOneBranch (tree/phylotree.cpp:2620-2670) with the Newton loop of
+  // Optimization::minimizeNewton (utils/optimization.cpp:422-499) run on the device.
+  int optimize_one(int node1, int node2, int clear_lh, int max_nr) {
+    const int k = find(node1, node2);
+    if (k < 0) return GEMS_ERR_BAD_ARG;
+    cur_u = node1;
+    cur_k = k;
+    const double cur = len[node1 * 3 + k];
+    theta_computed = false;
+    int n = node2, d = node1;
+    gems_branch br = branch(n, d);
+    double optx = cur;
+    int nev = 0;
+    int st = gems_newton_branch(s, ops.data(), (int)ops.size(), &br, 1, min_bl, max_bl, min_bl,
+                                max_nr, &optx, &nev);
+    newton_evals = nev;
+    if (st != GEMS_OK) return st;
+    theta_computed = true;
+    if (optx > max_bl * 0.95) {
+      double opt_lh = 0, orig_lh = 0;
+      if ((st = gems_lnl_from_buffer(s, optx, &opt_lh, nullptr))) return st;
+      if ((st = gems_lnl_from_buffer(s, cur, &orig_lh, nullptr))) return st;
+      if (orig_lh > opt_lh) optx = cur;
+    }
+    set_len(node1, node2, optx);
+    if (clear_lh && cur != optx) {
+      clear_reverse(node1, node2);
+      clear_reverse(node2, node1);
+    }
+    return GEMS_OK;
+  }
+
+  // PhyloTree::optimizeAllBranches(my_iterations, tolerance, maxNRStep)
+  // (tree/phylotree.cpp:2724-2800) with computeBestTraversal (:2710)
+  int optimize_all(int iterations, double tol, int max_nr, double *out) {
+    std::vector<int> h(nnode, 0), n1, n2;
+    const int far = far_leaf(0, -1, h);
+    far_leaf(far, -1, h);
+    preorder(far, -1, h, n1, n2);
+    double tree_lh = 0;
+    int st = lh_branch(n2[0], n1[0], &tree_lh, nullptr);
+    if (st) return st;
+    std::vector<double> saved(nedges);
+    for (int it = 0; it < iterations; it++) {
+      for (int e = 0; e < nedges; e++) saved[e] = len[eu[e] * 3 + find(eu[e], ev[e])];
+      for (size_t j = 0; j < n1.size(); j++)
+        if ((st = optimize_one(n1[j], n2[j], 1, max_nr))) return st;
+      double new_lh = 0;
+      if ((st = from_buffer(&new_lh))) return st;
+      if (new_lh < tree_lh - tol * 0.1) {
+        std::fill(computed.begin(), computed.end(), 0);
+        theta_computed = false;
+        for (int e = 0; e < nedges; e++) set_len(eu[e], ev[e], saved[e]);
+        if ((st = compute_likelihood(&new_lh, nullptr))) return st;
+        *out = new_lh;
+        return GEMS_OK;
+      }
+      if (tree_lh <= new_lh && new_lh <= tree_lh + tol) {
+        tree_lh = new_lh;
+        break;
+      }
+      tree_lh = new_lh;
+    }
+    *out = tree_lh;
+    return GEMS_OK;
+  }
+
+  // PhyloTree::computeLikelihood (tree/phylotree.cpp:1258-1295)
+  int compute_likelihood(double *lnl, double *pattern_lh) {
+    if (cur_u < 0) {
+      std::vector<int> h(nnode, 0);
+      cur_u = far_leaf(0, -1, h);
+      cur_k = 0;
+    }
+    const int v = adj[cur_u * 3 + cur_k];
+    return lh_branch(v, cur_u, lnl, pattern_lh);
+  }
+};
+
+}  // namespace
+
+struct gems_tree : public Tree {};
+
+extern "C" {
+
+int gems_tree_create(gems_session *s, int nedges, const int *eu, const int *ev,
+                     const double *len, gems_tree **out) {
+  if (!s || !eu || !ev || !len || !out || nedges < 3) return GEMS_ERR_BAD_ARG;
+  gems_tree *t = new gems_tree();
+  t->s = s;
+  t->nedges = nedges;
+  t->nnode = nedges + 1;
+  t->ntaxa = (t->nnode + 2) / 2;
+  t->deg.assign(t->nnode, 0);
+  t->adj.assign(t->nnode * 3, -1);
+  t->len.assign(t->nnode * 3, 0.0);
+  t->eu.assign(eu, eu + nedges);
+  t->ev.assign(ev, ev + nedges);
+  for (int e = 0; e < nedges; e++) {
+    const int u = eu[e], v = ev[e];
+    if (u < 0 || v < 0 || u >= t->nnode || v >= t->nnode || u == v || t->deg[u] >= 3 ||
+        t->deg[v] >= 3 || !(len[e] >= 0)) {
+      delete t;
+      return GEMS_ERR_BAD_ARG;
+    }
+    t->adj[u * 3 + t->deg[u]] = v;
+    t->len[u * 3 + t->deg[u]++] = len[e];
+    t->adj[v * 3 + t->deg[v]] = u;
+    t->len[v * 3 + t->deg[v]++] = len[e];
+  }
+  for (int u = 0; u < t->nnode; u++) {
+    const bool is_leaf_id = u < t->ntaxa;
+    if ((is_leaf_id && t->deg[u] != 1) || (!is_leaf_id && t->deg[u] != 3)) {
+      delete t;
+      return GEMS_ERR_BAD_ARG;  // binary unrooted tree with leaves 0..ntaxa-1 required
+    }
+  }
+  const int ninternal = t->nnode - t->ntaxa;
+  // the number of slots the session holds decides the memory mode
+  t->computed.assign(t->nnode * 3, 0);
+  t->node_slot.assign(t->nnode, -1);
+  t->dslot.assign(t->nnode * 3, -1);
+  gems_session_desc desc{};
+  if (gems_session_info(s, &desc) != GEMS_OK || desc.ntaxa != t->ntaxa) {
+    delete t;
+    return GEMS_ERR_BAD_ARG;
+  }
+  const int nslots = desc.nslots;
+  if (nslots < ninternal) {
+    delete t;
+    return GEMS_ERR_ADMISSION;
+  }
+  t->nslots = nslots;
+  int next = 0;
+  if (nslots >= 3 * ninternal) {
+    t->per_branch = true;
+    for (int u = 0; u < t->nnode; u++)
+      for (int k = 0; k < t->deg[u]; k++)
+        if (!t->leaf(t->adj[u * 3 + k])) t->dslot[u * 3 + k] = next++;
+  } else {
+    for (int u = t->ntaxa; u < t->nnode; u++) t->node_slot[u] = next++;
+  }
+  t->owner.assign(nslots, -1);
+  *out = t;
+  return GEMS_OK;
+}
+
+int gems_tree_destroy(gems_tree *t) {
+  delete t;
+  return GEMS_OK;
+}
+
+int gems_tree_set_branch_limits(gems_tree *t, double min_len, double max_len) {
+  if (!t || !(min_len >= 0) || !(max_len > min_len)) return GEMS_ERR_BAD_ARG;
+  t->min_bl = min_len;
+  t->max_bl = max_len;
+  return GEMS_OK;
+}
+
+int gems_tree_set_length(gems_tree *t, int u, int v, double x) {
+  if (!t || u < 0 || v < 0 || u >= t->nnode || v >= t->nnode || t->find(u, v) < 0 || !(x >= 0))
+    return GEMS_ERR_BAD_ARG;
+  t->set_len(u, v, x);
+  // a changed length invalidates partials looking across the branch
+  t->clear_reverse(u, v);
+  t->clear_reverse(v, u);
+  t->theta_computed = false;
+  return GEMS_OK;
+}
+
+int gems_tree_get_lengths(gems_tree *t, double *out) {
+  if (!t || !out) return GEMS_ERR_BAD_ARG;
+  for (int e = 0; e < t->nedges; e++) out[e] = t->len[t->eu[e] * 3 + t->find(t->eu[e], t->ev[e])];
+  return GEMS_OK;
+}
+
+int gems_tree_clear_all_partial_lh(gems_tree *t) {
+  if (!t) return GEMS_ERR_BAD_ARG;
+  std::fill(t->computed.begin(), t->computed.end(), 0);
+  t->theta_computed = false;
+  return GEMS_OK;
+}
+
+int gems_tree_compute_likelihood(gems_tree *t, double *lnl, double *pattern_lh) {
+  if (!t || !lnl) return GEMS_ERR_BAD_ARG;
+  return t->compute_likelihood(lnl, pattern_lh);
+}
+
+int gems_tree_compute_likelihood_branch(gems_tree *t, int node, int dad, double *lnl,
+                                        double *pattern_lh) {
+  if (!t || !lnl || node < 0 || dad < 0 || node >= t->nnode || dad >= t->nnode ||
+      t->find(node, dad) < 0)
+    return GEMS_ERR_BAD_ARG;
+  return t->lh_branch(node, dad, lnl, pattern_lh);
+}
+
+int gems_tree_compute_likelihood_derv(gems_tree *t, int node, int dad, double *df, double *ddf) {
+  if (!t || !df || !ddf || node < 0 || dad < 0 || node >= t->nnode || dad >= t->nnode ||
+      t->find(node, dad) < 0)
+    return GEMS_ERR_BAD_ARG;
+  return t->derv(node, dad, df, ddf);
+}
+
+int gems_tree_compute_likelihood_from_buffer(gems_tree *t, double *lnl) {
+  if (!t || !lnl) return GEMS_ERR_BAD_ARG;
+  return t->from_buffer(lnl);
+}
+
+int gems_tree_optimize_one_branch(gems_tree *t, int node1, int node2, int clear_lh,
+                                  int max_nr_step) {
+  if (!t || node1 < 0 || node2 < 0 || node1 >= t->nnode || node2 >= t->nnode ||
+      max_nr_step < 1)
+    return GEMS_ERR_BAD_ARG;
+  return t->optimize_one(node1, node2, clear_lh, max_nr_step);
+}
+
+int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double tolerance,
+                                    int max_nr_step, double *lnl) {
+  if (!t || !lnl || iterations < 1 || max_nr_step < 1) return GEMS_ERR_BAD_ARG;
+  return t->optimize_all(iterations, tolerance, max_nr_step, lnl);
+}
+
+int gems_tree_get_partial(gems_tree *t, int node, int dad, double *partial, uint16_t *scale) {
+  if (!t || node < 0 || dad < 0 || node >= t->nnode || dad >= t->nnode ||
+      t->find(dad, node) < 0 || t->leaf(node))
+    return GEMS_ERR_BAD_ARG;
+  const int d = t->dir(dad, node);
+  if (!t->computed[d]) return GEMS_ERR_STATE;
+  return gems_get_partial(t->s, t->slot_of(d), partial, scale);
+}
+
+int gems_tree_stats(gems_tree *t, long long *partial_ops, int *last_newton_evals) {
+  if (!t) return GEMS_ERR_BAD_ARG;
+  if (partial_ops) *partial_ops = t->partial_ops;
+  if (last_newton_evals) *last_newton_evals = t->newton_evals;
+  return GEMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,648 @@
+// session.cu -- C-ABI of the kernel set: device sessions, uploads, model, kernel calls.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gems_internal.cuh"
+
+namespace gems {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+int cuda_status(cudaError_t e, const char *what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return GEMS_ERR_OOM;
+  return GEMS_ERR_CUDA;
+}
+
+DevCtx Session::ctx() const {
+  DevCtx c{};
+  c.P = P;
+  c.nptn = desc.nptn;
+  c.n = desc.nstates;
+  c.C = desc.ncat;
+  c.block = block;
+  c.G = G;
+  c.unknown = unknown;
+  c.safe = desc.scaling == GEMS_SCALE_SAFE;
+  c.tips = d_tips;
+  c.freq = d_freq;
+  c.invar = d_invar;
+  c.partials = d_partials;
+  c.scale = d_scale;
+  const int n = desc.nstates;
+  c.eval = d_model;
+  c.evec = d_model + n;
+  c.inv_evec = d_model + n + n * n;
+  c.rates = d_model + n + 2 * n * n;
+  c.props = c.rates + desc.ncat;
+  c.tip = c.props + desc.ncat;
+  c.tip_real = c.tip + (size_t)(unknown + 1) * n;
+  c.theta = d_theta;
+  c.scale_all = d_scale_all;
+  c.pattern_lh = d_pattern_lh;
+  c.df_frac = d_df_frac;
+  c.red = d_red;
+  c.slot_elems = (size_t)P * block;
+  c.slot_scale = (size_t)P * (desc.scaling == GEMS_SCALE_SAFE ? desc.ncat : 1);
+  return c;
+}
+
+static cudaEvent_t prof_event(Session *s) {
+  cudaEvent_t e = nullptr;
+  if (!s->prof_free.empty()) {
+    e = s->prof_free.back();
+    s->prof_free.pop_back();
+  } else if (cudaEventCreate(&e) != cudaSuccess) {
+    e = nullptr;
+  }
+  return e;
+}
+
+int prof_begin(Session *s, int kernel, cudaEvent_t *a) {
+  (void)kernel;
+  *a = nullptr;
+  if (!s->prof_on) return GEMS_OK;
+  *a = prof_event(s);
+  if (*a) GEMS_CUDA(cudaEventRecord(*a, s->stream));
+  return GEMS_OK;
+}
+
+int prof_end(Session *s, int kernel, cudaEvent_t a) {
+  if (!a) return GEMS_OK;
+  cudaEvent_t b = prof_event(s);
+  if (!b) return GEMS_OK;
+  GEMS_CUDA(cudaEventRecord(b, s->stream));
+  s->prof_pending.push_back({a, b, kernel});
+  return GEMS_OK;
+}
+
+void prof_collect(Session *s) {
+  for (auto &pp : s->prof_pending) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(pp.b) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, pp.a, pp.b) == cudaSuccess && pp.kernel >= 0 &&
+        pp.kernel < Session::kProfKernels) {
+      s->prof_ms[pp.kernel] += ms;
+      s->prof_n[pp.kernel] += 1;
+    }
+    s->prof_free.push_back(pp.a);
+    s->prof_free.push_back(pp.b);
+  }
+  s->prof_pending.clear();
+}
+
+static int state_unknown(int n) { return n == 4 ? 18 : (n == 20 ? 23 : n); }
+static int pad_patterns(int nptn) { return ((nptn + 63) / 64) * 64; }
+static int pow2_at_least(int x) {
+  int g = 1;
+  while (g < x) g <<= 1;
+  return g;
+}
+
+struct Sizes {
+  size_t partial_bytes, scale_bytes, theta_bytes, opmats_bytes, branch_bytes, red_doubles,
+      model_doubles, total;
+  int nops_max;
+  size_t op_stride;
+};
+
+static Sizes compute_sizes(const gems_session_desc &d) {
+  Sizes z{};
+  const size_t P = pad_patterns(d.nptn);
+  const size_t blk = (size_t)d.nstates * d.ncat;
+  const int unk = state_unknown(d.nstates);
+  const size_t elem = d.precision == GEMS_PREC_MIXED ? sizeof(float) : sizeof(double);
+  z.partial_bytes = (size_t)d.nslots * P * blk * elem;
+  z.scale_bytes = (size_t)d.nslots * P * (d.scaling == GEMS_SCALE_SAFE ? d.ncat : 1) * 2;
+  z.theta_bytes = P * blk * sizeof(double) + 3 * P * sizeof(double);  // theta + scale_all, plh, G
+  z.nops_max = d.ntaxa + 8;
+  z.op_stride = 2 * (size_t)d.ncat * d.nstates * d.nstates + 2 * (size_t)(unk + 1) * blk;
+  z.opmats_bytes = (size_t)z.nops_max * z.op_stride * sizeof(double);
+  z.branch_bytes = (3 * blk + (size_t)(unk + 1) * blk) * sizeof(double);
+  z.red_doubles = 4 * (P * 16 / 256 + 1024);
+  z.model_doubles = d.nstates + 2 * (size_t)d.nstates * d.nstates + 2 * d.ncat +
+                    2 * (size_t)(unk + 1) * d.nstates;
+  z.total = z.partial_bytes + z.scale_bytes + z.theta_bytes + z.opmats_bytes + z.branch_bytes +
+            z.red_doubles * 8 + z.model_doubles * 8 + (size_t)d.ntaxa * P + 2 * P * 8 +
+            (size_t)z.nops_max * sizeof(DevOp);
+  return z;
+}
+
+static int validate(const gems_session_desc *d) {
+  if (!d) return GEMS_ERR_BAD_ARG;
+  if (d->ntaxa < 3 || d->nptn < 1 || d->nstates < 2 || d->nstates > kMaxStates || d->ncat < 1 ||
+      d->ncat > kMaxCat || d->nslots < 1 ||
+      (d->precision != GEMS_PREC_FP64 && d->precision != GEMS_PREC_MIXED) ||
+      (d->scaling != GEMS_SCALE_NORM && d->scaling != GEMS_SCALE_SAFE)) {
+    set_error("invalid session descriptor");
+    return GEMS_ERR_BAD_ARG;
+  }
+  if (d->nstates != 4 && d->nstates != 20 && d->nstates != 61) {
+    set_error("state count must be 4, 20 or 61");
+    return GEMS_ERR_BAD_ARG;
+  }
+  return GEMS_OK;
+}
+
+static void free_session(Session *s) {
+  cudaFree(s->d_tips);
+  cudaFree(s->d_freq);
+  cudaFree(s->d_invar);
+  cudaFree(s->d_partials);
+  cudaFree(s->d_scale);
+  cudaFree(s->d_theta);
+  cudaFree(s->d_model);
+  cudaFree(s->d_ops);
+  cudaFree(s->d_opmats);
+  cudaFree(s->d_branch);
+  cudaFree(s->d_red);
+  cudaFree(s->d_result);
+  cudaFree(s->d_flag);
+  cudaFree(s->d_bar);
+  cudaFreeHost(s->h_ops);
+  cudaFreeHost(s->h_result);
+  if (s->stream) {
+    cudaStreamSynchronize(s->stream);
+    prof_collect(s);
+    for (cudaEvent_t e : s->prof_free) cudaEventDestroy(e);
+    s->prof_free.clear();
+    cudaStreamDestroy(s->stream);
+  }
+}
+
+static int upload_ops(Session *s, const gems_op *ops, int nops) {
+  if (nops < 0 || nops > s->nops_max) {
+    set_error("too many traversal ops");
+    return GEMS_ERR_BAD_ARG;
+  }
+  if (nops == 0) return GEMS_OK;
+  for (int k = 0; k < nops; k++) {
+    const gems_op &o = ops[k];
+    auto bad_child = [&](int kind, int id) {
+      if (kind == GEMS_CHILD_TIP) return id < 0 || id >= s->desc.ntaxa;
+      if (kind == GEMS_CHILD_PARTIAL) return id < 0 || id >= s->desc.nslots || id == o.dst_slot;
+      return true;
+    };
+    if (o.dst_slot < 0 || o.dst_slot >= s->desc.nslots || bad_child(o.left_kind, o.left_id) ||
+        bad_child(o.right_kind, o.right_id) || !(o.left_len >= 0) || !(o.right_len >= 0)) {
+      set_error("invalid traversal op");
+      return GEMS_ERR_BAD_ARG;
+    }
+  }
+  // host staging: wait for any kernel still reading the previous op table
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  std::memcpy(s->h_ops, ops, sizeof(gems_op) * nops);
+  GEMS_CUDA(cudaMemcpyAsync(s->d_ops, s->h_ops, sizeof(DevOp) * nops, cudaMemcpyHostToDevice,
+                            s->stream));
+  return GEMS_OK;
+}
+
+static int check_branch(Session *s, const gems_branch *br) {
+  if (!br || br->dad_slot < 0 || br->dad_slot >= s->desc.nslots || !(br->length >= 0)) {
+    set_error("invalid branch");
+    return GEMS_ERR_BAD_ARG;
+  }
+  if (br->node_kind == GEMS_CHILD_TIP) {
+    if (br->node_id < 0 || br->node_id >= s->desc.ntaxa) return GEMS_ERR_BAD_ARG;
+  } else if (br->node_kind == GEMS_CHILD_PARTIAL) {
+    if (br->node_id < 0 || br->node_id >= s->desc.nslots || br->node_id == br->dad_slot)
+      return GEMS_ERR_BAD_ARG;
+  } else {
+    return GEMS_ERR_BAD_ARG;
+  }
+  return GEMS_OK;
+}
+
+static int run_ops(Session *s, const gems_op *ops, int nops) {
+  if (!s->model_set) {
+    set_error("model not set");
+    return GEMS_ERR_STATE;
+  }
+  int st = upload_ops(s, ops, nops);
+  if (st) return st;
+  if ((st = launch_prep_ops(s, nops))) return st;
+  if ((st = launch_traverse(s, nops))) return st;
+  for (int k = 0; k < nops; k++)
+    if (s->theta_valid &&
+        (ops[k].dst_slot == s->theta_branch.dad_slot ||
+         (s->theta_branch.node_kind == GEMS_CHILD_PARTIAL &&
+          ops[k].dst_slot == s->theta_branch.node_id)))
+      s->theta_valid = false;
+  return GEMS_OK;
+}
+
+static void copy_pattern_lh(Session *s, double *pattern_lh, double lnl_raw_finite) {
+  (void)lnl_raw_finite;
+  if (!pattern_lh) return;
+  cudaMemcpyAsync(pattern_lh, s->d_pattern_lh, sizeof(double) * s->desc.nptn,
+                  cudaMemcpyDeviceToHost, s->stream);
+  cudaStreamSynchronize(s->stream);
+  for (int p = 0; p < s->desc.nptn; p++)
+    if (!std::isfinite(pattern_lh[p])) pattern_lh[p] = 4.0 * kLogScaleThr;
+}
+
+}  // namespace gems
+
+using namespace gems;
+
+extern "C" {
+
+const char *gems_version(void) { return "gems_b200 0.1 (sm_100a)"; }
+const char *gems_last_error(void) { return gems::g_err.c_str(); }
+
+int gems_device_count(int *count) {
+  if (!count) return GEMS_ERR_BAD_ARG;
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) {
+    *count = 0;
+    cudaGetLastError();
+    set_error(cudaGetErrorString(e));
+    return GEMS_ERR_NO_DEVICE;
+  }
+  return GEMS_OK;
+}
+
+int gems_session_footprint(const gems_session_desc *desc, size_t *bytes) {
+  int st = validate(desc);
+  if (st) return st;
+  if (!bytes) return GEMS_ERR_BAD_ARG;
+  *bytes = compute_sizes(*desc).total;
+  return GEMS_OK;
+}
+
+int gems_session_create(const gems_session_desc *desc, gems_session **out) {
+  int st = validate(desc);
+  if (st) return st;
+  if (!out) return GEMS_ERR_BAD_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return GEMS_ERR_NO_DEVICE;
+  }
+  if (desc->device < 0 || desc->device >= ndev) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(desc->device));
+  Sizes z = compute_sizes(*desc);
+  size_t free_b = 0, total_b = 0;
+  GEMS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  if (z.total > free_b) {
+    set_error("session footprint exceeds free device memory");
+    return GEMS_ERR_ADMISSION;
+  }
+  gems_session *s = new gems_session();
+  s->desc = *desc;
+  s->P = pad_patterns(desc->nptn);
+  s->unknown = state_unknown(desc->nstates);
+  s->block = desc->nstates * desc->ncat;
+  s->G = pow2_at_least(desc->ncat);
+  s->nops_max = z.nops_max;
+  s->op_stride = z.op_stride;
+  s->nred = (int)z.red_doubles;
+  auto fail = [&](cudaError_t e, const char *what) {
+    int code = cuda_status(e, what);
+    free_session(s);
+    delete s;
+    return code;
+  };
+  cudaError_t e;
+#define ALLOC(ptr, bytes)                                           \
+  if ((e = cudaMalloc((void **)&(ptr), (bytes))) != cudaSuccess) \
+    return fail(e, "cudaMalloc " #ptr);
+  const size_t P = s->P;
+  ALLOC(s->d_tips, (size_t)desc->ntaxa * P);
+  ALLOC(s->d_freq, P * sizeof(double));
+  ALLOC(s->d_invar, P * sizeof(double));
+  ALLOC(s->d_partials, z.partial_bytes);
+  ALLOC(s->d_scale, z.scale_bytes);
+  ALLOC(s->d_theta, z.theta_bytes);
+  s->d_scale_all = s->d_theta + P * s->block;
+  s->d_pattern_lh = s->d_scale_all + P;
+  s->d_df_frac = s->d_pattern_lh + P;
+  ALLOC(s->d_model, z.model_doubles * sizeof(double));
+  ALLOC(s->d_ops, (size_t)z.nops_max * sizeof(DevOp));
+  ALLOC(s->d_opmats, z.opmats_bytes);
+  ALLOC(s->d_branch, z.branch_bytes);
+  ALLOC(s->d_red, z.red_doubles * sizeof(double));
+  ALLOC(s->d_result, 16 * sizeof(double));
+  ALLOC(s->d_flag, 16 * sizeof(int));
+  ALLOC(s->d_bar, 16 * sizeof(unsigned int));
+#undef ALLOC
+  if ((e = cudaHostAlloc((void **)&s->h_ops, (size_t)z.nops_max * sizeof(DevOp), 0)) !=
+      cudaSuccess)
+    return fail(e, "cudaHostAlloc ops");
+  if ((e = cudaHostAlloc((void **)&s->h_result, 16 * sizeof(double), 0)) != cudaSuccess)
+    return fail(e, "cudaHostAlloc result");
+  if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(e, "cudaStreamCreate");
+  // padded patterns: unknown state, weight 0, zero scale counters
+  if ((e = cudaMemsetAsync(s->d_tips, s->unknown, (size_t)desc->ntaxa * P, s->stream)) ||
+      (e = cudaMemsetAsync(s->d_freq, 0, P * sizeof(double), s->stream)) ||
+      (e = cudaMemsetAsync(s->d_invar, 0, P * sizeof(double), s->stream)) ||
+      (e = cudaMemsetAsync(s->d_scale, 0, z.scale_bytes, s->stream)) ||
+      (e = cudaStreamSynchronize(s->stream)))
+    return fail(e, "initialise session");
+  *out = s;
+  return GEMS_OK;
+}
+
+int gems_session_destroy(gems_session *s) {
+  if (!s) return GEMS_ERR_BAD_ARG;
+  cudaSetDevice(s->desc.device);
+  cudaStreamSynchronize(s->stream);
+  free_session(s);
+  delete s;
+  return GEMS_OK;
+}
+
+int gems_session_sync(gems_session *s) {
+  if (!s) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
+int gems_session_info(gems_session *s, gems_session_desc *desc) {
+  if (!s || !desc) return GEMS_ERR_BAD_ARG;
+  *desc = s->desc;
+  return GEMS_OK;
+}
+
+int gems_session_stream(gems_session *s, void **stream) {
+  if (!s || !stream) return GEMS_ERR_BAD_ARG;
+  *stream = (void *)s->stream;
+  return GEMS_OK;
+}
+
+int gems_upload_tips(gems_session *s, const uint8_t *states) {
+  if (!s || !states) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  const int unk = s->unknown;
+  for (size_t i = 0; i < (size_t)s->desc.ntaxa * s->desc.nptn; i++)
+    if (states[i] > unk) {
+      set_error("tip state byte out of range");
+      return GEMS_ERR_BAD_ARG;
+    }
+  GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips, s->P, states, s->desc.nptn, s->desc.nptn,
+                              s->desc.ntaxa, cudaMemcpyHostToDevice, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  s->theta_valid = false;
+  return GEMS_OK;
+}
+
+int gems_upload_patterns(gems_session *s, const double *ptn_freq, const double *ptn_invar) {
+  if (!s || !ptn_freq) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  const int n = s->desc.nptn;
+  GEMS_CUDA(cudaMemcpyAsync(s->d_freq, ptn_freq, n * sizeof(double), cudaMemcpyHostToDevice,
+                            s->stream));
+  if (ptn_invar) {
+    GEMS_CUDA(cudaMemcpyAsync(s->d_invar, ptn_invar, n * sizeof(double), cudaMemcpyHostToDevice,
+                              s->stream));
+  } else {
+    GEMS_CUDA(cudaMemsetAsync(s->d_invar, 0, n * sizeof(double), s->stream));
+  }
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  s->theta_valid = false;
+  return GEMS_OK;
+}
+
+// tip vectors for every state code: real-space indicator and eigen-space inv_evec . indicator
+// (phylotreesse.cpp:361-371, modelsubst.cpp:183-208, modeldna.cpp:462-474,
+//  modelprotein.cpp:1240-1255)
+static void build_tip_tables(int n, int unk, const double *inv_evec, std::vector<double> &tip,
+                             std::vector<double> &tip_real) {
+  tip.assign((size_t)(unk + 1) * n, 0.0);
+  tip_real.assign((size_t)(unk + 1) * n, 0.0);
+  static const int amb_aa[3][2] = {{2, 3}, {5, 6}, {9, 10}};
+  for (int s = 0; s <= unk; s++) {
+    double *ind = &tip_real[(size_t)s * n];
+    if (s < n) {
+      ind[s] = 1.0;
+    } else if (n == 4 && s < 18) {
+      const int cs = s - n + 1;
+      for (int j = 0; j < 4; j++)
+        if (cs & (1 << j)) ind[j] = 1.0;
+    } else if (n == 20 && s < 23) {
+      ind[amb_aa[s - 20][0]] = 1.0;
+      ind[amb_aa[s - 20][1]] = 1.0;
+    } else {
+      for (int j = 0; j < n; j++) ind[j] = 1.0;
+    }
+    for (int i = 0; i < n; i++) {
+      double acc = 0.0;
+      for (int j = 0; j < n; j++) acc += inv_evec[i * n + j] * ind[j];
+      tip[(size_t)s * n + i] = acc;
+    }
+  }
+}
+
+static int upload_model(gems_session *s, const double *eval, const double *evec,
+                        const double *inv_evec, const double *rates, const double *props) {
+  const int n = s->desc.nstates, C = s->desc.ncat;
+  std::vector<double> tip, tip_real;
+  build_tip_tables(n, s->unknown, inv_evec, tip, tip_real);
+  std::vector<double> m;
+  m.insert(m.end(), eval, eval + n);
+  m.insert(m.end(), evec, evec + n * n);
+  m.insert(m.end(), inv_evec, inv_evec + n * n);
+  m.insert(m.end(), rates, rates + C);
+  m.insert(m.end(), props, props + C);
+  m.insert(m.end(), tip.begin(), tip.end());
+  m.insert(m.end(), tip_real.begin(), tip_real.end());
+  GEMS_CUDA(cudaMemcpyAsync(s->d_model, m.data(), m.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  s->model_set = true;
+  s->theta_valid = false;
+  return GEMS_OK;
+}
+
+int gems_set_model(gems_session *s, const double *eval, const double *evec,
+                   const double *inv_evec, const double *rates, const double *props) {
+  if (!s || !eval || !evec || !inv_evec || !rates || !props) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  for (int c = 0; c < s->desc.ncat; c++)
+    if (!(rates[c] >= 0) || !(props[c] >= 0)) return GEMS_ERR_BAD_ARG;
+  return upload_model(s, eval, evec, inv_evec, rates, props);
+}
+
+int gems_set_model_from_rates(gems_session *s, const double *exch_upper, const double *freq,
+                              const double *rates, const double *props) {
+  if (!s || !exch_upper || !freq || !rates || !props) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  const int n = s->desc.nstates, C = s->desc.ncat;
+  int st = launch_eigen(s, exch_upper, freq);
+  if (st) return st;
+  std::vector<double> es((size_t)n + 2 * n * n);
+  GEMS_CUDA(cudaMemcpyAsync(es.data(), s->d_model, es.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  (void)C;
+  return upload_model(s, es.data(), es.data() + n, es.data() + n + n * n, rates, props);
+}
+
+int gems_get_eigensystem(gems_session *s, double *eval, double *evec, double *inv_evec) {
+  if (!s || !s->model_set) return GEMS_ERR_STATE;
+  const int n = s->desc.nstates;
+  std::vector<double> es((size_t)n + 2 * n * n);
+  GEMS_CUDA(cudaMemcpyAsync(es.data(), s->d_model, es.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  if (eval) std::memcpy(eval, es.data(), n * sizeof(double));
+  if (evec) std::memcpy(evec, es.data() + n, n * n * sizeof(double));
+  if (inv_evec) std::memcpy(inv_evec, es.data() + n + n * n, n * n * sizeof(double));
+  return GEMS_OK;
+}
+
+int gems_traverse(gems_session *s, const gems_op *ops, int nops) {
+  if (!s || (nops > 0 && !ops)) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = run_ops(s, ops, nops);
+  if (st) return st;
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
+int gems_branch_lnl(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
+                    double *lnl, double *pattern_lh) {
+  if (!s || !lnl || (nops > 0 && !ops)) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = check_branch(s, br);
+  if (st) return st;
+  if ((st = run_ops(s, ops, nops))) return st;
+  if ((st = launch_branch_lnl(s, br, lnl))) return st;
+  copy_pattern_lh(s, pattern_lh, *lnl);
+  return GEMS_OK;
+}
+
+int gems_branch_derv(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
+                     int compute_theta, double *df, double *ddf, double *df_frac) {
+  if (!s || !df || !ddf || (nops > 0 && !ops)) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = check_branch(s, br);
+  if (st) return st;
+  if (compute_theta) {
+    if ((st = run_ops(s, ops, nops))) return st;
+    if ((st = launch_theta(s, br))) return st;
+    s->theta_valid = true;
+    s->theta_branch = *br;
+  } else if (!s->theta_valid) {
+    set_error("theta not computed");
+    return GEMS_ERR_STATE;
+  }
+  if ((st = launch_derv(s, br->length, df, ddf))) return st;
+  if (df_frac) {
+    GEMS_CUDA(cudaMemcpyAsync(df_frac, s->d_df_frac, sizeof(double) * s->desc.nptn,
+                              cudaMemcpyDeviceToHost, s->stream));
+    GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return GEMS_OK;
+}
+
+int gems_lnl_from_buffer(gems_session *s, double length, double *lnl, double *pattern_lh) {
+  if (!s || !lnl || !(length >= 0)) return GEMS_ERR_BAD_ARG;
+  if (!s->theta_valid) {
+    set_error("theta not computed");
+    return GEMS_ERR_STATE;
+  }
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = launch_from_buffer(s, length, lnl);
+  if (st) return st;
+  copy_pattern_lh(s, pattern_lh, *lnl);
+  return GEMS_OK;
+}
+
+int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
+                       int compute_theta, double min_len, double max_len, double xacc,
+                       int max_steps, double *opt_len, int *nevals) {
+  if (!s || !opt_len || (nops > 0 && !ops) || !(min_len >= 0) || !(max_len >= min_len) ||
+      max_steps < 1)
+    return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = check_branch(s, br);
+  if (st) return st;
+  if (compute_theta) {
+    if ((st = run_ops(s, ops, nops))) return st;
+    if ((st = launch_theta(s, br))) return st;
+    s->theta_valid = true;
+    s->theta_branch = *br;
+  } else if (!s->theta_valid) {
+    set_error("theta not computed");
+    return GEMS_ERR_STATE;
+  }
+  int ne = 0;
+  st = launch_newton(s, br->length, min_len, max_len, xacc, max_steps, opt_len, &ne);
+  if (nevals) *nevals = ne;
+  return st;
+}
+
+int gems_get_partial(gems_session *s, int slot, double *partial, uint16_t *scale) {
+  if (!s || slot < 0 || slot >= s->desc.nslots) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  const size_t blk = s->block, n = (size_t)s->desc.nptn * blk;
+  if (partial) {
+    if (s->desc.precision == GEMS_PREC_FP64) {
+      const double *src = static_cast<const double *>(s->d_partials) + (size_t)slot * s->P * blk;
+      GEMS_CUDA(cudaMemcpyAsync(partial, src, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                s->stream));
+    } else {
+      std::vector<float> tmp(n);
+      const float *src = static_cast<const float *>(s->d_partials) + (size_t)slot * s->P * blk;
+      GEMS_CUDA(cudaMemcpyAsync(tmp.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost,
+                                s->stream));
+      GEMS_CUDA(cudaStreamSynchronize(s->stream));
+      for (size_t i = 0; i < n; i++) partial[i] = tmp[i];
+    }
+  }
+  if (scale) {
+    const size_t per = s->desc.scaling == GEMS_SCALE_SAFE ? s->desc.ncat : 1;
+    GEMS_CUDA(cudaMemcpyAsync(scale, s->d_scale + (size_t)slot * s->P * per,
+                              (size_t)s->desc.nptn * per * 2, cudaMemcpyDeviceToHost, s->stream));
+  }
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
+int gems_get_theta(gems_session *s, double *theta, double *scale_all) {
+  if (!s) return GEMS_ERR_BAD_ARG;
+  if (!s->theta_valid) return GEMS_ERR_STATE;
+  if (theta)
+    GEMS_CUDA(cudaMemcpyAsync(theta, s->d_theta, sizeof(double) * s->desc.nptn * s->block,
+                              cudaMemcpyDeviceToHost, s->stream));
+  if (scale_all)
+    GEMS_CUDA(cudaMemcpyAsync(scale_all, s->d_scale_all, sizeof(double) * s->desc.nptn,
+                              cudaMemcpyDeviceToHost, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
+int gems_launch_count(gems_session *s, long long *count) {
+  if (!s || !count) return GEMS_ERR_BAD_ARG;
+  *count = s->launches;
+  return GEMS_OK;
+}
+
+int gems_profile_enable(gems_session *s, int on) {
+  if (!s) return GEMS_ERR_BAD_ARG;
+  s->prof_on = on != 0;
+  return GEMS_OK;
+}
+
+int gems_profile_read(gems_session *s, int kernel_id, double *total_ms, long long *launches) {
+  if (!s || kernel_id < 0 || kernel_id >= Session::kProfKernels) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  prof_collect(s);
+  if (total_ms) *total_ms = s->prof_ms[kernel_id];
+  if (launches) *launches = s->prof_n[kernel_id];
+  s->prof_ms[kernel_id] = 0.0;
+  s->prof_n[kernel_id] = 0;
+  return GEMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,200 @@
+/*
+ * gems_b200.h -- C-ABI of the B200 (sm_100a) Felsenstein likelihood kernels.
+ *
+ * Two layers, both plain C (pointers, sizes, int status codes; no CUDA or torch types):
+ *
+ *  1. Kernel set ("gems_*"): what a new LikelihoodKernel value of IQ-TREE's PhyloTree
+ *     forwards its member-function pointers to.  The device session owns every partial
+ *     likelihood buffer, scale counter, theta buffer and tip byte; the caller keeps topology
+ *     and cache flags and names buffers by slot id.  Replaces the pointer targets that
+ *     PhyloTree::setLikelihoodKernel installs (tree/phylotreesse.cpp:91-199):
+ *        computePartialLikelihoodPointer   (tree/phylotree.h:902-903)   -> gems_traverse
+ *        computeLikelihoodBranchPointer    (tree/phylotree.h:948-950)   -> gems_branch_lnl
+ *        computeLikelihoodDervPointer      (tree/phylotree.h:1343-1345) -> gems_branch_derv
+ *        computeLikelihoodFromBufferPointer(tree/phylotree.h:1002-1003) -> gems_lnl_from_buffer
+ *     plus the Newton loop of PhyloTree::optimizeOneBranch (tree/phylotree.cpp:2620-2670,
+ *     utils/optimization.cpp:422-499) -> gems_newton_branch.
+ *
+ *  2. Tree mirror ("gems_tree_*"): a C++ re-statement of the PhyloTree calls on the path
+ *     (computeLikelihood, computeLikelihoodBranch, computeLikelihoodDerv,
+ *     computeLikelihoodFromBuffer, optimizeOneBranch, optimizeAllBranches, clearAllPartialLH)
+ *     driving layer 1, for callers that do not bring their own PhyloTree.
+ *
+ * Every call returns a gems_status.  Nothing exits the process; the reference's outError /
+ * ASSERT paths map onto these codes.  Calls on one session are not thread-safe; distinct
+ * sessions may be used from distinct threads (each session owns one CUDA stream).
+ */
+#ifndef GEMS_B200_H
+#define GEMS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GEMS_OK = 0,
+    GEMS_ERR_OOM = 1,               /* device allocation failed */
+    GEMS_ERR_ADMISSION = 2,         /* footprint exceeds the admission budget */
+    GEMS_ERR_NUMERIC_UNDERFLOW = 3, /* non-finite derivative (reference: "-safe" advice) */
+    GEMS_ERR_TIMEOUT = 4,           /* a bounded device wait ran out */
+    GEMS_ERR_BAD_ARG = 5,
+    GEMS_ERR_CUDA = 6,              /* CUDA runtime error (message in gems_last_error) */
+    GEMS_ERR_STATE = 7,             /* call out of order (e.g. no model, theta not computed) */
+    GEMS_ERR_NO_DEVICE = 8
+} gems_status;
+
+enum { GEMS_PREC_FP64 = 0, GEMS_PREC_MIXED = 1 };
+enum { GEMS_SCALE_NORM = 0, GEMS_SCALE_SAFE = 1 };
+enum { GEMS_CHILD_TIP = 0, GEMS_CHILD_PARTIAL = 1 };
+
+typedef struct gems_session gems_session;
+
+typedef struct {
+    int ntaxa;      /* leaves; tip rows 0..ntaxa-1 */
+    int nptn;       /* unique patterns (aln->size()) */
+    int nstates;    /* 4 (DNA), 20 (protein), 61 (codon) or any 2..64 */
+    int ncat;       /* rate categories, 1..16 (ncat_mix of the reference) */
+    int nslots;     /* partial-likelihood buffers the session allocates */
+    int precision;  /* GEMS_PREC_FP64 or GEMS_PREC_MIXED */
+    int scaling;    /* GEMS_SCALE_NORM or GEMS_SCALE_SAFE (reference SAFE_NUMERIC) */
+    int device;     /* CUDA device ordinal */
+} gems_session_desc;
+
+/* One node of a traversal: recompute the partial of slot dst from two children.
+ * Mirrors TraversalInfo (tree/phylotree.h) for a binary node: the children are
+ * (kind, id): GEMS_CHILD_TIP with a taxon id, or GEMS_CHILD_PARTIAL with a slot id;
+ * len_* is the branch length from the node to that child. */
+typedef struct {
+    int dst_slot;
+    int left_kind, left_id;
+    int right_kind, right_id;
+    int pad_;
+    double left_len, right_len;
+} gems_op;
+
+/* A branch for lnL / derivatives: dad side is always a partial slot ("dad_branch" partial);
+ * node side is a tip or a partial slot.  length is the branch length. */
+typedef struct {
+    int dad_slot;
+    int node_kind, node_id;
+    int pad_;
+    double length;
+} gems_branch;
+
+/* ---- session ---- */
+const char *gems_version(void);
+const char *gems_last_error(void);
+int gems_device_count(int *count);
+/* Bytes a session with this descriptor holds on the device (admission by footprint). */
+int gems_session_footprint(const gems_session_desc *desc, size_t *bytes);
+int gems_session_create(const gems_session_desc *desc, gems_session **out);
+int gems_session_destroy(gems_session *s);
+int gems_session_sync(gems_session *s);
+/* the descriptor the session was created with */
+int gems_session_info(gems_session *s, gems_session_desc *desc);
+/* the CUDA stream (cudaStream_t) the session launches on, for event timing by the caller */
+int gems_session_stream(gems_session *s, void **stream);
+
+/* Tip state bytes [ntaxa][nptn] (PhyloTree::getConvertedSequenceByNumber rows,
+ * tree/phylotree.cpp:3331): 0..n-1 states, DNA 4..17 ambiguity bitmask codes, protein
+ * 20..22 (B, Z, J), STATE_UNKNOWN (DNA 18, protein 23, else n) for gaps. */
+int gems_upload_tips(gems_session *s, const uint8_t *states);
+/* ptn_freq[nptn] and ptn_invar[nptn] (phylotreesse.cpp:537,549); invar may be NULL (zeros). */
+int gems_upload_patterns(gems_session *s, const double *ptn_freq, const double *ptn_invar);
+
+/* Model: eval[n], evec[n*n], inv_evec[n*n] row-major (ModelSubst getters,
+ * model/modelsubst.h:363-371); rates[ncat], props[ncat] (RateHeterogeneity getRate/getProp,
+ * model/rateheterogeneity.h:107-172).  Builds the tip tables on the device
+ * (phylotreesse.cpp:243-375). */
+int gems_set_model(gems_session *s, const double *eval, const double *evec,
+                   const double *inv_evec, const double *rates, const double *props);
+/* Same, but the FP64 eigendecomposition of the reversible rate matrix runs on the GPU
+ * (cyclic Jacobi on the sqrt(pi)-symmetrised matrix; replaces ModelMarkov::decomposeRateMatrix,
+ * model/modelmarkov.cpp:1389-1630).  exch_upper holds the n(n-1)/2 exchangeabilities. */
+int gems_set_model_from_rates(gems_session *s, const double *exch_upper, const double *freq,
+                              const double *rates, const double *props);
+/* Copy back the eigensystem in use (for inspection). */
+int gems_get_eigensystem(gems_session *s, double *eval, double *evec, double *inv_evec);
+
+/* ---- kernel set ---- */
+/* Postorder list of node updates (computePartialLikelihood over all patterns for each
+ * entry of traversal_info; tree/phylokernelnew.h:1293-2043). */
+int gems_traverse(gems_session *s, const gems_op *ops, int nops);
+/* Branch log-likelihood (computeLikelihoodBranchSIMD, tree/phylokernelnew.h:2658-3275),
+ * after running ops (may be 0).  pattern_lh[nptn] optional (log-likelihood per pattern
+ * including the scaling correction). */
+int gems_branch_lnl(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
+                    double *lnl, double *pattern_lh);
+/* Derivatives of lnL w.r.t. the branch length (computeLikelihoodDervSIMD,
+ * tree/phylokernelnew.h:2238-2650).  When compute_theta != 0 the ops run first and theta is
+ * rebuilt from the two partials (computeLikelihoodBufferSIMD, :2053-2235); otherwise the
+ * resident theta is reused at br->length.  df_frac[nptn] (G_matrix row) optional. */
+int gems_branch_derv(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
+                     int compute_theta, double *df, double *ddf, double *df_frac);
+/* lnL from the resident theta at a new length (computeLikelihoodFromBufferSIMD,
+ * tree/phylokernelnew.h:3285-3495). */
+int gems_lnl_from_buffer(gems_session *s, double length, double *lnl, double *pattern_lh);
+/* Safeguarded Newton on -lnL(t) in [min_len, max_len], starting from guess, over the resident
+ * theta of br (rebuilt first when compute_theta != 0).  Same iterate sequence as
+ * Optimization::minimizeNewton (utils/optimization.cpp:422-499); the loop runs on the device.
+ * opt_len receives the returned length, nevals the number of derivative evaluations. */
+int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
+                       int compute_theta, double min_len, double max_len, double xacc,
+                       int max_steps, double *opt_len, int *nevals);
+
+/* ---- inspection ---- */
+/* partial[nptn * ncat * nstates] (pattern-major, category-major, state-contiguous; FP64
+ * values, converted from the session precision) and scale[nptn] (NORM) or [nptn*ncat]
+ * (SAFE) counters of a slot.  Either pointer may be NULL. */
+int gems_get_partial(gems_session *s, int slot, double *partial, uint16_t *scale);
+/* theta[nptn * block] and per-pattern log scale (buffer_scale_all). */
+int gems_get_theta(gems_session *s, double *theta, double *scale_all);
+/* number of kernel launches issued by this session so far */
+int gems_launch_count(gems_session *s, long long *count);
+/* Kernel timing with CUDA events on the session stream: when enabled, every launch of the
+ * traversal kernel (kernel id 0), branch kernel (1), theta (2), derivative (3),
+ * from-buffer (4) and Newton (5) kernels is bracketed by events; gems_profile_read returns the
+ * summed device time in ms and the number of timed launches, then resets the counters. */
+int gems_profile_enable(gems_session *s, int on);
+int gems_profile_read(gems_session *s, int kernel_id, double *total_ms, long long *launches);
+
+/* ---- tree mirror (PhyloTree calls on the path) ---- */
+typedef struct gems_tree gems_tree;
+/* Unrooted binary tree: leaves 0..ntaxa-1, internal nodes ntaxa..nedges; each node's
+ * neighbour order follows the edge order.  The session must have been created with
+ * nslots >= ntaxa-2 (one partial per internal node, LM_PER_NODE) and may have up to
+ * 3*(ntaxa-2) (one per directed branch). */
+int gems_tree_create(gems_session *s, int nedges, const int *eu, const int *ev,
+                     const double *len, gems_tree **out);
+int gems_tree_destroy(gems_tree *t);
+int gems_tree_set_branch_limits(gems_tree *t, double min_len, double max_len);
+int gems_tree_set_length(gems_tree *t, int u, int v, double len);
+int gems_tree_get_lengths(gems_tree *t, double *len); /* in edge order */
+int gems_tree_clear_all_partial_lh(gems_tree *t);
+/* PhyloTree::computeLikelihood (tree/phylotree.cpp:1258) */
+int gems_tree_compute_likelihood(gems_tree *t, double *lnl, double *pattern_lh);
+/* computeLikelihoodBranch(dad->findNeighbor(node), dad) */
+int gems_tree_compute_likelihood_branch(gems_tree *t, int node, int dad, double *lnl,
+                                        double *pattern_lh);
+/* computeLikelihoodDerv(dad->findNeighbor(node), dad) */
+int gems_tree_compute_likelihood_derv(gems_tree *t, int node, int dad, double *df, double *ddf);
+int gems_tree_compute_likelihood_from_buffer(gems_tree *t, double *lnl);
+/* optimizeOneBranch(node1, node2, clearLH, maxNRStep) (tree/phylotree.cpp:2620) */
+int gems_tree_optimize_one_branch(gems_tree *t, int node1, int node2, int clear_lh,
+                                  int max_nr_step);
+/* optimizeAllBranches(my_iterations, tolerance, maxNRStep) (tree/phylotree.cpp:2724) */
+int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double tolerance,
+                                    int max_nr_step, double *lnl);
+/* partial of directed branch dad->node (subtree at node), if valid */
+int gems_tree_get_partial(gems_tree *t, int node, int dad, double *partial, uint16_t *scale);
+/* partial recomputations (traversal ops) executed so far, and Newton evaluations of the
+ * last optimize_one_branch */
+int gems_tree_stats(gems_tree *t, long long *partial_ops, int *last_newton_evals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

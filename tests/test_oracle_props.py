@@ -1,0 +1,60 @@
+"""Size-independent properties of the oracle itself (it is the checker, so it is checked):
+derivatives against finite differences, NORM vs SAFE, invariance to the evaluation branch,
+Newton returning a stationary point."""
+import numpy as np
+import pytest
+
+from gems_b200 import synth
+from oracle import oracle as orc
+
+
+def small_case(n=4, ntaxa=10, nsites=600, seed=3):
+    rng = np.random.default_rng(seed)
+    model = synth.dna_gtr(rng) if n == 4 else synth.protein(rng)
+    tree = synth.random_tree(ntaxa, 0.12, seed + 1)
+    aln = synth.simulate(tree, model, nsites, seed + 2)
+    return tree, model, aln
+
+
+@pytest.mark.parametrize("n", [4, 20])
+def test_lnl_same_on_every_branch(n):
+    tree, model, aln = small_case(n)
+    ot = orc.OracleTree(tree, model, aln)
+    vals = [ot.computeLikelihoodBranch(int(u), int(v)) for u, v in zip(tree.eu, tree.ev)]
+    assert np.ptp(vals) < 1e-9 * abs(vals[0])
+
+
+@pytest.mark.parametrize("n", [4, 20])
+def test_derivatives_match_finite_differences(n):
+    tree, model, aln = small_case(n)
+    ot = orc.OracleTree(tree, model, aln)
+    for e in (0, 3, len(tree.eu) - 1):
+        u, v = int(tree.eu[e]), int(tree.ev[e])
+        t0 = float(tree.length[e])
+        h = 1e-5
+        f = []
+        for t in (t0 - h, t0, t0 + h):
+            ot.setLength(u, v, t)
+            f.append(ot.computeLikelihoodBranch(v, u))
+        ot.setLength(u, v, t0)
+        ot.clearAllPartialLH()
+        df, ddf = ot.computeLikelihoodDerv(v, u)
+        assert abs(df - (f[2] - f[0]) / (2 * h)) < 1e-4 * max(1, abs(df))
+        assert abs(ddf - (f[2] - 2 * f[1] + f[0]) / h ** 2) < 1e-2 * max(1, abs(ddf))
+
+
+def test_norm_and_safe_agree():
+    tree, model, aln = small_case(4, ntaxa=120, nsites=300, seed=9)
+    a = orc.OracleTree(tree, model, aln, safe=False).computeLikelihood()
+    b = orc.OracleTree(tree, model, aln, safe=True).computeLikelihood()
+    assert abs(a - b) < 1e-9 * abs(a)
+
+
+def test_newton_reaches_stationary_point():
+    tree, model, aln = small_case(4)
+    ot = orc.OracleTree(tree, model, aln)
+    u, v = int(tree.eu[2]), int(tree.ev[2])
+    ot.optimizeOneBranch(u, v)
+    ot.clearAllPartialLH()
+    df, ddf = ot.computeLikelihoodDerv(v, u)
+    assert abs(df) < 1e-3 and ddf < 0
