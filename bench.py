@@ -284,8 +284,12 @@ def main():
     ms = float(t.item())
 
     # end to end through the public API from host buffers
-    pat_host = np.ascontiguousarray(aln.patterns)
-    w_host = np.ascontiguousarray(aln.weights)
+    pin_pat = torch.empty(aln.patterns.shape, dtype=torch.uint8, pin_memory=True)
+    pin_w = torch.empty(aln.weights.shape, dtype=torch.float64, pin_memory=True)
+    pat_host = pin_pat.numpy()
+    w_host = pin_w.numpy()
+    pat_host[:] = aln.patterns
+    w_host[:] = aln.weights
     h2d = pat_host.nbytes + w_host.nbytes
     d2h = 8 * P + 8
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -132,6 +132,11 @@ int launch_newton(Session *s, double length0, double min_len, double max_len, do
                   int max_steps, double *opt_len, int *nevals);
 int launch_eigen(Session *s, const double *exch_upper, const double *freq);
 int launch_unpack_partial(Session *s, int slot, double *d_out);
+// mixed precision (kernels_mixed.cu)
+int launch_prep_ops_mixed(Session *s, int nops);
+int launch_traverse_mixed(Session *s, int nops);
+int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta,
+                       double *lnl);
 
 }  // namespace gems
 

@@ -226,8 +226,13 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
   }
   int st = upload_ops(s, ops, nops);
   if (st) return st;
-  if ((st = launch_prep_ops(s, nops))) return st;
-  if ((st = launch_traverse(s, nops))) return st;
+  if (s->desc.precision == GEMS_PREC_MIXED) {
+    if ((st = launch_prep_ops_mixed(s, nops))) return st;
+    if ((st = launch_traverse_mixed(s, nops))) return st;
+  } else {
+    if ((st = launch_prep_ops(s, nops))) return st;
+    if ((st = launch_traverse(s, nops))) return st;
+  }
   for (int k = 0; k < nops; k++)
     if (s->theta_valid &&
         (ops[k].dst_slot == s->theta_branch.dad_slot ||
@@ -383,11 +388,13 @@ int gems_upload_tips(gems_session *s, const uint8_t *states) {
   if (!s || !states) return GEMS_ERR_BAD_ARG;
   GEMS_CUDA(cudaSetDevice(s->desc.device));
   const int unk = s->unknown;
-  for (size_t i = 0; i < (size_t)s->desc.ntaxa * s->desc.nptn; i++)
-    if (states[i] > unk) {
-      set_error("tip state byte out of range");
-      return GEMS_ERR_BAD_ARG;
-    }
+  uint8_t mx = 0;
+  const size_t total = (size_t)s->desc.ntaxa * s->desc.nptn;
+  for (size_t i = 0; i < total; i++) mx = states[i] > mx ? states[i] : mx;
+  if (mx > unk) {
+    set_error("tip state byte out of range");
+    return GEMS_ERR_BAD_ARG;
+  }
   GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips, s->P, states, s->desc.nptn, s->desc.nptn,
                               s->desc.ntaxa, cudaMemcpyHostToDevice, s->stream));
   GEMS_CUDA(cudaStreamSynchronize(s->stream));
@@ -516,7 +523,11 @@ int gems_branch_lnl(gems_session *s, const gems_op *ops, int nops, const gems_br
   int st = check_branch(s, br);
   if (st) return st;
   if ((st = run_ops(s, ops, nops))) return st;
-  if ((st = launch_branch_lnl(s, br, lnl))) return st;
+  if (s->desc.precision == GEMS_PREC_MIXED)
+    st = launch_theta_mixed(s, br, true, false, lnl);
+  else
+    st = launch_branch_lnl(s, br, lnl);
+  if (st) return st;
   copy_pattern_lh(s, pattern_lh, *lnl);
   return GEMS_OK;
 }
@@ -529,7 +540,9 @@ int gems_branch_derv(gems_session *s, const gems_op *ops, int nops, const gems_b
   if (st) return st;
   if (compute_theta) {
     if ((st = run_ops(s, ops, nops))) return st;
-    if ((st = launch_theta(s, br))) return st;
+    st = s->desc.precision == GEMS_PREC_MIXED ? launch_theta_mixed(s, br, false, true, nullptr)
+                                              : launch_theta(s, br);
+    if (st) return st;
     s->theta_valid = true;
     s->theta_branch = *br;
   } else if (!s->theta_valid) {
@@ -569,7 +582,9 @@ int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems
   if (st) return st;
   if (compute_theta) {
     if ((st = run_ops(s, ops, nops))) return st;
-    if ((st = launch_theta(s, br))) return st;
+    st = s->desc.precision == GEMS_PREC_MIXED ? launch_theta_mixed(s, br, false, true, nullptr)
+                                              : launch_theta(s, br);
+    if (st) return st;
     s->theta_valid = true;
     s->theta_branch = *br;
   } else if (!s->theta_valid) {

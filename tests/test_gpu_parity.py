@@ -175,3 +175,44 @@ def test_kernel_set_errors(gpu):
     with pytest.raises(GemsError) as e:
         s.upload_tips(np.full((5, 10), 99, np.uint8))  # state byte out of range
     assert e.value.status == 5
+
+
+# ---- mixed-precision form: FP32 real-space partials, FP64 theta / reductions / Newton ----
+MIXED_RTOL = 1e-6  # |dlnL| <= 1e-6 |lnL|
+
+
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_mixed_lnl_within_1e6(gpu, path):
+    tree, model, aln, z = load_golden(path)
+    safe = bool(z["safe"])
+    ot = orc.OracleTree(tree, model, aln, safe=safe, const_char=z["const_char"])
+    gt = gpu_tree(tree, model, aln, safe, precision="mixed")
+    lo, plo = ot.computeLikelihood(pattern_lh=True)
+    lg, plg = gt.computeLikelihood(pattern_lh=True)
+    assert abs(lg - lo) <= MIXED_RTOL * abs(lo), (lg, lo)
+    assert np.max(np.abs(plg - plo) / (np.abs(plo) + 1.0)) < 1e-5
+    u, v = int(tree.eu[1]), int(tree.ev[1])
+    ot.clearAllPartialLH()
+    gt.clearAllPartialLH()
+    dfo, ddfo = ot.computeLikelihoodDerv(v, u)
+    dfg, ddfg = gt.computeLikelihoodDerv(v, u)
+    assert abs(dfg - dfo) <= 1e-5 * max(1.0, abs(dfo)) + 1e-6 * abs(lo)
+    assert abs(ddfg - ddfo) <= 1e-5 * max(1.0, abs(ddfo)) + 1e-6 * abs(lo)
+
+
+@pytest.mark.parametrize("n", [4, 20, 61])
+def test_mixed_optimize_all(gpu, n):
+    rng = np.random.default_rng(40 + n)
+    model = {4: synth.dna_gtr, 20: synth.protein, 61: synth.codon_gy}[n](rng)
+    tree = synth.random_tree(24, 0.1, 7 + n)
+    aln = synth.simulate(tree, model, 1500, 9 + n)
+    safe = n == 61
+    ot = orc.OracleTree(tree, model, aln, safe=safe)
+    gt = gpu_tree(tree, model, aln, safe, precision="mixed")
+    lo = ot.optimizeAllBranches(100, 0.001, 100)
+    lg = gt.optimizeAllBranches(100, 0.001, 100)
+    assert abs(lg - lo) <= MIXED_RTOL * abs(lo)
+    # the mixed lengths are re-evaluated in FP64 by the oracle at its own precision
+    ot2 = orc.OracleTree(synth.Tree(tree.ntaxa, tree.eu, tree.ev, gt.getBranchLengths()),
+                         model, aln, safe=safe)
+    assert abs(ot2.computeLikelihood() - lo) <= MIXED_RTOL * abs(lo)
