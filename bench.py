@@ -40,9 +40,13 @@ from gems_b200 import synth  # noqa: E402
 
 NSITES = 1_000_000
 NTAXA = 512
-BYTES_II = 3 * 4 * 4 * 8 + 3 * 2   # internal-internal update, FP64, NORM
-BYTES_TI = 2 * 4 * 4 * 8 + 1 + 2 * 2
-BYTES_TT = 4 * 4 * 8 + 2 + 2
+
+
+def update_bytes(s):
+    """Algorithmic bytes of one site-partial update (C=4, n=4, NORM scale counters of 2 B):
+    internal-internal 3*C*n*s + 3*2, tip-internal 2*C*n*s + 1 + 2*2, tip-tip C*n*s + 2 + 2,
+    with s = 8 (FP64) or 4 (FP32 partials)."""
+    return 3 * 16 * s + 6, 2 * 16 * s + 5, 16 * s + 4
 
 
 def env_rank():
@@ -310,7 +314,8 @@ def main():
 
     ups = world * nops * P / (ms * 1e-3)
     ups_e2e = world * nops * P / (ms_e2e * 1e-3)
-    alg_bytes = P * (kinds[0] * BYTES_II + kinds[1] * BYTES_TI + kinds[2] * BYTES_TT)
+    b_ii, b_ti, b_tt = update_bytes(8 if args.precision == "fp64" else 4)
+    alg_bytes = P * (kinds[0] * b_ii + kinds[1] * b_ti + kinds[2] * b_tt)
     peak, peak_kind = read_peaks()
     achieved = alg_bytes / (trav_ms / max(trav_n, 1) * 1e-3) / 1e9 if trav_n else None
     line = {
@@ -334,7 +339,7 @@ def main():
                      "frac": (achieved / peak) if achieved else None,
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "avg_launch_ms": trav_ms / max(trav_n, 1),
-                     "traffic": read_traffic("traverse_fp64_dna512.md")},
+                     "traffic": read_traffic(f"traverse_{args.precision}_dna512.md")},
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu:

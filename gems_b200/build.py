@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                   "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
-CUDA_SOURCES = ["session.cu", "kernels_fp64.cu", "kernels_mixed.cu", "eigen.cu",
+CUDA_SOURCES = ["session.cu", "kernels_fp64.cu", "kernels_mixed.cu", "kernels_traverse.cu", "eigen.cu",
                 "phylotree.cpp"]
 HEADERS = ["gems_internal.cuh"]
 

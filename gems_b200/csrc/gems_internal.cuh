@@ -92,6 +92,7 @@ struct Session {
   DevOp *h_ops = nullptr;
   double *h_result = nullptr;
   int nred = 0;  // size of d_red in doubles
+  std::vector<double> h_evec, h_inv;  // host copy of the eigenvectors in use
   // kernel timing (gems_profile_*): event pairs recorded around launches
   static constexpr int kProfKernels = 8;
   bool prof_on = false;
@@ -137,6 +138,10 @@ int launch_prep_ops_mixed(Session *s, int nops);
 int launch_traverse_mixed(Session *s, int nops);
 int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta,
                        double *lnl);
+// factored whole-traversal kernels for 4 and 20 states (kernels_traverse.cu)
+bool traverse_v2_supported(const Session *s);
+int launch_prep_ops_v2(Session *s, int nops);
+int launch_traverse_v2(Session *s, int nops);
 
 }  // namespace gems
 

@@ -1,0 +1,398 @@
+// kernels_traverse.cu -- whole-traversal kernels for 4- and 20-state models (FP64 and mixed).
+//
+// One CTA owns a tile of patterns and runs every node update of the traversal over it, in
+// postorder; a pattern stays with one lane group for all ops, so a child written by an earlier
+// op is read back by the same warp (L2-resident in practice: the DRAM traffic of a traversal is
+// dominated by the partial writes).  Lane c of a group owns rate category c.
+//
+// FP64 form.  The reference precomputes E_c = evec . diag(exp(eval r_c t)) per child
+// (phylokernelnew.h:1043-1062) and applies it with a dense n x n product per category.  Here
+// the product is factored as
+//      E_c . L = evec . (d_c (*) L),        d_c[i] = exp(eval_i r_c t)
+// evec and inv_evec do not depend on the category or the op: they travel as kernel parameters,
+// so every lane of a warp reads the same element (uniform operand, no per-lane load), and an
+// op only loads its 2 x n exponential factors, stored category-fastest so the lanes of a
+// group read one 32-byte sector.  Tip children use the table sum_i E_c[x][i] tip[s][i]
+// (stored [s][x][c]).  The FP64 values agree with the reference form to rounding.
+//
+// Mixed form (FP32 real space): the transition matrices P_c(t) are op-dependent; they are
+// stored [x][y][c] so a warp-wide load of element (x, y) is one sector per 8 groups.
+#include <cmath>
+#include <string>
+
+#include "gems_internal.cuh"
+
+namespace gems {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <int N>
+struct EigPack {
+  double evec[N * N];
+  double inv[N * N];
+};
+
+__device__ __forceinline__ double group_max(double v, int G) {
+  for (int o = 1; o < G; o <<= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float group_maxf(float v, int G) {
+  for (int o = 1; o < G; o <<= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ---------------------------------------------------------------------------------------
+// FP64 op tables: d[side][i][c] = exp(eval_i r_c t_side); tip tables leaf[side][s][x][c]
+// table layout per op (doubles): [2][N][C] then [2][U1][N][C]
+// ---------------------------------------------------------------------------------------
+__global__ void k_prep_ops_f64(DevCtx c, const DevOp *ops, double *tab, size_t stride) {
+  extern __shared__ double dsh[];  // [N][C]
+  const int k = blockIdx.x, side = blockIdx.y;
+  const DevOp op = ops[k];
+  const int kind = side ? op.r_kind : op.l_kind;
+  const double len = side ? op.r_len : op.l_len;
+  const int n = c.n, C = c.C, blk = c.block;
+  double *d = tab + (size_t)k * stride + (size_t)side * blk;
+  for (int idx = threadIdx.x; idx < blk; idx += blockDim.x) {
+    const int i = idx / C, cc = idx - i * C;
+    const double v = exp(c.eval[i] * (c.rates[cc] * len));
+    d[idx] = v;
+    dsh[idx] = v;
+  }
+  if (kind != GEMS_CHILD_TIP) return;
+  __syncthreads();
+  double *leaf = tab + (size_t)k * stride + (size_t)2 * blk + (size_t)side * (c.unknown + 1) * blk;
+  const int rows = c.unknown * blk;
+  for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
+    const int s = idx / blk, r = idx - s * blk, x = r / C, cc = r - x * C;
+    const double *t = c.tip + (size_t)s * n;
+    double acc = 0.0;
+    for (int i = 0; i < n; i++) acc = fma(c.evec[x * n + i] * dsh[i * C + cc], t[i], acc);
+    leaf[idx] = acc;
+  }
+  for (int idx = threadIdx.x; idx < blk; idx += blockDim.x) leaf[rows + idx] = 1.0;
+}
+
+template <int N, bool SAFE>
+__device__ __forceinline__ void msg_f64(const DevCtx &c, const EigPack<N> &E, int kind, int id,
+                                        const double *__restrict__ d,
+                                        const double *__restrict__ leaf, long p, int gl,
+                                        double (&v)[N], int &s) {
+  const int C = c.C;
+  if (kind == GEMS_CHILD_TIP) {
+    const int st = c.tips[(size_t)id * c.P + p];
+    const double *lt = leaf + (size_t)st * c.block + gl;
+#pragma unroll
+    for (int x = 0; x < N; x++) v[x] = __ldg(lt + x * C);
+    s = 0;
+  } else {
+    const double *src = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems +
+                        (size_t)p * c.block + gl * N;
+    double L[N];
+    if constexpr (N % 2 == 0) {
+      const double2 *s2 = reinterpret_cast<const double2 *>(src);
+#pragma unroll
+      for (int i = 0; i < N / 2; i++) {
+        const double2 t = __ldcg(s2 + i);
+        L[2 * i] = t.x;
+        L[2 * i + 1] = t.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < N; i++) L[i] = __ldcg(src + i);
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) L[i] *= __ldg(d + i * C + gl);
+#pragma unroll
+    for (int x = 0; x < N; x++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int i = 0; i < N; i++) acc = fma(E.evec[x * N + i], L[i], acc);
+      v[x] = acc;
+    }
+    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+    s = SAFE ? sc[(size_t)p * C + gl] : sc[p];
+  }
+}
+
+template <int N, bool SAFE>
+__global__ void __launch_bounds__(kThreads) k_traverse_f64(DevCtx c, const DevOp *__restrict__ ops,
+                                                           int nops,
+                                                           const double *__restrict__ tab,
+                                                           size_t stride, const EigPack<N> E) {
+  const int G = c.G;
+  const int gl = threadIdx.x & (G - 1);
+  const long p = ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool act = p < c.P && gl < c.C;
+  const int C = c.C, blk = c.block;
+  double *part = static_cast<double *>(c.partials);
+  for (int k = 0; k < nops; k++) {
+    const DevOp op = ops[k];
+    const double *tk = tab + (size_t)k * stride;
+    const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
+    double out[N];
+    double lh_max = 0.0;
+    int sl = 0, sr = 0;
+    if (act) {
+      double tmp[N];
+      {
+        double vl[N], vr[N];
+        msg_f64<N, SAFE>(c, E, op.l_kind, op.l_id, tk, tk + 2 * blk, p, gl, vl, sl);
+        msg_f64<N, SAFE>(c, E, op.r_kind, op.r_id, tk + blk,
+                         tk + 2 * blk + (size_t)(c.unknown + 1) * blk, p, gl, vr, sr);
+#pragma unroll
+        for (int x = 0; x < N; x++) tmp[x] = vl[x] * vr[x];
+      }
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int x = 0; x < N; x++) acc = fma(E.inv[j * N + x], tmp[x], acc);
+        out[j] = acc;
+        lh_max = fmax(lh_max, fabs(acc));
+      }
+    }
+    if (!SAFE) lh_max = group_max(lh_max, G);
+    int s_out = sl + sr;
+    if (act) {
+      if (!tiptip && lh_max < kScaleThr && c.invar[p] == 0.0) {
+#pragma unroll
+        for (int j = 0; j < N; j++) out[j] = ldexp(out[j], kScaleExp);
+        s_out += 1;
+      }
+      double *dst = part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * blk + gl * N;
+      if constexpr (N % 2 == 0) {
+        double2 *d2 = reinterpret_cast<double2 *>(dst);
+#pragma unroll
+        for (int i = 0; i < N / 2; i++) d2[i] = make_double2(out[2 * i], out[2 * i + 1]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < N; i++) dst[i] = out[i];
+      }
+      uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
+      if (SAFE)
+        sc[(size_t)p * C + gl] = (uint16_t)s_out;
+      else if (gl == 0)
+        sc[p] = (uint16_t)s_out;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Mixed: P_c(t) = evec diag(exp(eval r_c t)) inv_evec in FP64, rounded to FP32, stored
+// [side][x][y][c]; tip tables [side][s][x][c] = P_c . indicator(s).
+// ---------------------------------------------------------------------------------------
+__global__ void k_prep_ops_mix(DevCtx c, const DevOp *ops, float *tab, size_t stride_f) {
+  extern __shared__ double ex[];  // [C][n]
+  const int k = blockIdx.x, side = blockIdx.y;
+  const DevOp op = ops[k];
+  const int kind = side ? op.r_kind : op.l_kind;
+  const double len = side ? op.r_len : op.l_len;
+  const int n = c.n, C = c.C, nnC = n * n * C;
+  for (int idx = threadIdx.x; idx < C * n; idx += blockDim.x) {
+    const int cc = idx / n, i = idx - cc * n;
+    ex[idx] = exp(c.eval[i] * (c.rates[cc] * len));
+  }
+  __syncthreads();
+  float *Pm = tab + (size_t)k * stride_f + (size_t)side * nnC;
+  for (int idx = threadIdx.x; idx < nnC; idx += blockDim.x) {
+    const int xy = idx / C, cc = idx - xy * C, x = xy / n, y = xy - x * n;
+    double acc = 0.0;
+    for (int i = 0; i < n; i++) acc = fma(c.evec[x * n + i] * ex[cc * n + i], c.inv_evec[i * n + y], acc);
+    Pm[idx] = (float)fmax(acc, 0.0);
+  }
+  if (kind != GEMS_CHILD_TIP) return;
+  __syncthreads();
+  float *leaf = tab + (size_t)k * stride_f + (size_t)2 * nnC + (size_t)side * (c.unknown + 1) * c.block;
+  const int rows = (c.unknown + 1) * c.block;
+  for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
+    const int s = idx / c.block, r = idx - s * c.block, x = r / C, cc = r - x * C;
+    const double *ind = c.tip_real + (size_t)s * n;
+    float acc = 0.f;
+    for (int y = 0; y < n; y++) acc = fmaf(Pm[(x * n + y) * C + cc], (float)ind[y], acc);
+    leaf[idx] = acc;
+  }
+}
+
+template <int N, bool SAFE>
+__device__ __forceinline__ void msg_mix(const DevCtx &c, int kind, int id,
+                                        const float *__restrict__ Pm,
+                                        const float *__restrict__ leaf, long p, int gl,
+                                        float (&v)[N], int &s) {
+  const int C = c.C;
+  if (kind == GEMS_CHILD_TIP) {
+    const int st = c.tips[(size_t)id * c.P + p];
+    const float *lt = leaf + (size_t)st * c.block + gl;
+#pragma unroll
+    for (int x = 0; x < N; x++) v[x] = __ldg(lt + x * C);
+    s = 0;
+  } else {
+    const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
+                       (size_t)p * c.block + gl * N;
+    float L[N];
+    if constexpr (N % 4 == 0) {
+      const float4 *s4 = reinterpret_cast<const float4 *>(src);
+#pragma unroll
+      for (int i = 0; i < N / 4; i++) {
+        const float4 t = __ldcg(s4 + i);
+        L[4 * i] = t.x;
+        L[4 * i + 1] = t.y;
+        L[4 * i + 2] = t.z;
+        L[4 * i + 3] = t.w;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < N; i++) L[i] = __ldcg(src + i);
+    }
+#pragma unroll
+    for (int x = 0; x < N; x++) {
+      float acc = 0.f;
+#pragma unroll
+      for (int y = 0; y < N; y++) acc = fmaf(__ldg(Pm + (x * N + y) * C + gl), L[y], acc);
+      v[x] = acc;
+    }
+    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+    s = SAFE ? sc[(size_t)p * C + gl] : sc[p];
+  }
+}
+
+template <int N, bool SAFE>
+__global__ void __launch_bounds__(kThreads) k_traverse_mix(DevCtx c, const DevOp *__restrict__ ops,
+                                                           int nops, const float *__restrict__ tab,
+                                                           size_t stride_f) {
+  const int G = c.G;
+  const int gl = threadIdx.x & (G - 1);
+  const long p = ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool act = p < c.P && gl < c.C;
+  const int C = c.C;
+  const size_t nnC = (size_t)N * N * C;
+  float *part = static_cast<float *>(c.partials);
+  for (int k = 0; k < nops; k++) {
+    const DevOp op = ops[k];
+    const float *tk = tab + (size_t)k * stride_f;
+    const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
+    float out[N];
+    float lh_max = 0.f;
+    int sl = 0, sr = 0;
+    if (act) {
+      float vl[N], vr[N];
+      msg_mix<N, SAFE>(c, op.l_kind, op.l_id, tk, tk + 2 * nnC, p, gl, vl, sl);
+      msg_mix<N, SAFE>(c, op.r_kind, op.r_id, tk + nnC,
+                       tk + 2 * nnC + (size_t)(c.unknown + 1) * c.block, p, gl, vr, sr);
+#pragma unroll
+      for (int x = 0; x < N; x++) {
+        out[x] = vl[x] * vr[x];
+        lh_max = fmaxf(lh_max, out[x]);
+      }
+    }
+    if (!SAFE) lh_max = group_maxf(lh_max, G);
+    int s_out = sl + sr;
+    if (act) {
+      if (!tiptip && lh_max < kScaleThrF && c.invar[p] == 0.0) {
+#pragma unroll
+        for (int x = 0; x < N; x++) out[x] *= 18446744073709551616.0f;  // 2^64
+        s_out += 1;
+      }
+      float *dst = part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * c.block + gl * N;
+      if constexpr (N % 4 == 0) {
+        float4 *d4 = reinterpret_cast<float4 *>(dst);
+#pragma unroll
+        for (int i = 0; i < N / 4; i++)
+          d4[i] = make_float4(out[4 * i], out[4 * i + 1], out[4 * i + 2], out[4 * i + 3]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < N; i++) dst[i] = out[i];
+      }
+      uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
+      if (SAFE)
+        sc[(size_t)p * C + gl] = (uint16_t)s_out;
+      else if (gl == 0)
+        sc[p] = (uint16_t)s_out;
+    }
+    __syncwarp();
+  }
+}
+
+inline int grid_for(const Session *s) {
+  const long threads = (long)s->P * s->G;
+  return (int)((threads + kThreads - 1) / kThreads);
+}
+
+template <int N>
+int launch_f64(Session *s, int nops) {
+  DevCtx c = s->ctx();
+  EigPack<N> E;
+  if (s->h_evec.size() != (size_t)N * N || s->h_inv.size() != (size_t)N * N) {
+    set_error("eigensystem not set");
+    return GEMS_ERR_STATE;
+  }
+  for (int i = 0; i < N * N; i++) {
+    E.evec[i] = s->h_evec[i];
+    E.inv[i] = s->h_inv[i];
+  }
+  const int grid = grid_for(s);
+  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  if (safe)
+    k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                               s->op_stride, E);
+  else
+    k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                                s->op_stride, E);
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  return GEMS_OK;
+}
+
+}  // namespace
+
+bool traverse_v2_supported(const Session *s) {
+  return s->desc.nstates == 4 || s->desc.nstates == 20;
+}
+
+int launch_prep_ops_v2(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  DevCtx c = s->ctx();
+  if (s->desc.precision == GEMS_PREC_MIXED) {
+    const size_t smem = sizeof(double) * s->block;
+    k_prep_ops_mix<<<dim3(nops, 2), 256, smem, s->stream>>>(
+        c, s->d_ops, reinterpret_cast<float *>(s->d_opmats), s->op_stride);
+  } else {
+    const size_t smem = sizeof(double) * s->block;
+    k_prep_ops_f64<<<dim3(nops, 2), 256, smem, s->stream>>>(c, s->d_ops, s->d_opmats,
+                                                             s->op_stride);
+  }
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  return GEMS_OK;
+}
+
+int launch_traverse_v2(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  cudaEvent_t ev0;
+  if (int st = prof_begin(s, 0, &ev0)) return st;
+  int st = GEMS_OK;
+  if (s->desc.precision == GEMS_PREC_MIXED) {
+    DevCtx c = s->ctx();
+    const int grid = grid_for(s);
+    const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+    const float *tab = reinterpret_cast<const float *>(s->d_opmats);
+    if (s->desc.nstates == 4) {
+      if (safe) k_traverse_mix<4, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+      else k_traverse_mix<4, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+    } else {
+      if (safe) k_traverse_mix<20, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+      else k_traverse_mix<20, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+    }
+    s->launches++;
+    GEMS_CUDA(cudaGetLastError());
+  } else {
+    st = s->desc.nstates == 4 ? launch_f64<4>(s, nops) : launch_f64<20>(s, nops);
+  }
+  if (st) return st;
+  return prof_end(s, 0, ev0);
+}
+
+}  // namespace gems

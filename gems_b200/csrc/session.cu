@@ -226,7 +226,10 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
   }
   int st = upload_ops(s, ops, nops);
   if (st) return st;
-  if (s->desc.precision == GEMS_PREC_MIXED) {
+  if (traverse_v2_supported(s)) {
+    if ((st = launch_prep_ops_v2(s, nops))) return st;
+    if ((st = launch_traverse_v2(s, nops))) return st;
+  } else if (s->desc.precision == GEMS_PREC_MIXED) {
     if ((st = launch_prep_ops_mixed(s, nops))) return st;
     if ((st = launch_traverse_mixed(s, nops))) return st;
   } else {
@@ -465,6 +468,8 @@ static int upload_model(gems_session *s, const double *eval, const double *evec,
   GEMS_CUDA(cudaMemcpyAsync(s->d_model, m.data(), m.size() * sizeof(double),
                             cudaMemcpyHostToDevice, s->stream));
   GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  s->h_evec.assign(evec, evec + n * n);
+  s->h_inv.assign(inv_evec, inv_evec + n * n);
   s->model_set = true;
   s->theta_valid = false;
   return GEMS_OK;
