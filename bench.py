@@ -42,11 +42,26 @@ NSITES = 1_000_000
 NTAXA = 512
 
 
-def update_bytes(s):
-    """Algorithmic bytes of one site-partial update (C=4, n=4, NORM scale counters of 2 B):
-    internal-internal 3*C*n*s + 3*2, tip-internal 2*C*n*s + 1 + 2*2, tip-tip C*n*s + 2 + 2,
-    with s = 8 (FP64) or 4 (FP32 partials)."""
-    return 3 * 16 * s + 6, 2 * 16 * s + 5, 16 * s + 4
+def update_bytes(s, n=4, C=4, safe=False):
+    """Algorithmic bytes of one site-partial update: internal-internal 3*C*n*s + 3*sigma,
+    tip-internal 2*C*n*s + 1 + 2*sigma, tip-tip C*n*s + 2 + sigma, with s = 8 (FP64) or 4
+    (FP32 partials) and sigma = 2 B (NORM counter) or 2*C B (SAFE counters)."""
+    sig = 2 * C if safe else 2
+    return 3 * C * n * s + 3 * sig, 2 * C * n * s + 1 + 2 * sig, C * n * s + 2 + sig
+
+
+def update_flops(n=4, C=4):
+    """Algorithmic flops of one site-partial update (eigen-space form): 6*C*n^2 + C*n."""
+    return 6 * C * n * n + C * n
+
+
+CONFIGS = {
+    "dna512": "DNA GTR+G4 (alpha 0.5), 512 taxa, Exp(0.05) lengths, {sites} sites/rank with 5% "
+              "gaps, from-scratch full-tree lnL",
+    "protein128": "20-state protein +G4 (alpha 0.8), log-normal exchangeabilities, Dirichlet "
+                  "frequencies, 128 taxa, Exp(0.15) lengths, {sites} sites/rank, from-scratch "
+                  "full-tree lnL",
+}
 
 
 def env_rank():
@@ -158,8 +173,14 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
 
 
-def make_workload(rank, nsites):
+def make_workload(rank, nsites, config="dna512"):
     """Same tree and model on every rank; each rank simulates its own site slab."""
+    if config == "protein128":
+        rng = np.random.default_rng(3)
+        model = synth.protein(rng, 4, 0.8)
+        tree = synth.random_tree(128, 0.15, 14)
+        aln = synth.simulate(tree, model, nsites, 26 + 1000 * rank)
+        return tree, model, aln
     rng = np.random.default_rng(2)
     model = synth.dna_gtr(rng, 4, 0.5)
     tree = synth.random_tree(NTAXA, 0.05, 13)
@@ -173,7 +194,7 @@ def cpu_baseline(tree, model, aln, target_s=12.0):
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
     nsamp = min(aln.npat, 40_000)
-    sub = synth.Alignment(aln.ntaxa, 4, int(aln.weights[:nsamp].sum()),
+    sub = synth.Alignment(aln.ntaxa, model.nstates, int(aln.weights[:nsamp].sum()),
                           np.ascontiguousarray(aln.patterns[:, :nsamp]), aln.weights[:nsamp])
     ot = orc.OracleTree(tree, model, sub)
     nops = sum(op_kinds(tree))
@@ -197,7 +218,7 @@ def run_reference(args):
     rank, world, _ = env_rank()
     if rank != 0:
         return
-    tree, model, aln = make_workload(0, args.sites)
+    tree, model, aln = make_workload(0, args.sites, args.config)
     for _ in range(args.warmup):
         pass
     res = []
@@ -226,10 +247,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gems", choices=["gems", "reference"])
-    ap.add_argument("--sites", type=int, default=NSITES)
+    ap.add_argument("--sites", type=int, default=None)
+    ap.add_argument("--config", default="dna512", choices=sorted(CONFIGS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
+    if args.sites is None:
+        args.sites = NSITES if args.config == "dna512" else 100_000
     if args.impl == "reference":
         return run_reference(args)
 
@@ -243,7 +267,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    tree, model, aln = make_workload(rank, args.sites)
+    tree, model, aln = make_workload(rank, args.sites, args.config)
     gt = PhyloTree.from_case(tree, model, aln, precision=args.precision, device=local)
     s = gt.session
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
@@ -314,7 +338,8 @@ def main():
 
     ups = world * nops * P / (ms * 1e-3)
     ups_e2e = world * nops * P / (ms_e2e * 1e-3)
-    b_ii, b_ti, b_tt = update_bytes(8 if args.precision == "fp64" else 4)
+    b_ii, b_ti, b_tt = update_bytes(8 if args.precision == "fp64" else 4, model.nstates,
+                                    model.ncat)
     alg_bytes = P * (kinds[0] * b_ii + kinds[1] * b_ti + kinds[2] * b_tt)
     peak, peak_kind = read_peaks()
     achieved = alg_bytes / (trav_ms / max(trav_n, 1) * 1e-3) / 1e9 if trav_n else None
@@ -324,8 +349,7 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (seeded generator; no public dataset)",
-        "config": {"workload": "DNA GTR+G4 (alpha 0.5), 512 taxa, Exp(0.05) lengths, "
-                               "1,000,000 sites/rank with 5% gaps, from-scratch full-tree lnL",
+        "config": {"workload": CONFIGS[args.config].format(sites=f"{args.sites:,}"),
                    "npat_per_rank": P, "node_updates_per_step": nops,
                    "precision": args.precision, "parallelism": f"pattern-shard x{world}",
                    "l2": "inputs larger than L2 (partials ~39 GB)"},
@@ -339,7 +363,7 @@ def main():
                      "frac": (achieved / peak) if achieved else None,
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "avg_launch_ms": trav_ms / max(trav_n, 1),
-                     "traffic": read_traffic(f"traverse_{args.precision}_dna512.md")},
+                     "traffic": read_traffic(f"traverse_{args.precision}_{args.config}.md")},
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu:

@@ -123,6 +123,7 @@ static Sizes compute_sizes(const gems_session_desc &d) {
   z.theta_bytes = P * blk * sizeof(double) + 3 * P * sizeof(double);  // theta + scale_all, plh, G
   z.nops_max = d.ntaxa + 8;
   z.op_stride = 2 * (size_t)d.ncat * d.nstates * d.nstates + 2 * (size_t)(unk + 1) * blk;
+  z.op_stride = (z.op_stride + 7) & ~(size_t)7;  // 64-byte aligned op tables
   z.opmats_bytes = (size_t)z.nops_max * z.op_stride * sizeof(double);
   z.branch_bytes = (3 * blk + (size_t)(unk + 1) * blk) * sizeof(double);
   z.red_doubles = 4 * (P * 16 / 256 + 1024);
