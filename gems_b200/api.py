@@ -181,6 +181,11 @@ class Session:
         _check(self.lib.gems_launch_count(self.handle, byref(n)), "gems_launch_count")
         return n.value
 
+    def set_tensor_cores(self, on=True):
+        """20-state mixed traversal on tcgen05 split-TF32 products (default) or FP32 CUDA
+        cores."""
+        _check(self.lib.gems_session_set_option(self.handle, 1, int(on)), "set_option")
+
     def stream_handle(self):
         p = c_void_p()
         _check(self.lib.gems_session_stream(self.handle, byref(p)), "gems_session_stream")

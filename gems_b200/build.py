@@ -24,8 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                   "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
-CUDA_SOURCES = ["session.cu", "kernels_fp64.cu", "kernels_mixed.cu", "kernels_traverse.cu", "eigen.cu",
-                "phylotree.cpp"]
+CUDA_SOURCES = ["session.cu", "kernels_fp64.cu", "kernels_mixed.cu", "kernels_traverse.cu",
+                "kernels_tc.cu", "eigen.cu", "phylotree.cpp"]
 HEADERS = ["gems_internal.cuh"]
 
 LIB = os.path.join(HERE, "libgems_b200.so")
@@ -70,7 +70,7 @@ def build_cuda(force=False, verbose=False):
             if verbose:
                 sys.stderr.write(r.stderr)
     if force or _newer(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"])
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
     return LIB
 
 

@@ -93,6 +93,11 @@ struct Session {
   double *h_result = nullptr;
   int nred = 0;  // size of d_red in doubles
   std::vector<double> h_evec, h_inv;  // host copy of the eigenvectors in use
+  // tensor-core path (20 states, mixed): per-op table stride in floats, TMA descriptor
+  bool tc_enabled = true;
+  size_t op_stride_tc = 0;
+  alignas(64) unsigned char tmap_storage[128] = {};
+  bool tmap_ready = false;
   // kernel timing (gems_profile_*): event pairs recorded around launches
   static constexpr int kProfKernels = 8;
   bool prof_on = false;
@@ -142,6 +147,11 @@ int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool st
 bool traverse_v2_supported(const Session *s);
 int launch_prep_ops_v2(Session *s, int nops);
 int launch_traverse_v2(Session *s, int nops);
+// tcgen05 split-TF32 traversal for 20 states (kernels_tc.cu)
+size_t tc20_op_floats(int ncat, int unknown);
+bool tc20_supported(const Session *s);
+int launch_prep_ops_tc20(Session *s, int nops);
+int launch_traverse_tc20(Session *s, int nops);
 
 }  // namespace gems
 

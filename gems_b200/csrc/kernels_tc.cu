@@ -1,0 +1,528 @@
+// kernels_tc.cu -- 20-state mixed-precision traversal on the 5th-generation tensor cores.
+//
+// Node update per category c (real space, FP32 storage):
+//     out[p][c][:] = (P_c(t_L) . L[p][c][:]) (*) (P_c(t_R) . R[p][c][:])
+// For a tile of 128 patterns each child product is a GEMM  D[128 x 32] = A[128 x 24] . B^T,
+// A = the child partial rows of category c (K = 20 states padded to 24), B = P_c (20 x 20
+// padded to 32 x 24, zero padding).  FP32 accuracy comes from split TF32 ("3xTF32"):
+//     A.B ~= A_hi.B_hi + A_hi.B_lo + A_lo.B_hi,  x_hi = rna_tf32(x), x_lo = rna_tf32(x - x_hi)
+// issued as tcgen05.mma kind::tf32 (M=128, N=32, K=8) by one thread, accumulators in TMEM
+// (2 sides x C categories x 32 columns), read back with tcgen05.ld for the epilogue (product,
+// per-pattern 2^64 rescaling, FP32 store).
+//
+// Data movement per op and tile: the child tiles come from HBM/L2 with TMA (2D tensor map over
+// all slots: 80 floats per pattern row, 16-byte boxes of 4 states x 128 rows, which is exactly
+// the no-swizzle K-major core-matrix layout the MMA reads: LBO = 2048 B between K chunks,
+// SBO = 128 B between 8-row groups).  The split B images are precomputed per op in the same
+// layout and copied with cp.async.bulk.  Tip children need no product: the message is the
+// tip table row.
+//
+// Every mbarrier wait is bounded by a clock budget; on expiry the kernel records
+// GEMS_ERR_TIMEOUT, stops issuing work, waits (bounded) for its own MMAs, frees its TMEM and
+// returns.
+#include <cuda.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "gems_internal.cuh"
+
+namespace gems {
+
+namespace {
+
+constexpr int kN = 20;        // states
+constexpr int kNP = 32;       // MMA N (padded states)
+constexpr int kKP = 24;       // padded K (3 x 8)
+constexpr int kTile = 128;    // patterns per CTA = MMA M
+constexpr int kChunks = kN * 4 / 4 * 1;  // 16-byte K chunks per category row: 20 floats = 5
+constexpr int kRowChunks = 20;           // chunks per pattern row (4 categories x 5)
+constexpr int kAChunk = kTile * 16;      // bytes of one K chunk of an A tile (128 rows x 16 B)
+constexpr int kABytes = (kRowChunks + 1) * kAChunk;   // + one zero chunk for the last category
+constexpr int kBImg = (kKP / 4) * kNP * 16;           // 6 chunks x 32 rows x 16 B = 3072
+constexpr long long kWaitCycles = 4000000000LL;       // ~2 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t sptr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t cnt) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(cnt) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major, no swizzle (Blackwell version field = 1)
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// instruction descriptor: D f32, A/B tf32, both K-major, N = 32, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNP >> 3) << 17) |
+                            ((uint32_t)(kTile >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t dtm, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtm),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+// 32 consecutive TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-op tables for the tensor-core path (floats, per op):
+//   B images [2 sides][C][hi, lo][6 chunks][32 rows][4]   (row n = target state x, K = y)
+//   tip tables [2 sides][U1][C][20]
+// ---------------------------------------------------------------------------------------
+__global__ void k_prep_ops_tc(DevCtx c, const DevOp *ops, float *tab, size_t stride_f) {
+  extern __shared__ double sm[];
+  double *ex = sm;                         // [C][n]
+  float *Pm = reinterpret_cast<float *>(ex + c.C * kN);  // [C][n][n]
+  const int k = blockIdx.x, side = blockIdx.y;
+  const DevOp op = ops[k];
+  const int kind = side ? op.r_kind : op.l_kind;
+  const double len = side ? op.r_len : op.l_len;
+  const int C = c.C, n = kN;
+  for (int idx = threadIdx.x; idx < C * n; idx += blockDim.x) {
+    const int cc = idx / n, i = idx - cc * n;
+    ex[idx] = exp(c.eval[i] * (c.rates[cc] * len));
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < C * n * n; idx += blockDim.x) {
+    const int cc = idx / (n * n), r = idx - cc * n * n, x = r / n, y = r - x * n;
+    double acc = 0.0;
+    for (int i = 0; i < n; i++) acc = fma(c.evec[x * n + i] * ex[cc * n + i], c.inv_evec[i * n + y], acc);
+    Pm[idx] = (float)fmax(acc, 0.0);
+  }
+  __syncthreads();
+  float *img = tab + (size_t)k * stride_f + (size_t)side * C * 2 * (kBImg / 4);
+  for (int idx = threadIdx.x; idx < C * (kBImg / 4); idx += blockDim.x) {
+    const int cc = idx / (kBImg / 4), r = idx - cc * (kBImg / 4);
+    const int chunk = r / (kNP * 4), rr = r - chunk * kNP * 4, row = rr / 4, e = rr - row * 4;
+    const int x = row, y = chunk * 4 + e;
+    const float v = (x < n && y < n) ? Pm[(cc * n + x) * n + y] : 0.f;
+    const float hi = tf32_rna(v);
+    const float lo = tf32_rna(v - hi);
+    img[(size_t)cc * 2 * (kBImg / 4) + r] = hi;
+    img[(size_t)cc * 2 * (kBImg / 4) + (kBImg / 4) + r] = lo;
+  }
+  if (kind != GEMS_CHILD_TIP) return;
+  float *leaf = tab + (size_t)k * stride_f + (size_t)2 * C * 2 * (kBImg / 4) +
+                (size_t)side * (c.unknown + 1) * C * n;
+  for (int idx = threadIdx.x; idx < (c.unknown + 1) * C * n; idx += blockDim.x) {
+    const int s = idx / (C * n), r = idx - s * C * n, cc = r / n, x = r - cc * n;
+    const double *ind = c.tip_real + (size_t)s * n;
+    float acc = 0.f;
+    for (int y = 0; y < n; y++) acc = fmaf(Pm[(cc * n + x) * n + y], (float)ind[y], acc);
+    leaf[idx] = acc;
+  }
+}
+
+struct TcShared {
+  uint64_t bar_tma;
+  uint64_t bar_mma;
+  uint32_t tmem_base;
+};
+
+template <bool SAFE>
+__global__ void __launch_bounds__(kTile, 1)
+    k_traverse_tc20(DevCtx c, const DevOp *__restrict__ ops, int nops,
+                    const float *__restrict__ tab, size_t stride_f,
+                    const __grid_constant__ CUtensorMap tmap, int *flag) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // carve: A[2] | Alo[2] | B[2][C][2] | control
+  unsigned char *base = smem_raw;
+  float *A[2], *Alo[2];
+  A[0] = reinterpret_cast<float *>(base);
+  A[1] = reinterpret_cast<float *>(base + kABytes);
+  Alo[0] = reinterpret_cast<float *>(base + 2 * kABytes);
+  Alo[1] = reinterpret_cast<float *>(base + 3 * kABytes);
+  const int C = c.C;
+  unsigned char *Bbase = base + 4 * kABytes;
+  TcShared *ctl = reinterpret_cast<TcShared *>(Bbase + (size_t)2 * C * 2 * kBImg);
+
+  const int t = threadIdx.x, warp = t >> 5;
+  const long p0 = (long)blockIdx.x * kTile;
+  const long p = p0 + t;
+  const bool act = p < c.P;
+  const uint32_t bar_tma = sptr(&ctl->bar_tma), bar_mma = sptr(&ctl->bar_mma);
+
+  if (t == 0) {
+    mbar_init(bar_tma, 1);
+    mbar_init(bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // zero the spare chunk after each A tile (read by the last category's padded K step)
+  for (int s = 0; s < 2; s++) {
+    reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(A[s]) + kRowChunks * kAChunk)[t] =
+        make_float4(0.f, 0.f, 0.f, 0.f);
+    reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(Alo[s]) + kRowChunks * kAChunk)[t] =
+        make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     sptr(&ctl->tmem_base)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = ctl->tmem_base;
+  uint32_t ph_tma = 0, ph_mma = 0;
+  bool ok = true, tma_pending = false, mma_pending = false;
+  float *part = static_cast<float *>(c.partials);
+  const size_t imgf = kBImg / 4;
+
+  for (int k = 0; k < nops && ok; k++) {
+    const DevOp op = ops[k];
+    const float *tk = tab + (size_t)k * stride_f;
+    const bool inL = op.l_kind == GEMS_CHILD_PARTIAL, inR = op.r_kind == GEMS_CHILD_PARTIAL;
+    const int nin = (int)inL + (int)inR;
+    // ---- 1. bring the internal children's tiles and the B images into shared memory
+    if (nin > 0) {
+      if (t == 0) {
+        const uint32_t bytes = nin * (kRowChunks * kAChunk + (uint32_t)C * 2 * kBImg);
+        mbar_expect_tx(bar_tma, bytes);
+        for (int s = 0; s < 2; s++) {
+          const bool in = s ? inR : inL;
+          if (!in) continue;
+          const int slot = s ? op.r_id : op.l_id;
+          const int row = slot * c.P + (int)p0;
+          for (int j = 0; j < kRowChunks; j++)
+            tma_load_2d(sptr(A[s]) + j * kAChunk, &tmap, 4 * j, row, bar_tma);
+          const float *src = tk + (size_t)s * C * 2 * imgf;
+          bulk_g2s(sptr(Bbase + (size_t)s * C * 2 * kBImg), src, (uint32_t)C * 2 * kBImg, bar_tma);
+        }
+      }
+      tma_pending = true;
+      // every thread must take the same branch: vote on the bounded wait
+      if (__syncthreads_or(!mbar_wait(bar_tma, ph_tma))) {
+        ok = false;
+        if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+        break;
+      }
+      tma_pending = false;
+      ph_tma ^= 1;
+      // ---- 2. split each loaded tile: A <- rna_tf32(A), Alo <- rna_tf32(A - hi)
+      for (int s = 0; s < 2; s++) {
+        if (!(s ? inR : inL)) continue;
+        float4 *a4 = reinterpret_cast<float4 *>(A[s]);
+        float4 *l4 = reinterpret_cast<float4 *>(Alo[s]);
+#pragma unroll 4
+        for (int j = 0; j < kRowChunks; j++) {
+          float4 v = a4[j * kTile + t];
+          float4 h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
+          a4[j * kTile + t] = h;
+          l4[j * kTile + t] = make_float4(tf32_rna(v.x - h.x), tf32_rna(v.y - h.y),
+                                          tf32_rna(v.z - h.z), tf32_rna(v.w - h.w));
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      // ---- 3. one thread issues the split-TF32 products into TMEM
+      if (t == 0) {
+        for (int s = 0; s < 2; s++) {
+          if (!(s ? inR : inL)) continue;
+          for (int cc = 0; cc < C; cc++) {
+            const uint32_t dtm = tmem + (uint32_t)((s * C + cc) * kNP);
+            const uint32_t bh = sptr(Bbase + ((size_t)(s * C + cc) * 2) * kBImg);
+            const uint32_t bl = bh + kBImg;
+            for (int ks = 0; ks < kKP / 8; ks++) {
+              const uint32_t koff = (uint32_t)(cc * 5 + 2 * ks) * kAChunk;
+              const uint64_t ah = sdesc(sptr(A[s]) + koff, kAChunk, 128);
+              const uint64_t al = sdesc(sptr(Alo[s]) + koff, kAChunk, 128);
+              const uint64_t dbh = sdesc(bh + (uint32_t)(2 * ks) * (kNP * 16), kNP * 16, 128);
+              const uint64_t dbl = sdesc(bl + (uint32_t)(2 * ks) * (kNP * 16), kNP * 16, 128);
+              mma_tf32(dtm, ah, dbh, ks > 0 ? 1u : 0u);
+              mma_tf32(dtm, ah, dbl, 1u);
+              mma_tf32(dtm, al, dbh, 1u);
+            }
+          }
+        }
+        mma_commit(bar_mma);
+      }
+      mma_pending = true;
+      if (__syncthreads_or(!mbar_wait(bar_mma, ph_mma))) {
+        ok = false;
+        if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+        break;
+      }
+      mma_pending = false;
+      ph_mma ^= 1;
+      tc_fence_after();
+    }
+    // ---- 4. epilogue: messages, product, rescaling, FP32 store of this thread's row
+    const float *leafL = tk + (size_t)2 * C * 2 * imgf;
+    const float *leafR = leafL + (size_t)(c.unknown + 1) * C * kN;
+    int stL = 0, stR = 0, sL = 0, sR = 0;
+    if (act) {
+      if (!inL) stL = c.tips[(size_t)op.l_id * c.P + p];
+      if (!inR) stR = c.tips[(size_t)op.r_id * c.P + p];
+    }
+    float out[4][kN];
+    float lh_max_all = 0.f;
+    float lh_max_c[4] = {0.f, 0.f, 0.f, 0.f};
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+#pragma unroll
+    for (int cc = 0; cc < 4; cc++) {
+      if (cc >= C) break;
+      float mL[32], mR[32];
+      if (inL) {
+        tmem_ld32(tmem + lane_off + (uint32_t)(cc * kNP), mL);
+      } else {
+        const float *lt = leafL + ((size_t)stL * C + cc) * kN;
+#pragma unroll
+        for (int x = 0; x < kN; x++) mL[x] = __ldg(lt + x);
+      }
+      if (inR) {
+        tmem_ld32(tmem + lane_off + (uint32_t)((C + cc) * kNP), mR);
+      } else {
+        const float *rt = leafR + ((size_t)stR * C + cc) * kN;
+#pragma unroll
+        for (int x = 0; x < kN; x++) mR[x] = __ldg(rt + x);
+      }
+#pragma unroll
+      for (int x = 0; x < kN; x++) {
+        const float v = fmaxf(mL[x], 0.f) * fmaxf(mR[x], 0.f);
+        out[cc][x] = v;
+        lh_max_c[cc] = fmaxf(lh_max_c[cc], v);
+      }
+      lh_max_all = fmaxf(lh_max_all, lh_max_c[cc]);
+    }
+    if (act) {
+      const uint16_t *scl = c.scale + (size_t)op.l_id * c.slot_scale;
+      const uint16_t *scr = c.scale + (size_t)op.r_id * c.slot_scale;
+      const bool tiptip = !inL && !inR;
+      uint16_t *sd = c.scale + (size_t)op.dst_slot * c.slot_scale;
+      float *dst = part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * c.block;
+      if (SAFE) {
+        for (int cc = 0; cc < C; cc++) {
+          int s_out = (inL ? scl[(size_t)p * C + cc] : 0) + (inR ? scr[(size_t)p * C + cc] : 0);
+          float f = 1.f;
+          if (!tiptip && lh_max_c[cc] < kScaleThrF && c.invar[p] == 0.0) {
+            f = 18446744073709551616.0f;
+            s_out += 1;
+          }
+          float4 *d4 = reinterpret_cast<float4 *>(dst + cc * kN);
+#pragma unroll
+          for (int i = 0; i < kN / 4; i++)
+            d4[i] = make_float4(out[cc][4 * i] * f, out[cc][4 * i + 1] * f,
+                                out[cc][4 * i + 2] * f, out[cc][4 * i + 3] * f);
+          sd[(size_t)p * C + cc] = (uint16_t)s_out;
+        }
+      } else {
+        sL = inL ? scl[p] : 0;
+        sR = inR ? scr[p] : 0;
+        int s_out = sL + sR;
+        float f = 1.f;
+        if (!tiptip && lh_max_all < kScaleThrF && c.invar[p] == 0.0) {
+          f = 18446744073709551616.0f;
+          s_out += 1;
+        }
+#pragma unroll
+        for (int cc = 0; cc < 4; cc++) {
+          if (cc >= C) break;
+          float4 *d4 = reinterpret_cast<float4 *>(dst + cc * kN);
+#pragma unroll
+          for (int i = 0; i < kN / 4; i++)
+            d4[i] = make_float4(out[cc][4 * i] * f, out[cc][4 * i + 1] * f,
+                                out[cc][4 * i + 2] * f, out[cc][4 * i + 3] * f);
+        }
+        sd[p] = (uint16_t)s_out;
+      }
+    }
+    // the next op's TMA reads must see these generic-proxy stores
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  if (!ok && t == 0) {
+    // stop cleanly: wait (bounded) for the copies and products this CTA still has in flight
+    if (tma_pending) mbar_wait(bar_tma, ph_tma);
+    if (mma_pending) mbar_wait(bar_mma, ph_mma);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256)
+                 : "memory");
+}
+
+}  // namespace
+
+size_t tc20_op_floats(int ncat, int unknown) {
+  return (size_t)2 * ncat * 2 * (kBImg / 4) + (size_t)2 * (unknown + 1) * ncat * kN;
+}
+
+bool tc20_supported(const Session *s) {
+  return s->desc.nstates == 20 && s->desc.precision == GEMS_PREC_MIXED && s->desc.ncat <= 4 &&
+         s->tc_enabled;
+}
+
+static size_t tc_smem(int C) { return 4 * (size_t)kABytes + (size_t)2 * C * 2 * kBImg + 64; }
+
+int tc20_make_tmap(Session *s) {
+  // 2D view of all partial slots: rows = nslots * P patterns, 80 floats per row
+  CUtensorMap *map = reinterpret_cast<CUtensorMap *>(s->tmap_storage);
+  const cuuint64_t dims[2] = {(cuuint64_t)kN * s->desc.ncat, (cuuint64_t)s->P * s->desc.nslots};
+  const cuuint64_t strides[1] = {(cuuint64_t)kN * s->desc.ncat * sizeof(float)};
+  const cuuint32_t box[2] = {4, (cuuint32_t)kTile};
+  const cuuint32_t estr[2] = {1, 1};
+  // the driver entry point is resolved through the runtime, so the library does not link
+  // libcuda (it still loads on hosts without a driver)
+  using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    set_error("cuTensorMapEncodeTiled entry point not available");
+    return GEMS_ERR_CUDA;
+  }
+  CUresult r = reinterpret_cast<EncodeFn>(fn)(
+      map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->d_partials, dims, strides, box, estr,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for the partial buffer");
+    return GEMS_ERR_CUDA;
+  }
+  s->tmap_ready = true;
+  return GEMS_OK;
+}
+
+int launch_prep_ops_tc20(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  DevCtx c = s->ctx();
+  const size_t smem = sizeof(double) * s->desc.ncat * kN + sizeof(float) * s->desc.ncat * kN * kN;
+  k_prep_ops_tc<<<dim3(nops, 2), 256, smem, s->stream>>>(
+      c, s->d_ops, reinterpret_cast<float *>(s->d_opmats), s->op_stride_tc);
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  return GEMS_OK;
+}
+
+int launch_traverse_tc20(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  if (!s->tmap_ready) {
+    int st = tc20_make_tmap(s);
+    if (st) return st;
+  }
+  DevCtx c = s->ctx();
+  const size_t smem = tc_smem(s->desc.ncat);
+  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  void *fn = safe ? (void *)k_traverse_tc20<true> : (void *)k_traverse_tc20<false>;
+  GEMS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GEMS_CUDA(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
+  const int grid = (s->P + kTile - 1) / kTile;
+  CUtensorMap map;
+  std::memcpy(&map, s->tmap_storage, sizeof(map));
+  cudaEvent_t ev0;
+  if (int st = prof_begin(s, 0, &ev0)) return st;
+  const float *tab = reinterpret_cast<const float *>(s->d_opmats);
+  if (safe)
+    k_traverse_tc20<true><<<grid, kTile, smem, s->stream>>>(c, s->d_ops, nops, tab,
+                                                             s->op_stride_tc, map, s->d_flag);
+  else
+    k_traverse_tc20<false><<<grid, kTile, smem, s->stream>>>(c, s->d_ops, nops, tab,
+                                                              s->op_stride_tc, map, s->d_flag);
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  if (int st = prof_end(s, 0, ev0)) return st;
+  int flag = 0;
+  GEMS_CUDA(cudaMemcpyAsync(&flag, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  if (flag) {
+    set_error("tensor-core traversal: bounded wait expired");
+    return GEMS_ERR_TIMEOUT;
+  }
+  return GEMS_OK;
+}
+
+}  // namespace gems

@@ -182,144 +182,6 @@ __global__ void __launch_bounds__(kThreads) k_traverse_f64(DevCtx c, const DevOp
 }
 
 // ---------------------------------------------------------------------------------------
-// 4-state FP64 traversal with one op of look-ahead: the child partials (or tip bytes) of op
-// k+1 are requested before op k is computed, so two ops' worth of L2/HBM reads are in flight
-// per lane.  A child of op k+1 that op k produces is taken from registers (forwarded) instead
-// of being read back.  Same arithmetic as k_traverse_f64<4>.
-// ---------------------------------------------------------------------------------------
-struct Fetch4 {
-  double raw[4];
-  int scale;
-  int state;
-};
-
-template <bool SAFE>
-__device__ __forceinline__ void fetch4(const DevCtx &c, int kind, int id, int fwd_slot, long p,
-                                       int gl, bool act, Fetch4 &f) {
-  f.scale = 0;
-  f.state = 0;
-  if (!act) return;
-  if (kind == GEMS_CHILD_TIP) {
-    f.state = c.tips[(size_t)id * c.P + p];
-  } else if (id != fwd_slot) {
-    const double2 *s2 = reinterpret_cast<const double2 *>(
-        static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems +
-        (size_t)p * c.block + gl * 4);
-    const double2 a = __ldcg(s2), b = __ldcg(s2 + 1);
-    f.raw[0] = a.x;
-    f.raw[1] = a.y;
-    f.raw[2] = b.x;
-    f.raw[3] = b.y;
-    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
-    f.scale = SAFE ? sc[(size_t)p * c.C + gl] : sc[p];
-  }
-}
-
-__device__ __forceinline__ void msg4(const DevCtx &c, const EigPack<4> &E, int kind,
-                                     const double *__restrict__ d,
-                                     const double *__restrict__ leaf, int gl, const Fetch4 &f,
-                                     double (&v)[4]) {
-  const int C = c.C;
-  if (kind == GEMS_CHILD_TIP) {
-    const double *lt = leaf + (size_t)f.state * c.block + gl;
-#pragma unroll
-    for (int x = 0; x < 4; x++) v[x] = __ldg(lt + x * C);
-  } else {
-    double L[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) L[i] = f.raw[i] * __ldg(d + i * C + gl);
-#pragma unroll
-    for (int x = 0; x < 4; x++) {
-      double acc = 0.0;
-#pragma unroll
-      for (int i = 0; i < 4; i++) acc = fma(E.evec[x * 4 + i], L[i], acc);
-      v[x] = acc;
-    }
-  }
-}
-
-template <bool SAFE>
-__global__ void __launch_bounds__(kThreads) k_traverse4_pf(DevCtx c, const DevOp *__restrict__ ops,
-                                                           int nops,
-                                                           const double *__restrict__ tab,
-                                                           size_t stride, const EigPack<4> E) {
-  const int G = c.G;
-  const int gl = threadIdx.x & (G - 1);
-  const long p = ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const bool act = p < c.P && gl < c.C;
-  const int C = c.C, blk = c.block;
-  double *part = static_cast<double *>(c.partials);
-  DevOp cur = ops[0];
-  Fetch4 fl, fr;
-  fetch4<SAFE>(c, cur.l_kind, cur.l_id, -1, p, gl, act, fl);
-  fetch4<SAFE>(c, cur.r_kind, cur.r_id, -1, p, gl, act, fr);
-  for (int k = 0; k < nops; k++) {
-    DevOp nxt;
-    const bool has_next = k + 1 < nops;
-    Fetch4 gl2, gr2;
-    if (has_next) {
-      nxt = ops[k + 1];
-      fetch4<SAFE>(c, nxt.l_kind, nxt.l_id, cur.dst_slot, p, gl, act, gl2);
-      fetch4<SAFE>(c, nxt.r_kind, nxt.r_id, cur.dst_slot, p, gl, act, gr2);
-    }
-    const double *tk = tab + (size_t)k * stride;
-    const bool tiptip = cur.l_kind == GEMS_CHILD_TIP && cur.r_kind == GEMS_CHILD_TIP;
-    double out[4] = {0.0, 0.0, 0.0, 0.0};
-    double lh_max = 0.0;
-    if (act) {
-      double vl[4], vr[4], tmp[4];
-      msg4(c, E, cur.l_kind, tk, tk + 2 * blk, gl, fl, vl);
-      msg4(c, E, cur.r_kind, tk + blk, tk + 2 * blk + (size_t)(c.unknown + 1) * blk, gl, fr, vr);
-#pragma unroll
-      for (int x = 0; x < 4; x++) tmp[x] = vl[x] * vr[x];
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int x = 0; x < 4; x++) acc = fma(E.inv[j * 4 + x], tmp[x], acc);
-        out[j] = acc;
-        lh_max = fmax(lh_max, fabs(acc));
-      }
-    }
-    if (!SAFE) lh_max = group_max(lh_max, G);
-    int s_out = fl.scale + fr.scale;
-    if (act) {
-      if (!tiptip && lh_max < kScaleThr && c.invar[p] == 0.0) {
-#pragma unroll
-        for (int j = 0; j < 4; j++) out[j] = ldexp(out[j], kScaleExp);
-        s_out += 1;
-      }
-      double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)cur.dst_slot * c.slot_elems +
-                                                (size_t)p * blk + gl * 4);
-      d2[0] = make_double2(out[0], out[1]);
-      d2[1] = make_double2(out[2], out[3]);
-      uint16_t *sc = c.scale + (size_t)cur.dst_slot * c.slot_scale;
-      if (SAFE)
-        sc[(size_t)p * C + gl] = (uint16_t)s_out;
-      else if (gl == 0)
-        sc[p] = (uint16_t)s_out;
-    }
-    __syncwarp();
-    if (has_next) {
-      // forward this op's output to the next op when it is one of its children
-      if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) {
-#pragma unroll
-        for (int i = 0; i < 4; i++) gl2.raw[i] = out[i];
-        gl2.scale = s_out;
-      }
-      if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) {
-#pragma unroll
-        for (int i = 0; i < 4; i++) gr2.raw[i] = out[i];
-        gr2.scale = s_out;
-      }
-      fl = gl2;
-      fr = gr2;
-      cur = nxt;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------------------
 // Mixed: P_c(t) = evec diag(exp(eval r_c t)) inv_evec in FP64, rounded to FP32, stored
 // [side][x][y][c]; tip tables [side][s][x][c] = P_c . indicator(s).
 // ---------------------------------------------------------------------------------------
@@ -489,21 +351,12 @@ int launch_f64(Session *s, int nops) {
   }
   const int grid = grid_for(s);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
-  if constexpr (N == 4) {
-    if (safe)
-      k_traverse4_pf<true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                              s->op_stride, E);
-    else
-      k_traverse4_pf<false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+  if (safe)
+    k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
                                                                s->op_stride, E);
-  } else {
-    if (safe)
-      k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                                 s->op_stride, E);
-    else
-      k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                                  s->op_stride, E);
-  }
+  else
+    k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                                s->op_stride, E);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   return GEMS_OK;

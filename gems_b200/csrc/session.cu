@@ -123,6 +123,11 @@ static Sizes compute_sizes(const gems_session_desc &d) {
   z.theta_bytes = P * blk * sizeof(double) + 3 * P * sizeof(double);  // theta + scale_all, plh, G
   z.nops_max = d.ntaxa + 8;
   z.op_stride = 2 * (size_t)d.ncat * d.nstates * d.nstates + 2 * (size_t)(unk + 1) * blk;
+  if (d.nstates == 20 && d.precision == GEMS_PREC_MIXED && d.ncat <= 4) {
+    // the tensor-core tables (floats) share the buffer
+    const size_t need = (tc20_op_floats(d.ncat, unk) + 1) / 2;
+    if (z.op_stride < need) z.op_stride = need;
+  }
   z.op_stride = (z.op_stride + 7) & ~(size_t)7;  // 64-byte aligned op tables
   z.opmats_bytes = (size_t)z.nops_max * z.op_stride * sizeof(double);
   z.branch_bytes = (3 * blk + (size_t)(unk + 1) * blk) * sizeof(double);
@@ -227,7 +232,10 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
   }
   int st = upload_ops(s, ops, nops);
   if (st) return st;
-  if (traverse_v2_supported(s)) {
+  if (tc20_supported(s)) {
+    if ((st = launch_prep_ops_tc20(s, nops))) return st;
+    if ((st = launch_traverse_tc20(s, nops))) return st;
+  } else if (traverse_v2_supported(s)) {
     if ((st = launch_prep_ops_v2(s, nops))) return st;
     if ((st = launch_traverse_v2(s, nops))) return st;
   } else if (s->desc.precision == GEMS_PREC_MIXED) {
@@ -313,6 +321,7 @@ int gems_session_create(const gems_session_desc *desc, gems_session **out) {
   s->G = pow2_at_least(desc->ncat);
   s->nops_max = z.nops_max;
   s->op_stride = z.op_stride;
+  s->op_stride_tc = 2 * z.op_stride;  // same buffer viewed as floats
   s->nred = (int)z.red_doubles;
   auto fail = [&](cudaError_t e, const char *what) {
     int code = cuda_status(e, what);
@@ -380,6 +389,17 @@ int gems_session_info(gems_session *s, gems_session_desc *desc) {
   if (!s || !desc) return GEMS_ERR_BAD_ARG;
   *desc = s->desc;
   return GEMS_OK;
+}
+
+int gems_session_set_option(gems_session *s, int option, int value) {
+  if (!s) return GEMS_ERR_BAD_ARG;
+  switch (option) {
+    case GEMS_OPT_TENSOR_CORES:
+      s->tc_enabled = value != 0;
+      return GEMS_OK;
+    default:
+      return GEMS_ERR_BAD_ARG;
+  }
 }
 
 int gems_session_stream(gems_session *s, void **stream) {

@@ -97,6 +97,10 @@ int gems_session_sync(gems_session *s);
 int gems_session_info(gems_session *s, gems_session_desc *desc);
 /* the CUDA stream (cudaStream_t) the session launches on, for event timing by the caller */
 int gems_session_stream(gems_session *s, void **stream);
+/* Session options.  GEMS_OPT_TENSOR_CORES (default 1): the mixed-precision 20-state traversal
+ * runs on tcgen05 split-TF32 products; 0 selects the FP32 CUDA-core kernel. */
+enum { GEMS_OPT_TENSOR_CORES = 1 };
+int gems_session_set_option(gems_session *s, int option, int value);
 
 /* Tip state bytes [ntaxa][nptn] (PhyloTree::getConvertedSequenceByNumber rows,
  * tree/phylotree.cpp:3331): 0..n-1 states, DNA 4..17 ambiguity bitmask codes, protein

@@ -216,3 +216,24 @@ def test_mixed_optimize_all(gpu, n):
     ot2 = orc.OracleTree(synth.Tree(tree.ntaxa, tree.eu, tree.ev, gt.getBranchLengths()),
                          model, aln, safe=safe)
     assert abs(ot2.computeLikelihood() - lo) <= MIXED_RTOL * abs(lo)
+
+
+def test_tensor_core_path_matches_cuda_core_path(gpu):
+    """20-state mixed traversal: tcgen05 split-TF32 products against the FP32 CUDA-core
+    kernel and the FP64 oracle, NORM and SAFE, including tip-tip, tip-internal and
+    internal-internal nodes and pattern counts that are not a multiple of the 128-row tile."""
+    rng = np.random.default_rng(77)
+    model = synth.protein(rng, 4, 0.8)
+    for safe, ntaxa, nsites in ((False, 30, 700), (True, 45, 333)):
+        tree = synth.random_tree(ntaxa, 0.15, ntaxa)
+        aln = synth.simulate(tree, model, nsites, ntaxa + 1)
+        ot = orc.OracleTree(tree, model, aln, safe=safe)
+        lo = ot.computeLikelihood()
+        res = []
+        for tc in (True, False):
+            gt = gpu_tree(tree, model, aln, safe, precision="mixed")
+            gt.session.set_tensor_cores(tc)
+            lg, plg = gt.computeLikelihood(pattern_lh=True)
+            assert abs(lg - lo) <= MIXED_RTOL * abs(lo), (tc, lg, lo)
+            res.append(plg)
+        assert np.max(np.abs(res[0] - res[1]) / (np.abs(res[1]) + 1)) < 1e-5
