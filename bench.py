@@ -251,6 +251,8 @@ def main():
     ap.add_argument("--config", default="dna512", choices=sorted(CONFIGS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tc", action="store_true",
+                    help="20-state mixed traversal on CUDA cores instead of tcgen05")
     args = ap.parse_args()
     if args.sites is None:
         args.sites = NSITES if args.config == "dna512" else 100_000
@@ -270,6 +272,8 @@ def main():
     tree, model, aln = make_workload(rank, args.sites, args.config)
     gt = PhyloTree.from_case(tree, model, aln, precision=args.precision, device=local)
     s = gt.session
+    if args.no_tc:
+        s.set_tensor_cores(False)
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
     kinds = op_kinds(tree)
     nops = sum(kinds)

@@ -1,4 +1,4 @@
-// kernels_tc.cu -- 20-state mixed-precision traversal on the 5th-generation tensor cores.
+// kernels_tc20.cu -- 20-state mixed-precision traversal on the 5th-generation tensor cores.
 //
 // Node update per category c (real space, FP32 storage):
 //     out[p][c][:] = (P_c(t_L) . L[p][c][:]) (*) (P_c(t_R) . R[p][c][:])
@@ -8,18 +8,25 @@
 //     A.B ~= A_hi.B_hi + A_hi.B_lo + A_lo.B_hi,  x_hi = rna_tf32(x), x_lo = rna_tf32(x - x_hi)
 // issued as tcgen05.mma kind::tf32 (M=128, N=32, K=8) by one thread, accumulators in TMEM
 // (2 sides x C categories x 32 columns), read back with tcgen05.ld for the epilogue (product,
-// per-pattern 2^64 rescaling, FP32 store).
+// 2^64 rescaling, FP32 store).
 //
-// Data movement per op and tile: the child tiles come from HBM/L2 with TMA (2D tensor map over
-// all slots: 80 floats per pattern row, 16-byte boxes of 4 states x 128 rows, which is exactly
-// the no-swizzle K-major core-matrix layout the MMA reads: LBO = 2048 B between K chunks,
-// SBO = 128 B between 8-row groups).  The split B images are precomputed per op in the same
-// layout and copied with cp.async.bulk.  Tip children need no product: the message is the
-// tip table row.
+// Operands in shared memory use the no-swizzle K-major core-matrix layout: 16-byte chunks of
+// 4 states x 128 rows, LBO = 2048 B between K chunks, SBO = 128 B between 8-row groups.  That
+// is exactly what a TMA box of {4 states, 128 rows} over the partial buffer (2D tensor map:
+// 80 floats per pattern row, rows of all slots stacked) writes, one box per chunk.  The split
+// B images are precomputed per op in the same layout and copied with cp.async.bulk.
 //
-// Every mbarrier wait is bounded by a clock budget; on expiry the kernel records
-// GEMS_ERR_TIMEOUT, stops issuing work, waits (bounded) for its own MMAs, frees its TMEM and
-// returns.
+// Pipeline per op (one CTA per SM, 8 warps; warps w and w+4 share TMEM lane quadrant w%4 and
+// each handles two of the four categories of a row):
+//   wait(TMA of this op) -> split the loaded tiles into hi/lo -> MMAs -> wait(MMA)
+//   -> issue the next op's TMA/bulk copies (operand buffers are free again)
+//   -> epilogue; when the next op consumes this op's output, the epilogue also writes the
+//      row, already split, into the next op's operand buffer (no round trip through L2).
+// Tip children need no product: the message is the tip table row.
+//
+// Every mbarrier wait is bounded by a clock budget; on expiry the CTA records
+// GEMS_ERR_TIMEOUT, stops issuing work, waits (bounded) for what it has in flight, frees its
+// TMEM and returns.
 #include <cuda.h>
 
 #include <cmath>
@@ -32,21 +39,20 @@ namespace gems {
 
 namespace {
 
-constexpr int kN = 20;        // states
-constexpr int kNP = 32;       // MMA N (padded states)
-constexpr int kKP = 24;       // padded K (3 x 8)
-constexpr int kTile = 128;    // patterns per CTA = MMA M
-constexpr int kChunks = kN * 4 / 4 * 1;  // 16-byte K chunks per category row: 20 floats = 5
-constexpr int kRowChunks = 20;           // chunks per pattern row (4 categories x 5)
-constexpr int kAChunk = kTile * 16;      // bytes of one K chunk of an A tile (128 rows x 16 B)
-constexpr int kABytes = (kRowChunks + 1) * kAChunk;   // + one zero chunk for the last category
-constexpr int kBImg = (kKP / 4) * kNP * 16;           // 6 chunks x 32 rows x 16 B = 3072
-constexpr long long kWaitCycles = 4000000000LL;       // ~2 s at 1.9 GHz
+constexpr int kN = 20;                          // states
+constexpr int kNP = 32;                         // MMA N (padded states)
+constexpr int kKP = 24;                         // padded K (3 x 8)
+constexpr int kTile = 128;                      // patterns per CTA = MMA M
+constexpr int kThreadsTc = 256;                 // 2 threads per pattern row
+constexpr int kRowChunks = 20;                  // 16-byte chunks per row (4 categories x 5)
+constexpr int kAChunk = kTile * 16;             // one chunk of an A tile (128 rows x 16 B)
+constexpr int kABytes = (kRowChunks + 1) * kAChunk;  // + a zero chunk for the last category
+constexpr int kBImg = (kKP / 4) * kNP * 16;     // 6 chunks x 32 rows x 16 B = 3072
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
 __device__ __forceinline__ uint32_t sptr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t cnt) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(cnt) : "memory");
 }
@@ -71,7 +77,6 @@ __device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (clock64() - t0 > kWaitCycles) return false;
   return true;
 }
-
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
                                             uint32_t bar) {
   asm volatile(
@@ -88,7 +93,6 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
 }
-
 // UMMA shared-memory descriptor, K-major, no swizzle (Blackwell version field = 1)
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = 0;
@@ -98,7 +102,6 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   d |= (uint64_t)1 << 46;
   return d;
 }
-
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 32, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNP >> 3) << 17) |
                             ((uint32_t)(kTile >> 4) << 24);
@@ -122,7 +125,6 @@ __device__ __forceinline__ void tc_fence_after() {
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
-
 // 32 consecutive TMEM columns of this thread's lane
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   uint32_t r[32];
@@ -140,11 +142,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 #pragma unroll
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
-
 __device__ __forceinline__ float tf32_rna(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
+}
+__device__ __forceinline__ void split4(float4 v, float4 &h, float4 &l) {
+  h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
+  l = make_float4(tf32_rna(v.x - h.x), tf32_rna(v.y - h.y), tf32_rna(v.z - h.z),
+                  tf32_rna(v.w - h.w));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -154,7 +160,7 @@ __device__ __forceinline__ float tf32_rna(float x) {
 // ---------------------------------------------------------------------------------------
 __global__ void k_prep_ops_tc(DevCtx c, const DevOp *ops, float *tab, size_t stride_f) {
   extern __shared__ double sm[];
-  double *ex = sm;                         // [C][n]
+  double *ex = sm;                                        // [C][n]
   float *Pm = reinterpret_cast<float *>(ex + c.C * kN);  // [C][n][n]
   const int k = blockIdx.x, side = blockIdx.y;
   const DevOp op = ops[k];
@@ -200,15 +206,50 @@ struct TcShared {
   uint64_t bar_tma;
   uint64_t bar_mma;
   uint32_t tmem_base;
+  float rowmax[2][kTile];
 };
 
+// which children of op `nx` the TMA must bring (the one equal to `fwd_slot` is forwarded)
+__device__ __forceinline__ int tma_mask(const DevOp &nx, int fwd_slot) {
+  int m = 0;
+  if (nx.l_kind == GEMS_CHILD_PARTIAL && nx.l_id != fwd_slot) m |= 1;
+  if (nx.r_kind == GEMS_CHILD_PARTIAL && nx.r_id != fwd_slot) m |= 2;
+  return m;
+}
+
+// thread 0: copies for op `nx` (children in `mask`, B images of every internal side)
+__device__ __forceinline__ void issue_copies(const DevCtx &c, const DevOp &nx, int mask,
+                                             const float *tk, const CUtensorMap *tmap,
+                                             float *const *A, unsigned char *Bbase, long p0,
+                                             uint32_t bar) {
+  const int C = c.C;
+  const size_t imgf = kBImg / 4;
+  const bool inL = nx.l_kind == GEMS_CHILD_PARTIAL, inR = nx.r_kind == GEMS_CHILD_PARTIAL;
+  uint32_t bytes = 0;
+  for (int s = 0; s < 2; s++) {
+    if (mask & (1 << s)) bytes += kRowChunks * kAChunk;
+    if (s ? inR : inL) bytes += (uint32_t)C * 2 * kBImg;
+  }
+  mbar_expect_tx(bar, bytes);
+  for (int s = 0; s < 2; s++) {
+    if (mask & (1 << s)) {
+      const int slot = s ? nx.r_id : nx.l_id;
+      const int row = slot * c.P + (int)p0;
+      for (int j = 0; j < kRowChunks; j++)
+        tma_load_2d(sptr(A[s]) + j * kAChunk, tmap, 4 * j, row, bar);
+    }
+    if (s ? inR : inL)
+      bulk_g2s(sptr(Bbase + (size_t)s * C * 2 * kBImg), tk + (size_t)s * C * 2 * imgf,
+               (uint32_t)C * 2 * kBImg, bar);
+  }
+}
+
 template <bool SAFE>
-__global__ void __launch_bounds__(kTile, 1)
+__global__ void __launch_bounds__(kThreadsTc, 1)
     k_traverse_tc20(DevCtx c, const DevOp *__restrict__ ops, int nops,
                     const float *__restrict__ tab, size_t stride_f,
                     const __grid_constant__ CUtensorMap tmap, int *flag) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // carve: A[2] | Alo[2] | B[2][C][2] | control
   unsigned char *base = smem_raw;
   float *A[2], *Alo[2];
   A[0] = reinterpret_cast<float *>(base);
@@ -220,22 +261,26 @@ __global__ void __launch_bounds__(kTile, 1)
   TcShared *ctl = reinterpret_cast<TcShared *>(Bbase + (size_t)2 * C * 2 * kBImg);
 
   const int t = threadIdx.x, warp = t >> 5;
+  const int row = ((warp & 3) << 5) | (t & 31);  // TMEM lane = pattern row of the tile
+  const int half = warp >> 2;                    // categories {2h, 2h+1}
   const long p0 = (long)blockIdx.x * kTile;
-  const long p = p0 + t;
+  const long p = p0 + row;
   const bool act = p < c.P;
   const uint32_t bar_tma = sptr(&ctl->bar_tma), bar_mma = sptr(&ctl->bar_mma);
+  const size_t imgf = kBImg / 4;
 
   if (t == 0) {
     mbar_init(bar_tma, 1);
     mbar_init(bar_mma, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // zero the spare chunk after each A tile (read by the last category's padded K step)
-  for (int s = 0; s < 2; s++) {
-    reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(A[s]) + kRowChunks * kAChunk)[t] =
-        make_float4(0.f, 0.f, 0.f, 0.f);
-    reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(Alo[s]) + kRowChunks * kAChunk)[t] =
-        make_float4(0.f, 0.f, 0.f, 0.f);
+  if (t < kTile) {  // zero chunk after each operand tile (read by the last category's K pad)
+    for (int s = 0; s < 2; s++) {
+      reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(A[s]) + kRowChunks * kAChunk)[t] =
+          make_float4(0.f, 0.f, 0.f, 0.f);
+      reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(Alo[s]) + kRowChunks * kAChunk)[t] =
+          make_float4(0.f, 0.f, 0.f, 0.f);
+    }
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -248,60 +293,68 @@ __global__ void __launch_bounds__(kTile, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = ctl->tmem_base;
+  const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
   uint32_t ph_tma = 0, ph_mma = 0;
   bool ok = true, tma_pending = false, mma_pending = false;
   float *part = static_cast<float *>(c.partials);
-  const size_t imgf = kBImg / 4;
+  const bool inv0 = act ? c.invar[p] == 0.0 : false;
+
+  DevOp cur = ops[0];
+  int cur_mask = tma_mask(cur, -1);
+  bool cur_copies = (cur.l_kind == GEMS_CHILD_PARTIAL) || (cur.r_kind == GEMS_CHILD_PARTIAL);
+  if (t == 0 && cur_copies) issue_copies(c, cur, cur_mask, tab, &tmap, A, Bbase, p0, bar_tma);
 
   for (int k = 0; k < nops && ok; k++) {
-    const DevOp op = ops[k];
     const float *tk = tab + (size_t)k * stride_f;
-    const bool inL = op.l_kind == GEMS_CHILD_PARTIAL, inR = op.r_kind == GEMS_CHILD_PARTIAL;
-    const int nin = (int)inL + (int)inR;
-    // ---- 1. bring the internal children's tiles and the B images into shared memory
-    if (nin > 0) {
-      if (t == 0) {
-        const uint32_t bytes = nin * (kRowChunks * kAChunk + (uint32_t)C * 2 * kBImg);
-        mbar_expect_tx(bar_tma, bytes);
-        for (int s = 0; s < 2; s++) {
-          const bool in = s ? inR : inL;
-          if (!in) continue;
-          const int slot = s ? op.r_id : op.l_id;
-          const int row = slot * c.P + (int)p0;
-          for (int j = 0; j < kRowChunks; j++)
-            tma_load_2d(sptr(A[s]) + j * kAChunk, &tmap, 4 * j, row, bar_tma);
-          const float *src = tk + (size_t)s * C * 2 * imgf;
-          bulk_g2s(sptr(Bbase + (size_t)s * C * 2 * kBImg), src, (uint32_t)C * 2 * kBImg, bar_tma);
+    const bool inL = cur.l_kind == GEMS_CHILD_PARTIAL, inR = cur.r_kind == GEMS_CHILD_PARTIAL;
+    // epilogue inputs that do not depend on the products: issue their loads first
+    int stL = 0, stR = 0, scL[2] = {0, 0}, scR[2] = {0, 0};
+    if (act) {
+      if (!inL) stL = c.tips[(size_t)cur.l_id * c.P + p];
+      if (!inR) stR = c.tips[(size_t)cur.r_id * c.P + p];
+      const uint16_t *sl = c.scale + (size_t)cur.l_id * c.slot_scale;
+      const uint16_t *sr = c.scale + (size_t)cur.r_id * c.slot_scale;
+      // (a forwarded child's counters were stored by the previous epilogue, before the barrier
+      // that ended it)
+      if (SAFE) {
+        for (int j = 0; j < 2; j++) {
+          const int cc = 2 * half + j;
+          if (cc < C && inL) scL[j] = sl[(size_t)p * C + cc];
+          if (cc < C && inR) scR[j] = sr[(size_t)p * C + cc];
         }
+      } else {
+        if (inL) scL[0] = sl[p];
+        if (inR) scR[0] = sr[p];
       }
-      tma_pending = true;
-      // every thread must take the same branch: vote on the bounded wait
-      if (__syncthreads_or(!mbar_wait(bar_tma, ph_tma))) {
-        ok = false;
-        if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
-        break;
+    }
+    if (inL || inR) {
+      if (cur_copies) {
+        tma_pending = true;
+        if (__syncthreads_or(!mbar_wait(bar_tma, ph_tma))) {
+          ok = false;
+          if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+          break;
+        }
+        tma_pending = false;
+        ph_tma ^= 1;
       }
-      tma_pending = false;
-      ph_tma ^= 1;
-      // ---- 2. split each loaded tile: A <- rna_tf32(A), Alo <- rna_tf32(A - hi)
+      // split the tiles the TMA brought: A <- hi in place, Alo <- lo
       for (int s = 0; s < 2; s++) {
-        if (!(s ? inR : inL)) continue;
+        if (!(cur_mask & (1 << s))) continue;
         float4 *a4 = reinterpret_cast<float4 *>(A[s]);
         float4 *l4 = reinterpret_cast<float4 *>(Alo[s]);
-#pragma unroll 4
-        for (int j = 0; j < kRowChunks; j++) {
-          float4 v = a4[j * kTile + t];
-          float4 h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
-          a4[j * kTile + t] = h;
-          l4[j * kTile + t] = make_float4(tf32_rna(v.x - h.x), tf32_rna(v.y - h.y),
-                                          tf32_rna(v.z - h.z), tf32_rna(v.w - h.w));
+#pragma unroll 5
+        for (int j = half * 10; j < half * 10 + 10; j++) {
+          float4 h, l;
+          split4(a4[j * kTile + row], h, l);
+          a4[j * kTile + row] = h;
+          l4[j * kTile + row] = l;
         }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       tc_fence_before();
       __syncthreads();
       tc_fence_after();
-      // ---- 3. one thread issues the split-TF32 products into TMEM
       if (t == 0) {
         for (int s = 0; s < 2; s++) {
           if (!(s ? inR : inL)) continue;
@@ -333,21 +386,34 @@ __global__ void __launch_bounds__(kTile, 1)
       ph_mma ^= 1;
       tc_fence_after();
     }
-    // ---- 4. epilogue: messages, product, rescaling, FP32 store of this thread's row
+    // operand buffers are free: start the next op's copies under this op's epilogue
+    const bool has_next = k + 1 < nops;
+    DevOp nxt = cur;
+    int nxt_mask = 0, nxt_fwd = -1;
+    bool nxt_copies = false;
+    if (has_next) {
+      nxt = ops[k + 1];
+      nxt_mask = tma_mask(nxt, cur.dst_slot);
+      if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) nxt_fwd = 0;
+      if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) nxt_fwd = 1;
+      nxt_copies = (nxt.l_kind == GEMS_CHILD_PARTIAL) || (nxt.r_kind == GEMS_CHILD_PARTIAL);
+      if (t == 0 && nxt_copies)
+        issue_copies(c, nxt, nxt_mask, tab + (size_t)(k + 1) * stride_f, &tmap, A, Bbase, p0,
+                     bar_tma);
+    }
+    // ---- epilogue: this thread's row, categories 2*half and 2*half+1
     const float *leafL = tk + (size_t)2 * C * 2 * imgf;
     const float *leafR = leafL + (size_t)(c.unknown + 1) * C * kN;
-    int stL = 0, stR = 0, sL = 0, sR = 0;
-    if (act) {
-      if (!inL) stL = c.tips[(size_t)op.l_id * c.P + p];
-      if (!inR) stR = c.tips[(size_t)op.r_id * c.P + p];
-    }
-    float out[4][kN];
-    float lh_max_all = 0.f;
-    float lh_max_c[4] = {0.f, 0.f, 0.f, 0.f};
-    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    float out[2][kN];
+    float mx[2] = {0.f, 0.f};
 #pragma unroll
-    for (int cc = 0; cc < 4; cc++) {
-      if (cc >= C) break;
+    for (int j = 0; j < 2; j++) {
+      const int cc = 2 * half + j;
+      if (cc >= C) {
+#pragma unroll
+        for (int x = 0; x < kN; x++) out[j][x] = 0.f;
+        continue;
+      }
       float mL[32], mR[32];
       if (inL) {
         tmem_ld32(tmem + lane_off + (uint32_t)(cc * kNP), mL);
@@ -366,61 +432,81 @@ __global__ void __launch_bounds__(kTile, 1)
 #pragma unroll
       for (int x = 0; x < kN; x++) {
         const float v = fmaxf(mL[x], 0.f) * fmaxf(mR[x], 0.f);
-        out[cc][x] = v;
-        lh_max_c[cc] = fmaxf(lh_max_c[cc], v);
+        out[j][x] = v;
+        mx[j] = fmaxf(mx[j], v);
       }
-      lh_max_all = fmaxf(lh_max_all, lh_max_c[cc]);
+    }
+    const bool tiptip = !inL && !inR;
+    float f[2] = {1.f, 1.f};
+    int s_out[2];
+    if (!SAFE) ctl->rowmax[half][row] = fmaxf(mx[0], mx[1]);  // the row max spans both halves
+    __syncthreads();
+    if (SAFE) {
+      for (int j = 0; j < 2; j++) {
+        const int cc = 2 * half + j;
+        s_out[j] = scL[j] + scR[j];
+        if (cc < C && !tiptip && mx[j] < kScaleThrF && inv0) {
+          f[j] = 18446744073709551616.0f;  // 2^64
+          s_out[j] += 1;
+        }
+      }
+    } else {
+      const float m = fmaxf(ctl->rowmax[0][row], ctl->rowmax[1][row]);
+      s_out[0] = scL[0] + scR[0];
+      if (!tiptip && m < kScaleThrF && inv0) {
+        f[0] = f[1] = 18446744073709551616.0f;  // 2^64
+        s_out[0] += 1;
+      }
+      s_out[1] = s_out[0];
     }
     if (act) {
-      const uint16_t *scl = c.scale + (size_t)op.l_id * c.slot_scale;
-      const uint16_t *scr = c.scale + (size_t)op.r_id * c.slot_scale;
-      const bool tiptip = !inL && !inR;
-      uint16_t *sd = c.scale + (size_t)op.dst_slot * c.slot_scale;
-      float *dst = part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * c.block;
-      if (SAFE) {
-        for (int cc = 0; cc < C; cc++) {
-          int s_out = (inL ? scl[(size_t)p * C + cc] : 0) + (inR ? scr[(size_t)p * C + cc] : 0);
-          float f = 1.f;
-          if (!tiptip && lh_max_c[cc] < kScaleThrF && c.invar[p] == 0.0) {
-            f = 18446744073709551616.0f;
-            s_out += 1;
+      float *dst = part + (size_t)cur.dst_slot * c.slot_elems + (size_t)p * c.block;
+      uint16_t *sd = c.scale + (size_t)cur.dst_slot * c.slot_scale;
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int cc = 2 * half + j;
+        if (cc >= C) continue;
+        float4 *d4 = reinterpret_cast<float4 *>(dst + cc * kN);
+#pragma unroll
+        for (int i = 0; i < kN / 4; i++) {
+          const float4 v = make_float4(out[j][4 * i] * f[j], out[j][4 * i + 1] * f[j],
+                                       out[j][4 * i + 2] * f[j], out[j][4 * i + 3] * f[j]);
+          d4[i] = v;
+          if (nxt_fwd >= 0) {  // the next op reads this row: hand it over already split
+            float4 h, l;
+            split4(v, h, l);
+            reinterpret_cast<float4 *>(A[nxt_fwd])[(cc * 5 + i) * kTile + row] = h;
+            reinterpret_cast<float4 *>(Alo[nxt_fwd])[(cc * 5 + i) * kTile + row] = l;
           }
-          float4 *d4 = reinterpret_cast<float4 *>(dst + cc * kN);
-#pragma unroll
-          for (int i = 0; i < kN / 4; i++)
-            d4[i] = make_float4(out[cc][4 * i] * f, out[cc][4 * i + 1] * f,
-                                out[cc][4 * i + 2] * f, out[cc][4 * i + 3] * f);
-          sd[(size_t)p * C + cc] = (uint16_t)s_out;
         }
-      } else {
-        sL = inL ? scl[p] : 0;
-        sR = inR ? scr[p] : 0;
-        int s_out = sL + sR;
-        float f = 1.f;
-        if (!tiptip && lh_max_all < kScaleThrF && c.invar[p] == 0.0) {
-          f = 18446744073709551616.0f;
-          s_out += 1;
-        }
+        if (SAFE) sd[(size_t)p * C + cc] = (uint16_t)s_out[j];
+      }
+      if (!SAFE && half == 0) sd[p] = (uint16_t)s_out[0];
+    } else if (nxt_fwd >= 0) {
 #pragma unroll
-        for (int cc = 0; cc < 4; cc++) {
-          if (cc >= C) break;
-          float4 *d4 = reinterpret_cast<float4 *>(dst + cc * kN);
+      for (int j = 0; j < 2; j++) {
+        const int cc = 2 * half + j;
+        if (cc >= C) continue;
 #pragma unroll
-          for (int i = 0; i < kN / 4; i++)
-            d4[i] = make_float4(out[cc][4 * i] * f, out[cc][4 * i + 1] * f,
-                                out[cc][4 * i + 2] * f, out[cc][4 * i + 3] * f);
+        for (int i = 0; i < kN / 4; i++) {
+          reinterpret_cast<float4 *>(A[nxt_fwd])[(cc * 5 + i) * kTile + row] =
+              make_float4(0.f, 0.f, 0.f, 0.f);
+          reinterpret_cast<float4 *>(Alo[nxt_fwd])[(cc * 5 + i) * kTile + row] =
+              make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        sd[p] = (uint16_t)s_out;
       }
     }
-    // the next op's TMA reads must see these generic-proxy stores
+    // later ops may TMA this output from global; the next MMA reads the forwarded operand
     asm volatile("fence.proxy.async.global;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    cur = nxt;
+    cur_mask = nxt_mask;
+    cur_copies = nxt_copies;
   }
   if (!ok && t == 0) {
-    // stop cleanly: wait (bounded) for the copies and products this CTA still has in flight
     if (tma_pending) mbar_wait(bar_tma, ph_tma);
     if (mma_pending) mbar_wait(bar_mma, ph_mma);
   }
@@ -439,10 +525,12 @@ size_t tc20_op_floats(int ncat, int unknown) {
 
 bool tc20_supported(const Session *s) {
   return s->desc.nstates == 20 && s->desc.precision == GEMS_PREC_MIXED && s->desc.ncat <= 4 &&
-         s->tc_enabled;
+         s->tc_enabled && (long long)s->P * s->desc.nslots < (1LL << 31);
 }
 
-static size_t tc_smem(int C) { return 4 * (size_t)kABytes + (size_t)2 * C * 2 * kBImg + 64; }
+static size_t tc_smem(int C) {
+  return 4 * (size_t)kABytes + (size_t)2 * C * 2 * kBImg + sizeof(TcShared) + 64;
+}
 
 int tc20_make_tmap(Session *s) {
   // 2D view of all partial slots: rows = nslots * P patterns, 80 floats per row
@@ -507,11 +595,11 @@ int launch_traverse_tc20(Session *s, int nops) {
   if (int st = prof_begin(s, 0, &ev0)) return st;
   const float *tab = reinterpret_cast<const float *>(s->d_opmats);
   if (safe)
-    k_traverse_tc20<true><<<grid, kTile, smem, s->stream>>>(c, s->d_ops, nops, tab,
-                                                             s->op_stride_tc, map, s->d_flag);
+    k_traverse_tc20<true><<<grid, kThreadsTc, smem, s->stream>>>(c, s->d_ops, nops, tab,
+                                                                  s->op_stride_tc, map, s->d_flag);
   else
-    k_traverse_tc20<false><<<grid, kTile, smem, s->stream>>>(c, s->d_ops, nops, tab,
-                                                              s->op_stride_tc, map, s->d_flag);
+    k_traverse_tc20<false><<<grid, kThreadsTc, smem, s->stream>>>(c, s->d_ops, nops, tab,
+                                                                   s->op_stride_tc, map, s->d_flag);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   if (int st = prof_end(s, 0, ev0)) return st;
