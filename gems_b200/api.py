@@ -181,6 +181,25 @@ class Session:
         _check(self.lib.gems_launch_count(self.handle, byref(n)), "gems_launch_count")
         return n.value
 
+    def upload_reweightings(self, weights):
+        """weights: [R][nptn] pattern counts of R bootstrap replicates (kept in HBM)."""
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        assert w.ndim == 2 and w.shape[1] == self.nptn
+        _check(self.lib.gems_upload_reweightings(self.handle, _dptr(w), w.shape[0]),
+               "gems_upload_reweightings")
+        self.rell_R = w.shape[0]
+
+    def reweighted_lnl(self):
+        out = np.zeros(self.rell_R)
+        _check(self.lib.gems_reweighted_lnl(self.handle, _dptr(out)), "gems_reweighted_lnl")
+        return out
+
+    def reweighted_derv(self):
+        df, ddf = np.zeros(self.rell_R), np.zeros(self.rell_R)
+        _check(self.lib.gems_reweighted_derv(self.handle, _dptr(df), _dptr(ddf)),
+               "gems_reweighted_derv")
+        return df, ddf
+
     def set_tensor_cores(self, on=True):
         """20-state mixed traversal on tcgen05 split-TF32 products (default) or FP32 CUDA
         cores."""

@@ -56,6 +56,7 @@ struct DevCtx {
   double *scale_all;       // [P]
   double *pattern_lh;      // [P]
   double *df_frac;         // [P]
+  double *ddf_term;        // [P] ddf_frac - df_frac^2 (reweighted derivatives)
   double *red;             // reduction partials
   size_t slot_elems;       // P * block
   size_t slot_scale;       // P * (safe ? C : 1)
@@ -80,6 +81,11 @@ struct Session {
   void *d_partials = nullptr;
   uint16_t *d_scale = nullptr;
   double *d_theta = nullptr, *d_scale_all = nullptr, *d_pattern_lh = nullptr, *d_df_frac = nullptr;
+  double *d_ddf_term = nullptr;
+  // bootstrap reweightings (RELL): R rows of P pattern counts
+  float *d_rell_w = nullptr;
+  int rell_R = 0;
+  size_t rell_ld = 0;
   double *d_model = nullptr;  // eval | evec | inv_evec | rates | props | tip | tip_real
   DevOp *d_ops = nullptr;
   double *d_opmats = nullptr;
@@ -152,6 +158,9 @@ size_t tc20_op_floats(int ncat, int unknown);
 bool tc20_supported(const Session *s);
 int launch_prep_ops_tc20(Session *s, int nops);
 int launch_traverse_tc20(Session *s, int nops);
+// bootstrap reweighting (kernels_rell.cu)
+int launch_rell_lnl(Session *s, double *d_out);
+int launch_rell_derv(Session *s, double *d_out);
 
 }  // namespace gems
 

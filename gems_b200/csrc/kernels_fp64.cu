@@ -403,7 +403,10 @@ __device__ __forceinline__ void derv_pattern(const DevCtx &c, long p, int gl, bo
     const double t1 = dff * f, t2 = ddff * f;
     a += t1;
     b += fma(-t1, dff, t2);
-    if (store_g) c.df_frac[p] = dff;
+    if (store_g) {
+      c.df_frac[p] = dff;
+      c.ddf_term[p] = fma(-dff, dff, ddff);
+    }
   }
 }
 

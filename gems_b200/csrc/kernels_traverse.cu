@@ -332,257 +332,6 @@ __global__ void __launch_bounds__(kThreads) k_traverse_mix(DevCtx c, const DevOp
   }
 }
 
-// ---------------------------------------------------------------------------------------
-// Look-ahead versions for 4 states.  Every op is a dependent round trip to L2 (the children
-// were written by earlier ops of the same CTA), so the kernels above stall on it.  Here each
-// lane requests the child rows of op k+1 with cp.async into a two-stage shared-memory ring
-// before computing op k, and reads them from shared memory one op later; a child that op k
-// itself produces is forwarded from registers instead.  A lane only ever reads the bytes it
-// copied, so a per-thread cp.async.wait_group orders it (no CTA barrier), and the copies cost
-// no registers.  The next op's scale counters and tip bytes are loaded into registers early.
-// ---------------------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                   static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))),
-               "l"(gsrc)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int K>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(K) : "memory");
-}
-
-// what a lane knows about one child of the next op before computing the current one
-struct Next {
-  int scale;
-  int state;
-  bool fwd;  // the child is the current op's output
-};
-
-// ELEM = double (FP64 eigen-space) or float (mixed real-space); VB = bytes of one lane's row
-template <typename ELEM, bool SAFE>
-__device__ __forceinline__ void request(const DevCtx &c, int kind, int id, int cur_dst, long p,
-                                        int gl, bool act, ELEM *ring_slot, Next &nx) {
-  nx.scale = 0;
-  nx.state = 0;
-  nx.fwd = false;
-  if (!act) return;
-  if (kind == GEMS_CHILD_TIP) {
-    nx.state = c.tips[(size_t)id * c.P + p];
-  } else if (id == cur_dst) {
-    nx.fwd = true;
-  } else {
-    const ELEM *src = static_cast<const ELEM *>(c.partials) + (size_t)id * c.slot_elems +
-                      (size_t)p * c.block + gl * 4;
-#pragma unroll
-    for (int i = 0; i < (int)(4 * sizeof(ELEM)) / 16; i++)
-      cp_async16(ring_slot + i * (16 / sizeof(ELEM)), src + i * (16 / sizeof(ELEM)));
-    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
-    nx.scale = SAFE ? sc[(size_t)p * c.C + gl] : sc[p];
-  }
-}
-
-template <bool SAFE>
-__global__ void __launch_bounds__(kThreads) k_traverse4_la(DevCtx c, const DevOp *__restrict__ ops,
-                                                           int nops,
-                                                           const double *__restrict__ tab,
-                                                           size_t stride, const EigPack<4> E) {
-  __shared__ __align__(16) double ring[2][2][kThreads][4];  // [stage][side][lane][state]
-  const int G = c.G;
-  const int t = threadIdx.x;
-  const int gl = t & (G - 1);
-  const long p = ((long)blockIdx.x * blockDim.x + t) / G;
-  const bool act = p < c.P && gl < c.C;
-  const int C = c.C, blk = c.block;
-  const bool inv0 = act ? c.invar[p] == 0.0 : false;
-  double *part = static_cast<double *>(c.partials);
-  DevOp cur = ops[0];
-  Next nl, nr;
-  request<double, SAFE>(c, cur.l_kind, cur.l_id, -1, p, gl, act, ring[0][0][t], nl);
-  request<double, SAFE>(c, cur.r_kind, cur.r_id, -1, p, gl, act, ring[0][1][t], nr);
-  cp_async_commit();
-  double fwd[4] = {0.0, 0.0, 0.0, 0.0};
-  int fwd_s = 0;
-  for (int k = 0; k < nops; k++) {
-    const int st = k & 1;
-    DevOp nxt = cur;
-    Next ml, mr;
-    const bool has_next = k + 1 < nops;
-    if (has_next) {
-      nxt = ops[k + 1];
-      request<double, SAFE>(c, nxt.l_kind, nxt.l_id, cur.dst_slot, p, gl, act, ring[st ^ 1][0][t], ml);
-      request<double, SAFE>(c, nxt.r_kind, nxt.r_id, cur.dst_slot, p, gl, act, ring[st ^ 1][1][t], mr);
-    }
-    cp_async_commit();
-    cp_async_wait<1>();  // this op's rows have landed; the next op's may still be in flight
-    const double *tk = tab + (size_t)k * stride;
-    const bool tiptip = cur.l_kind == GEMS_CHILD_TIP && cur.r_kind == GEMS_CHILD_TIP;
-    double out[4] = {0.0, 0.0, 0.0, 0.0};
-    double lh_max = 0.0;
-    const int sl = nl.fwd ? fwd_s : nl.scale, sr = nr.fwd ? fwd_s : nr.scale;
-    if (act) {
-      double v[2][4];
-#pragma unroll
-      for (int side = 0; side < 2; side++) {
-        const int kind = side ? cur.r_kind : cur.l_kind;
-        const Next &nx = side ? nr : nl;
-        const double *d = tk + side * blk;
-        if (kind == GEMS_CHILD_TIP) {
-          const double *lt = tk + 2 * blk + (size_t)side * (c.unknown + 1) * blk +
-                             (size_t)nx.state * blk + gl;
-#pragma unroll
-          for (int x = 0; x < 4; x++) v[side][x] = __ldg(lt + x * C);
-        } else {
-          double L[4];
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-            L[i] = (nx.fwd ? fwd[i] : ring[st][side][t][i]) * __ldg(d + i * C + gl);
-#pragma unroll
-          for (int x = 0; x < 4; x++) {
-            double acc = 0.0;
-#pragma unroll
-            for (int i = 0; i < 4; i++) acc = fma(E.evec[x * 4 + i], L[i], acc);
-            v[side][x] = acc;
-          }
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int x = 0; x < 4; x++) acc = fma(E.inv[j * 4 + x], v[0][x] * v[1][x], acc);
-        out[j] = acc;
-        lh_max = fmax(lh_max, fabs(acc));
-      }
-    }
-    if (!SAFE) lh_max = group_max(lh_max, G);
-    int s_out = sl + sr;
-    if (act) {
-      if (!tiptip && lh_max < kScaleThr && inv0) {
-#pragma unroll
-        for (int j = 0; j < 4; j++) out[j] = ldexp(out[j], kScaleExp);
-        s_out += 1;
-      }
-      double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)cur.dst_slot * c.slot_elems +
-                                                (size_t)p * blk + gl * 4);
-      d2[0] = make_double2(out[0], out[1]);
-      d2[1] = make_double2(out[2], out[3]);
-      uint16_t *sc = c.scale + (size_t)cur.dst_slot * c.slot_scale;
-      if (SAFE)
-        sc[(size_t)p * C + gl] = (uint16_t)s_out;
-      else if (gl == 0)
-        sc[p] = (uint16_t)s_out;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) fwd[i] = out[i];
-    fwd_s = s_out;
-    __syncwarp();
-    cur = nxt;
-    nl = ml;
-    nr = mr;
-  }
-  cp_async_wait<0>();
-}
-
-template <bool SAFE>
-__global__ void __launch_bounds__(kThreads) k_traverse_mix4_la(DevCtx c,
-                                                               const DevOp *__restrict__ ops,
-                                                               int nops,
-                                                               const float *__restrict__ tab,
-                                                               size_t stride_f) {
-  __shared__ __align__(16) float ring[2][2][kThreads][4];
-  const int G = c.G;
-  const int t = threadIdx.x;
-  const int gl = t & (G - 1);
-  const long p = ((long)blockIdx.x * blockDim.x + t) / G;
-  const bool act = p < c.P && gl < c.C;
-  const int C = c.C;
-  const size_t nnC = (size_t)16 * C;
-  const bool inv0 = act ? c.invar[p] == 0.0 : false;
-  float *part = static_cast<float *>(c.partials);
-  DevOp cur = ops[0];
-  Next nl, nr;
-  request<float, SAFE>(c, cur.l_kind, cur.l_id, -1, p, gl, act, ring[0][0][t], nl);
-  request<float, SAFE>(c, cur.r_kind, cur.r_id, -1, p, gl, act, ring[0][1][t], nr);
-  cp_async_commit();
-  float fwd[4] = {0.f, 0.f, 0.f, 0.f};
-  int fwd_s = 0;
-  for (int k = 0; k < nops; k++) {
-    const int st = k & 1;
-    DevOp nxt = cur;
-    Next ml, mr;
-    const bool has_next = k + 1 < nops;
-    if (has_next) {
-      nxt = ops[k + 1];
-      request<float, SAFE>(c, nxt.l_kind, nxt.l_id, cur.dst_slot, p, gl, act, ring[st ^ 1][0][t], ml);
-      request<float, SAFE>(c, nxt.r_kind, nxt.r_id, cur.dst_slot, p, gl, act, ring[st ^ 1][1][t], mr);
-    }
-    cp_async_commit();
-    cp_async_wait<1>();
-    const float *tk = tab + (size_t)k * stride_f;
-    const bool tiptip = cur.l_kind == GEMS_CHILD_TIP && cur.r_kind == GEMS_CHILD_TIP;
-    float out[4] = {0.f, 0.f, 0.f, 0.f};
-    float lh_max = 0.f;
-    const int sl = nl.fwd ? fwd_s : nl.scale, sr = nr.fwd ? fwd_s : nr.scale;
-    if (act) {
-      float v[2][4];
-#pragma unroll
-      for (int side = 0; side < 2; side++) {
-        const int kind = side ? cur.r_kind : cur.l_kind;
-        const Next &nx = side ? nr : nl;
-        if (kind == GEMS_CHILD_TIP) {
-          const float *lt = tk + 2 * nnC + (size_t)side * (c.unknown + 1) * c.block +
-                            (size_t)nx.state * c.block + gl;
-#pragma unroll
-          for (int x = 0; x < 4; x++) v[side][x] = __ldg(lt + x * C);
-        } else {
-          float L[4];
-#pragma unroll
-          for (int i = 0; i < 4; i++) L[i] = nx.fwd ? fwd[i] : ring[st][side][t][i];
-          const float *Pm = tk + side * nnC;
-#pragma unroll
-          for (int x = 0; x < 4; x++) {
-            const float4 pr = __ldg(reinterpret_cast<const float4 *>(Pm + ((size_t)x * C + gl) * 4));
-            v[side][x] = fmaf(pr.w, L[3], fmaf(pr.z, L[2], fmaf(pr.y, L[1], pr.x * L[0])));
-          }
-        }
-      }
-#pragma unroll
-      for (int x = 0; x < 4; x++) {
-        out[x] = v[0][x] * v[1][x];
-        lh_max = fmaxf(lh_max, out[x]);
-      }
-    }
-    if (!SAFE) lh_max = group_maxf(lh_max, G);
-    int s_out = sl + sr;
-    if (act) {
-      if (!tiptip && lh_max < kScaleThrF && inv0) {
-#pragma unroll
-        for (int x = 0; x < 4; x++) out[x] *= 18446744073709551616.0f;  // 2^64
-        s_out += 1;
-      }
-      *reinterpret_cast<float4 *>(part + (size_t)cur.dst_slot * c.slot_elems + (size_t)p * c.block +
-                                  gl * 4) = make_float4(out[0], out[1], out[2], out[3]);
-      uint16_t *sc = c.scale + (size_t)cur.dst_slot * c.slot_scale;
-      if (SAFE)
-        sc[(size_t)p * C + gl] = (uint16_t)s_out;
-      else if (gl == 0)
-        sc[p] = (uint16_t)s_out;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) fwd[i] = out[i];
-    fwd_s = s_out;
-    __syncwarp();
-    cur = nxt;
-    nl = ml;
-    nr = mr;
-  }
-  cp_async_wait<0>();
-}
-
 inline int grid_for(const Session *s) {
   const long threads = (long)s->P * s->G;
   return (int)((threads + kThreads - 1) / kThreads);
@@ -602,21 +351,12 @@ int launch_f64(Session *s, int nops) {
   }
   const int grid = grid_for(s);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
-  if constexpr (N == 4) {
-    if (safe)
-      k_traverse4_la<true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                              s->op_stride, E);
-    else
-      k_traverse4_la<false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+  if (safe)
+    k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
                                                                s->op_stride, E);
-  } else {
-    if (safe)
-      k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                                 s->op_stride, E);
-    else
-      k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                                  s->op_stride, E);
-  }
+  else
+    k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                                s->op_stride, E);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   return GEMS_OK;
@@ -656,8 +396,8 @@ int launch_traverse_v2(Session *s, int nops) {
     const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
     const float *tab = reinterpret_cast<const float *>(s->d_opmats);
     if (s->desc.nstates == 4) {
-      if (safe) k_traverse_mix4_la<true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
-      else k_traverse_mix4_la<false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+      if (safe) k_traverse_mix<4, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+      else k_traverse_mix<4, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
     } else {
       if (safe) k_traverse_mix<20, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
       else k_traverse_mix<20, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);

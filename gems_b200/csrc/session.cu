@@ -47,6 +47,7 @@ DevCtx Session::ctx() const {
   c.scale_all = d_scale_all;
   c.pattern_lh = d_pattern_lh;
   c.df_frac = d_df_frac;
+  c.ddf_term = d_ddf_term;
   c.red = d_red;
   c.slot_elems = (size_t)P * block;
   c.slot_scale = (size_t)P * (desc.scaling == GEMS_SCALE_SAFE ? desc.ncat : 1);
@@ -120,7 +121,8 @@ static Sizes compute_sizes(const gems_session_desc &d) {
   const size_t elem = d.precision == GEMS_PREC_MIXED ? sizeof(float) : sizeof(double);
   z.partial_bytes = (size_t)d.nslots * P * blk * elem;
   z.scale_bytes = (size_t)d.nslots * P * (d.scaling == GEMS_SCALE_SAFE ? d.ncat : 1) * 2;
-  z.theta_bytes = P * blk * sizeof(double) + 3 * P * sizeof(double);  // theta + scale_all, plh, G
+  // theta + scale_all, pattern_lh, df_frac, ddf_term
+  z.theta_bytes = P * blk * sizeof(double) + 4 * P * sizeof(double);
   z.nops_max = d.ntaxa + 8;
   z.op_stride = 2 * (size_t)d.ncat * d.nstates * d.nstates + 2 * (size_t)(unk + 1) * blk;
   if (d.nstates == 20 && d.precision == GEMS_PREC_MIXED && d.ncat <= 4) {
@@ -163,6 +165,7 @@ static void free_session(Session *s) {
   cudaFree(s->d_partials);
   cudaFree(s->d_scale);
   cudaFree(s->d_theta);
+  cudaFree(s->d_rell_w);
   cudaFree(s->d_model);
   cudaFree(s->d_ops);
   cudaFree(s->d_opmats);
@@ -343,6 +346,7 @@ int gems_session_create(const gems_session_desc *desc, gems_session **out) {
   s->d_scale_all = s->d_theta + P * s->block;
   s->d_pattern_lh = s->d_scale_all + P;
   s->d_df_frac = s->d_pattern_lh + P;
+  s->d_ddf_term = s->d_df_frac + P;
   ALLOC(s->d_model, z.model_doubles * sizeof(double));
   ALLOC(s->d_ops, (size_t)z.nops_max * sizeof(DevOp));
   ALLOC(s->d_opmats, z.opmats_bytes);
@@ -660,6 +664,62 @@ int gems_get_theta(gems_session *s, double *theta, double *scale_all) {
     GEMS_CUDA(cudaMemcpyAsync(scale_all, s->d_scale_all, sizeof(double) * s->desc.nptn,
                               cudaMemcpyDeviceToHost, s->stream));
   GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
+int gems_upload_reweightings(gems_session *s, const float *weights, int R) {
+  if (!s || !weights || R < 1 || 2 * R > s->nred) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  if (s->d_rell_w && s->rell_R != R) {
+    cudaFree(s->d_rell_w);
+    s->d_rell_w = nullptr;
+    s->rell_R = 0;
+  }
+  const size_t ld = (size_t)s->P;
+  if (!s->d_rell_w) {
+    size_t free_b = 0, total_b = 0;
+    GEMS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if ((size_t)R * ld * sizeof(float) > free_b) {
+      set_error("reweightings exceed free device memory");
+      return GEMS_ERR_ADMISSION;
+    }
+    GEMS_CUDA(cudaMalloc((void **)&s->d_rell_w, (size_t)R * ld * sizeof(float)));
+    GEMS_CUDA(cudaMemsetAsync(s->d_rell_w, 0, (size_t)R * ld * sizeof(float), s->stream));
+  }
+  s->rell_R = R;
+  s->rell_ld = ld;
+  GEMS_CUDA(cudaMemcpy2DAsync(s->d_rell_w, ld * sizeof(float), weights,
+                              (size_t)s->desc.nptn * sizeof(float),
+                              (size_t)s->desc.nptn * sizeof(float), R, cudaMemcpyHostToDevice,
+                              s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
+int gems_reweighted_lnl(gems_session *s, double *lnl) {
+  if (!s || !lnl) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = launch_rell_lnl(s, s->d_red);
+  if (st) return st;
+  GEMS_CUDA(cudaMemcpyAsync(lnl, s->d_red, sizeof(double) * s->rell_R, cudaMemcpyDeviceToHost,
+                            s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
+int gems_reweighted_derv(gems_session *s, double *df, double *ddf) {
+  if (!s || !df || !ddf) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = launch_rell_derv(s, s->d_red);
+  if (st) return st;
+  std::vector<double> tmp(2 * (size_t)s->rell_R);
+  GEMS_CUDA(cudaMemcpyAsync(tmp.data(), s->d_red, sizeof(double) * tmp.size(),
+                            cudaMemcpyDeviceToHost, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  for (int r = 0; r < s->rell_R; r++) {
+    df[r] = tmp[2 * r];
+    ddf[r] = tmp[2 * r + 1];
+  }
   return GEMS_OK;
 }
 

@@ -149,6 +149,18 @@ int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems
                        int compute_theta, double min_len, double max_len, double xacc,
                        int max_steps, double *opt_len, int *nevals);
 
+/* ---- bootstrap reweighting (UFBoot RELL) ---- */
+/* Upload R replicates of pattern counts, weights[R][nptn] (FP32), resident until replaced. */
+int gems_upload_reweightings(gems_session *s, const float *weights, int R);
+/* lnl[r] = sum_p weights[r][p] * pattern_lh[p] for the per-pattern log-likelihoods of the last
+ * branch lnL / lnL-from-buffer call: the dotProduct(pattern_lh, boot_sample) of UFBoot
+ * (tree/iqtree.cpp:3870-3916, tree/phylokernel.h:65; pattern_lh taken in FP32 as there,
+ * accumulated in FP64).  One launch for all R replicates. */
+int gems_reweighted_lnl(gems_session *s, double *lnl);
+/* Reweighted derivatives of the last gems_branch_derv call: df[r] = sum_p w_rp df_frac_p,
+ * ddf[r] = sum_p w_rp (ddf_frac_p - df_frac_p^2). */
+int gems_reweighted_derv(gems_session *s, double *df, double *ddf);
+
 /* ---- inspection ---- */
 /* partial[nptn * ncat * nstates] (pattern-major, category-major, state-contiguous; FP64
  * values, converted from the session precision) and scale[nptn] (NORM) or [nptn*ncat]
