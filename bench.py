@@ -1,24 +1,30 @@
 #!/usr/bin/env python
 """Benchmark of the likelihood path on one B200 (or N, pattern-sharded).
 
-Workload: DNA GTR+G4 (Gamma shape 0.5) on a seeded 512-taxon tree with branch lengths
-~Exp(0.05), 1,000,000 simulated sites with 5% gap cells, compressed to unique patterns
-(the "FP64 vs mixed-precision DNA at scale" configuration).  A step is one full-tree
-log-likelihood evaluated from scratch: every partial of the tree recomputed (510 node
-updates over all patterns), then the branch log-likelihood and its pattern-weighted sum.
+Workload (the "FP64 vs mixed-precision DNA at scale" configuration): DNA GTR+G4 (Gamma shape
+0.5) on a seeded 512-taxon tree with branch lengths ~Exp(0.05), 1,000,000 simulated sites
+with 5% gap cells, compressed to unique patterns (with random gaps nearly every column is
+unique).  A step is one full-tree log-likelihood evaluated from scratch: every partial of the
+tree recomputed (510 node updates over all patterns), then the branch log-likelihood and its
+pattern-weighted sum.  Both precision forms are timed in the same run:
+  * fp64  -- the plain drop-in (eigen-space FP64 partials, reference arithmetic);
+  * mixed -- FP32 real-space partials with per-pattern scaling, FP64 branch terms.
+`value` is the mixed form's site-partial updates/s when its lnL is within 1e-6 relative of
+the FP64 lnL of the same run (reported as `lnl_rel_err_mixed`), else the FP64 form's.
+`e2e` runs the same step through the public PhyloTree API from pinned host buffers (tips and
+weights up, pattern lnL down).  Timing uses CUDA events on the session's stream; the partial
+buffers (65 GB FP64, 33 GB mixed) exceed L2 many times over, so no flush is needed.
 
-Metric: site-partial updates/s (patterns x node updates per second, whole job) and lnL
-evaluations/s.  `value` is measured with the inputs resident in HBM; `e2e` runs the same
-step through the public PhyloTree API from host buffers (tips, weights up; pattern lnL
-down) every step.  Timing uses CUDA events on the session's stream; partial buffers
-(~39 GB) exceed L2 many times over, so no flush is needed between steps.
+Also reported (same run): one Newton branch optimisation (optimizeOneBranch) per branch, and
+the 20-state protein +G4 configuration (128 taxa, 100,000 sites) FP64 vs mixed (tcgen05
+split-TF32) with its lnL error.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gems|reference]
 
-Under torchrun each rank holds its own 1,000,000-site slab of the same tree and model
-(weak scaling); the per-evaluation exchange is one NCCL all-reduce of the lnL.
-`--impl reference` times the CPU restatement of the reference kernels (oracle/, FP64, all
-host threads) on the same workload, bounded to a pattern sample per step.
+Under torchrun each rank holds its own 1,000,000-site slab of the same tree and model (weak
+scaling); the per-evaluation exchange is one NCCL all-reduce of the lnL.  `--impl reference`
+times the CPU restatement of the reference kernels (oracle/, FP64, all host threads) on the
+same workload, bounded to a pattern sample per step.
 """
 from __future__ import annotations
 
@@ -40,6 +46,15 @@ from gems_b200 import synth  # noqa: E402
 
 NSITES = 1_000_000
 NTAXA = 512
+MIXED_RTOL = 1e-6
+
+CONFIGS = {
+    "dna512": "DNA GTR+G4 (alpha 0.5), 512 taxa, Exp(0.05) lengths, {sites} sites/rank with 5% "
+              "gaps, from-scratch full-tree lnL",
+    "protein128": "20-state protein +G4 (alpha 0.8), log-normal exchangeabilities, Dirichlet "
+                  "frequencies, 128 taxa, Exp(0.15) lengths, {sites} sites/rank, from-scratch "
+                  "full-tree lnL",
+}
 
 
 def update_bytes(s, n=4, C=4, safe=False):
@@ -53,15 +68,6 @@ def update_bytes(s, n=4, C=4, safe=False):
 def update_flops(n=4, C=4):
     """Algorithmic flops of one site-partial update (eigen-space form): 6*C*n^2 + C*n."""
     return 6 * C * n * n + C * n
-
-
-CONFIGS = {
-    "dna512": "DNA GTR+G4 (alpha 0.5), 512 taxa, Exp(0.05) lengths, {sites} sites/rank with 5% "
-              "gaps, from-scratch full-tree lnL",
-    "protein128": "20-state protein +G4 (alpha 0.8), log-normal exchangeabilities, Dirichlet "
-                  "frequencies, 128 taxa, Exp(0.15) lengths, {sites} sites/rank, from-scratch "
-                  "full-tree lnL",
-}
 
 
 def env_rank():
@@ -113,13 +119,13 @@ def read_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         d = json.load(open(path))
-        return float(d["hbm_gbs"]), "measured"
+        return float(d["hbm_gbs"]), float(d.get("bf16_tflops", 1590.0)), "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return 6650.0, 1590.0, "fallback"
 
 
 def read_traffic(name):
-    """traffic (DRAM bytes per launch) from the committed ncu summary, if present."""
+    """traffic (DRAM bytes per launch, scaled to this workload) from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
@@ -188,6 +194,13 @@ def make_workload(rank, nsites, config="dna512"):
     return tree, model, aln
 
 
+def config_block(args, aln, nops):
+    return {"workload": CONFIGS[args.config].format(sites=f"{args.sites:,}"),
+            "npat_per_rank": aln.npat, "node_updates_per_step": nops,
+            "parallelism": f"pattern-shard x{env_rank()[1]}",
+            "l2": "inputs larger than L2 (partials 33-65 GB), no flush needed"}
+
+
 def cpu_baseline(tree, model, aln, target_s=12.0):
     """The oracle (CPU restatement of the reference kernels) on a bounded pattern sample."""
     from oracle import oracle as orc
@@ -198,6 +211,7 @@ def cpu_baseline(tree, model, aln, target_s=12.0):
                           np.ascontiguousarray(aln.patterns[:, :nsamp]), aln.weights[:nsamp])
     ot = orc.OracleTree(tree, model, sub)
     nops = sum(op_kinds(tree))
+    ot.computeLikelihood()  # warm-up (allocation of the oracle's buffers)
     t0 = time.perf_counter()
     k = 0
     while True:
@@ -219,11 +233,9 @@ def run_reference(args):
     if rank != 0:
         return
     tree, model, aln = make_workload(0, args.sites, args.config)
-    for _ in range(args.warmup):
-        pass
-    res = []
-    for _ in range(args.steps):
-        res.append(cpu_baseline(tree, model, aln, target_s=max(3.0, 30.0 / args.steps)))
+    cpu_baseline(tree, model, aln, target_s=1.0)  # warm-up
+    res = [cpu_baseline(tree, model, aln, target_s=max(3.0, 30.0 / args.steps))
+           for _ in range(args.steps)]
     v = statistics.median(r["value"] for r in res)
     nops = sum(op_kinds(tree))
     line = {
@@ -231,14 +243,100 @@ def run_reference(args):
         "unit": "site-partial updates/s", "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "ms_per_step": 1e3 * nops * aln.npat / v, "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded)",
-        "config": {"workload": "DNA GTR+G4, 512 taxa, 1,000,000 sites (5% gaps), "
-                               "from-scratch full-tree lnL", "npat": aln.npat},
+        "data": "synthetic (seeded generator; no public dataset)",
+        "config": config_block(args, aln, nops),
         "cpu_baseline": {**res[0], "value": v},
         "e2e": {"value": v, "unit": "site-partial updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def time_lnl(gt, steps, warmup, stream, dist, lnl_buf):
+    """K from-scratch lnL evaluations timed with CUDA events on the session stream; returns
+    (ms per step (max over ranks), lnL, traversal kernel ms per launch, launches)."""
+    import torch
+    s = gt.session
+
+    def step():
+        gt.clearAllPartialLH()
+        v = gt.computeLikelihood()
+        if dist is not None:
+            lnl_buf.fill_(v)
+            dist.all_reduce(lnl_buf)
+            return float(lnl_buf.item())
+        return v
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    s.profile(True)
+    s.profile_read(0)
+    l0 = s.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        lnl = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    s.profile(False)
+    ms = e0.elapsed_time(e1) / steps
+    trav_ms, trav_n = s.profile_read(0)
+    launches = s.launch_count() - l0
+    t = torch.tensor([ms], dtype=torch.float64, device=lnl_buf.device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), lnl, trav_ms / max(trav_n, 1), launches
+
+
+def time_newton(gt, tree, stream, nbranch=24):
+    """optimizeOneBranch on nbranch branches (traversal of stale partials, theta, the whole
+    Newton loop on device); ms per branch."""
+    import torch
+    gt.clearAllPartialLH()
+    gt.computeLikelihood()
+    br = [(int(u), int(v)) for u, v in zip(tree.eu, tree.ev)][:nbranch]
+    gt.optimizeOneBranch(*br[0])  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    nev = 0
+    for u, v in br:
+        gt.optimizeOneBranch(u, v)
+        nev += gt.stats()[1]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return {"branches": len(br), "ms_per_branch": e0.elapsed_time(e1) / len(br),
+            "derivative_evals_per_branch": nev / len(br)}
+
+
+def protein_comparison(args, local):
+    """20-state +G4: FP64 vs mixed (tcgen05 split-TF32) and mixed on CUDA cores."""
+    import torch
+    from gems_b200 import PhyloTree
+    tree, model, aln = make_workload(0, 100_000, "protein128")
+    out = {"workload": CONFIGS["protein128"].format(sites="100,000"), "npat": aln.npat}
+    nops = sum(op_kinds(tree))
+    lnl_buf = torch.zeros(1, dtype=torch.float64, device=f"cuda:{local}")
+    res = {}
+    for name, prec, tc in (("fp64", "fp64", True), ("mixed_tcgen05", "mixed", True),
+                           ("mixed_cuda_cores", "mixed", False)):
+        gt = PhyloTree.from_case(tree, model, aln, precision=prec, device=local)
+        gt.session.set_tensor_cores(tc)
+        stream = torch.cuda.ExternalStream(gt.session.stream_handle(), device=local)
+        ms, lnl, kms, _ = time_lnl(gt, max(args.steps, 5), 3, stream, None, lnl_buf)
+        res[name] = {"ms_per_step": ms, "traverse_ms": kms,
+                     "site_partial_updates_per_s": nops * aln.npat / (ms * 1e-3), "lnl": lnl}
+        gt.close()
+        gt.session.close()
+    base = res["fp64"]
+    for k in ("mixed_tcgen05", "mixed_cuda_cores"):
+        res[k]["speedup_vs_fp64"] = base["ms_per_step"] / res[k]["ms_per_step"]
+        res[k]["lnl_rel_err_vs_fp64"] = abs(res[k]["lnl"] - base["lnl"]) / abs(base["lnl"])
+    out.update(res)
+    return out
 
 
 def main():
@@ -249,8 +347,10 @@ def main():
     ap.add_argument("--impl", default="gems", choices=["gems", "reference"])
     ap.add_argument("--sites", type=int, default=None)
     ap.add_argument("--config", default="dna512", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the Newton timing and the protein comparison")
     ap.add_argument("--no-tc", action="store_true",
                     help="20-state mixed traversal on CUDA cores instead of tcgen05")
     args = ap.parse_args()
@@ -270,68 +370,76 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     tree, model, aln = make_workload(rank, args.sites, args.config)
-    gt = PhyloTree.from_case(tree, model, aln, precision=args.precision, device=local)
-    s = gt.session
-    if args.no_tc:
-        s.set_tensor_cores(False)
-    stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
     kinds = op_kinds(tree)
     nops = sum(kinds)
     P = aln.npat
     lnl_buf = torch.zeros(1, dtype=torch.float64, device=f"cuda:{local}")
-
-    def step():
-        gt.clearAllPartialLH()
-        v = gt.computeLikelihood()
-        if dist is not None:
-            lnl_buf.fill_(v)
-            dist.all_reduce(lnl_buf)
-            return float(lnl_buf.item())
-        return v
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    s.profile(True)
-    s.profile_read(0)
-    l0 = s.launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hbm_peak, _, peak_src = read_peaks()
+    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    forms = {}
+    keep = None
     with Clocks(local) as clk:
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(args.steps):
-            lnl = step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-    s.profile(False)
-    ms = e0.elapsed_time(e1) / args.steps
-    trav_ms, trav_n = s.profile_read(0)
-    launches = s.launch_count() - l0
-    # max over ranks
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+        for prec in precisions:
+            gt = PhyloTree.from_case(tree, model, aln, precision=prec, device=local)
+            if args.no_tc:
+                gt.session.set_tensor_cores(False)
+            stream = torch.cuda.ExternalStream(gt.session.stream_handle(), device=local)
+            ms, lnl, kms, launches = time_lnl(gt, args.steps, args.warmup, stream, dist, lnl_buf)
+            s_bytes = 8 if prec == "fp64" else 4
+            b_ii, b_ti, b_tt = update_bytes(s_bytes, model.nstates, model.ncat)
+            alg = P * (kinds[0] * b_ii + kinds[1] * b_ti + kinds[2] * b_tt)
+            ach = alg / (kms * 1e-3) / 1e9
+            forms[prec] = {
+                "ms_per_step": ms, "value": world * nops * P / (ms * 1e-3), "lnl": lnl,
+                "gpu_launches": launches,
+                "roofline": {"bound": "hbm", "kernel": "traversal (one launch per step)",
+                             "achieved": ach, "peak": hbm_peak,
+                             "peak_source": peak_src, "unit": "GB/s", "frac": ach / hbm_peak,
+                             "algorithmic_bytes_per_launch": alg, "avg_launch_ms": kms,
+                             "traffic": read_traffic(f"traverse_{prec}_{args.config}.md")},
+            }
+            if not args.no_extras and rank == 0:
+                forms[prec]["newton"] = time_newton(gt, tree, stream)
+            if keep is not None:
+                keep[0].close()
+                keep[0].session.close()
+            keep = (gt, stream, prec)
+    fp = forms.get("fp64")
+    mx = forms.get("mixed")
+    head = "fp64"
+    if mx is not None and fp is not None:
+        err = abs(mx["lnl"] - fp["lnl"]) / abs(fp["lnl"])
+        mx["lnl_rel_err_vs_fp64"] = err
+        if err <= MIXED_RTOL:
+            head = "mixed"
+    elif mx is not None:
+        head = "mixed"
+    H = forms[head]
 
-    # end to end through the public API from host buffers
+    # end to end through the public API from pinned host buffers, on the headline form
+    gt, stream, prec = keep
+    if prec != head:
+        gt.close()
+        gt.session.close()
+        gt = PhyloTree.from_case(tree, model, aln, precision=head, device=local)
+        stream = torch.cuda.ExternalStream(gt.session.stream_handle(), device=local)
+    s = gt.session
     pin_pat = torch.empty(aln.patterns.shape, dtype=torch.uint8, pin_memory=True)
     pin_w = torch.empty(aln.weights.shape, dtype=torch.float64, pin_memory=True)
-    pat_host = pin_pat.numpy()
-    w_host = pin_w.numpy()
+    pat_host, w_host = pin_pat.numpy(), pin_w.numpy()
     pat_host[:] = aln.patterns
     w_host[:] = aln.weights
     h2d = pat_host.nbytes + w_host.nbytes
     d2h = 8 * P + 8
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.upload_tips(pat_host)
     torch.cuda.synchronize()
     e2.record(stream)
     for _ in range(args.steps):
         s.upload_tips(pat_host)
         s.upload_patterns(w_host)
         gt.clearAllPartialLH()
-        lnl_e2e, plh = gt.computeLikelihood(pattern_lh=True)
+        gt.computeLikelihood(pattern_lh=True)
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3) / args.steps
@@ -339,43 +447,31 @@ def main():
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
+    gt.close()
+    s.close()
 
-    ups = world * nops * P / (ms * 1e-3)
-    ups_e2e = world * nops * P / (ms_e2e * 1e-3)
-    b_ii, b_ti, b_tt = update_bytes(8 if args.precision == "fp64" else 4, model.nstates,
-                                    model.ncat)
-    alg_bytes = P * (kinds[0] * b_ii + kinds[1] * b_ti + kinds[2] * b_tt)
-    peak, peak_kind = read_peaks()
-    achieved = alg_bytes / (trav_ms / max(trav_n, 1) * 1e-3) / 1e9 if trav_n else None
     line = {
-        "metric": "site-partial updates/s", "value": ups, "unit": "site-partial updates/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "metric": "site-partial updates/s", "value": H["value"],
+        "unit": "site-partial updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": H["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if head == "fp64" else "f32 partials + f64 branch terms",
         "data": "synthetic (seeded generator; no public dataset)",
-        "config": {"workload": CONFIGS[args.config].format(sites=f"{args.sites:,}"),
-                   "npat_per_rank": P, "node_updates_per_step": nops,
-                   "precision": args.precision, "parallelism": f"pattern-shard x{world}",
-                   "l2": "inputs larger than L2 (partials ~39 GB)"},
-        "lnl_evals_per_s": 1.0 / (ms * 1e-3),
-        "lnl": lnl,
-        "gpu_launches": launches,
-        "e2e": {"value": ups_e2e, "unit": "site-partial updates/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
-        "roofline": {"bound": "hbm", "kernel": "k_traverse", "achieved": achieved,
-                     "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None,
-                     "algorithmic_bytes_per_launch": alg_bytes,
-                     "avg_launch_ms": trav_ms / max(trav_n, 1),
-                     "traffic": read_traffic(f"traverse_{args.precision}_{args.config}.md")},
+        "config": {**config_block(args, aln, nops), "precision": head},
+        "lnl_evals_per_s": 1.0 / (H["ms_per_step"] * 1e-3), "lnl": H["lnl"],
+        "gpu_launches": H["gpu_launches"],
+        "e2e": {"value": world * nops * P / (ms_e2e * 1e-3), "unit": "site-partial updates/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+        "roofline": H["roofline"],
+        "forms": forms,
         "clocks": clk.summary(),
     }
+    if rank == 0 and not args.no_extras and args.config == "dna512":
+        line["protein20"] = protein_comparison(args, local)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tree, model, aln)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    gt.close()
-    s.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -318,6 +318,19 @@ class PhyloTree:
                                                         byref(out)), "optimizeAllBranches")
         return out.value
 
+    def getBranchLength(self, u, v):
+        for i, (a, b) in enumerate(zip(self.eu, self.ev)):
+            if (a == u and b == v) or (a == v and b == u):
+                return float(self.getBranchLengths()[i])
+        raise KeyError((u, v))
+
+    def computeFuncDerv(self, node1, node2, value, new_branch=False):
+        f, df = c_double(), c_double()
+        _check(self.lib.gems_tree_compute_func_derv(self.handle, node1, node2, c_double(value),
+                                                    int(new_branch), byref(f), byref(df)),
+               "computeFuncDerv")
+        return f.value, df.value
+
     def getPartial(self, node, dad):
         s = self.session
         part = np.zeros((s.nptn, s.ncat, s.nstates))

@@ -405,6 +405,25 @@ int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double toleran
   return t->optimize_all(iterations, tolerance, max_nr_step, lnl);
 }
 
+int gems_tree_compute_func_derv(gems_tree *t, int node1, int node2, double value,
+                                int new_branch, double *f, double *df) {
+  if (!t || !f || !df || node1 < 0 || node2 < 0 || node1 >= t->nnode || node2 >= t->nnode ||
+      t->find(node1, node2) < 0 || !(value >= 0))
+    return GEMS_ERR_BAD_ARG;
+  // PhyloTree::computeFuncDerv (tree/phylotree.cpp:2555): current_it = node1 -> node2, both
+  // lengths set to value without invalidating partials (theta does not depend on the length)
+  t->cur_u = node1;
+  t->cur_k = t->find(node1, node2);
+  if (new_branch) t->theta_computed = false;
+  t->set_len(node1, node2, value);
+  double d1 = 0, d2 = 0;
+  const int st = t->derv(node2, node1, &d1, &d2);
+  if (st) return st;
+  *f = -d1;
+  *df = -d2;
+  return GEMS_OK;
+}
+
 int gems_tree_get_partial(gems_tree *t, int node, int dad, double *partial, uint16_t *scale) {
   if (!t || node < 0 || dad < 0 || node >= t->nnode || dad >= t->nnode ||
       t->find(dad, node) < 0 || t->leaf(node))

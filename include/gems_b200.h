@@ -204,6 +204,12 @@ int gems_tree_optimize_one_branch(gems_tree *t, int node1, int node2, int clear_
 /* optimizeAllBranches(my_iterations, tolerance, maxNRStep) (tree/phylotree.cpp:2724) */
 int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double tolerance,
                                     int max_nr_step, double *lnl);
+/* PhyloTree::computeFuncDerv (tree/phylotree.cpp:2555): set the length of branch
+ * (node1, node2) to value without invalidating partials and return f = -dlnL/dt,
+ * df = -d2lnL/dt2; new_branch != 0 rebuilds theta for this branch first.  Used to drive a
+ * Newton iteration from outside, e.g. in lock-step over pattern shards. */
+int gems_tree_compute_func_derv(gems_tree *t, int node1, int node2, double value,
+                                int new_branch, double *f, double *df);
 /* partial of directed branch dad->node (subtree at node), if valid */
 int gems_tree_get_partial(gems_tree *t, int node, int dad, double *partial, uint16_t *scale);
 /* partial recomputations (traversal ops) executed so far, and Newton evaluations of the

@@ -1107,6 +1107,14 @@ static void func_derv(orc_tree *t, double x, double *f, double *df) {
     t->newton_evals++;
 }
 
+void orc_compute_func_derv(orc_tree *t, int node1, int node2, double value, int new_branch,
+                           double *f, double *df) {
+    t->cur_u = node1;
+    t->cur_k = find_nei(t, node1, node2);
+    if (new_branch) t->theta_computed = 0;
+    func_derv(t, value, f, df);
+}
+
 /* minimizeNewton (utils/optimization.cpp:422-499) */
 static double minimize_newton(orc_tree *t, double x1, double xguess, double x2, double xacc,
                               int maxstep) {

@@ -126,6 +126,15 @@ class OracleTree:
     def computeLikelihoodFromBuffer(self):
         return self.L.orc_compute_likelihood_from_buffer(self.h)
 
+    def getBranchLength(self, u, v):
+        return self.L.orc_get_length(self.h, u, v)
+
+    def computeFuncDerv(self, node1, node2, value, new_branch=False):
+        f, df = c_double(), c_double()
+        self.L.orc_compute_func_derv(self.h, node1, node2, c_double(value), int(new_branch),
+                                     byref(f), byref(df))
+        return f.value, df.value
+
     def optimizeOneBranch(self, n1, n2, clearLH=True, maxNRStep=100):
         self.L.orc_optimize_one_branch(self.h, n1, n2, int(clearLH), maxNRStep)
 
