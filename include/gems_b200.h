@@ -149,6 +149,26 @@ int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems
                        int compute_theta, double min_len, double max_len, double xacc,
                        int max_steps, double *opt_len, int *nevals);
 
+/* ---- allocation-free evaluation ---- */
+/* No counterpart in the reference.  lnL at branch length `length` from a theta buffer the
+ * caller owns, for callers that cannot allocate device memory when they evaluate (inside a
+ * stream capture, under a memory pool that owns the device, or in a loop that must not touch
+ * the allocator).  It computes what gems_lnl_from_buffer computes, over caller-owned device
+ * arrays: theta[nptn][ncat][nstates] and scale_all[nptn] (the layout gems_get_theta returns),
+ * freq[nptn] and invar[nptn] (invar may be NULL); eval[nstates], rates[ncat], props[ncat]
+ * are host arrays.  stream is a cudaStream_t (NULL: the default stream); lnl (host) receives
+ * the result after the stream synchronises.  No cudaMalloc, cudaFree or allocating library
+ * call is made: the reduction scratch is a fixed device array of this library (256 KiB per
+ * GPU, held until exit), which limits nptn to 4194304 / G (G = smallest power of two >=
+ * ncat); larger calls return GEMS_ERR_BAD_ARG.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+int gems_lnl_from_theta_noalloc(const double *theta, const double *scale_all,
+                                const double *freq, const double *invar, int nptn,
+                                int nstates, int ncat, const double *eval,
+                                const double *rates, const double *props, double length,
+                                void *stream, double *lnl);
+
 /* ---- bootstrap reweighting (UFBoot RELL) ---- */
 /* Upload R replicates of pattern counts, weights[R][nptn] (FP32), resident until replaced. */
 int gems_upload_reweightings(gems_session *s, const float *weights, int R);
