@@ -18,11 +18,15 @@
 //
 // Pipeline per op (one CTA per SM, 8 warps; warps w and w+4 share TMEM lane quadrant w%4 and
 // each handles two of the four categories of a row):
-//   wait(TMA of this op) -> split the loaded tiles into hi/lo -> MMAs -> wait(MMA)
-//   -> issue the next op's TMA/bulk copies (operand buffers are free again)
-//   -> epilogue; when the next op consumes this op's output, the epilogue also writes the
-//      row, already split, into the next op's operand buffer (no round trip through L2).
-// Tip children need no product: the message is the tip table row.
+//   wait(copies of this op) -> split the loaded tiles into hi/lo -> MMAs -> wait(MMA)
+//   -> epilogue part 1 (TMEM / tip-table reads, products) -> barrier
+//   -> issue the next op's TMA/bulk copies (operand buffers and tables are free again)
+//   -> epilogue part 2 (rescaling, stores); when the next op consumes this op's output, the
+//      row is also written, already split, into the next op's operand buffer (no round trip
+//      through L2), and its counters stay in registers
+//   -> loads of the next op's tip bytes and counters, issued a whole op ahead of their use.
+// Tip children need no product: the message is a row of the op's tip table, which the same
+// bulk copy brings into the side's table region.  The op descriptors are read two ops ahead.
 //
 // Every mbarrier wait is bounded by a clock budget; on expiry the CTA records
 // GEMS_ERR_TIMEOUT, stops issuing work, waits (bounded) for what it has in flight, frees its
@@ -217,30 +221,72 @@ __device__ __forceinline__ int tma_mask(const DevOp &nx, int fwd_slot) {
   return m;
 }
 
-// thread 0: copies for op `nx` (children in `mask`, B images of every internal side)
+// bytes of a side's op table: split B images (internal child) or its tip table (tip child)
+__device__ __forceinline__ uint32_t side_table_bytes(bool internal, int C, int unknown) {
+  return internal ? (uint32_t)C * 2 * kBImg : (uint32_t)(unknown + 1) * C * kN * 4;
+}
+
+// thread 0: copies for op `nx`: TMA tiles of the children in `mask`, and for each side its
+// op table (B images of an internal child, tip table of a tip child) into that side's region
 __device__ __forceinline__ void issue_copies(const DevCtx &c, const DevOp &nx, int mask,
                                              const float *tk, const CUtensorMap *tmap,
                                              float *const *A, unsigned char *Bbase, long p0,
                                              uint32_t bar) {
   const int C = c.C;
   const size_t imgf = kBImg / 4;
-  const bool inL = nx.l_kind == GEMS_CHILD_PARTIAL, inR = nx.r_kind == GEMS_CHILD_PARTIAL;
   uint32_t bytes = 0;
   for (int s = 0; s < 2; s++) {
+    const bool in = (s ? nx.r_kind : nx.l_kind) == GEMS_CHILD_PARTIAL;
     if (mask & (1 << s)) bytes += kRowChunks * kAChunk;
-    if (s ? inR : inL) bytes += (uint32_t)C * 2 * kBImg;
+    bytes += side_table_bytes(in, C, c.unknown);
   }
   mbar_expect_tx(bar, bytes);
   for (int s = 0; s < 2; s++) {
+    const bool in = (s ? nx.r_kind : nx.l_kind) == GEMS_CHILD_PARTIAL;
     if (mask & (1 << s)) {
       const int slot = s ? nx.r_id : nx.l_id;
       const int row = slot * c.P + (int)p0;
       for (int j = 0; j < kRowChunks; j++)
         tma_load_2d(sptr(A[s]) + j * kAChunk, tmap, 4 * j, row, bar);
     }
-    if (s ? inR : inL)
-      bulk_g2s(sptr(Bbase + (size_t)s * C * 2 * kBImg), tk + (size_t)s * C * 2 * imgf,
-               (uint32_t)C * 2 * kBImg, bar);
+    const float *src = in ? tk + (size_t)s * C * 2 * imgf
+                          : tk + (size_t)2 * C * 2 * imgf + (size_t)s * (c.unknown + 1) * C * kN;
+    bulk_g2s(sptr(Bbase + (size_t)s * C * 2 * kBImg), src, side_table_bytes(in, C, c.unknown),
+             bar);
+  }
+}
+
+// what a thread loads for an op before its products are ready: tip bytes and the counters of
+// internal children (a forwarded child's counters come from the previous op's registers)
+struct OpIn {
+  int st[2];
+  int sc[2][2];  // [side][category of this thread]
+};
+
+template <bool SAFE>
+__device__ __forceinline__ void load_op_inputs(const DevCtx &c, const DevOp &op, int fwd_side,
+                                               const int (&fwd_s)[2], long p, int half,
+                                               bool act, OpIn &in) {
+  const int C = c.C;
+  for (int s = 0; s < 2; s++) {
+    in.st[s] = 0;
+    in.sc[s][0] = in.sc[s][1] = 0;
+    if (!act) continue;
+    const int kind = s ? op.r_kind : op.l_kind, id = s ? op.r_id : op.l_id;
+    if (kind == GEMS_CHILD_TIP) {
+      in.st[s] = c.tips[(size_t)id * c.P + p];
+    } else if (s == fwd_side) {
+      in.sc[s][0] = fwd_s[0];
+      in.sc[s][1] = fwd_s[1];
+    } else {
+      const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+      if (SAFE) {
+        for (int j = 0; j < 2; j++)
+          if (2 * half + j < C) in.sc[s][j] = sc[(size_t)p * C + 2 * half + j];
+      } else {
+        in.sc[s][0] = in.sc[s][1] = sc[p];
+      }
+    }
   }
 }
 
@@ -267,7 +313,6 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   const long p = p0 + row;
   const bool act = p < c.P;
   const uint32_t bar_tma = sptr(&ctl->bar_tma), bar_mma = sptr(&ctl->bar_mma);
-  const size_t imgf = kBImg / 4;
 
   if (t == 0) {
     mbar_init(bar_tma, 1);
@@ -294,50 +339,38 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   tc_fence_after();
   const uint32_t tmem = ctl->tmem_base;
   const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
+  // MMA descriptors of the first K step of category 0; the others are these plus offsets
+  // (the 14-bit address field counts 16-byte units and the whole buffer is < 256 KiB)
+  const uint64_t dA0[2] = {sdesc(sptr(A[0]), kAChunk, 128), sdesc(sptr(A[1]), kAChunk, 128)};
+  const uint64_t dL0[2] = {sdesc(sptr(Alo[0]), kAChunk, 128), sdesc(sptr(Alo[1]), kAChunk, 128)};
+  const uint64_t dB0 = sdesc(sptr(Bbase), kNP * 16, 128);
   uint32_t ph_tma = 0, ph_mma = 0;
   bool ok = true, tma_pending = false, mma_pending = false;
   float *part = static_cast<float *>(c.partials);
   const bool inv0 = act ? c.invar[p] == 0.0 : false;
 
   DevOp cur = ops[0];
+  DevOp nxt = nops > 1 ? ops[1] : cur;
   int cur_mask = tma_mask(cur, -1);
-  bool cur_copies = (cur.l_kind == GEMS_CHILD_PARTIAL) || (cur.r_kind == GEMS_CHILD_PARTIAL);
-  if (t == 0 && cur_copies) issue_copies(c, cur, cur_mask, tab, &tmap, A, Bbase, p0, bar_tma);
+  if (t == 0) issue_copies(c, cur, cur_mask, tab, &tmap, A, Bbase, p0, bar_tma);
+  OpIn in;
+  const int zero2[2] = {0, 0};
+  load_op_inputs<SAFE>(c, cur, -1, zero2, p, half, act, in);
 
   for (int k = 0; k < nops && ok; k++) {
-    const float *tk = tab + (size_t)k * stride_f;
     const bool inL = cur.l_kind == GEMS_CHILD_PARTIAL, inR = cur.r_kind == GEMS_CHILD_PARTIAL;
-    // epilogue inputs that do not depend on the products: issue their loads first
-    int stL = 0, stR = 0, scL[2] = {0, 0}, scR[2] = {0, 0};
-    if (act) {
-      if (!inL) stL = c.tips[(size_t)cur.l_id * c.P + p];
-      if (!inR) stR = c.tips[(size_t)cur.r_id * c.P + p];
-      const uint16_t *sl = c.scale + (size_t)cur.l_id * c.slot_scale;
-      const uint16_t *sr = c.scale + (size_t)cur.r_id * c.slot_scale;
-      // (a forwarded child's counters were stored by the previous epilogue, before the barrier
-      // that ended it)
-      if (SAFE) {
-        for (int j = 0; j < 2; j++) {
-          const int cc = 2 * half + j;
-          if (cc < C && inL) scL[j] = sl[(size_t)p * C + cc];
-          if (cc < C && inR) scR[j] = sr[(size_t)p * C + cc];
-        }
-      } else {
-        if (inL) scL[0] = sl[p];
-        if (inR) scR[0] = sr[p];
-      }
+    const bool has_next = k + 1 < nops;
+    // the op after next: its descriptor is needed one op from now
+    const DevOp nxt2 = (k + 2 < nops) ? ops[k + 2] : nxt;
+    tma_pending = true;
+    if (__syncthreads_or(!mbar_wait(bar_tma, ph_tma))) {
+      ok = false;
+      if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+      break;
     }
+    tma_pending = false;
+    ph_tma ^= 1;
     if (inL || inR) {
-      if (cur_copies) {
-        tma_pending = true;
-        if (__syncthreads_or(!mbar_wait(bar_tma, ph_tma))) {
-          ok = false;
-          if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
-          break;
-        }
-        tma_pending = false;
-        ph_tma ^= 1;
-      }
       // split the tiles the TMA brought: A <- hi in place, Alo <- lo
       for (int s = 0; s < 2; s++) {
         if (!(cur_mask & (1 << s))) continue;
@@ -356,21 +389,22 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       __syncthreads();
       tc_fence_after();
       if (t == 0) {
+#pragma unroll
         for (int s = 0; s < 2; s++) {
           if (!(s ? inR : inL)) continue;
-          for (int cc = 0; cc < C; cc++) {
+#pragma unroll
+          for (int cc = 0; cc < 4; cc++) {
+            if (cc >= C) break;
             const uint32_t dtm = tmem + (uint32_t)((s * C + cc) * kNP);
-            const uint32_t bh = sptr(Bbase + ((size_t)(s * C + cc) * 2) * kBImg);
-            const uint32_t bl = bh + kBImg;
+            const uint64_t bh = dB0 + (uint64_t)((((s * C + cc) * 2) * kBImg) >> 4);
+            const uint64_t bl = bh + (uint64_t)(kBImg >> 4);
+#pragma unroll
             for (int ks = 0; ks < kKP / 8; ks++) {
-              const uint32_t koff = (uint32_t)(cc * 5 + 2 * ks) * kAChunk;
-              const uint64_t ah = sdesc(sptr(A[s]) + koff, kAChunk, 128);
-              const uint64_t al = sdesc(sptr(Alo[s]) + koff, kAChunk, 128);
-              const uint64_t dbh = sdesc(bh + (uint32_t)(2 * ks) * (kNP * 16), kNP * 16, 128);
-              const uint64_t dbl = sdesc(bl + (uint32_t)(2 * ks) * (kNP * 16), kNP * 16, 128);
-              mma_tf32(dtm, ah, dbh, ks > 0 ? 1u : 0u);
-              mma_tf32(dtm, ah, dbl, 1u);
-              mma_tf32(dtm, al, dbh, 1u);
+              const uint64_t ko = (uint64_t)(((cc * 5 + 2 * ks) * kAChunk) >> 4);
+              const uint64_t kb = (uint64_t)((2 * ks * kNP * 16) >> 4);
+              mma_tf32(dtm, dA0[s] + ko, bh + kb, ks > 0 ? 1u : 0u);
+              mma_tf32(dtm, dA0[s] + ko, bl + kb, 1u);
+              mma_tf32(dtm, dL0[s] + ko, bh + kb, 1u);
             }
           }
         }
@@ -386,24 +420,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       ph_mma ^= 1;
       tc_fence_after();
     }
-    // operand buffers are free: start the next op's copies under this op's epilogue
-    const bool has_next = k + 1 < nops;
-    DevOp nxt = cur;
-    int nxt_mask = 0, nxt_fwd = -1;
-    bool nxt_copies = false;
-    if (has_next) {
-      nxt = ops[k + 1];
-      nxt_mask = tma_mask(nxt, cur.dst_slot);
-      if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) nxt_fwd = 0;
-      if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) nxt_fwd = 1;
-      nxt_copies = (nxt.l_kind == GEMS_CHILD_PARTIAL) || (nxt.r_kind == GEMS_CHILD_PARTIAL);
-      if (t == 0 && nxt_copies)
-        issue_copies(c, nxt, nxt_mask, tab + (size_t)(k + 1) * stride_f, &tmap, A, Bbase, p0,
-                     bar_tma);
-    }
-    // ---- epilogue: this thread's row, categories 2*half and 2*half+1
-    const float *leafL = tk + (size_t)2 * C * 2 * imgf;
-    const float *leafR = leafL + (size_t)(c.unknown + 1) * C * kN;
+    // ---- epilogue, part 1: messages and products into registers (the tip tables of this op
+    // are in the side regions of shared memory; read them before the next copies land)
     float out[2][kN];
     float mx[2] = {0.f, 0.f};
 #pragma unroll
@@ -414,37 +432,53 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         for (int x = 0; x < kN; x++) out[j][x] = 0.f;
         continue;
       }
-      float mL[32], mR[32];
-      if (inL) {
-        tmem_ld32(tmem + lane_off + (uint32_t)(cc * kNP), mL);
-      } else {
-        const float *lt = leafL + ((size_t)stL * C + cc) * kN;
+      float m[2][32];
 #pragma unroll
-        for (int x = 0; x < kN; x++) mL[x] = __ldg(lt + x);
-      }
-      if (inR) {
-        tmem_ld32(tmem + lane_off + (uint32_t)((C + cc) * kNP), mR);
-      } else {
-        const float *rt = leafR + ((size_t)stR * C + cc) * kN;
+      for (int s = 0; s < 2; s++) {
+        if (s ? inR : inL) {
+          tmem_ld32(tmem + lane_off + (uint32_t)((s * C + cc) * kNP), m[s]);
+        } else {
+          const float4 *lt = reinterpret_cast<const float4 *>(
+              Bbase + (size_t)s * C * 2 * kBImg + (((size_t)in.st[s] * C + cc) * kN) * 4);
 #pragma unroll
-        for (int x = 0; x < kN; x++) mR[x] = __ldg(rt + x);
+          for (int i = 0; i < kN / 4; i++) {
+            const float4 v = lt[i];
+            m[s][4 * i] = v.x;
+            m[s][4 * i + 1] = v.y;
+            m[s][4 * i + 2] = v.z;
+            m[s][4 * i + 3] = v.w;
+          }
+        }
       }
 #pragma unroll
       for (int x = 0; x < kN; x++) {
-        const float v = fmaxf(mL[x], 0.f) * fmaxf(mR[x], 0.f);
+        const float v = fmaxf(m[0][x], 0.f) * fmaxf(m[1][x], 0.f);
         out[j][x] = v;
         mx[j] = fmaxf(mx[j], v);
       }
     }
     const bool tiptip = !inL && !inR;
+    if (!SAFE) ctl->rowmax[half][row] = fmaxf(mx[0], mx[1]);  // the row max spans both halves
+    tc_fence_before();
+    __syncthreads();  // operand buffers, tables and TMEM of this op are no longer read
+    tc_fence_after();
+    // start the next op's copies under the rest of this epilogue
+    int nxt_mask = 0, nxt_fwd = -1;
+    if (has_next) {
+      nxt_mask = tma_mask(nxt, cur.dst_slot);
+      if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) nxt_fwd = 0;
+      if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) nxt_fwd = 1;
+      if (t == 0)
+        issue_copies(c, nxt, nxt_mask, tab + (size_t)(k + 1) * stride_f, &tmap, A, Bbase, p0,
+                     bar_tma);
+    }
+    // ---- epilogue, part 2: rescaling, counters, stores, forwarding
     float f[2] = {1.f, 1.f};
     int s_out[2];
-    if (!SAFE) ctl->rowmax[half][row] = fmaxf(mx[0], mx[1]);  // the row max spans both halves
-    __syncthreads();
     if (SAFE) {
       for (int j = 0; j < 2; j++) {
         const int cc = 2 * half + j;
-        s_out[j] = scL[j] + scR[j];
+        s_out[j] = in.sc[0][j] + in.sc[1][j];
         if (cc < C && !tiptip && mx[j] < kScaleThrF && inv0) {
           f[j] = 18446744073709551616.0f;  // 2^64
           s_out[j] += 1;
@@ -452,7 +486,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       }
     } else {
       const float m = fmaxf(ctl->rowmax[0][row], ctl->rowmax[1][row]);
-      s_out[0] = scL[0] + scR[0];
+      s_out[0] = in.sc[0][0] + in.sc[1][0];
       if (!tiptip && m < kScaleThrF && inv0) {
         f[0] = f[1] = 18446744073709551616.0f;  // 2^64
         s_out[0] += 1;
@@ -496,6 +530,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         }
       }
     }
+    // next op's tip bytes and counters (a forwarded child's counters are this op's s_out)
+    if (has_next) load_op_inputs<SAFE>(c, nxt, nxt_fwd, s_out, p, half, act, in);
     // later ops may TMA this output from global; the next MMA reads the forwarded operand
     asm volatile("fence.proxy.async.global;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -503,8 +539,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     __syncthreads();
     tc_fence_after();
     cur = nxt;
+    nxt = nxt2;
     cur_mask = nxt_mask;
-    cur_copies = nxt_copies;
   }
   if (!ok && t == 0) {
     if (tma_pending) mbar_wait(bar_tma, ph_tma);
