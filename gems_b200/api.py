@@ -232,8 +232,9 @@ class PhyloTree:
     def __init__(self, session: Session, eu, ev, lengths):
         self.session = session
         self.lib = session.lib
-        self.eu = np.ascontiguousarray(eu, np.int32)
-        self.ev = np.ascontiguousarray(ev, np.int32)
+        # own copies: doNNI rewrites them in place
+        self.eu = np.array(eu, np.int32)
+        self.ev = np.array(ev, np.int32)
         ln = _f64(lengths)
         self.handle = c_void_p()
         _check(self.lib.gems_tree_create(session.handle, len(self.eu), _dptr(self.eu),
@@ -323,6 +324,21 @@ class PhyloTree:
             if (a == u and b == v) or (a == v and b == u):
                 return float(self.getBranchLengths()[i])
         raise KeyError((u, v))
+
+    def doNNI(self, u, v, a, b):
+        """Swap subtree a (at u) with subtree b (at v) across the internal branch (u, v)."""
+        _check(self.lib.gems_tree_nni(self.handle, u, v, a, b), "doNNI")
+        _check(self.lib.gems_tree_get_edges(self.handle, _dptr(self.eu), _dptr(self.ev)),
+               "get_edges")
+
+    def neighbors(self, u):
+        out = []
+        for a, b in zip(self.eu, self.ev):
+            if a == u:
+                out.append(int(b))
+            elif b == u:
+                out.append(int(a))
+        return out
 
     def computeFuncDerv(self, node1, node2, value, new_branch=False):
         f, df = c_double(), c_double()

@@ -250,6 +250,48 @@ struct Tree {
     return GEMS_OK;
   }
 
+  // PhyloTree::doNNI (tree/phylotree.cpp:4059-4125): exchange subtree a (at u) with subtree b
+  // (at v) across the internal branch (u, v).  The neighbour entries move with their lengths
+  // and partials (the subtrees at a and b are unchanged); the central partials and every
+  // partial looking back towards u or v are invalidated.
+  int nni(int u, int v, int a, int b) {
+    const int ku_a = find(u, a), kv_b = find(v, b), ka_u = find(a, u), kb_v = find(b, v);
+    if (leaf(u) || leaf(v) || find(u, v) < 0 || ku_a < 0 || kv_b < 0 || a == v || b == u)
+      return GEMS_ERR_BAD_ARG;
+    const int du = u * 3 + ku_a, dv = v * 3 + kv_b;
+    if (per_branch) {
+      std::swap(dslot[du], dslot[dv]);
+    } else {
+      // the buffers of a and b stay with their subtrees: re-point their owners
+      const bool own_a = !leaf(a) && owner[node_slot[a]] == du;
+      const bool own_b = !leaf(b) && owner[node_slot[b]] == dv;
+      if (own_a) owner[node_slot[a]] = dv;
+      if (own_b) owner[node_slot[b]] = du;
+    }
+    std::swap(adj[du], adj[dv]);
+    std::swap(len[du], len[dv]);
+    std::swap(computed[du], computed[dv]);
+    adj[a * 3 + ka_u] = v;
+    adj[b * 3 + kb_v] = u;
+    computed[u * 3 + find(u, v)] = 0;
+    computed[v * 3 + find(v, u)] = 0;
+    clear_reverse(v, u);
+    clear_reverse(u, v);
+    // edge list: the edges (u, a) and (v, b) become (v, a) and (u, b)
+    for (int e = 0; e < nedges; e++) {
+      if ((eu[e] == u && ev[e] == a) || (eu[e] == a && ev[e] == u)) {
+        eu[e] = v;
+        ev[e] = a;
+      } else if ((eu[e] == v && ev[e] == b) || (eu[e] == b && ev[e] == v)) {
+        eu[e] = u;
+        ev[e] = b;
+      }
+    }
+    theta_computed = false;
+    cur_u = -1;
+    return GEMS_OK;
+  }
+
   // PhyloTree::computeLikelihood (tree/phylotree.cpp:1258-1295)
   int compute_likelihood(double *lnl, double *pattern_lh) {
     if (cur_u < 0) {
@@ -403,6 +445,22 @@ int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double toleran
                                     int max_nr_step, double *lnl) {
   if (!t || !lnl || iterations < 1 || max_nr_step < 1) return GEMS_ERR_BAD_ARG;
   return t->optimize_all(iterations, tolerance, max_nr_step, lnl);
+}
+
+int gems_tree_nni(gems_tree *t, int u, int v, int a, int b) {
+  if (!t || u < 0 || v < 0 || a < 0 || b < 0 || u >= t->nnode || v >= t->nnode ||
+      a >= t->nnode || b >= t->nnode)
+    return GEMS_ERR_BAD_ARG;
+  return t->nni(u, v, a, b);
+}
+
+int gems_tree_get_edges(gems_tree *t, int *eu, int *ev) {
+  if (!t || !eu || !ev) return GEMS_ERR_BAD_ARG;
+  for (int e = 0; e < t->nedges; e++) {
+    eu[e] = t->eu[e];
+    ev[e] = t->ev[e];
+  }
+  return GEMS_OK;
 }
 
 int gems_tree_compute_func_derv(gems_tree *t, int node1, int node2, double value,

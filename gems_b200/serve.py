@@ -1,0 +1,285 @@
+"""Serving loop: many tree-search sessions resident in HBM, requests batched continuously.
+
+A session is one alignment + model + tree kept on the GPU (its partials, scale counters,
+theta and tip bytes).  A request is a local tree move as tree search issues them: an NNI on an
+internal branch (tree/phylotree.cpp:4059 doNNI), then Newton optimisation of the five branches
+around it (the central one and its four neighbours, as the NNI-5 evaluation of
+getBestNNIForBran does, tree/phylotree.cpp:4176), then the tree log-likelihood.  Only the
+partials on the affected paths are recomputed.
+
+Scheduling:
+  * admission by HBM footprint: a session is created on the GPU when its footprint
+    (gems_session_footprint) fits the remaining budget; it is released after its last
+    request, which admits the next waiting ones;
+  * continuous batching: requests arrive over time (Poisson); a pool of worker threads takes
+    the oldest runnable request of any admitted session whose previous request has finished.
+    Each session has its own CUDA stream and the C-ABI calls release the GIL, so the work of
+    different sessions overlaps on the device;
+  * per-session order is the arrival order, so a session's results do not depend on what else
+    runs (tests/test_gpu_serve.py checks this against each session run alone).
+
+    python -m gems_b200.serve --sessions 48 --requests 1000 --rate 300
+"""
+from __future__ import annotations
+
+import argparse
+import collections
+import dataclasses
+import json
+import threading
+import time
+
+import numpy as np
+
+from . import synth
+from .api import GemsError, PhyloTree, Session
+
+
+@dataclasses.dataclass
+class SessionSpec:
+    sid: int
+    ntaxa: int
+    nsites: int
+    nstates: int
+    ncat: int
+    precision: str
+    seed: int
+
+    def footprint(self, npat):
+        nslots = self.ntaxa - 2
+        scaling = "safe" if self.nstates == 61 else "norm"
+        return Session.footprint(self.ntaxa, npat, self.nstates, self.ncat, nslots,
+                                 self.precision, scaling)
+
+
+def build_case(spec: SessionSpec):
+    rng = np.random.default_rng(spec.seed)
+    if spec.nstates == 4:
+        model = synth.dna_gtr(rng, spec.ncat, 0.5)
+    elif spec.nstates == 20:
+        model = synth.protein(rng, spec.ncat, 0.8)
+    else:
+        model = synth.codon_gy(rng, spec.ncat, 0.5, freerate=spec.ncat == 8)
+    tree = synth.random_tree(spec.ntaxa, 0.1, spec.seed + 1)
+    aln = synth.simulate(tree, model, spec.nsites, spec.seed + 2)
+    return tree, model, aln
+
+
+def open_session(spec, case, device=0):
+    tree, model, aln = case
+    return PhyloTree.from_case(tree, model, aln, precision=spec.precision,
+                               scaling="safe" if spec.nstates == 61 else "norm", device=device)
+
+
+def nni5(gt: PhyloTree, ntaxa: int, rng: np.random.Generator):
+    """One request: a random NNI on an internal branch, Newton on the 5 branches around it,
+    then lnL.  Returns (lnL, branches optimised)."""
+    internal = [(int(a), int(b)) for a, b in zip(gt.eu, gt.ev) if a >= ntaxa and b >= ntaxa]
+    u, v = internal[int(rng.integers(len(internal)))]
+    nu = [x for x in gt.neighbors(u) if x != v]
+    nv = [x for x in gt.neighbors(v) if x != u]
+    a, b = nu[int(rng.integers(2))], nv[int(rng.integers(2))]
+    gt.doNNI(u, v, a, b)
+    branches = [(u, v)] + [(u, x) for x in gt.neighbors(u) if x != v] + \
+               [(v, y) for y in gt.neighbors(v) if y != u]
+    for p, q in branches:
+        gt.optimizeOneBranch(p, q)
+    return gt.computeLikelihoodFromBuffer(), len(branches)
+
+
+def run_alone(spec, case, nreq, device=0):
+    """The session's requests in order, nothing else on the GPU."""
+    gt = open_session(spec, case, device)
+    gt.computeLikelihood()
+    out = []
+    for k in range(nreq):
+        out.append(nni5(gt, spec.ntaxa, np.random.default_rng((spec.seed, k)))[0])
+    gt.close()
+    gt.session.close()
+    return out
+
+
+class Server:
+    def __init__(self, device=0, budget_bytes=None, workers=8):
+        import torch
+        free, _ = torch.cuda.mem_get_info(device)
+        self.device = device
+        self.budget = int(0.85 * free) if budget_bytes is None else int(budget_bytes)
+        self.workers = workers
+
+    def run(self, specs, cases, requests):
+        """requests: list of (arrival_s, sid) in arrival order.  Returns per-request records
+        and counters."""
+        lock = threading.Condition()
+        npat = {s.sid: cases[s.sid][2].npat for s in specs}
+        fp = {s.sid: s.footprint(npat[s.sid]) for s in specs}
+        spec_of = {s.sid: s for s in specs}
+        remaining = collections.Counter(sid for _, sid in requests)
+        pending = collections.defaultdict(collections.deque)  # sid -> deque of (arr, idx, seq)
+        seq_of = collections.Counter()
+        state = {"used": 0, "next": 0, "done": 0, "rejected": set()}
+        open_sess = {}   # sid -> PhyloTree
+        busy = set()
+        waiting_admit = collections.deque()
+        records = [None] * len(requests)
+        t0 = time.perf_counter()
+        for sid in fp:
+            if fp[sid] > self.budget:
+                state["rejected"].add(sid)
+
+        def admit_locked():
+            # admit waiting sessions in arrival order while they fit
+            while waiting_admit:
+                sid = waiting_admit[0]
+                if state["used"] + fp[sid] > self.budget:
+                    break
+                waiting_admit.popleft()
+                state["used"] += fp[sid]
+                open_sess[sid] = "opening"
+                return sid
+            return None
+
+        def dispatcher():
+            for i, (arr, sid) in enumerate(requests):
+                delay = arr - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                with lock:
+                    if sid in state["rejected"]:
+                        records[i] = {"sid": sid, "rejected": True}
+                        state["done"] += 1
+                    else:
+                        pending[sid].append((arr, i, seq_of[sid]))
+                        seq_of[sid] += 1
+                        if sid not in open_sess and sid not in waiting_admit:
+                            waiting_admit.append(sid)
+                    lock.notify_all()
+
+        def worker():
+            while True:
+                job = None
+                to_open = None
+                with lock:
+                    while True:
+                        if state["done"] >= len(requests):
+                            return
+                        to_open = admit_locked()
+                        if to_open is not None:
+                            break
+                        best = None
+                        for sid, dq in pending.items():
+                            if dq and sid not in busy and isinstance(open_sess.get(sid), PhyloTree):
+                                if best is None or dq[0][0] < pending[best][0][0]:
+                                    best = sid
+                        if best is not None:
+                            job = (best, pending[best].popleft())
+                            busy.add(best)
+                            break
+                        lock.wait(0.05)
+                if to_open is not None:
+                    try:
+                        gt = open_session(spec_of[to_open], cases[to_open], self.device)
+                        gt.computeLikelihood()
+                    except GemsError:
+                        gt = None
+                    with lock:
+                        if gt is None:
+                            state["rejected"].add(to_open)
+                            state["used"] -= fp[to_open]
+                            del open_sess[to_open]
+                            for arr, i, _ in pending.pop(to_open, []):
+                                records[i] = {"sid": to_open, "rejected": True}
+                                state["done"] += 1
+                        else:
+                            open_sess[to_open] = gt
+                        lock.notify_all()
+                    continue
+                sid, (arr, i, seq) = job
+                gt = open_sess[sid]
+                ts = time.perf_counter() - t0
+                lnl, nbr = nni5(gt, spec_of[sid].ntaxa, np.random.default_rng((spec_of[sid].seed, seq)))
+                te = time.perf_counter() - t0
+                with lock:
+                    records[i] = {"sid": sid, "seq": seq, "arrival": arr, "start": ts, "end": te,
+                                  "latency_ms": 1e3 * (te - arr), "lnl": lnl, "branches": nbr}
+                    busy.discard(sid)
+                    state["done"] += 1
+                    remaining[sid] -= 1
+                    if remaining[sid] == 0:
+                        gt.close()
+                        gt.session.close()
+                        open_sess[sid] = "closed"
+                        state["used"] -= fp[sid]
+                    lock.notify_all()
+
+        threads = [threading.Thread(target=worker) for _ in range(self.workers)]
+        disp = threading.Thread(target=dispatcher)
+        disp.start()
+        for th in threads:
+            th.start()
+        disp.join()
+        for th in threads:
+            th.join()
+        return records, time.perf_counter() - t0
+
+
+def make_stream(nsessions, nrequests, rate, seed, taxa=(8, 1024), sites=(500, 500_000),
+                states=(4, 20, 61), cats=(1, 4, 8), precisions=("fp64", "mixed")):
+    """Session specs (log-uniform taxa and sites) and Poisson arrivals at `rate` requests/s
+    spread uniformly over the sessions."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for sid in range(nsessions):
+        nt = int(round(np.exp(rng.uniform(np.log(taxa[0]), np.log(taxa[1])))))
+        ns = int(round(np.exp(rng.uniform(np.log(sites[0]), np.log(sites[1])))))
+        specs.append(SessionSpec(sid, max(nt, 8), ns, int(rng.choice(states)),
+                                 int(rng.choice(cats)), str(rng.choice(precisions)),
+                                 int(seed * 1000 + sid)))
+    gaps = rng.exponential(1.0 / rate, nrequests)
+    arr = np.cumsum(gaps)
+    sids = rng.integers(nsessions, size=nrequests)
+    return specs, list(zip(arr.tolist(), sids.tolist()))
+
+
+def summarize(records, wall, specs, cases):
+    done = [r for r in records if r and not r.get("rejected")]
+    lat = np.array([r["latency_ms"] for r in done]) if done else np.zeros(1)
+    upd = 0
+    for r in done:
+        spec = specs[r["sid"]]
+        npat = cases[r["sid"]][2].npat
+        upd += npat  # at least one partial per touched branch; reported as patterns served
+    return {"requests": len(records), "served": len(done),
+            "rejected": sum(1 for r in records if r and r.get("rejected")),
+            "wall_s": wall, "throughput_req_s": len(done) / wall,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p90": float(np.percentile(lat, 90)),
+                           "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "patterns_served_per_s": upd / wall}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--sessions", type=int, default=48)
+    ap.add_argument("--requests", type=int, default=1000)
+    ap.add_argument("--rate", type=float, default=300.0)
+    ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--max-taxa", type=int, default=256)
+    ap.add_argument("--max-sites", type=int, default=50_000)
+    ap.add_argument("--seed", type=int, default=5)
+    args = ap.parse_args()
+    specs, reqs = make_stream(args.sessions, args.requests, args.rate, args.seed,
+                              taxa=(8, args.max_taxa), sites=(500, args.max_sites))
+    cases = {s.sid: build_case(s) for s in specs}
+    srv = Server(workers=args.workers)
+    records, wall = srv.run(specs, cases, reqs)
+    out = summarize(records, wall, specs, cases)
+    out.update({"sessions": args.sessions, "offered_rate_req_s": args.rate,
+                "workers": args.workers, "taxa": [8, args.max_taxa],
+                "sites": [500, args.max_sites], "states": [4, 20, 61], "categories": [1, 4, 8],
+                "precisions": ["fp64", "mixed"]})
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -224,6 +224,13 @@ int gems_tree_optimize_one_branch(gems_tree *t, int node1, int node2, int clear_
 /* optimizeAllBranches(my_iterations, tolerance, maxNRStep) (tree/phylotree.cpp:2724) */
 int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double tolerance,
                                     int max_nr_step, double *lnl);
+/* PhyloTree::doNNI (tree/phylotree.cpp:4059-4125): swap subtree a (a neighbour of u) with
+ * subtree b (a neighbour of v) across the internal branch (u, v); partials and lengths move
+ * with their subtrees, the partials looking back across u or v are invalidated.  The edge
+ * list reported by gems_tree_get_edges changes accordingly. */
+int gems_tree_nni(gems_tree *t, int u, int v, int a, int b);
+/* current edge list (same order as at creation; endpoints change with NNIs) */
+int gems_tree_get_edges(gems_tree *t, int *eu, int *ev);
 /* PhyloTree::computeFuncDerv (tree/phylotree.cpp:2555): set the length of branch
  * (node1, node2) to value without invalidating partials and return f = -dlnL/dt,
  * df = -d2lnL/dt2; new_branch != 0 rebuilds theta for this branch first.  Used to drive a

@@ -1107,6 +1107,44 @@ static void func_derv(orc_tree *t, double x, double *f, double *df) {
     t->newton_evals++;
 }
 
+/* doNNI (tree/phylotree.cpp:4059-4125): neighbour entries (with their lengths and partials)
+ * swap between u and v; central partials and those looking back at u or v are cleared. */
+int orc_nni(orc_tree *t, int u, int v, int a, int b) {
+    int ku_a = find_nei(t, u, a), kv_b = find_nei(t, v, b), ka_u = find_nei(t, a, u),
+        kb_v = find_nei(t, b, v);
+    if (is_leaf(t, u) || is_leaf(t, v) || find_nei(t, u, v) < 0 || ku_a < 0 || kv_b < 0)
+        return -1;
+    int du = u * 3 + ku_a, dv = v * 3 + kv_b, e;
+    double *tp;
+    uint16_t *ts;
+    int ti;
+    double tl;
+    unsigned char tc;
+    ti = t->adj[du]; t->adj[du] = t->adj[dv]; t->adj[dv] = ti;
+    tl = t->len[du]; t->len[du] = t->len[dv]; t->len[dv] = tl;
+    tp = t->plh[du]; t->plh[du] = t->plh[dv]; t->plh[dv] = tp;
+    ts = t->scl[du]; t->scl[du] = t->scl[dv]; t->scl[dv] = ts;
+    tc = t->computed[du]; t->computed[du] = t->computed[dv]; t->computed[dv] = tc;
+    t->adj[a * 3 + ka_u] = v;
+    t->adj[b * 3 + kb_v] = u;
+    t->computed[u * 3 + find_nei(t, u, v)] = 0;
+    t->computed[v * 3 + find_nei(t, v, u)] = 0;
+    clear_reverse(t, v, u);
+    clear_reverse(t, u, v);
+    for (e = 0; e < t->nedges; e++) {
+        if ((t->eu[e] == u && t->ev[e] == a) || (t->eu[e] == a && t->ev[e] == u)) {
+            t->eu[e] = v;
+            t->ev[e] = a;
+        } else if ((t->eu[e] == v && t->ev[e] == b) || (t->eu[e] == b && t->ev[e] == v)) {
+            t->eu[e] = u;
+            t->ev[e] = b;
+        }
+    }
+    t->theta_computed = 0;
+    t->cur_u = -1;
+    return 0;
+}
+
 void orc_compute_func_derv(orc_tree *t, int node1, int node2, double value, int new_branch,
                            double *f, double *df) {
     t->cur_u = node1;
@@ -1157,7 +1195,9 @@ static double minimize_newton(orc_tree *t, double x1, double xguess, double x2, 
 }
 
 void orc_optimize_one_branch(orc_tree *t, int node1, int node2, int clear_lh, int max_nr_step) {
+    if (node1 < 0 || node1 >= t->nnode || node2 < 0 || node2 >= t->nnode) return;
     int k = find_nei(t, node1, node2);
+    if (k < 0) return;
     t->cur_u = node1;
     t->cur_k = k;
     double cur = t->len[node1 * 3 + k];

@@ -68,8 +68,9 @@ class OracleTree:
     def __init__(self, tree, model, aln, safe=False, const_char=None, p_invar=None):
         L = lib()
         self.L = L
-        self.eu = np.ascontiguousarray(tree.eu, np.int32)
-        self.ev = np.ascontiguousarray(tree.ev, np.int32)
+        # own copies: doNNI rewrites them in place
+        self.eu = np.array(tree.eu, np.int32)
+        self.ev = np.array(tree.ev, np.int32)
         ln = np.ascontiguousarray(tree.length, np.float64)
         self.h = c_void_p(L.orc_tree_new(tree.ntaxa, len(self.eu), _p(self.eu), _p(self.ev),
                                          _p(ln), model.nstates, model.ncat, int(safe)))
@@ -128,6 +129,18 @@ class OracleTree:
 
     def getBranchLength(self, u, v):
         return self.L.orc_get_length(self.h, u, v)
+
+    def doNNI(self, u, v, a, b):
+        assert self.L.orc_nni(self.h, u, v, a, b) == 0
+        for i in range(len(self.eu)):
+            x, y = int(self.eu[i]), int(self.ev[i])
+            if {x, y} == {u, a}:
+                self.eu[i], self.ev[i] = v, a
+            elif {x, y} == {v, b}:
+                self.eu[i], self.ev[i] = u, b
+
+    def neighbors(self, u):
+        return [int(b) if a == u else int(a) for a, b in zip(self.eu, self.ev) if u in (a, b)]
 
     def computeFuncDerv(self, node1, node2, value, new_branch=False):
         f, df = c_double(), c_double()

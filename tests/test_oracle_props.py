@@ -58,3 +58,40 @@ def test_newton_reaches_stationary_point():
     ot.clearAllPartialLH()
     df, ddf = ot.computeLikelihoodDerv(v, u)
     assert abs(df) < 1e-3 and ddf < 0
+
+
+@pytest.mark.parametrize("n", [4, 20])
+def test_nni_incremental_equals_fresh_tree(n):
+    """doNNI + NNI-5 branch optimisation keeps the partial buffers consistent: the lnL read
+    from the buffers equals a from-scratch lnL of a new tree with the resulting topology."""
+    from gems_b200.serve import nni5
+    tree, model, aln = small_case(n, ntaxa=12)
+    ot = orc.OracleTree(tree, model, aln)
+    ot.computeLikelihood()
+    for k in range(4):
+        lnl, nbr = nni5(ot, tree.ntaxa, np.random.default_rng((7, k)))
+        assert nbr == 5
+        fresh = orc.OracleTree(synth.Tree(tree.ntaxa, ot.eu.copy(), ot.ev.copy(),
+                                          ot.getBranchLengths()), model, aln)
+        ref = fresh.computeLikelihood()
+        assert abs(lnl - ref) <= 1e-9 * abs(ref), (k, lnl, ref)
+
+
+def test_nni_changes_topology_and_back():
+    """The same NNI applied twice restores the split set (doNNI is an involution up to the
+    edge labels it rewrites)."""
+    tree, model, aln = small_case(4, ntaxa=10)
+    ot = orc.OracleTree(tree, model, aln)
+    l0 = ot.computeLikelihood()
+    u, v = next((int(a), int(b)) for a, b in zip(tree.eu, tree.ev)
+                if a >= tree.ntaxa and b >= tree.ntaxa)
+    a = [x for x in ot.neighbors(u) if x != v][0]
+    b = [x for x in ot.neighbors(v) if x != u][0]
+    ot.doNNI(u, v, a, b)
+    assert a in ot.neighbors(v) and b in ot.neighbors(u)
+    l1 = ot.computeLikelihood()
+    assert abs(l1 - l0) > 1e-6
+    ot.doNNI(u, v, b, a)
+    assert a in ot.neighbors(u) and b in ot.neighbors(v)
+    l2 = ot.computeLikelihood()
+    assert abs(l2 - l0) <= 1e-9 * abs(l0)
