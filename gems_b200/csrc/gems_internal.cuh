@@ -43,7 +43,7 @@ struct DevCtx {
   const uint8_t *tips;   // [ntaxa][P]
   const double *freq;    // [P]
   const double *invar;   // [P]
-  void *partials;        // [nslots][P][block]  (double, or float in mixed)
+  void *partials;        // [nslots][P][block] (double, or float in mixed; see mix_off)
   uint16_t *scale;       // [nslots][P * (safe ? C : 1)]
   const double *inv_evec;  // [n][n]
   const double *evec;      // [n][n]
@@ -58,9 +58,30 @@ struct DevCtx {
   double *df_frac;         // [P]
   double *ddf_term;        // [P] ddf_frac - df_frac^2 (reweighted derivatives)
   double *red;             // reduction partials
-  size_t slot_elems;       // P * block
+  size_t slot_elems;       // P * block (tiled: P rounded up to 128, times block)
   size_t slot_scale;       // P * (safe ? C : 1)
 };
+
+// Layout of FP32 partials.  The 20-state mixed form stores each slot tile-major:
+//   [tile of 128 patterns][chunk = category * 5 + state / 4][128 rows][4 states]
+// which is the tensor-core operand layout (one contiguous 40 KB block per tile and slot, so a
+// tile moves with one bulk copy, and a warp's 32 rows of one chunk are 512 contiguous bytes).
+// Every other form is pattern-major [P][C][n].  mix_off<N>: offset of state 0 of category cc
+// of pattern p within a slot of N-state FP32 partials; mix_cs<N>: floats between consecutive
+// 4-state chunks of that row.
+constexpr int kMixTile = 128;
+template <int N>
+__host__ __device__ inline size_t mix_off(const DevCtx &c, long p, int cc) {
+  if constexpr (N == 20)
+    return (size_t)(p / kMixTile) * ((size_t)c.C * 5 * kMixTile * 4) +
+           (size_t)cc * 5 * kMixTile * 4 + (size_t)(p % kMixTile) * 4;
+  else
+    return (size_t)p * c.block + (size_t)cc * N;
+}
+template <int N>
+__host__ __device__ constexpr int mix_cs() {
+  return N == 20 ? kMixTile * 4 : 4;
+}
 
 struct Session {
   gems_session_desc desc;
@@ -99,11 +120,12 @@ struct Session {
   double *h_result = nullptr;
   int nred = 0;  // size of d_red in doubles
   std::vector<double> h_evec, h_inv;  // host copy of the eigenvectors in use
-  // tensor-core path (20 states, mixed): per-op table stride in floats, TMA descriptor
+  // tensor-core path (20 states, mixed): per-op table stride in floats
   bool tc_enabled = true;
   size_t op_stride_tc = 0;
-  alignas(64) unsigned char tmap_storage[128] = {};
-  bool tmap_ready = false;
+  // FP32 partials stored tile-major (20-state mixed form); elements per slot
+  bool tiled = false;
+  size_t slot_elems = 0;
   // kernel timing (gems_profile_*): event pairs recorded around launches
   static constexpr int kProfKernels = 8;
   bool prof_on = false;

@@ -91,13 +91,13 @@ __global__ void k_prep_ops_mixed(DevCtx c, const DevOp *ops, float *opm, size_t 
   }
 }
 
+// N states of one (pattern, category) row; cs = floats between 4-state chunks (mix_cs)
 template <int N>
-__device__ __forceinline__ void load_vecf(const float *__restrict__ src, float (&v)[N]) {
+__device__ __forceinline__ void load_vecf(const float *__restrict__ src, float (&v)[N], int cs) {
   if constexpr (N % 4 == 0) {
-    const float4 *s4 = reinterpret_cast<const float4 *>(src);
 #pragma unroll
     for (int i = 0; i < N / 4; i++) {
-      float4 t = __ldcg(s4 + i);
+      float4 t = __ldcg(reinterpret_cast<const float4 *>(src + (size_t)i * cs));
       v[4 * i] = t.x;
       v[4 * i + 1] = t.y;
       v[4 * i + 2] = t.z;
@@ -110,12 +110,12 @@ __device__ __forceinline__ void load_vecf(const float *__restrict__ src, float (
 }
 
 template <int N>
-__device__ __forceinline__ void store_vecf(float *__restrict__ dst, const float (&v)[N]) {
+__device__ __forceinline__ void store_vecf(float *__restrict__ dst, const float (&v)[N], int cs) {
   if constexpr (N % 4 == 0) {
-    float4 *d4 = reinterpret_cast<float4 *>(dst);
 #pragma unroll
     for (int i = 0; i < N / 4; i++)
-      d4[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+      *reinterpret_cast<float4 *>(dst + (size_t)i * cs) =
+          make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
   } else {
 #pragma unroll
     for (int i = 0; i < N; i++) dst[i] = v[i];
@@ -134,9 +134,9 @@ __device__ __forceinline__ void child_msg_f(const DevCtx &c, int kind, int id, c
     s = 0;
   } else {
     const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
-                       (size_t)p * c.block + gl * N;
+                       mix_off<N>(c, p, gl);
     float L[N];
-    load_vecf<N>(src, L);
+    load_vecf<N>(src, L, mix_cs<N>());
     const float *pm = Pm + (size_t)gl * N * N;
 #pragma unroll
     for (int x = 0; x < N; x++) {
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_traverse_mixed(DevCtx c, const Dev
         for (int x = 0; x < N; x++) out[x] *= 18446744073709551616.0f;  // 2^64
         s_out += 1;
       }
-      store_vecf<N>(part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * c.block + gl * N, out);
+      store_vecf<N>(part + (size_t)op.dst_slot * c.slot_elems + mix_off<N>(c, p, gl), out, mix_cs<N>());
       uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
       if (SAFE)
         sc[(size_t)p * C + gl] = (uint16_t)s_out;
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kThreads) k_theta_mixed(DevCtx c, gems_branch 
   double th[N];
   if (act) {
     float a[N];
-    load_vecf<N>(part + (size_t)br.dad_slot * c.slot_elems + (size_t)p * c.block + gl * N, a);
+    load_vecf<N>(part + (size_t)br.dad_slot * c.slot_elems + mix_off<N>(c, p, gl), a, mix_cs<N>());
     double de[N];
     lift<N>(c, a, de);
     const uint16_t *sd = c.scale + (size_t)br.dad_slot * c.slot_scale;
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kThreads) k_theta_mixed(DevCtx c, gems_branch 
       for (int i = 0; i < N; i++) th[i] = __ldg(tp + i) * de[i];
     } else {
       float b[N];
-      load_vecf<N>(part + (size_t)br.node_id * c.slot_elems + (size_t)p * c.block + gl * N, b);
+      load_vecf<N>(part + (size_t)br.node_id * c.slot_elems + mix_off<N>(c, p, gl), b, mix_cs<N>());
       double ne[N];
       lift<N>(c, b, ne);
 #pragma unroll

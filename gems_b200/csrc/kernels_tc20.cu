@@ -11,19 +11,20 @@
 // 2^64 rescaling, FP32 store).
 //
 // Operands in shared memory use the no-swizzle K-major core-matrix layout: 16-byte chunks of
-// 4 states x 128 rows, LBO = 2048 B between K chunks, SBO = 128 B between 8-row groups.  That
-// is exactly what a TMA box of {4 states, 128 rows} over the partial buffer (2D tensor map:
-// 80 floats per pattern row, rows of all slots stacked) writes, one box per chunk.  The split
-// B images are precomputed per op in the same layout and copied with cp.async.bulk.
+// 4 states x 128 rows, LBO = 2048 B between K chunks, SBO = 128 B between 8-row groups.  The
+// 20-state mixed partials are stored in global memory in exactly this layout (tile-major,
+// see mix_off), so a child's tile is one contiguous 5C x 2 KB block brought by one
+// cp.async.bulk, and the output rows go out as coalesced 16-byte stores (a warp writes 512
+// contiguous bytes per chunk).  The split B images are precomputed per op in the same layout.
 //
 // Pipeline per op (one CTA per SM, 8 warps; warps w and w+4 share TMEM lane quadrant w%4 and
 // each handles two of the four categories of a row):
 //   wait(copies of this op) -> split the loaded tiles into hi/lo -> MMAs -> wait(MMA)
 //   -> epilogue part 1 (TMEM / tip-table reads, products) -> barrier
-//   -> issue the next op's TMA/bulk copies (operand buffers and tables are free again)
-//   -> epilogue part 2 (rescaling, stores); when the next op consumes this op's output, the
-//      row is also written, already split, into the next op's operand buffer (no round trip
-//      through L2), and its counters stay in registers
+//   -> issue the next op's bulk copies (operand buffers and tables are free again)
+//   -> epilogue part 2 (rescaling, split, stores); when the next op consumes this op's output,
+//      the split row also goes into the next op's operand buffer (no round trip through
+//      global memory), and its counters stay in registers
 //   -> loads of the next op's tip bytes and counters, issued a whole op ahead of their use.
 // Tip children need no product: the message is a row of the op's tip table, which the same
 // bulk copy brings into the side's table region.  The op descriptors are read two ops ahead.
@@ -31,8 +32,6 @@
 // Every mbarrier wait is bounded by a clock budget; on expiry the CTA records
 // GEMS_ERR_TIMEOUT, stops issuing work, waits (bounded) for what it has in flight, frees its
 // TMEM and returns.
-#include <cuda.h>
-
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -80,14 +79,6 @@ __device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   while (!mbar_try_wait(bar, parity))
     if (clock64() - t0 > kWaitCycles) return false;
   return true;
-}
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
-                                            uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-      : "memory");
 }
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
                                          uint32_t bar) {
@@ -146,15 +137,22 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 #pragma unroll
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
+// Round a finite FP32 value to TF32 (10 fraction bits), to nearest with ties away from zero:
+// adding half a TF32 ulp (bit 12) to the sign-magnitude bits and clearing the 13 low bits
+// rounds the magnitude up exactly when the dropped bits are at least half an ulp (a carry
+// into the exponent gives the next binade correctly).  Two integer operations.
 __device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 __device__ __forceinline__ void split4(float4 v, float4 &h, float4 &l) {
   h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
   l = make_float4(tf32_rna(v.x - h.x), tf32_rna(v.y - h.y), tf32_rna(v.z - h.z),
                   tf32_rna(v.w - h.w));
+}
+// the value a row is stored as: hi + lo of its split (exact in FP32), so that a later split
+// of the stored value gives the same hi and lo again
+__device__ __forceinline__ float4 join4(float4 h, float4 l) {
+  return make_float4(h.x + l.x, h.y + l.y, h.z + l.z, h.w + l.w);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -229,25 +227,24 @@ __device__ __forceinline__ uint32_t side_table_bytes(bool internal, int C, int u
 // thread 0: copies for op `nx`: TMA tiles of the children in `mask`, and for each side its
 // op table (B images of an internal child, tip table of a tip child) into that side's region
 __device__ __forceinline__ void issue_copies(const DevCtx &c, const DevOp &nx, int mask,
-                                             const float *tk, const CUtensorMap *tmap,
-                                             float *const *A, unsigned char *Bbase, long p0,
-                                             uint32_t bar) {
+                                             const float *tk, uint32_t sA0, uint32_t sA1,
+                                             unsigned char *Bbase, int tile, uint32_t bar) {
   const int C = c.C;
   const size_t imgf = kBImg / 4;
   uint32_t bytes = 0;
   for (int s = 0; s < 2; s++) {
     const bool in = (s ? nx.r_kind : nx.l_kind) == GEMS_CHILD_PARTIAL;
-    if (mask & (1 << s)) bytes += kRowChunks * kAChunk;
+    if (mask & (1 << s)) bytes += 5 * C * kAChunk;
     bytes += side_table_bytes(in, C, c.unknown);
   }
   mbar_expect_tx(bar, bytes);
   for (int s = 0; s < 2; s++) {
     const bool in = (s ? nx.r_kind : nx.l_kind) == GEMS_CHILD_PARTIAL;
-    if (mask & (1 << s)) {
-      const int slot = s ? nx.r_id : nx.l_id;
-      const int row = slot * c.P + (int)p0;
-      for (int j = 0; j < kRowChunks; j++)
-        tma_load_2d(sptr(A[s]) + j * kAChunk, tmap, 4 * j, row, bar);
+    if (mask & (1 << s)) {  // the child's tile: one contiguous block of the tile-major slot
+      const float *src = static_cast<const float *>(c.partials) +
+                         (size_t)(s ? nx.r_id : nx.l_id) * c.slot_elems +
+                         (size_t)tile * (5 * C * kAChunk / 4);
+      bulk_g2s(s ? sA1 : sA0, src, 5 * C * kAChunk, bar);
     }
     const float *src = in ? tk + (size_t)s * C * 2 * imgf
                           : tk + (size_t)2 * C * 2 * imgf + (size_t)s * (c.unknown + 1) * C * kN;
@@ -293,8 +290,7 @@ __device__ __forceinline__ void load_op_inputs(const DevCtx &c, const DevOp &op,
 template <bool SAFE>
 __global__ void __launch_bounds__(kThreadsTc, 1)
     k_traverse_tc20(DevCtx c, const DevOp *__restrict__ ops, int nops,
-                    const float *__restrict__ tab, size_t stride_f,
-                    const __grid_constant__ CUtensorMap tmap, int *flag) {
+                    const float *__restrict__ tab, size_t stride_f, int *flag) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = smem_raw;
   float *A[2], *Alo[2];
@@ -309,7 +305,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   const int t = threadIdx.x, warp = t >> 5;
   const int row = ((warp & 3) << 5) | (t & 31);  // TMEM lane = pattern row of the tile
   const int half = warp >> 2;                    // categories {2h, 2h+1}
-  const long p0 = (long)blockIdx.x * kTile;
+  const int p0 = blockIdx.x * kTile;
   const long p = p0 + row;
   const bool act = p < c.P;
   const uint32_t bar_tma = sptr(&ctl->bar_tma), bar_mma = sptr(&ctl->bar_mma);
@@ -319,12 +315,13 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     mbar_init(bar_mma, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (t < kTile) {  // zero chunk after each operand tile (read by the last category's K pad)
+  // chunks 5C..20 of every operand buffer stay zero for the whole kernel (the K padding of
+  // the last category, and categories the session does not have): nothing writes them again
+  for (int i = t; i < (kRowChunks + 1 - 5 * C) * kTile; i += kThreadsTc) {
+    const int off = 5 * C * kTile + i;
     for (int s = 0; s < 2; s++) {
-      reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(A[s]) + kRowChunks * kAChunk)[t] =
-          make_float4(0.f, 0.f, 0.f, 0.f);
-      reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(Alo[s]) + kRowChunks * kAChunk)[t] =
-          make_float4(0.f, 0.f, 0.f, 0.f);
+      reinterpret_cast<float4 *>(A[s])[off] = make_float4(0.f, 0.f, 0.f, 0.f);
+      reinterpret_cast<float4 *>(Alo[s])[off] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   }
   if (warp == 0) {
@@ -346,13 +343,13 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   const uint64_t dB0 = sdesc(sptr(Bbase), kNP * 16, 128);
   uint32_t ph_tma = 0, ph_mma = 0;
   bool ok = true, tma_pending = false, mma_pending = false;
-  float *part = static_cast<float *>(c.partials);
+  const uint32_t sA0 = sptr(A[0]), sA1 = sptr(A[1]);
   const bool inv0 = act ? c.invar[p] == 0.0 : false;
 
   DevOp cur = ops[0];
   DevOp nxt = nops > 1 ? ops[1] : cur;
   int cur_mask = tma_mask(cur, -1);
-  if (t == 0) issue_copies(c, cur, cur_mask, tab, &tmap, A, Bbase, p0, bar_tma);
+  if (t == 0) issue_copies(c, cur, cur_mask, tab, sA0, sA1, Bbase, blockIdx.x, bar_tma);
   OpIn in;
   const int zero2[2] = {0, 0};
   load_op_inputs<SAFE>(c, cur, -1, zero2, p, half, act, in);
@@ -374,10 +371,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       // split the tiles the TMA brought: A <- hi in place, Alo <- lo
       for (int s = 0; s < 2; s++) {
         if (!(cur_mask & (1 << s))) continue;
-        float4 *a4 = reinterpret_cast<float4 *>(A[s]);
-        float4 *l4 = reinterpret_cast<float4 *>(Alo[s]);
+        float4 *a4 = reinterpret_cast<float4 *>(s ? A[1] : A[0]);
+        float4 *l4 = reinterpret_cast<float4 *>(s ? Alo[1] : Alo[0]);
+        const int jend = min(half * 10 + 10, 5 * C);
 #pragma unroll 5
-        for (int j = half * 10; j < half * 10 + 10; j++) {
+        for (int j = half * 10; j < jend; j++) {
           float4 h, l;
           split4(a4[j * kTile + row], h, l);
           a4[j * kTile + row] = h;
@@ -469,8 +467,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) nxt_fwd = 0;
       if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) nxt_fwd = 1;
       if (t == 0)
-        issue_copies(c, nxt, nxt_mask, tab + (size_t)(k + 1) * stride_f, &tmap, A, Bbase, p0,
-                     bar_tma);
+        issue_copies(c, nxt, nxt_mask, tab + (size_t)(k + 1) * stride_f, sA0, sA1, Bbase,
+                     blockIdx.x, bar_tma);
     }
     // ---- epilogue, part 2: rescaling, counters, stores, forwarding
     float f[2] = {1.f, 1.f};
@@ -493,46 +491,41 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       }
       s_out[1] = s_out[0];
     }
-    if (act) {
-      float *dst = part + (size_t)cur.dst_slot * c.slot_elems + (size_t)p * c.block;
+    // The output rows are stored as hi + lo of their split (so that a later split of the stored
+    // value gives the same operands), straight into the tile-major slot: for one chunk a warp
+    // writes 32 consecutive rows, 512 contiguous bytes.  When the next op consumes this output
+    // the split rows also go into its operand buffers.
+    float *dtile = static_cast<float *>(c.partials) + (size_t)cur.dst_slot * c.slot_elems +
+                   (size_t)blockIdx.x * (5 * C * kAChunk / 4);
+    float *fa = nxt_fwd == 1 ? A[1] : A[0];
+    float *fl = nxt_fwd == 1 ? Alo[1] : Alo[0];
+    {
       uint16_t *sd = c.scale + (size_t)cur.dst_slot * c.slot_scale;
 #pragma unroll
       for (int j = 0; j < 2; j++) {
         const int cc = 2 * half + j;
         if (cc >= C) continue;
-        float4 *d4 = reinterpret_cast<float4 *>(dst + cc * kN);
 #pragma unroll
         for (int i = 0; i < kN / 4; i++) {
           const float4 v = make_float4(out[j][4 * i] * f[j], out[j][4 * i + 1] * f[j],
                                        out[j][4 * i + 2] * f[j], out[j][4 * i + 3] * f[j]);
-          d4[i] = v;
-          if (nxt_fwd >= 0) {  // the next op reads this row: hand it over already split
-            float4 h, l;
-            split4(v, h, l);
-            reinterpret_cast<float4 *>(A[nxt_fwd])[(cc * 5 + i) * kTile + row] = h;
-            reinterpret_cast<float4 *>(Alo[nxt_fwd])[(cc * 5 + i) * kTile + row] = l;
+          float4 h, l;
+          split4(v, h, l);
+          const int idx = (cc * 5 + i) * kTile + row;
+          reinterpret_cast<float4 *>(dtile)[idx] = join4(h, l);
+          if (nxt_fwd >= 0) {
+            reinterpret_cast<float4 *>(fa)[idx] = h;
+            reinterpret_cast<float4 *>(fl)[idx] = l;
           }
         }
-        if (SAFE) sd[(size_t)p * C + cc] = (uint16_t)s_out[j];
+        if (SAFE && act) sd[(size_t)p * C + cc] = (uint16_t)s_out[j];
       }
-      if (!SAFE && half == 0) sd[p] = (uint16_t)s_out[0];
-    } else if (nxt_fwd >= 0) {
-#pragma unroll
-      for (int j = 0; j < 2; j++) {
-        const int cc = 2 * half + j;
-        if (cc >= C) continue;
-#pragma unroll
-        for (int i = 0; i < kN / 4; i++) {
-          reinterpret_cast<float4 *>(A[nxt_fwd])[(cc * 5 + i) * kTile + row] =
-              make_float4(0.f, 0.f, 0.f, 0.f);
-          reinterpret_cast<float4 *>(Alo[nxt_fwd])[(cc * 5 + i) * kTile + row] =
-              make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      }
+      if (!SAFE && act && half == 0) sd[p] = (uint16_t)s_out[0];
     }
     // next op's tip bytes and counters (a forwarded child's counters are this op's s_out)
     if (has_next) load_op_inputs<SAFE>(c, nxt, nxt_fwd, s_out, p, half, act, in);
-    // later ops may TMA this output from global; the next MMA reads the forwarded operand
+    // later ops bulk-copy this output from global memory, and the next MMA reads the forwarded
+    // operands: both through the async proxy
     asm volatile("fence.proxy.async.global;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
@@ -561,44 +554,11 @@ size_t tc20_op_floats(int ncat, int unknown) {
 
 bool tc20_supported(const Session *s) {
   return s->desc.nstates == 20 && s->desc.precision == GEMS_PREC_MIXED && s->desc.ncat <= 4 &&
-         s->tc_enabled && (long long)s->P * s->desc.nslots < (1LL << 31);
+         s->tc_enabled && s->tiled;
 }
 
 static size_t tc_smem(int C) {
   return 4 * (size_t)kABytes + (size_t)2 * C * 2 * kBImg + sizeof(TcShared) + 64;
-}
-
-int tc20_make_tmap(Session *s) {
-  // 2D view of all partial slots: rows = nslots * P patterns, 80 floats per row
-  CUtensorMap *map = reinterpret_cast<CUtensorMap *>(s->tmap_storage);
-  const cuuint64_t dims[2] = {(cuuint64_t)kN * s->desc.ncat, (cuuint64_t)s->P * s->desc.nslots};
-  const cuuint64_t strides[1] = {(cuuint64_t)kN * s->desc.ncat * sizeof(float)};
-  const cuuint32_t box[2] = {4, (cuuint32_t)kTile};
-  const cuuint32_t estr[2] = {1, 1};
-  // the driver entry point is resolved through the runtime, so the library does not link
-  // libcuda (it still loads on hosts without a driver)
-  using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  void *fn = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
-          cudaSuccess ||
-      q != cudaDriverEntryPointSuccess || !fn) {
-    set_error("cuTensorMapEncodeTiled entry point not available");
-    return GEMS_ERR_CUDA;
-  }
-  CUresult r = reinterpret_cast<EncodeFn>(fn)(
-      map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->d_partials, dims, strides, box, estr,
-      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    set_error("cuTensorMapEncodeTiled failed for the partial buffer");
-    return GEMS_ERR_CUDA;
-  }
-  s->tmap_ready = true;
-  return GEMS_OK;
 }
 
 int launch_prep_ops_tc20(Session *s, int nops) {
@@ -614,10 +574,6 @@ int launch_prep_ops_tc20(Session *s, int nops) {
 
 int launch_traverse_tc20(Session *s, int nops) {
   if (nops <= 0) return GEMS_OK;
-  if (!s->tmap_ready) {
-    int st = tc20_make_tmap(s);
-    if (st) return st;
-  }
   DevCtx c = s->ctx();
   const size_t smem = tc_smem(s->desc.ncat);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
@@ -625,17 +581,15 @@ int launch_traverse_tc20(Session *s, int nops) {
   GEMS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   GEMS_CUDA(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
   const int grid = (s->P + kTile - 1) / kTile;
-  CUtensorMap map;
-  std::memcpy(&map, s->tmap_storage, sizeof(map));
   cudaEvent_t ev0;
   if (int st = prof_begin(s, 0, &ev0)) return st;
   const float *tab = reinterpret_cast<const float *>(s->d_opmats);
   if (safe)
     k_traverse_tc20<true><<<grid, kThreadsTc, smem, s->stream>>>(c, s->d_ops, nops, tab,
-                                                                  s->op_stride_tc, map, s->d_flag);
+                                                                  s->op_stride_tc, s->d_flag);
   else
     k_traverse_tc20<false><<<grid, kThreadsTc, smem, s->stream>>>(c, s->d_ops, nops, tab,
-                                                                   s->op_stride_tc, map, s->d_flag);
+                                                                   s->op_stride_tc, s->d_flag);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   if (int st = prof_end(s, 0, ev0)) return st;

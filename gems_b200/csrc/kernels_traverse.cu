@@ -232,13 +232,13 @@ __device__ __forceinline__ void msg_mix(const DevCtx &c, int kind, int id,
     s = 0;
   } else {
     const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
-                       (size_t)p * c.block + gl * N;
+                       mix_off<N>(c, p, gl);
+    const int cs = mix_cs<N>();
     float L[N];
     if constexpr (N % 4 == 0) {
-      const float4 *s4 = reinterpret_cast<const float4 *>(src);
 #pragma unroll
       for (int i = 0; i < N / 4; i++) {
-        const float4 t = __ldcg(s4 + i);
+        const float4 t = __ldcg(reinterpret_cast<const float4 *>(src + (size_t)i * cs));
         L[4 * i] = t.x;
         L[4 * i + 1] = t.y;
         L[4 * i + 2] = t.z;
@@ -312,12 +312,13 @@ __global__ void __launch_bounds__(kThreads) k_traverse_mix(DevCtx c, const DevOp
         for (int x = 0; x < N; x++) out[x] *= 18446744073709551616.0f;  // 2^64
         s_out += 1;
       }
-      float *dst = part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * c.block + gl * N;
+      float *dst = part + (size_t)op.dst_slot * c.slot_elems + mix_off<N>(c, p, gl);
       if constexpr (N % 4 == 0) {
-        float4 *d4 = reinterpret_cast<float4 *>(dst);
+        const int cs = mix_cs<N>();
 #pragma unroll
         for (int i = 0; i < N / 4; i++)
-          d4[i] = make_float4(out[4 * i], out[4 * i + 1], out[4 * i + 2], out[4 * i + 3]);
+          *reinterpret_cast<float4 *>(dst + (size_t)i * cs) =
+              make_float4(out[4 * i], out[4 * i + 1], out[4 * i + 2], out[4 * i + 3]);
       } else {
 #pragma unroll
         for (int i = 0; i < N; i++) dst[i] = out[i];

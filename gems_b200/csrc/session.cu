@@ -49,7 +49,7 @@ DevCtx Session::ctx() const {
   c.df_frac = d_df_frac;
   c.ddf_term = d_ddf_term;
   c.red = d_red;
-  c.slot_elems = (size_t)P * block;
+  c.slot_elems = slot_elems;
   c.slot_scale = (size_t)P * (desc.scaling == GEMS_SCALE_SAFE ? desc.ncat : 1);
   return c;
 }
@@ -107,6 +107,8 @@ static int pow2_at_least(int x) {
 }
 
 struct Sizes {
+  bool tiled;
+  size_t slot_elems;
   size_t partial_bytes, scale_bytes, theta_bytes, opmats_bytes, branch_bytes, red_doubles,
       model_doubles, total;
   int nops_max;
@@ -119,7 +121,10 @@ static Sizes compute_sizes(const gems_session_desc &d) {
   const size_t blk = (size_t)d.nstates * d.ncat;
   const int unk = state_unknown(d.nstates);
   const size_t elem = d.precision == GEMS_PREC_MIXED ? sizeof(float) : sizeof(double);
-  z.partial_bytes = (size_t)d.nslots * P * blk * elem;
+  // 20-state mixed partials are tile-major in 128-pattern tiles (the tensor-core layout)
+  z.tiled = d.nstates == 20 && d.precision == GEMS_PREC_MIXED;
+  z.slot_elems = (z.tiled ? (P + kMixTile - 1) / kMixTile * kMixTile : P) * blk;
+  z.partial_bytes = (size_t)d.nslots * z.slot_elems * elem;
   z.scale_bytes = (size_t)d.nslots * P * (d.scaling == GEMS_SCALE_SAFE ? d.ncat : 1) * 2;
   // theta + scale_all, pattern_lh, df_frac, ddf_term
   z.theta_bytes = P * blk * sizeof(double) + 4 * P * sizeof(double);
@@ -326,6 +331,8 @@ int gems_session_create(const gems_session_desc *desc, gems_session **out) {
   s->op_stride = z.op_stride;
   s->op_stride_tc = 2 * z.op_stride;  // same buffer viewed as floats
   s->nred = (int)z.red_doubles;
+  s->tiled = z.tiled;
+  s->slot_elems = z.slot_elems;
   auto fail = [&](cudaError_t e, const char *what) {
     int code = cuda_status(e, what);
     free_session(s);
@@ -637,12 +644,21 @@ int gems_get_partial(gems_session *s, int slot, double *partial, uint16_t *scale
       GEMS_CUDA(cudaMemcpyAsync(partial, src, n * sizeof(double), cudaMemcpyDeviceToHost,
                                 s->stream));
     } else {
-      std::vector<float> tmp(n);
-      const float *src = static_cast<const float *>(s->d_partials) + (size_t)slot * s->P * blk;
-      GEMS_CUDA(cudaMemcpyAsync(tmp.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost,
-                                s->stream));
+      std::vector<float> tmp(s->slot_elems);
+      const float *src = static_cast<const float *>(s->d_partials) + (size_t)slot * s->slot_elems;
+      GEMS_CUDA(cudaMemcpyAsync(tmp.data(), src, s->slot_elems * sizeof(float),
+                                cudaMemcpyDeviceToHost, s->stream));
       GEMS_CUDA(cudaStreamSynchronize(s->stream));
-      for (size_t i = 0; i < n; i++) partial[i] = tmp[i];
+      const DevCtx c = s->ctx();
+      const int nst = s->desc.nstates;
+      for (long p = 0; p < s->desc.nptn; p++)
+        for (int cc = 0; cc < s->desc.ncat; cc++) {
+          for (int x = 0; x < nst; x++) {
+            const size_t o = s->tiled ? mix_off<20>(c, p, cc) + (size_t)(x / 4) * mix_cs<20>() + x % 4
+                                      : (size_t)p * blk + (size_t)cc * nst + x;
+            partial[(size_t)p * blk + (size_t)cc * nst + x] = tmp[o];
+          }
+        }
     }
   }
   if (scale) {
