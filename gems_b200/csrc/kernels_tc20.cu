@@ -52,6 +52,13 @@ constexpr int kAChunk = kTile * 16;             // one chunk of an A tile (128 r
 constexpr int kABytes = (kRowChunks + 1) * kAChunk;  // + a zero chunk for the last category
 constexpr int kBImg = (kKP / 4) * kNP * 16;     // 6 chunks x 32 rows x 16 B = 3072
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+// TMEM columns: accumulators D[side][category] (32 columns each) in [0, 256), the hi part of
+// the operand rows A_hi[side][category] (K = 24 columns each) in [256, 448)
+constexpr int kTmemCols = 512;
+constexpr int kAhiCol = 256;
+// tip tables: one row of C x 20 floats per state code, padded by 4 floats so that rows of
+// consecutive state codes start in different shared-memory bank groups
+__host__ __device__ constexpr int tip_row_floats(int C) { return C * kN + 4; }
 
 __device__ __forceinline__ uint32_t sptr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -109,10 +116,28 @@ __device__ __forceinline__ void mma_tf32(uint32_t dtm, uint64_t a, uint64_t b, u
       "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
       : "memory");
 }
+// same, A read from tensor memory (lane = row, one column per K element)
+__device__ __forceinline__ void mma_tf32_ta(uint32_t dtm, uint32_t atm, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(dtm),
+      "r"(atm), "l"(b), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    bar)
                : "memory");
+}
+// one lane of a converged warp (the MMA and copy instructions are issued by a single thread;
+// issuing them from a warp-uniform branch keeps their operands in uniform registers)
+__device__ __forceinline__ bool elect_one() {
+  uint32_t pred = 0;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\telect.sync _|P, 0xffffffff;\n\tselp.u32 %0, 1, 0, P;\n\t}\n"
+      : "=r"(pred));
+  return pred != 0;
 }
 __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -141,6 +166,25 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 // adding half a TF32 ulp (bit 12) to the sign-magnitude bits and clearing the 13 low bits
 // rounds the magnitude up exactly when the dropped bits are at least half an ulp (a carry
 // into the exponent gives the next binade correctly).  Two integer operations.
+// the hi part of a row of one category (20 states and 4 zero columns of K padding) into its
+// 24 TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_st_row(uint32_t taddr, const float4 (&h)[5]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "f"(h[0].x), "f"(h[0].y), "f"(h[0].z), "f"(h[0].w), "f"(h[1].x), "f"(h[1].y), "f"(h[1].z),
+      "f"(h[1].w), "f"(h[2].x), "f"(h[2].y), "f"(h[2].z), "f"(h[2].w), "f"(h[3].x), "f"(h[3].y),
+      "f"(h[3].z), "f"(h[3].w)
+      : "memory");
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %5, %5, %5};" ::"r"(
+          taddr + 16),
+      "f"(h[4].x), "f"(h[4].y), "f"(h[4].z), "f"(h[4].w), "f"(0.f)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
 __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
@@ -193,10 +237,15 @@ __global__ void k_prep_ops_tc(DevCtx c, const DevOp *ops, float *tab, size_t str
     img[(size_t)cc * 2 * (kBImg / 4) + (kBImg / 4) + r] = lo;
   }
   if (kind != GEMS_CHILD_TIP) return;
+  const int trow = tip_row_floats(C);
   float *leaf = tab + (size_t)k * stride_f + (size_t)2 * C * 2 * (kBImg / 4) +
-                (size_t)side * (c.unknown + 1) * C * n;
-  for (int idx = threadIdx.x; idx < (c.unknown + 1) * C * n; idx += blockDim.x) {
-    const int s = idx / (C * n), r = idx - s * C * n, cc = r / n, x = r - cc * n;
+                (size_t)side * (c.unknown + 1) * trow;
+  for (int idx = threadIdx.x; idx < (c.unknown + 1) * trow; idx += blockDim.x) {
+    const int s = idx / trow, r = idx - s * trow, cc = r / n, x = r - cc * n;
+    if (cc >= C) {  // row padding
+      leaf[idx] = 0.f;
+      continue;
+    }
     const double *ind = c.tip_real + (size_t)s * n;
     float acc = 0.f;
     for (int y = 0; y < n; y++) acc = fmaf(Pm[(cc * n + x) * n + y], (float)ind[y], acc);
@@ -221,7 +270,7 @@ __device__ __forceinline__ int tma_mask(const DevOp &nx, int fwd_slot) {
 
 // bytes of a side's op table: split B images (internal child) or its tip table (tip child)
 __device__ __forceinline__ uint32_t side_table_bytes(bool internal, int C, int unknown) {
-  return internal ? (uint32_t)C * 2 * kBImg : (uint32_t)(unknown + 1) * C * kN * 4;
+  return internal ? (uint32_t)C * 2 * kBImg : (uint32_t)(unknown + 1) * tip_row_floats(C) * 4;
 }
 
 // thread 0: copies for op `nx`: TMA tiles of the children in `mask`, and for each side its
@@ -247,7 +296,7 @@ __device__ __forceinline__ void issue_copies(const DevCtx &c, const DevOp &nx, i
       bulk_g2s(s ? sA1 : sA0, src, 5 * C * kAChunk, bar);
     }
     const float *src = in ? tk + (size_t)s * C * 2 * imgf
-                          : tk + (size_t)2 * C * 2 * imgf + (size_t)s * (c.unknown + 1) * C * kN;
+                          : tk + (size_t)2 * C * 2 * imgf + (size_t)s * (c.unknown + 1) * tip_row_floats(C);
     bulk_g2s(sptr(Bbase + (size_t)s * C * 2 * kBImg), src, side_table_bytes(in, C, c.unknown),
              bar);
   }
@@ -327,7 +376,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      sptr(&ctl->tmem_base)),
-                 "r"(256)
+                 "r"(kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -338,7 +387,6 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
   // MMA descriptors of the first K step of category 0; the others are these plus offsets
   // (the 14-bit address field counts 16-byte units and the whole buffer is < 256 KiB)
-  const uint64_t dA0[2] = {sdesc(sptr(A[0]), kAChunk, 128), sdesc(sptr(A[1]), kAChunk, 128)};
   const uint64_t dL0[2] = {sdesc(sptr(Alo[0]), kAChunk, 128), sdesc(sptr(Alo[1]), kAChunk, 128)};
   const uint64_t dB0 = sdesc(sptr(Bbase), kNP * 16, 128);
   uint32_t ph_tma = 0, ph_mma = 0;
@@ -349,7 +397,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   DevOp cur = ops[0];
   DevOp nxt = nops > 1 ? ops[1] : cur;
   int cur_mask = tma_mask(cur, -1);
-  if (t == 0) issue_copies(c, cur, cur_mask, tab, sA0, sA1, Bbase, blockIdx.x, bar_tma);
+  if (warp == 0 && elect_one())
+    issue_copies(c, cur, cur_mask, tab, sA0, sA1, Bbase, blockIdx.x, bar_tma);
   OpIn in;
   const int zero2[2] = {0, 0};
   load_op_inputs<SAFE>(c, cur, -1, zero2, p, half, act, in);
@@ -368,25 +417,32 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     tma_pending = false;
     ph_tma ^= 1;
     if (inL || inR) {
-      // split the tiles the TMA brought: A <- hi in place, Alo <- lo
+      // split the tiles the bulk copies brought: hi -> the side's TMEM operand columns,
+      // lo -> Alo (shared memory)
       for (int s = 0; s < 2; s++) {
         if (!(cur_mask & (1 << s))) continue;
-        float4 *a4 = reinterpret_cast<float4 *>(s ? A[1] : A[0]);
+        const float4 *a4 = reinterpret_cast<const float4 *>(s ? A[1] : A[0]);
         float4 *l4 = reinterpret_cast<float4 *>(s ? Alo[1] : Alo[0]);
-        const int jend = min(half * 10 + 10, 5 * C);
-#pragma unroll 5
-        for (int j = half * 10; j < jend; j++) {
-          float4 h, l;
-          split4(a4[j * kTile + row], h, l);
-          a4[j * kTile + row] = h;
-          l4[j * kTile + row] = l;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          const int cc = 2 * half + j;
+          if (cc >= C) continue;
+          float4 h[5];
+#pragma unroll
+          for (int i = 0; i < 5; i++) {
+            float4 l;
+            split4(a4[(cc * 5 + i) * kTile + row], h[i], l);
+            l4[(cc * 5 + i) * kTile + row] = l;
+          }
+          tmem_st_row(tmem + lane_off + (uint32_t)(kAhiCol + (s * 4 + cc) * kKP), h);
         }
       }
+      tmem_st_wait();
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       tc_fence_before();
       __syncthreads();
       tc_fence_after();
-      if (t == 0) {
+      if (warp == 0 && elect_one()) {
 #pragma unroll
         for (int s = 0; s < 2; s++) {
           if (!(s ? inR : inL)) continue;
@@ -394,14 +450,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           for (int cc = 0; cc < 4; cc++) {
             if (cc >= C) break;
             const uint32_t dtm = tmem + (uint32_t)((s * C + cc) * kNP);
+            const uint32_t atm = tmem + (uint32_t)(kAhiCol + (s * 4 + cc) * kKP);
             const uint64_t bh = dB0 + (uint64_t)((((s * C + cc) * 2) * kBImg) >> 4);
             const uint64_t bl = bh + (uint64_t)(kBImg >> 4);
 #pragma unroll
             for (int ks = 0; ks < kKP / 8; ks++) {
               const uint64_t ko = (uint64_t)(((cc * 5 + 2 * ks) * kAChunk) >> 4);
               const uint64_t kb = (uint64_t)((2 * ks * kNP * 16) >> 4);
-              mma_tf32(dtm, dA0[s] + ko, bh + kb, ks > 0 ? 1u : 0u);
-              mma_tf32(dtm, dA0[s] + ko, bl + kb, 1u);
+              mma_tf32_ta(dtm, atm + 8 * ks, bh + kb, ks > 0 ? 1u : 0u);
+              mma_tf32_ta(dtm, atm + 8 * ks, bl + kb, 1u);
               mma_tf32(dtm, dL0[s] + ko, bh + kb, 1u);
             }
           }
@@ -437,7 +494,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           tmem_ld32(tmem + lane_off + (uint32_t)((s * C + cc) * kNP), m[s]);
         } else {
           const float4 *lt = reinterpret_cast<const float4 *>(
-              Bbase + (size_t)s * C * 2 * kBImg + (((size_t)in.st[s] * C + cc) * kN) * 4);
+              Bbase + (size_t)s * C * 2 * kBImg +
+              ((size_t)in.st[s] * tip_row_floats(C) + (size_t)cc * kN) * 4);
 #pragma unroll
           for (int i = 0; i < kN / 4; i++) {
             const float4 v = lt[i];
@@ -466,7 +524,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       nxt_mask = tma_mask(nxt, cur.dst_slot);
       if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) nxt_fwd = 0;
       if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) nxt_fwd = 1;
-      if (t == 0)
+      if (warp == 0 && elect_one())
         issue_copies(c, nxt, nxt_mask, tab + (size_t)(k + 1) * stride_f, sA0, sA1, Bbase,
                      blockIdx.x, bar_tma);
     }
@@ -497,7 +555,6 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     // the split rows also go into its operand buffers.
     float *dtile = static_cast<float *>(c.partials) + (size_t)cur.dst_slot * c.slot_elems +
                    (size_t)blockIdx.x * (5 * C * kAChunk / 4);
-    float *fa = nxt_fwd == 1 ? A[1] : A[0];
     float *fl = nxt_fwd == 1 ? Alo[1] : Alo[0];
     {
       uint16_t *sd = c.scale + (size_t)cur.dst_slot * c.slot_scale;
@@ -505,19 +562,19 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       for (int j = 0; j < 2; j++) {
         const int cc = 2 * half + j;
         if (cc >= C) continue;
+        float4 h[5];
 #pragma unroll
         for (int i = 0; i < kN / 4; i++) {
           const float4 v = make_float4(out[j][4 * i] * f[j], out[j][4 * i + 1] * f[j],
                                        out[j][4 * i + 2] * f[j], out[j][4 * i + 3] * f[j]);
-          float4 h, l;
-          split4(v, h, l);
+          float4 l;
+          split4(v, h[i], l);
           const int idx = (cc * 5 + i) * kTile + row;
-          reinterpret_cast<float4 *>(dtile)[idx] = join4(h, l);
-          if (nxt_fwd >= 0) {
-            reinterpret_cast<float4 *>(fa)[idx] = h;
-            reinterpret_cast<float4 *>(fl)[idx] = l;
-          }
+          reinterpret_cast<float4 *>(dtile)[idx] = join4(h[i], l);
+          if (nxt_fwd >= 0) reinterpret_cast<float4 *>(fl)[idx] = l;
         }
+        if (nxt_fwd >= 0)
+          tmem_st_row(tmem + lane_off + (uint32_t)(kAhiCol + (nxt_fwd * 4 + cc) * kKP), h);
         if (SAFE && act) sd[(size_t)p * C + cc] = (uint16_t)s_out[j];
       }
       if (!SAFE && act && half == 0) sd[p] = (uint16_t)s_out[0];
@@ -526,6 +583,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     if (has_next) load_op_inputs<SAFE>(c, nxt, nxt_fwd, s_out, p, half, act, in);
     // later ops bulk-copy this output from global memory, and the next MMA reads the forwarded
     // operands: both through the async proxy
+    if (nxt_fwd >= 0) tmem_st_wait();
     asm volatile("fence.proxy.async.global;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
@@ -542,14 +600,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
                  : "memory");
 }
 
 }  // namespace
 
 size_t tc20_op_floats(int ncat, int unknown) {
-  return (size_t)2 * ncat * 2 * (kBImg / 4) + (size_t)2 * (unknown + 1) * ncat * kN;
+  return (size_t)2 * ncat * 2 * (kBImg / 4) + (size_t)2 * (unknown + 1) * tip_row_floats(ncat);
 }
 
 bool tc20_supported(const Session *s) {
