@@ -145,27 +145,31 @@ __device__ __forceinline__ void tc_fence_after() {
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
-// 32 consecutive TMEM columns of this thread's lane
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
+// the 20 state columns of one accumulator (columns 20..31 are padding) of this thread's lane;
+// the registers are valid after tmem_ld_wait on them
+__device__ __forceinline__ void tmem_ld20(uint32_t taddr, uint32_t (&r)[20]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
-      "%30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19])
+               : "r"(taddr + 16));
 }
-// Round a finite FP32 value to TF32 (10 fraction bits), to nearest with ties away from zero:
-// adding half a TF32 ulp (bit 12) to the sign-magnitude bits and clearing the 13 low bits
-// rounds the magnitude up exactly when the dropped bits are at least half an ulp (a carry
-// into the exponent gives the next binade correctly).  Two integer operations.
+// waits for this thread's TMEM loads; the register operands make every later use of the
+// loaded values depend on the wait
+__device__ __forceinline__ void tmem_ld_wait(uint32_t (&r)[20]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19])
+               :
+               : "memory");
+}
 // the hi part of a row of one category (20 states and 4 zero columns of K padding) into its
 // 24 TMEM columns of this thread's lane
 __device__ __forceinline__ void tmem_st_row(uint32_t taddr, const float4 (&h)[5]) {
@@ -185,6 +189,10 @@ __device__ __forceinline__ void tmem_st_row(uint32_t taddr, const float4 (&h)[5]
 __device__ __forceinline__ void tmem_st_wait() {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
+// Round a finite FP32 value to TF32 (10 fraction bits), to nearest with ties away from zero:
+// adding half a TF32 ulp (bit 12) to the sign-magnitude bits and clearing the 13 low bits
+// rounds the magnitude up exactly when the dropped bits are at least half an ulp (a carry
+// into the exponent gives the next binade correctly).  Two integer operations.
 __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
@@ -253,8 +261,31 @@ __global__ void k_prep_ops_tc(DevCtx c, const DevOp *ops, float *tab, size_t str
   }
 }
 
+// MMAs of one side: for each category, D[128 x 32] = A_hi.B_hi + A_hi.B_lo + A_lo.B_hi over
+// three K steps (A_hi in TMEM, A_lo and the B images in shared memory)
+__device__ __forceinline__ void issue_side_mmas(int s, int C, uint32_t tmem, uint64_t dB0,
+                                                uint64_t dL0s) {
+#pragma unroll
+  for (int cc = 0; cc < 4; cc++) {
+    if (cc >= C) break;
+    const uint32_t dtm = tmem + (uint32_t)((s * C + cc) * kNP);
+    const uint32_t atm = tmem + (uint32_t)(kAhiCol + (s * 4 + cc) * kKP);
+    const uint64_t bh = dB0 + (uint64_t)((((s * C + cc) * 2) * kBImg) >> 4);
+    const uint64_t bl = bh + (uint64_t)(kBImg >> 4);
+#pragma unroll
+    for (int ks = 0; ks < kKP / 8; ks++) {
+      const uint64_t ko = (uint64_t)(((cc * 5 + 2 * ks) * kAChunk) >> 4);
+      const uint64_t kb = (uint64_t)((2 * ks * kNP * 16) >> 4);
+      mma_tf32_ta(dtm, atm + 8 * ks, bh + kb, ks > 0 ? 1u : 0u);
+      mma_tf32_ta(dtm, atm + 8 * ks, bl + kb, 1u);
+      mma_tf32(dtm, dL0s + ko, bh + kb, 1u);
+    }
+  }
+}
+
 struct TcShared {
-  uint64_t bar_tma;
+  uint64_t bar_tile;  // operand tiles of the next op (landing buffers)
+  uint64_t bar_tab;   // tables of the next op (B images / tip tables)
   uint64_t bar_mma;
   uint32_t tmem_base;
   float rowmax[2][kTile];
@@ -273,67 +304,81 @@ __device__ __forceinline__ uint32_t side_table_bytes(bool internal, int C, int u
   return internal ? (uint32_t)C * 2 * kBImg : (uint32_t)(unknown + 1) * tip_row_floats(C) * 4;
 }
 
-// thread 0: copies for op `nx`: TMA tiles of the children in `mask`, and for each side its
-// op table (B images of an internal child, tip table of a tip child) into that side's region
-__device__ __forceinline__ void issue_copies(const DevCtx &c, const DevOp &nx, int mask,
-                                             const float *tk, uint32_t sA0, uint32_t sA1,
-                                             unsigned char *Bbase, int tile, uint32_t bar) {
+// Copies for op `nx`, issued by one thread.  issue_tiles: the tiles of the children in `mask`
+// (one contiguous block of the tile-major slot each) into the landing buffers; it runs as soon
+// as the current op no longer reads those.  issue_tables: for each side its op table (B
+// images of an internal child, tip table of a tip child) into that side's region, once the
+// current op's MMAs and table reads are done.  Each completes its barrier once per op.
+__device__ __forceinline__ void issue_tiles(const DevCtx &c, const DevOp &nx, int mask,
+                                            uint32_t sA0, uint32_t sA1, int tile, uint32_t bar) {
+  const int C = c.C;
+  const uint32_t tb = 5 * C * kAChunk;
+  mbar_expect_tx(bar, (uint32_t)__popc(mask) * tb);
+  for (int s = 0; s < 2; s++) {
+    if (!(mask & (1 << s))) continue;
+    const float *src = static_cast<const float *>(c.partials) +
+                       (size_t)(s ? nx.r_id : nx.l_id) * c.slot_elems + (size_t)tile * (tb / 4);
+    bulk_g2s(s ? sA1 : sA0, src, tb, bar);
+  }
+}
+__device__ __forceinline__ void issue_tables(const DevCtx &c, const DevOp &nx, const float *tk,
+                                             unsigned char *Bbase, uint32_t bar) {
   const int C = c.C;
   const size_t imgf = kBImg / 4;
   uint32_t bytes = 0;
-  for (int s = 0; s < 2; s++) {
-    const bool in = (s ? nx.r_kind : nx.l_kind) == GEMS_CHILD_PARTIAL;
-    if (mask & (1 << s)) bytes += 5 * C * kAChunk;
-    bytes += side_table_bytes(in, C, c.unknown);
-  }
+  for (int s = 0; s < 2; s++)
+    bytes += side_table_bytes((s ? nx.r_kind : nx.l_kind) == GEMS_CHILD_PARTIAL, C, c.unknown);
   mbar_expect_tx(bar, bytes);
   for (int s = 0; s < 2; s++) {
     const bool in = (s ? nx.r_kind : nx.l_kind) == GEMS_CHILD_PARTIAL;
-    if (mask & (1 << s)) {  // the child's tile: one contiguous block of the tile-major slot
-      const float *src = static_cast<const float *>(c.partials) +
-                         (size_t)(s ? nx.r_id : nx.l_id) * c.slot_elems +
-                         (size_t)tile * (5 * C * kAChunk / 4);
-      bulk_g2s(s ? sA1 : sA0, src, 5 * C * kAChunk, bar);
-    }
     const float *src = in ? tk + (size_t)s * C * 2 * imgf
-                          : tk + (size_t)2 * C * 2 * imgf + (size_t)s * (c.unknown + 1) * tip_row_floats(C);
+                          : tk + (size_t)2 * C * 2 * imgf +
+                                (size_t)s * (c.unknown + 1) * tip_row_floats(C);
     bulk_g2s(sptr(Bbase + (size_t)s * C * 2 * kBImg), src, side_table_bytes(in, C, c.unknown),
              bar);
   }
 }
 
 // what a thread loads for an op before its products are ready: tip bytes and the counters of
-// internal children (a forwarded child's counters come from the previous op's registers)
+// internal children (a forwarded child's counters come from the previous op's registers).
+// Plain named scalars, so that everything stays in registers and the loads stay in flight
+// until their first use a whole op later.
+struct SideIn {
+  int st;        // tip state code (tip child)
+  int sc0, sc1;  // counters of this thread's two categories (internal child)
+};
 struct OpIn {
-  int st[2];
-  int sc[2][2];  // [side][category of this thread]
+  SideIn L, R;
 };
 
 template <bool SAFE>
-__device__ __forceinline__ void load_op_inputs(const DevCtx &c, const DevOp &op, int fwd_side,
-                                               const int (&fwd_s)[2], long p, int half,
-                                               bool act, OpIn &in) {
-  const int C = c.C;
-  for (int s = 0; s < 2; s++) {
-    in.st[s] = 0;
-    in.sc[s][0] = in.sc[s][1] = 0;
-    if (!act) continue;
-    const int kind = s ? op.r_kind : op.l_kind, id = s ? op.r_id : op.l_id;
-    if (kind == GEMS_CHILD_TIP) {
-      in.st[s] = c.tips[(size_t)id * c.P + p];
-    } else if (s == fwd_side) {
-      in.sc[s][0] = fwd_s[0];
-      in.sc[s][1] = fwd_s[1];
+__device__ __forceinline__ SideIn load_side(const DevCtx &c, int kind, int id, bool fwd,
+                                            int fs0, int fs1, long p, int half, bool act) {
+  SideIn r{0, 0, 0};
+  if (!act) return r;
+  if (kind == GEMS_CHILD_TIP) {
+    r.st = c.tips[(size_t)id * c.P + p];
+  } else if (fwd) {
+    r.sc0 = fs0;
+    r.sc1 = fs1;
+  } else {
+    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+    if (SAFE) {
+      if (2 * half < c.C) r.sc0 = sc[(size_t)p * c.C + 2 * half];
+      if (2 * half + 1 < c.C) r.sc1 = sc[(size_t)p * c.C + 2 * half + 1];
     } else {
-      const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
-      if (SAFE) {
-        for (int j = 0; j < 2; j++)
-          if (2 * half + j < C) in.sc[s][j] = sc[(size_t)p * C + 2 * half + j];
-      } else {
-        in.sc[s][0] = in.sc[s][1] = sc[p];
-      }
+      r.sc0 = r.sc1 = sc[p];
     }
   }
+  return r;
+}
+
+template <bool SAFE>
+__device__ __forceinline__ void load_op_inputs(const DevCtx &c, const DevOp &op, int fwd_side,
+                                               int fs0, int fs1, long p, int half, bool act,
+                                               OpIn &in) {
+  in.L = load_side<SAFE>(c, op.l_kind, op.l_id, fwd_side == 0, fs0, fs1, p, half, act);
+  in.R = load_side<SAFE>(c, op.r_kind, op.r_id, fwd_side == 1, fs0, fs1, p, half, act);
 }
 
 template <bool SAFE>
@@ -357,10 +402,12 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   const int p0 = blockIdx.x * kTile;
   const long p = p0 + row;
   const bool act = p < c.P;
-  const uint32_t bar_tma = sptr(&ctl->bar_tma), bar_mma = sptr(&ctl->bar_mma);
+  const uint32_t bar_tile = sptr(&ctl->bar_tile), bar_tab = sptr(&ctl->bar_tab);
+  const uint32_t bar_mma = sptr(&ctl->bar_mma);
 
   if (t == 0) {
-    mbar_init(bar_tma, 1);
+    mbar_init(bar_tile, 1);
+    mbar_init(bar_tab, 1);
     mbar_init(bar_mma, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -389,82 +436,90 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   // (the 14-bit address field counts 16-byte units and the whole buffer is < 256 KiB)
   const uint64_t dL0[2] = {sdesc(sptr(Alo[0]), kAChunk, 128), sdesc(sptr(Alo[1]), kAChunk, 128)};
   const uint64_t dB0 = sdesc(sptr(Bbase), kNP * 16, 128);
-  uint32_t ph_tma = 0, ph_mma = 0;
-  bool ok = true, tma_pending = false, mma_pending = false;
+  uint32_t ph_tile = 0, ph_tab = 0, ph_mma = 0;
+  bool ok = true, tile_pending = false, tab_pending = false, mma_pending = false;
   const uint32_t sA0 = sptr(A[0]), sA1 = sptr(A[1]);
   const bool inv0 = act ? c.invar[p] == 0.0 : false;
 
   DevOp cur = ops[0];
   DevOp nxt = nops > 1 ? ops[1] : cur;
   int cur_mask = tma_mask(cur, -1);
-  if (warp == 0 && elect_one())
-    issue_copies(c, cur, cur_mask, tab, sA0, sA1, Bbase, blockIdx.x, bar_tma);
+  if (warp == 0 && elect_one()) {
+    issue_tiles(c, cur, cur_mask, sA0, sA1, blockIdx.x, bar_tile);
+    issue_tables(c, cur, tab, Bbase, bar_tab);
+  }
+  tile_pending = tab_pending = true;
   OpIn in;
-  const int zero2[2] = {0, 0};
-  load_op_inputs<SAFE>(c, cur, -1, zero2, p, half, act, in);
+  load_op_inputs<SAFE>(c, cur, -1, 0, 0, p, half, act, in);
 
   for (int k = 0; k < nops && ok; k++) {
     const bool inL = cur.l_kind == GEMS_CHILD_PARTIAL, inR = cur.r_kind == GEMS_CHILD_PARTIAL;
     const bool has_next = k + 1 < nops;
     // the op after next: its descriptor is needed one op from now
     const DevOp nxt2 = (k + 2 < nops) ? ops[k + 2] : nxt;
-    tma_pending = true;
-    if (__syncthreads_or(!mbar_wait(bar_tma, ph_tma))) {
+    if (__syncthreads_or(!mbar_wait(bar_tile, ph_tile) || !mbar_wait(bar_tab, ph_tab))) {
       ok = false;
       if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
       break;
     }
-    tma_pending = false;
-    ph_tma ^= 1;
+    tile_pending = tab_pending = false;
+    ph_tile ^= 1;
+    ph_tab ^= 1;
+    // the next op's children: the one this op produces is forwarded, the others are copied
+    int nxt_mask = 0, nxt_fwd = -1;
+    if (has_next) {
+      nxt_mask = tma_mask(nxt, cur.dst_slot);
+      if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) nxt_fwd = 0;
+      if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) nxt_fwd = 1;
+    }
     if (inL || inR) {
-      // split the tiles the bulk copies brought: hi -> the side's TMEM operand columns,
-      // lo -> Alo (shared memory)
-      for (int s = 0; s < 2; s++) {
-        if (!(cur_mask & (1 << s))) continue;
-        const float4 *a4 = reinterpret_cast<const float4 *>(s ? A[1] : A[0]);
-        float4 *l4 = reinterpret_cast<float4 *>(s ? Alo[1] : Alo[0]);
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-          const int cc = 2 * half + j;
-          if (cc >= C) continue;
-          float4 h[5];
-#pragma unroll
-          for (int i = 0; i < 5; i++) {
-            float4 l;
-            split4(a4[(cc * 5 + i) * kTile + row], h[i], l);
-            l4[(cc * 5 + i) * kTile + row] = l;
-          }
-          tmem_st_row(tmem + lane_off + (uint32_t)(kAhiCol + (s * 4 + cc) * kKP), h);
-        }
-      }
-      tmem_st_wait();
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
+      // The forwarded child's operands are already in place (written by the previous op's
+      // epilogue): its MMAs go first and run while the loaded child is split.
+      const int fwd_side = (inL && !(cur_mask & 1)) ? 0 : ((inR && !(cur_mask & 2)) ? 1 : -1);
       if (warp == 0 && elect_one()) {
-#pragma unroll
+        if (fwd_side >= 0) issue_side_mmas(fwd_side, C, tmem, dB0, fwd_side ? dL0[1] : dL0[0]);
+        if (cur_mask == 0) {
+          mma_commit(bar_mma);
+          // nothing to split: the landing buffers are free for the next op's tiles
+          if (has_next) issue_tiles(c, nxt, nxt_mask, sA0, sA1, blockIdx.x, bar_tile);
+        }
+      }
+      if (cur_mask) {
+        // split the tiles the bulk copies brought: hi -> the side's TMEM operand columns,
+        // lo -> Alo (shared memory)
         for (int s = 0; s < 2; s++) {
-          if (!(s ? inR : inL)) continue;
+          if (!(cur_mask & (1 << s))) continue;
+          const float4 *a4 = reinterpret_cast<const float4 *>(s ? A[1] : A[0]);
+          float4 *l4 = reinterpret_cast<float4 *>(s ? Alo[1] : Alo[0]);
 #pragma unroll
-          for (int cc = 0; cc < 4; cc++) {
-            if (cc >= C) break;
-            const uint32_t dtm = tmem + (uint32_t)((s * C + cc) * kNP);
-            const uint32_t atm = tmem + (uint32_t)(kAhiCol + (s * 4 + cc) * kKP);
-            const uint64_t bh = dB0 + (uint64_t)((((s * C + cc) * 2) * kBImg) >> 4);
-            const uint64_t bl = bh + (uint64_t)(kBImg >> 4);
+          for (int j = 0; j < 2; j++) {
+            const int cc = 2 * half + j;
+            if (cc >= C) continue;
+            float4 h[5];
 #pragma unroll
-            for (int ks = 0; ks < kKP / 8; ks++) {
-              const uint64_t ko = (uint64_t)(((cc * 5 + 2 * ks) * kAChunk) >> 4);
-              const uint64_t kb = (uint64_t)((2 * ks * kNP * 16) >> 4);
-              mma_tf32_ta(dtm, atm + 8 * ks, bh + kb, ks > 0 ? 1u : 0u);
-              mma_tf32_ta(dtm, atm + 8 * ks, bl + kb, 1u);
-              mma_tf32(dtm, dL0[s] + ko, bh + kb, 1u);
+            for (int i = 0; i < 5; i++) {
+              float4 l;
+              split4(a4[(cc * 5 + i) * kTile + row], h[i], l);
+              l4[(cc * 5 + i) * kTile + row] = l;
             }
+            tmem_st_row(tmem + lane_off + (uint32_t)(kAhiCol + (s * 4 + cc) * kKP), h);
           }
         }
-        mma_commit(bar_mma);
+        tmem_st_wait();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        // the same elected lane (the lowest) commits every MMA of this op
+        if (warp == 0 && elect_one()) {
+          if (cur_mask & 1) issue_side_mmas(0, C, tmem, dB0, dL0[0]);
+          if (cur_mask & 2) issue_side_mmas(1, C, tmem, dB0, dL0[1]);
+          mma_commit(bar_mma);
+          // the split has read the landing buffers: the next op's tiles can come in
+          if (has_next) issue_tiles(c, nxt, nxt_mask, sA0, sA1, blockIdx.x, bar_tile);
+        }
       }
+      tile_pending = has_next;
       mma_pending = true;
       if (__syncthreads_or(!mbar_wait(bar_mma, ph_mma))) {
         ok = false;
@@ -474,6 +529,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       mma_pending = false;
       ph_mma ^= 1;
       tc_fence_after();
+    } else {
+      if (has_next && warp == 0 && elect_one())
+        issue_tiles(c, nxt, nxt_mask, sA0, sA1, blockIdx.x, bar_tile);
+      tile_pending = has_next;
     }
     // ---- epilogue, part 1: messages and products into registers (the tip tables of this op
     // are in the side regions of shared memory; read them before the next copies land)
@@ -487,15 +546,22 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         for (int x = 0; x < kN; x++) out[j][x] = 0.f;
         continue;
       }
-      float m[2][32];
+      float m[2][kN];
+      // both sides' accumulator loads in flight together, then the wait
+      uint32_t r[2][20];
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+        if (s ? inR : inL) tmem_ld20(tmem + lane_off + (uint32_t)((s * C + cc) * kNP), r[s]);
 #pragma unroll
       for (int s = 0; s < 2; s++) {
         if (s ? inR : inL) {
-          tmem_ld32(tmem + lane_off + (uint32_t)((s * C + cc) * kNP), m[s]);
+          tmem_ld_wait(r[s]);
+#pragma unroll
+          for (int x = 0; x < kN; x++) m[s][x] = __uint_as_float(r[s][x]);
         } else {
           const float4 *lt = reinterpret_cast<const float4 *>(
               Bbase + (size_t)s * C * 2 * kBImg +
-              ((size_t)in.st[s] * tip_row_floats(C) + (size_t)cc * kN) * 4);
+              ((size_t)(s ? in.R.st : in.L.st) * tip_row_floats(C) + (size_t)cc * kN) * 4);
 #pragma unroll
           for (int i = 0; i < kN / 4; i++) {
             const float4 v = lt[i];
@@ -518,23 +584,22 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     tc_fence_before();
     __syncthreads();  // operand buffers, tables and TMEM of this op are no longer read
     tc_fence_after();
-    // start the next op's copies under the rest of this epilogue
-    int nxt_mask = 0, nxt_fwd = -1;
+    // the tables of this op are no longer read: the next op's tables come in under the rest
+    // of this epilogue
     if (has_next) {
-      nxt_mask = tma_mask(nxt, cur.dst_slot);
-      if (nxt.l_kind == GEMS_CHILD_PARTIAL && nxt.l_id == cur.dst_slot) nxt_fwd = 0;
-      if (nxt.r_kind == GEMS_CHILD_PARTIAL && nxt.r_id == cur.dst_slot) nxt_fwd = 1;
       if (warp == 0 && elect_one())
-        issue_copies(c, nxt, nxt_mask, tab + (size_t)(k + 1) * stride_f, sA0, sA1, Bbase,
-                     blockIdx.x, bar_tma);
+        issue_tables(c, nxt, tab + (size_t)(k + 1) * stride_f, Bbase, bar_tab);
+      tab_pending = true;
     }
     // ---- epilogue, part 2: rescaling, counters, stores, forwarding
     float f[2] = {1.f, 1.f};
     int s_out[2];
     if (SAFE) {
+      s_out[0] = in.L.sc0 + in.R.sc0;
+      s_out[1] = in.L.sc1 + in.R.sc1;
+#pragma unroll
       for (int j = 0; j < 2; j++) {
         const int cc = 2 * half + j;
-        s_out[j] = in.sc[0][j] + in.sc[1][j];
         if (cc < C && !tiptip && mx[j] < kScaleThrF && inv0) {
           f[j] = 18446744073709551616.0f;  // 2^64
           s_out[j] += 1;
@@ -542,7 +607,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       }
     } else {
       const float m = fmaxf(ctl->rowmax[0][row], ctl->rowmax[1][row]);
-      s_out[0] = in.sc[0][0] + in.sc[1][0];
+      s_out[0] = in.L.sc0 + in.R.sc0;
       if (!tiptip && m < kScaleThrF && inv0) {
         f[0] = f[1] = 18446744073709551616.0f;  // 2^64
         s_out[0] += 1;
@@ -580,7 +645,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       if (!SAFE && act && half == 0) sd[p] = (uint16_t)s_out[0];
     }
     // next op's tip bytes and counters (a forwarded child's counters are this op's s_out)
-    if (has_next) load_op_inputs<SAFE>(c, nxt, nxt_fwd, s_out, p, half, act, in);
+    if (has_next) load_op_inputs<SAFE>(c, nxt, nxt_fwd, s_out[0], s_out[1], p, half, act, in);
     // later ops bulk-copy this output from global memory, and the next MMA reads the forwarded
     // operands: both through the async proxy
     if (nxt_fwd >= 0) tmem_st_wait();
@@ -594,7 +659,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     cur_mask = nxt_mask;
   }
   if (!ok && t == 0) {
-    if (tma_pending) mbar_wait(bar_tma, ph_tma);
+    if (tile_pending) mbar_wait(bar_tile, ph_tile);
+    if (tab_pending) mbar_wait(bar_tab, ph_tab);
     if (mma_pending) mbar_wait(bar_mma, ph_mma);
   }
   tc_fence_before();
