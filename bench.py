@@ -312,13 +312,19 @@ def time_newton(gt, tree, stream, nbranch=24):
             "derivative_evals_per_branch": nev / len(br)}
 
 
-def protein_comparison(args, local):
-    """20-state +G4: FP64 vs mixed (tcgen05 split-TF32) and mixed on CUDA cores."""
+def protein_comparison(args, local, peaks):
+    """20-state +G4: FP64 vs mixed (tcgen05 split-TF32) and mixed on CUDA cores, each with its
+    HBM roofline (algorithmic bytes) and compute roofline (algorithmic flops 6Cn^2 + Cn per
+    update, credited alike to every form, against the measured peak of the unit it runs on)."""
     import torch
     from gems_b200 import PhyloTree
     tree, model, aln = make_workload(0, 100_000, "protein128")
     out = {"workload": CONFIGS["protein128"].format(sites="100,000"), "npat": aln.npat}
-    nops = sum(op_kinds(tree))
+    kinds = op_kinds(tree)
+    nops = sum(kinds)
+    hbm_peak, _, peak_src = read_peaks()
+    n, C = model.nstates, model.ncat
+    flops = aln.npat * nops * update_flops(n, C)
     lnl_buf = torch.zeros(1, dtype=torch.float64, device=f"cuda:{local}")
     res = {}
     for name, prec, tc in (("fp64", "fp64", True), ("mixed_tcgen05", "mixed", True),
@@ -327,8 +333,24 @@ def protein_comparison(args, local):
         gt.session.set_tensor_cores(tc)
         stream = torch.cuda.ExternalStream(gt.session.stream_handle(), device=local)
         ms, lnl, kms, _ = time_lnl(gt, max(args.steps, 5), 3, stream, None, lnl_buf)
+        b_ii, b_ti, b_tt = update_bytes(8 if prec == "fp64" else 4, n, C)
+        alg = aln.npat * (kinds[0] * b_ii + kinds[1] * b_ti + kinds[2] * b_tt)
+        unit, pk = {"fp64": ("fp64 FMA", peaks["fp64_tflops"]),
+                    "mixed_tcgen05": ("tcgen05 TF32 (3 products issued per credited one)",
+                                      peaks["tf32_tflops"]),
+                    "mixed_cuda_cores": ("fp32 FMA", peaks["fp32_tflops"])}[name]
         res[name] = {"ms_per_step": ms, "traverse_ms": kms,
-                     "site_partial_updates_per_s": nops * aln.npat / (ms * 1e-3), "lnl": lnl}
+                     "site_partial_updates_per_s": nops * aln.npat / (ms * 1e-3),
+                     "lnl_evals_per_s": 1e3 / ms, "lnl": lnl,
+                     "roofline": {"bound": "hbm", "achieved": alg / (kms * 1e-3) / 1e9,
+                                  "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s",
+                                  "frac": alg / (kms * 1e-3) / 1e9 / hbm_peak,
+                                  "algorithmic_bytes_per_launch": alg,
+                                  "traffic": read_traffic("traverse_mixed_protein128.md")
+                                  if name == "mixed_tcgen05" else None},
+                     "compute": {"unit_used": unit, "achieved_tflops": flops / (kms * 1e-3) / 1e12,
+                                 "peak_tflops": pk, "frac": flops / (kms * 1e-3) / 1e12 / pk,
+                                 "algorithmic_flops_per_launch": flops}}
         gt.close()
         gt.session.close()
     base = res["fp64"]
@@ -336,6 +358,56 @@ def protein_comparison(args, local):
         res[k]["speedup_vs_fp64"] = base["ms_per_step"] / res[k]["ms_per_step"]
         res[k]["lnl_rel_err_vs_fp64"] = abs(res[k]["lnl"] - base["lnl"]) / abs(base["lnl"])
     out.update(res)
+    return out
+
+
+def rell_block(gt, aln, stream, R=256, reps=5):
+    """UFBoot RELL on the resident pattern log-likelihoods: R multinomial reweightings
+    (seeded) of the pattern counts, replicate lnL and derivative sums in one launch each."""
+    import torch
+    s = gt.session
+    # multinomial resampling of the sites (as UFBoot draws them), counted per pattern
+    rng = np.random.default_rng(11)
+    site_ptn = np.repeat(np.arange(aln.npat), aln.weights.astype(np.int64))
+    nsites = len(site_ptn)
+    W = np.empty((R, aln.npat), np.float32)
+    for r in range(R):
+        W[r] = np.bincount(site_ptn[rng.integers(nsites, size=nsites)], minlength=aln.npat)
+    s.upload_reweightings(W)
+    _, plh = gt.computeLikelihood(pattern_lh=True)
+    ref = W.astype(np.float64) @ plh
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    got = s.reweighted_lnl()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        got = s.reweighted_lnl()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    hbm_peak, _, _ = read_peaks()
+    byts = R * aln.npat * 4 + aln.npat * 8
+    return {"replicates": R, "npat": aln.npat, "ms_per_call": ms,
+            "replicate_lnl_evals_per_s": R / (ms * 1e-3),
+            "max_rel_err_vs_fp64_dot": float(np.max(np.abs(got - ref) / np.abs(ref))),
+            "roofline": {"bound": "hbm", "achieved": byts / (ms * 1e-3) / 1e9, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": byts / (ms * 1e-3) / 1e9 / hbm_peak}}
+
+
+def serving_block(local, nsess=48, nreq=800, rate=250.0):
+    """The serving loop on a seeded stream: sessions of 8-256 taxa and 500-50,000 sites
+    (log-uniform), 4/20/61 states, 1/4/8 categories, FP64/mixed; NNI + 5-branch Newton + lnL
+    per request; Poisson arrivals at `rate` requests/s."""
+    from gems_b200 import serve
+    specs, reqs = serve.make_stream(nsess, nreq, rate, seed=5, taxa=(8, 256), sites=(500, 50_000))
+    cases = {sp.sid: serve.build_case(sp) for sp in specs}
+    srv = serve.Server(device=local, workers=16)
+    records, wall = srv.run(specs, cases, reqs)
+    out = serve.summarize(records, wall, specs, cases)
+    out.update({"sessions": nsess, "offered_rate_req_s": rate, "workers": 16,
+                "stream": "seeded; taxa 8-256, sites 500-50,000 (log-uniform), states {4,20,61}, "
+                          "categories {1,4,8}, fp64/mixed; request = NNI + Newton on the 5 "
+                          "branches around it + lnL"})
     return out
 
 
@@ -369,6 +441,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    from gems_b200 import measure_peaks
+    peaks = measure_peaks(local)
     tree, model, aln = make_workload(rank, args.sites, args.config)
     kinds = op_kinds(tree)
     nops = sum(kinds)
@@ -447,6 +521,7 @@ def main():
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
+    rell = rell_block(gt, aln, stream) if (rank == 0 and not args.no_extras) else None
     gt.close()
     s.close()
 
@@ -465,9 +540,13 @@ def main():
         "roofline": H["roofline"],
         "forms": forms,
         "clocks": clk.summary(),
+        "peaks_measured": peaks,
     }
+    if rell is not None:
+        line["rell"] = rell
     if rank == 0 and not args.no_extras and args.config == "dna512":
-        line["protein20"] = protein_comparison(args, local)
+        line["protein20"] = protein_comparison(args, local, peaks)
+        line["serving"] = serving_block(local)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tree, model, aln)
     if rank == 0:

@@ -66,6 +66,14 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def measure_peaks(device=0):
+    """Measured FP64 / FP32 FMA and dense TF32 tensor-core peaks of a device (TFLOP/s)."""
+    lib = _lib.gems()
+    a, b, c = c_double(), c_double(), c_double()
+    _check(lib.gems_measure_peaks(device, byref(a), byref(b), byref(c)), "gems_measure_peaks")
+    return {"fp64_tflops": a.value, "fp32_tflops": b.value, "tf32_tflops": c.value}
+
+
 class Session:
     """A device session: tips, pattern weights, model and partial slots resident in HBM."""
 

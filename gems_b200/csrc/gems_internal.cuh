@@ -93,6 +93,7 @@ struct Session {
   size_t op_stride = 0;  // doubles per op in opmats
   cudaStream_t stream = nullptr;
   bool model_set = false;
+  bool tips_ok = true;  // false after a rejected tip upload
   bool theta_valid = false;
   gems_branch theta_branch{};
   long long launches = 0;

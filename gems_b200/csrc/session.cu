@@ -238,6 +238,10 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
     set_error("model not set");
     return GEMS_ERR_STATE;
   }
+  if (!s->tips_ok) {
+    set_error("tip states invalid (last upload was rejected)");
+    return GEMS_ERR_STATE;
+  }
   int st = upload_ops(s, ops, nops);
   if (st) return st;
   if (tc20_supported(s)) {
@@ -419,21 +423,47 @@ int gems_session_stream(gems_session *s, void **stream) {
   return GEMS_OK;
 }
 
+// largest state byte of the uploaded tips (rows of P bytes, the first nptn of each valid)
+__global__ void k_tips_max(const uint8_t *__restrict__ tips, int P, int nptn, int ntaxa,
+                           unsigned int *out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;  // 4-byte word of a row
+  unsigned int m = 0;
+  for (int row = blockIdx.y; row < ntaxa; row += gridDim.y) {
+    if (4 * q < nptn) {
+      const uint32_t w = reinterpret_cast<const uint32_t *>(tips + (size_t)row * P)[q];
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+        if (4 * q + b < nptn) m = max(m, (w >> (8 * b)) & 0xFFu);
+    }
+  }
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 int gems_upload_tips(gems_session *s, const uint8_t *states) {
   if (!s || !states) return GEMS_ERR_BAD_ARG;
   GEMS_CUDA(cudaSetDevice(s->desc.device));
-  const int unk = s->unknown;
-  uint8_t mx = 0;
-  const size_t total = (size_t)s->desc.ntaxa * s->desc.nptn;
-  for (size_t i = 0; i < total; i++) mx = states[i] > mx ? states[i] : mx;
-  if (mx > unk) {
+  // the bytes are checked on the device after the copy: on a bad byte the tips of the session
+  // are invalid (traversals are refused) until the next successful upload
+  unsigned int *d_max = reinterpret_cast<unsigned int *>(s->d_flag) + 8;
+  GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), s->stream));
+  GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips, s->P, states, s->desc.nptn, s->desc.nptn,
+                              s->desc.ntaxa, cudaMemcpyHostToDevice, s->stream));
+  const int words = (s->desc.nptn + 3) / 4;
+  const dim3 grid((words + 255) / 256, s->desc.ntaxa < 65535 ? s->desc.ntaxa : 65535);
+  k_tips_max<<<grid, 256, 0, s->stream>>>(s->d_tips, s->P, s->desc.nptn, s->desc.ntaxa, d_max);
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  unsigned int mx = 0;
+  GEMS_CUDA(cudaMemcpyAsync(&mx, d_max, sizeof(mx), cudaMemcpyDeviceToHost, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  s->theta_valid = false;
+  if ((int)mx > s->unknown) {
+    s->tips_ok = false;
     set_error("tip state byte out of range");
     return GEMS_ERR_BAD_ARG;
   }
-  GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips, s->P, states, s->desc.nptn, s->desc.nptn,
-                              s->desc.ntaxa, cudaMemcpyHostToDevice, s->stream));
-  GEMS_CUDA(cudaStreamSynchronize(s->stream));
-  s->theta_valid = false;
+  s->tips_ok = true;
   return GEMS_OK;
 }
 

@@ -196,6 +196,10 @@ int gems_launch_count(gems_session *s, long long *count);
  * summed device time in ms and the number of timed launches, then resets the counters. */
 int gems_profile_enable(gems_session *s, int on);
 int gems_profile_read(gems_session *s, int kernel_id, double *total_ms, long long *launches);
+/* Measured compute peaks of a device (no counterpart in the reference: the denominators of the
+ * compute rooflines): FP64 and FP32 FMA throughput of the CUDA cores and the dense TF32 rate of
+ * the tcgen05 tensor cores, in TFLOP/s.  Takes a few tens of milliseconds. */
+int gems_measure_peaks(int device, double *fp64_tflops, double *fp32_tflops, double *tf32_tflops);
 
 /* ---- tree mirror (PhyloTree calls on the path) ---- */
 typedef struct gems_tree gems_tree;

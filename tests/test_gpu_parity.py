@@ -175,6 +175,11 @@ def test_kernel_set_errors(gpu):
     with pytest.raises(GemsError) as e:
         s.upload_tips(np.full((5, 10), 99, np.uint8))  # state byte out of range
     assert e.value.status == 5
+    with pytest.raises(GemsError) as e:  # tips are invalid until the next good upload
+        s.traverse([(0, 0, 1, 0, 2, 0.1, 0.1)])
+    assert e.value.status == 7
+    s.upload_tips(np.zeros((5, 10), np.uint8))
+    s.traverse([(0, 0, 1, 0, 2, 0.1, 0.1)])
 
 
 # ---- mixed-precision form: FP32 real-space partials, FP64 theta / reductions / Newton ----
