@@ -74,6 +74,56 @@ def measure_peaks(device=0):
     return {"fp64_tflops": a.value, "fp32_tflops": b.value, "tf32_tflops": c.value}
 
 
+def full_traversal(tree):
+    """Ops of a from-scratch traversal with one slot per internal node (slot = node - ntaxa),
+    rooted at the branch between leaf 0 and its neighbour, and that branch: (ops, branch)."""
+    nt = tree.ntaxa
+    adj = {}
+    for u, v, ln in zip(tree.eu, tree.ev, tree.length):
+        adj.setdefault(int(u), []).append((int(v), float(ln)))
+        adj.setdefault(int(v), []).append((int(u), float(ln)))
+    root, rlen = adj[0][0]
+    ops = []
+    stack = [(root, 0, False)]
+    while stack:
+        x, dad, done = stack.pop()
+        kids = [(y, ln) for y, ln in adj[x] if y != dad]
+        if not done:
+            stack.append((x, dad, True))
+            stack.extend((y, x, False) for y, _ in kids if y >= nt)
+            continue
+        (a, la), (b, lb) = kids
+        kind = lambda y: (GEMS_CHILD_TIP, y) if y < nt else (GEMS_CHILD_PARTIAL, y - nt)
+        (ka, ia), (kb, ib) = kind(a), kind(b)
+        ops.append((x - nt, ka, ia, kb, ib, la, lb))
+    return ops, branch_struct(root - nt, GEMS_CHILD_TIP, 0, rlen)
+
+
+def _session_array(sessions):
+    arr = (c_void_p * len(sessions))()
+    for i, s in enumerate(sessions):
+        arr[i] = s.handle.value
+    return arr
+
+
+def traverse_batch(sessions, ops):
+    """One batched traversal over sessions that share the tree (gems_traverse_batch)."""
+    arr, n = op_array(ops)
+    lib = sessions[0].lib
+    _check(lib.gems_traverse_batch(_session_array(sessions), len(sessions), arr, n),
+           "gems_traverse_batch")
+
+
+def branch_lnl_batch(sessions, ops, br):
+    """Batched traversal, then each session's branch lnL (gems_branch_lnl_batch)."""
+    arr, n = op_array(ops)
+    lib = sessions[0].lib
+    out = np.zeros(len(sessions))
+    _check(lib.gems_branch_lnl_batch(_session_array(sessions), len(sessions), arr, n, byref(br),
+                                     _dptr(out)), "gems_branch_lnl_batch")
+    return out
+
+
 class Session:
     """A device session: tips, pattern weights, model and partial slots resident in HBM."""
 

@@ -62,26 +62,41 @@ struct DevCtx {
   size_t slot_scale;       // P * (safe ? C : 1)
 };
 
-// Layout of FP32 partials.  The 20-state mixed form stores each slot tile-major:
-//   [tile of 128 patterns][chunk = category * 5 + state / 4][128 rows][4 states]
-// which is the tensor-core operand layout (one contiguous 40 KB block per tile and slot, so a
-// tile moves with one bulk copy, and a warp's 32 rows of one chunk are 512 contiguous bytes).
-// Every other form is pattern-major [P][C][n].  mix_off<N>: offset of state 0 of category cc
-// of pattern p within a slot of N-state FP32 partials; mix_cs<N>: floats between consecutive
-// 4-state chunks of that row.
+// Layout of FP32 partials.  The 20- and 61-state mixed forms store each slot tile-major:
+//   [tile of 128 patterns][chunk = category * K + state / 4][128 rows][4 states]
+// with K = 5 (20 states) or 16 (61 states padded to 64, the pad stored as zeros).  This is
+// the tensor-core operand layout: one contiguous block per (tile, slot) -- or per (tile, slot,
+// category) for 61 states -- so a tile moves with one bulk copy, and a warp's 32 rows of one
+// chunk are 512 contiguous bytes.  The 4-state form is pattern-major [P][C][n].
+// mix_off<N>: offset of state 0 of category cc of pattern p within a slot; mix_cs<N>: floats
+// between consecutive 4-state chunks of that row; mix_k<N>: chunks per category (0: not tiled).
 constexpr int kMixTile = 128;
 template <int N>
+__host__ __device__ constexpr int mix_k() {
+  return N == 20 ? 5 : (N == 61 ? 16 : 0);
+}
+template <int N>
 __host__ __device__ inline size_t mix_off(const DevCtx &c, long p, int cc) {
-  if constexpr (N == 20)
-    return (size_t)(p / kMixTile) * ((size_t)c.C * 5 * kMixTile * 4) +
-           (size_t)cc * 5 * kMixTile * 4 + (size_t)(p % kMixTile) * 4;
-  else
+  if constexpr (mix_k<N>() > 0) {
+    constexpr int K = mix_k<N>();
+    return (size_t)(p / kMixTile) * ((size_t)c.C * K * kMixTile * 4) +
+           (size_t)cc * K * kMixTile * 4 + (size_t)(p % kMixTile) * 4;
+  } else {
     return (size_t)p * c.block + (size_t)cc * N;
+  }
 }
 template <int N>
 __host__ __device__ constexpr int mix_cs() {
-  return N == 20 ? kMixTile * 4 : 4;
+  return mix_k<N>() > 0 ? kMixTile * 4 : 4;
 }
+
+// one session of a batched tensor-core launch (sessions that share the op list: the same tree
+// and lengths, e.g. candidate models on one alignment)
+struct TcJob {
+  DevCtx c;
+  const DevOp *ops;
+  const float *tab;
+};
 
 struct Session {
   gems_session_desc desc;
@@ -116,6 +131,10 @@ struct Session {
   double *d_result = nullptr;  // final scalars
   int *d_flag = nullptr;       // device status flags (barrier timeouts)
   unsigned int *d_bar = nullptr;  // grid barrier counters
+  // batched launches led by this session: job table (device and pinned host copies)
+  static constexpr int kMaxBatch = 128;
+  TcJob *d_jobs = nullptr;
+  TcJob *h_jobs = nullptr;
   // pinned host staging
   DevOp *h_ops = nullptr;
   double *h_result = nullptr;
@@ -124,7 +143,7 @@ struct Session {
   // tensor-core path (20 states, mixed): per-op table stride in floats
   bool tc_enabled = true;
   size_t op_stride_tc = 0;
-  // FP32 partials stored tile-major (20-state mixed form); elements per slot
+  // FP32 partials stored tile-major (20- and 61-state mixed forms); elements per slot
   bool tiled = false;
   size_t slot_elems = 0;
   // kernel timing (gems_profile_*): event pairs recorded around launches
@@ -181,6 +200,12 @@ size_t tc20_op_floats(int ncat, int unknown);
 bool tc20_supported(const Session *s);
 int launch_prep_ops_tc20(Session *s, int nops);
 int launch_traverse_tc20(Session *s, int nops);
+// tcgen05 split-TF32 traversal for 61 states, SAFE (kernels_tc61.cu)
+size_t tc61_op_floats(int ncat);
+bool tc61_supported(const Session *s);
+int launch_prep_ops_tc61(Session *s, int nops);
+int launch_traverse_tc61(Session *s, int nops);
+int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops);
 // bootstrap reweighting (kernels_rell.cu)
 int launch_rell_lnl(Session *s, double *d_out);
 int launch_rell_derv(Session *s, double *d_out);

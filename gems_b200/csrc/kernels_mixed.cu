@@ -105,7 +105,7 @@ __device__ __forceinline__ void load_vecf(const float *__restrict__ src, float (
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < N; i++) v[i] = __ldcg(src + i);
+    for (int i = 0; i < N; i++) v[i] = __ldcg(src + (size_t)(i / 4) * cs + i % 4);
   }
 }
 
@@ -117,8 +117,24 @@ __device__ __forceinline__ void store_vecf(float *__restrict__ dst, const float 
       *reinterpret_cast<float4 *>(dst + (size_t)i * cs) =
           make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
   } else {
+    // whole 4-state chunks; in the tile-major form the padding states are stored as zeros
+    // (they meet zero rows of P in the tensor-core products)
 #pragma unroll
-    for (int i = 0; i < N; i++) dst[i] = v[i];
+    for (int i = 0; i < (N + 3) / 4; i++) {
+      float4 w;
+      w.x = v[4 * i];
+      w.y = 4 * i + 1 < N ? v[4 * i + 1] : 0.f;
+      w.z = 4 * i + 2 < N ? v[4 * i + 2] : 0.f;
+      w.w = 4 * i + 3 < N ? v[4 * i + 3] : 0.f;
+      if (mix_k<N>() > 0) {
+        *reinterpret_cast<float4 *>(dst + (size_t)i * cs) = w;
+      } else {
+        dst[4 * i] = w.x;
+        if (4 * i + 1 < N) dst[4 * i + 1] = w.y;
+        if (4 * i + 2 < N) dst[4 * i + 2] = w.z;
+        if (4 * i + 3 < N) dst[4 * i + 3] = w.w;
+      }
+    }
   }
 }
 

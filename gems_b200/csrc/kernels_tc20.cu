@@ -37,10 +37,13 @@
 #include <string>
 
 #include "gems_internal.cuh"
+#include "tc_common.cuh"
 
 namespace gems {
 
 namespace {
+
+using namespace tc;
 
 constexpr int kN = 20;                          // states
 constexpr int kNP = 32;                         // MMA N (padded states)
@@ -51,7 +54,6 @@ constexpr int kRowChunks = 20;                  // 16-byte chunks per row (4 cat
 constexpr int kAChunk = kTile * 16;             // one chunk of an A tile (128 rows x 16 B)
 constexpr int kABytes = (kRowChunks + 1) * kAChunk;  // + a zero chunk for the last category
 constexpr int kBImg = (kKP / 4) * kNP * 16;     // 6 chunks x 32 rows x 16 B = 3072
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 // TMEM columns: accumulators D[side][category] (32 columns each) in [0, 256), the hi part of
 // the operand rows A_hi[side][category] (K = 24 columns each) in [256, 448)
 constexpr int kTmemCols = 512;
@@ -60,91 +62,17 @@ constexpr int kAhiCol = 256;
 // consecutive state codes start in different shared-memory bank groups
 __host__ __device__ constexpr int tip_row_floats(int C) { return C * kN + 4; }
 
-__device__ __forceinline__ uint32_t sptr(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t cnt) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(cnt) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > kWaitCycles) return false;
-  return true;
-}
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
-                                         uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(dst),
-      "l"(src), "r"(bytes), "r"(bar)
-      : "memory");
-}
-// UMMA shared-memory descriptor, K-major, no swizzle (Blackwell version field = 1)
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;
-}
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 32, M = 128
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kNP >> 3) << 17) |
-                            ((uint32_t)(kTile >> 4) << 24);
-
+constexpr uint32_t kIdesc = tc::idesc_tf32(kNP);
 __device__ __forceinline__ void mma_tf32(uint32_t dtm, uint64_t a, uint64_t b, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtm),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
-      : "memory");
+  tc::mma_ss(dtm, a, b, kIdesc, acc);
 }
-// same, A read from tensor memory (lane = row, one column per K element)
 __device__ __forceinline__ void mma_tf32_ta(uint32_t dtm, uint32_t atm, uint64_t b, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(dtm),
-      "r"(atm), "l"(b), "r"(kIdesc), "r"(acc)
-      : "memory");
+  tc::mma_ts(dtm, atm, b, kIdesc, acc);
 }
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   bar)
-               : "memory");
-}
-// one lane of a converged warp (the MMA and copy instructions are issued by a single thread;
-// issuing them from a warp-uniform branch keeps their operands in uniform registers)
-__device__ __forceinline__ bool elect_one() {
-  uint32_t pred = 0;
-  asm volatile(
-      "{\n\t.reg .pred P;\n\telect.sync _|P, 0xffffffff;\n\tselp.u32 %0, 1, 0, P;\n\t}\n"
-      : "=r"(pred));
-  return pred != 0;
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
+__device__ __forceinline__ void tc_fence_after() { tc::fence_after(); }
+__device__ __forceinline__ void tc_fence_before() { tc::fence_before(); }
+
 // the 20 state columns of one accumulator (columns 20..31 are padding) of this thread's lane;
 // the registers are valid after tmem_ld_wait on them
 __device__ __forceinline__ void tmem_ld20(uint32_t taddr, uint32_t (&r)[20]) {
@@ -186,27 +114,6 @@ __device__ __forceinline__ void tmem_st_row(uint32_t taddr, const float4 (&h)[5]
       "f"(h[4].x), "f"(h[4].y), "f"(h[4].z), "f"(h[4].w), "f"(0.f)
       : "memory");
 }
-__device__ __forceinline__ void tmem_st_wait() {
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-// Round a finite FP32 value to TF32 (10 fraction bits), to nearest with ties away from zero:
-// adding half a TF32 ulp (bit 12) to the sign-magnitude bits and clearing the 13 low bits
-// rounds the magnitude up exactly when the dropped bits are at least half an ulp (a carry
-// into the exponent gives the next binade correctly).  Two integer operations.
-__device__ __forceinline__ float tf32_rna(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-}
-__device__ __forceinline__ void split4(float4 v, float4 &h, float4 &l) {
-  h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
-  l = make_float4(tf32_rna(v.x - h.x), tf32_rna(v.y - h.y), tf32_rna(v.z - h.z),
-                  tf32_rna(v.w - h.w));
-}
-// the value a row is stored as: hi + lo of its split (exact in FP32), so that a later split
-// of the stored value gives the same hi and lo again
-__device__ __forceinline__ float4 join4(float4 h, float4 l) {
-  return make_float4(h.x + l.x, h.y + l.y, h.z + l.z, h.w + l.w);
-}
-
 // ---------------------------------------------------------------------------------------
 // Per-op tables for the tensor-core path (floats, per op):
 //   B images [2 sides][C][hi, lo][6 chunks][32 rows][4]   (row n = target state x, K = y)

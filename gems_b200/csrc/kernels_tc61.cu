@@ -1,0 +1,457 @@
+// kernels_tc61.cu -- 61-state (codon) mixed-precision traversal on the tcgen05 tensor cores.
+//
+// Node update per category c (real space, FP32 storage, SAFE scaling per category -- the
+// reference always uses SAFE for 61 states, phylotreesse.cpp:95-96):
+//     out[p][c][:] = (P_c(t_L) . L[p][c][:]) (*) (P_c(t_R) . R[p][c][:])
+// For a tile of 128 patterns each child product is D[128 x 64] = A[128 x 64] . B^T (61 states
+// padded to 64 in K and N; the padding rows of B are zero), issued as tcgen05.mma kind::tf32
+// M=128 N=64 K=8, FP32 accuracy from split TF32 (A.B ~ A_hi.B_hi + A_hi.B_lo + A_lo.B_hi).
+// A tip child is a one-hot (or all-ones for the unknown state) operand row, exact in TF32, so it
+// needs only the first two products and no table.
+//
+// The work of one op is done category by category ("steps"): one category of a child tile is
+// 16 chunks x 2 KB = 32 KB, contiguous in the tile-major layout (mix_off<61>), brought by one
+// cp.async.bulk.  Per step (one CTA per SM, 256 threads, 2 per pattern row):
+//   wait(operand tiles, B images of this step)
+//   -> split: hi -> TMEM operand columns (tcgen05.st), lo -> shared memory; one-hot rows of tips
+//   -> the next step's operand tiles start copying (landing buffers free)
+//   -> MMAs (issued by an elected lane), wait -> the next step's B images start copying
+//   -> epilogue: tcgen05.ld of the accumulators, products, SAFE rescaling by 2^64 with uint16
+//      counters, coalesced stores of the rows (stored as hi + lo of their split)
+// The step after the last category of an op may need that op's output of the same category
+// (one category: C = 1); that copy is issued after the epilogue's stores instead.
+//
+// The kernel takes an array of jobs (sessions that share one tree and op list: ModelFinder's
+// candidate models on one alignment), grid (tiles, jobs), so many small sessions fill the GPU
+// in one launch.  Every mbarrier wait is bounded; on expiry the CTA records GEMS_ERR_TIMEOUT,
+// waits (bounded) for its copies in flight, frees its TMEM and returns.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gems_internal.cuh"
+#include "tc_common.cuh"
+
+namespace gems {
+
+namespace {
+
+using namespace tc;
+
+constexpr int kN = 61;
+constexpr int kNP = 64;                   // MMA N and K (padded states)
+constexpr int kTile = 128;                // patterns per CTA = MMA M
+constexpr int kThreads61 = 256;           // 2 threads per pattern row, 32 states each
+constexpr int kK = 16;                    // 4-state chunks per category row
+constexpr int kAChunk = kTile * 16;       // one chunk of a tile (128 rows x 16 B)
+constexpr int kATile = kK * kAChunk;      // one category of one child tile: 32 KB
+constexpr int kBImg = (kNP / 4) * kNP * 16;  // 16 K chunks x 64 rows x 16 B = 16 KB
+constexpr int kBSide = 2 * kBImg;         // hi + lo images of one side: 32 KB
+constexpr uint32_t kIdesc61 = idesc_tf32(kNP);
+constexpr int kTmemCols61 = 256;          // D[side] at side*64, A_hi[side] at 128 + side*64
+constexpr int kAhi61 = 128;
+
+// op tables: B images [side][C][hi, lo][16 K chunks][64 rows][4] (row = target state x,
+// K = source state y), floats per op
+__host__ __device__ constexpr size_t op_floats61(int C) { return (size_t)2 * C * (kBSide / 4); }
+
+__global__ void k_prep_ops_tc61(DevCtx c, const DevOp *ops, float *tab, size_t stride_f) {
+  extern __shared__ double ex[];  // [C][n] exp terms
+  const int k = blockIdx.x, side = blockIdx.y;
+  const DevOp op = ops[k];
+  const double len = side ? op.r_len : op.l_len;
+  const int C = c.C, n = kN;
+  for (int idx = threadIdx.x; idx < C * n; idx += blockDim.x) {
+    const int cc = idx / n, i = idx - cc * n;
+    ex[idx] = exp(c.eval[i] * (c.rates[cc] * len));
+  }
+  __syncthreads();
+  float *img = tab + (size_t)k * stride_f + (size_t)side * C * (kBSide / 4);
+  const int per = kBImg / 4;  // floats of one image
+  for (int idx = threadIdx.x; idx < C * per; idx += blockDim.x) {
+    const int cc = idx / per, r = idx - cc * per;
+    const int chunk = r / (kNP * 4), rr = r - chunk * kNP * 4, x = rr / 4, y = chunk * 4 + (rr & 3);
+    float v = 0.f;
+    if (x < n && y < n) {
+      double acc = 0.0;
+      for (int i = 0; i < n; i++) acc = fma(c.evec[x * n + i] * ex[cc * n + i], c.inv_evec[i * n + y], acc);
+      v = (float)fmax(acc, 0.0);
+    }
+    const float hi = tf32_rna(v);
+    img[(size_t)cc * 2 * per + r] = hi;
+    img[(size_t)cc * 2 * per + per + r] = tf32_rna(v - hi);
+  }
+}
+
+struct Tc61Shared {
+  uint64_t bar_land, bar_b, bar_mma;
+  uint32_t tmem_base;
+  float rowmax[2][kTile];
+};
+
+// 32 TMEM columns of this thread's lane; valid after tmem_ld32_wait on the same registers
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld32_wait(uint32_t (&r)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31])
+               :
+               : "memory");
+}
+// 32 consecutive TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, "
+      "%29, %30, %31, %32};" ::"r"(taddr),
+      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]),
+      "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]),
+      "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]),
+      "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]),
+      "f"(v[29]), "f"(v[30]), "f"(v[31])
+      : "memory");
+}
+
+
+// step t of an op list: op t / C, category t % C
+struct Step {
+  DevOp op;
+  int cat;
+};
+
+// copies of the operand tiles of step `st` (internal children, category st.cat) into the
+// landing buffers; `late_slot`: a child equal to it is left for a late copy (issued by the
+// caller after the current step's stores); the barrier expects all bytes now
+__device__ __forceinline__ void issue_land(const DevCtx &c, const Step &st, int late_slot,
+                                           uint32_t sL0, uint32_t sL1, int tile, uint32_t bar) {
+  uint32_t bytes = 0;
+  for (int s = 0; s < 2; s++)
+    if ((s ? st.op.r_kind : st.op.l_kind) == GEMS_CHILD_PARTIAL) bytes += kATile;
+  mbar_expect_tx(bar, bytes);
+  for (int s = 0; s < 2; s++) {
+    const int kind = s ? st.op.r_kind : st.op.l_kind, id = s ? st.op.r_id : st.op.l_id;
+    if (kind != GEMS_CHILD_PARTIAL || id == late_slot) continue;
+    const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
+                       mix_off<61>(c, (long)tile * kTile, st.cat);
+    bulk_g2s(s ? sL1 : sL0, src, kATile, bar);
+  }
+}
+__device__ __forceinline__ void issue_late(const DevCtx &c, const Step &st, int late_slot,
+                                           uint32_t sL0, uint32_t sL1, int tile, uint32_t bar) {
+  for (int s = 0; s < 2; s++) {
+    const int kind = s ? st.op.r_kind : st.op.l_kind, id = s ? st.op.r_id : st.op.l_id;
+    if (kind != GEMS_CHILD_PARTIAL || id != late_slot) continue;
+    const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
+                       mix_off<61>(c, (long)tile * kTile, st.cat);
+    bulk_g2s(s ? sL1 : sL0, src, kATile, bar);
+  }
+}
+// B images (hi and lo, both sides) of step `st`
+__device__ __forceinline__ void issue_b(const float *tab_op, int C, int cat, unsigned char *Bbase,
+                                        uint32_t bar) {
+  mbar_expect_tx(bar, 2 * kBSide);
+  for (int s = 0; s < 2; s++)
+    bulk_g2s(sptr(Bbase + (size_t)s * kBSide),
+             tab_op + ((size_t)s * C + cat) * (kBSide / 4), kBSide, bar);
+}
+
+__global__ void __launch_bounds__(kThreads61, 1)
+    k_traverse_tc61(const TcJob *__restrict__ jobs, int nops, size_t stride_f, int *flag) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ TcJob sj;
+  unsigned char *land = smem_raw;                     // [2][32 KB] raw operand tiles
+  unsigned char *alo = smem_raw + 2 * kATile;         // [2][32 KB] lo parts
+  unsigned char *Bbase = smem_raw + 4 * kATile;       // [2][hi 16 KB, lo 16 KB]
+  Tc61Shared *ctl = reinterpret_cast<Tc61Shared *>(smem_raw + 4 * kATile + 2 * kBSide);
+
+  const int t = threadIdx.x, warp = t >> 5;
+  const int row = ((warp & 3) << 5) | (t & 31);
+  const int half = warp >> 2;  // states [32h, 32h + 32) = chunks [8h, 8h + 8)
+  if (t == 0) sj = jobs[blockIdx.y];
+  const uint32_t bar_land = sptr(&ctl->bar_land), bar_b = sptr(&ctl->bar_b),
+                 bar_mma = sptr(&ctl->bar_mma);
+  if (t == 0) {
+    mbar_init(bar_land, 1);
+    mbar_init(bar_b, 1);
+    mbar_init(bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(sptr(&ctl->tmem_base), kTmemCols61);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const DevCtx &c = sj.c;
+  const DevOp *ops = sj.ops;
+  const float *tab = sj.tab;
+  const int C = c.C;
+  const int tile = blockIdx.x;
+  const long p = (long)tile * kTile + row;
+  const bool act = p < c.P;
+  const bool inv0 = act ? c.invar[p] == 0.0 : false;
+  const uint32_t tmem = ctl->tmem_base;
+  const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
+  const uint32_t sL0 = sptr(land), sL1 = sptr(land + kATile);
+  const uint64_t dLo[2] = {sdesc(sptr(alo), kAChunk, 128), sdesc(sptr(alo + kATile), kAChunk, 128)};
+  const uint64_t dB[2] = {sdesc(sptr(Bbase), kNP * 16, 128),
+                          sdesc(sptr(Bbase + kBSide), kNP * 16, 128)};
+  float *part = static_cast<float *>(c.partials);
+  const int nsteps = nops * C;
+  uint32_t ph_land = 0, ph_b = 0, ph_mma = 0;
+  bool ok = true, land_pending = false, b_pending = false, mma_pending = false;
+
+  Step cur{ops[0], 0};
+  if (warp == 0 && elect_one()) {
+    issue_land(c, cur, -1, sL0, sL1, tile, bar_land);
+    issue_b(tab, C, 0, Bbase, bar_b);
+  }
+  land_pending = b_pending = true;
+  int st_l = 0, st_r = 0;  // tip state codes of the current op
+  if (act) {
+    if (cur.op.l_kind == GEMS_CHILD_TIP) st_l = c.tips[(size_t)cur.op.l_id * c.P + p];
+    if (cur.op.r_kind == GEMS_CHILD_TIP) st_r = c.tips[(size_t)cur.op.r_id * c.P + p];
+  }
+
+  for (int step = 0; step < nsteps && ok; step++) {
+    const int k = step / C;
+    const bool inL = cur.op.l_kind == GEMS_CHILD_PARTIAL, inR = cur.op.r_kind == GEMS_CHILD_PARTIAL;
+    const bool has_next = step + 1 < nsteps;
+    Step nxt = cur;
+    if (has_next) {
+      if (cur.cat + 1 < C) {
+        nxt.cat = cur.cat + 1;
+      } else {
+        nxt.op = ops[k + 1];
+        nxt.cat = 0;
+      }
+    }
+    // the next step needs this step's output (same slot and category): copied after the stores
+    const int late = (has_next && nxt.cat == cur.cat) ? cur.op.dst_slot : -1;
+    // children's counters of this category (SAFE: per pattern and category)
+    int scl = 0, scr = 0;
+    if (act) {
+      if (inL) scl = c.scale[(size_t)cur.op.l_id * c.slot_scale + (size_t)p * C + cur.cat];
+      if (inR) scr = c.scale[(size_t)cur.op.r_id * c.slot_scale + (size_t)p * C + cur.cat];
+    }
+    if (__syncthreads_or(!mbar_wait(bar_land, ph_land) || !mbar_wait(bar_b, ph_b))) {
+      ok = false;
+      if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+      break;
+    }
+    land_pending = b_pending = false;
+    ph_land ^= 1;
+    ph_b ^= 1;
+    // operand rows: hi -> TMEM, lo -> shared memory; tips as one-hot rows
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      float h[32];
+      if (s ? inR : inL) {
+        const float4 *a4 = reinterpret_cast<const float4 *>(land + (size_t)s * kATile);
+        float4 *l4 = reinterpret_cast<float4 *>(alo + (size_t)s * kATile);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int ch = 8 * half + i;
+          float4 hv, lv;
+          split4(a4[ch * kTile + row], hv, lv);
+          l4[ch * kTile + row] = lv;
+          h[4 * i] = hv.x;
+          h[4 * i + 1] = hv.y;
+          h[4 * i + 2] = hv.z;
+          h[4 * i + 3] = hv.w;
+        }
+      } else {
+        const int st = s ? st_r : st_l;
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+          const int x = 32 * half + i;
+          h[i] = (x < kN && (st == x || st >= kN)) ? 1.f : 0.f;
+        }
+      }
+      tmem_st32(tmem + lane_off + (uint32_t)(kAhi61 + s * kNP + 32 * half), h);
+    }
+    tmem_st_wait();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0 && elect_one()) {
+      // the landing buffers have been read: the next step's tiles come in
+      if (has_next) issue_land(c, nxt, late, sL0, sL1, tile, bar_land);
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        const bool in = s ? inR : inL;
+        const uint32_t dtm = tmem + (uint32_t)(s * kNP);
+        const uint32_t atm = tmem + (uint32_t)(kAhi61 + s * kNP);
+#pragma unroll
+        for (int ks = 0; ks < kNP / 8; ks++) {
+          const uint64_t kb = (uint64_t)((2 * ks * kNP * 16) >> 4);
+          const uint64_t ko = (uint64_t)((2 * ks * kAChunk) >> 4);
+          const uint64_t bh = dB[s] + kb, bl = dB[s] + kb + (uint64_t)(kBImg >> 4);
+          mma_ts(dtm, atm + 8 * ks, bh, kIdesc61, ks > 0 ? 1u : 0u);
+          mma_ts(dtm, atm + 8 * ks, bl, kIdesc61, 1u);
+          if (in) mma_ss(dtm, dLo[s] + ko, bh, kIdesc61, 1u);
+        }
+      }
+      mma_commit(bar_mma);
+    }
+    land_pending = has_next;
+    mma_pending = true;
+    if (__syncthreads_or(!mbar_wait(bar_mma, ph_mma))) {
+      ok = false;
+      if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+      break;
+    }
+    mma_pending = false;
+    ph_mma ^= 1;
+    fence_after();
+    // B images of this step are no longer read: the next step's come in under the epilogue
+    if (has_next) {
+      if (warp == 0 && elect_one())
+        issue_b(tab + (size_t)(cur.cat + 1 < C ? k : k + 1) * stride_f, C, nxt.cat, Bbase, bar_b);
+      b_pending = true;
+    }
+    // ---- epilogue: products, SAFE rescaling of this category, stores
+    uint32_t rl[32], rr[32];
+    tmem_ld32(tmem + lane_off + (uint32_t)(0 * kNP + 32 * half), rl);
+    tmem_ld32(tmem + lane_off + (uint32_t)(1 * kNP + 32 * half), rr);
+    tmem_ld32_wait(rl);
+    tmem_ld32_wait(rr);
+    float v[32];
+    float mx = 0.f;
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      v[i] = fmaxf(__uint_as_float(rl[i]), 0.f) * fmaxf(__uint_as_float(rr[i]), 0.f);
+      mx = fmaxf(mx, v[i]);
+    }
+    ctl->rowmax[half][row] = mx;
+    __syncthreads();
+    const float m = fmaxf(ctl->rowmax[0][row], ctl->rowmax[1][row]);
+    int s_out = scl + scr;
+    float f = 1.f;
+    if ((inL || inR) && m < kScaleThrF && inv0) {
+      f = 18446744073709551616.0f;  // 2^64
+      s_out += 1;
+    }
+    float *dst = part + (size_t)cur.op.dst_slot * c.slot_elems + mix_off<61>(c, (long)tile * kTile, cur.cat);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int x = 32 * half + 4 * i;
+      float4 w = make_float4(v[4 * i] * f, v[4 * i + 1] * f, v[4 * i + 2] * f, v[4 * i + 3] * f);
+      if (x + 3 >= kN) {  // padding states stored as zeros
+        if (x + 1 >= kN) w.y = 0.f;
+        if (x + 2 >= kN) w.z = 0.f;
+        if (x + 3 >= kN) w.w = 0.f;
+        if (x >= kN) w.x = 0.f;
+      }
+      float4 h, l;
+      split4(w, h, l);
+      reinterpret_cast<float4 *>(dst)[(8 * half + i) * kTile + row] = join4(h, l);
+    }
+    if (act && half == 0)
+      c.scale[(size_t)cur.op.dst_slot * c.slot_scale + (size_t)p * C + cur.cat] = (uint16_t)s_out;
+    // later steps bulk-copy this output from global memory
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (late >= 0 && warp == 0 && elect_one()) issue_late(c, nxt, late, sL0, sL1, tile, bar_land);
+    if (has_next && nxt.cat == 0 && act) {  // the next op's tip state codes
+      st_l = nxt.op.l_kind == GEMS_CHILD_TIP ? c.tips[(size_t)nxt.op.l_id * c.P + p] : 0;
+      st_r = nxt.op.r_kind == GEMS_CHILD_TIP ? c.tips[(size_t)nxt.op.r_id * c.P + p] : 0;
+    }
+    cur = nxt;
+  }
+  if (!ok && t == 0) {
+    if (land_pending) mbar_wait(bar_land, ph_land);
+    if (b_pending) mbar_wait(bar_b, ph_b);
+    if (mma_pending) mbar_wait(bar_mma, ph_mma);
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTmemCols61);
+}
+
+size_t tc61_smem() { return 4 * (size_t)kATile + 2 * (size_t)kBSide + sizeof(Tc61Shared) + 64; }
+
+}  // namespace
+
+size_t tc61_op_floats(int ncat) { return op_floats61(ncat); }
+
+bool tc61_supported(const Session *s) {
+  return s->desc.nstates == 61 && s->desc.precision == GEMS_PREC_MIXED &&
+         s->desc.scaling == GEMS_SCALE_SAFE && s->tc_enabled && s->tiled;
+}
+
+int launch_prep_ops_tc61(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  DevCtx c = s->ctx();
+  const size_t smem = sizeof(double) * s->desc.ncat * kN;
+  k_prep_ops_tc61<<<dim3(nops, 2), 256, smem, s->stream>>>(
+      c, s->d_ops, reinterpret_cast<float *>(s->d_opmats), s->op_stride_tc);
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  return GEMS_OK;
+}
+
+// one launch over the tiles of every session in `ss` (all with the same op list, pattern
+// count, categories and device), on the stream of ss[0]
+int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops) {
+  if (nops <= 0 || nsess <= 0) return GEMS_OK;
+  Session *s0 = ss[0];
+  if (nsess > Session::kMaxBatch) {
+    set_error("too many sessions in one batched launch");
+    return GEMS_ERR_BAD_ARG;
+  }
+  std::vector<TcJob> jobs(nsess);
+  for (int i = 0; i < nsess; i++) {
+    jobs[i].c = ss[i]->ctx();
+    jobs[i].ops = ss[i]->d_ops;
+    jobs[i].tab = reinterpret_cast<const float *>(ss[i]->d_opmats);
+  }
+  // host staging (pinned), then one copy; the previous launch that read it has completed
+  GEMS_CUDA(cudaStreamSynchronize(s0->stream));
+  std::memcpy(s0->h_jobs, jobs.data(), sizeof(TcJob) * nsess);
+  GEMS_CUDA(cudaMemcpyAsync(s0->d_jobs, s0->h_jobs, sizeof(TcJob) * nsess,
+                            cudaMemcpyHostToDevice, s0->stream));
+  const size_t smem = tc61_smem();
+  GEMS_CUDA(cudaFuncSetAttribute(k_traverse_tc61, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  GEMS_CUDA(cudaMemsetAsync(s0->d_flag, 0, sizeof(int), s0->stream));
+  const dim3 grid((s0->P + kTile - 1) / kTile, nsess);
+  cudaEvent_t ev0;
+  if (int st = prof_begin(s0, 0, &ev0)) return st;
+  k_traverse_tc61<<<grid, kThreads61, smem, s0->stream>>>(
+      reinterpret_cast<const TcJob *>(s0->d_jobs), nops, s0->op_stride_tc, s0->d_flag);
+  s0->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  if (int st = prof_end(s0, 0, ev0)) return st;
+  int flag = 0;
+  GEMS_CUDA(cudaMemcpyAsync(&flag, s0->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s0->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s0->stream));
+  if (flag) {
+    set_error("tensor-core traversal: bounded wait expired");
+    return GEMS_ERR_TIMEOUT;
+  }
+  return GEMS_OK;
+}
+
+int launch_traverse_tc61(Session *s, int nops) {
+  Session *one[1] = {s};
+  return launch_traverse_tc61_batch(one, 1, nops);
+}
+
+}  // namespace gems

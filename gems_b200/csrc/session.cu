@@ -121,9 +121,12 @@ static Sizes compute_sizes(const gems_session_desc &d) {
   const size_t blk = (size_t)d.nstates * d.ncat;
   const int unk = state_unknown(d.nstates);
   const size_t elem = d.precision == GEMS_PREC_MIXED ? sizeof(float) : sizeof(double);
-  // 20-state mixed partials are tile-major in 128-pattern tiles (the tensor-core layout)
-  z.tiled = d.nstates == 20 && d.precision == GEMS_PREC_MIXED;
-  z.slot_elems = (z.tiled ? (P + kMixTile - 1) / kMixTile * kMixTile : P) * blk;
+  // 20- and 61-state mixed partials are tile-major in 128-pattern tiles (the tensor-core
+  // layout; 61 states padded to 64)
+  z.tiled = (d.nstates == 20 || d.nstates == 61) && d.precision == GEMS_PREC_MIXED;
+  z.slot_elems = z.tiled ? (P + kMixTile - 1) / kMixTile * kMixTile * d.ncat *
+                               (d.nstates == 20 ? 20 : 64)
+                         : P * blk;
   z.partial_bytes = (size_t)d.nslots * z.slot_elems * elem;
   z.scale_bytes = (size_t)d.nslots * P * (d.scaling == GEMS_SCALE_SAFE ? d.ncat : 1) * 2;
   // theta + scale_all, pattern_lh, df_frac, ddf_term
@@ -133,6 +136,10 @@ static Sizes compute_sizes(const gems_session_desc &d) {
   if (d.nstates == 20 && d.precision == GEMS_PREC_MIXED && d.ncat <= 4) {
     // the tensor-core tables (floats) share the buffer
     const size_t need = (tc20_op_floats(d.ncat, unk) + 1) / 2;
+    if (z.op_stride < need) z.op_stride = need;
+  }
+  if (d.nstates == 61 && d.precision == GEMS_PREC_MIXED && d.scaling == GEMS_SCALE_SAFE) {
+    const size_t need = (tc61_op_floats(d.ncat) + 1) / 2;
     if (z.op_stride < need) z.op_stride = need;
   }
   z.op_stride = (z.op_stride + 7) & ~(size_t)7;  // 64-byte aligned op tables
@@ -180,6 +187,8 @@ static void free_session(Session *s) {
   cudaFree(s->d_flag);
   cudaFree(s->d_bar);
   cudaFreeHost(s->h_ops);
+  cudaFree(s->d_jobs);
+  cudaFreeHost(s->h_jobs);
   cudaFreeHost(s->h_result);
   if (s->stream) {
     cudaStreamSynchronize(s->stream);
@@ -233,6 +242,15 @@ static int check_branch(Session *s, const gems_branch *br) {
   return GEMS_OK;
 }
 
+static void invalidate_theta(Session *s, const gems_op *ops, int nops) {
+  for (int k = 0; k < nops; k++)
+    if (s->theta_valid &&
+        (ops[k].dst_slot == s->theta_branch.dad_slot ||
+         (s->theta_branch.node_kind == GEMS_CHILD_PARTIAL &&
+          ops[k].dst_slot == s->theta_branch.node_id)))
+      s->theta_valid = false;
+}
+
 static int run_ops(Session *s, const gems_op *ops, int nops) {
   if (!s->model_set) {
     set_error("model not set");
@@ -247,6 +265,9 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
   if (tc20_supported(s)) {
     if ((st = launch_prep_ops_tc20(s, nops))) return st;
     if ((st = launch_traverse_tc20(s, nops))) return st;
+  } else if (tc61_supported(s)) {
+    if ((st = launch_prep_ops_tc61(s, nops))) return st;
+    if ((st = launch_traverse_tc61(s, nops))) return st;
   } else if (traverse_v2_supported(s)) {
     if ((st = launch_prep_ops_v2(s, nops))) return st;
     if ((st = launch_traverse_v2(s, nops))) return st;
@@ -257,12 +278,7 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
     if ((st = launch_prep_ops(s, nops))) return st;
     if ((st = launch_traverse(s, nops))) return st;
   }
-  for (int k = 0; k < nops; k++)
-    if (s->theta_valid &&
-        (ops[k].dst_slot == s->theta_branch.dad_slot ||
-         (s->theta_branch.node_kind == GEMS_CHILD_PARTIAL &&
-          ops[k].dst_slot == s->theta_branch.node_id)))
-      s->theta_valid = false;
+  invalidate_theta(s, ops, nops);
   return GEMS_OK;
 }
 
@@ -370,6 +386,11 @@ int gems_session_create(const gems_session_desc *desc, gems_session **out) {
   if ((e = cudaHostAlloc((void **)&s->h_ops, (size_t)z.nops_max * sizeof(DevOp), 0)) !=
       cudaSuccess)
     return fail(e, "cudaHostAlloc ops");
+  if ((e = cudaMalloc((void **)&s->d_jobs, sizeof(TcJob) * Session::kMaxBatch)) != cudaSuccess)
+    return fail(e, "cudaMalloc jobs");
+  if ((e = cudaHostAlloc((void **)&s->h_jobs, sizeof(TcJob) * Session::kMaxBatch, 0)) !=
+      cudaSuccess)
+    return fail(e, "cudaHostAlloc jobs");
   if ((e = cudaHostAlloc((void **)&s->h_result, 16 * sizeof(double), 0)) != cudaSuccess)
     return fail(e, "cudaHostAlloc result");
   if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -583,6 +604,59 @@ int gems_traverse(gems_session *s, const gems_op *ops, int nops) {
   return GEMS_OK;
 }
 
+int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, int nops) {
+  if (!ss || nsess <= 0 || nsess > Session::kMaxBatch || (nops > 0 && !ops))
+    return GEMS_ERR_BAD_ARG;
+  Session *s0 = ss[0];
+  if (!s0) return GEMS_ERR_BAD_ARG;
+  bool tc = true;
+  for (int i = 0; i < nsess; i++) {
+    Session *s = ss[i];
+    if (!s || s->desc.device != s0->desc.device || s->desc.nptn != s0->desc.nptn ||
+        s->desc.nstates != s0->desc.nstates || s->desc.ncat != s0->desc.ncat ||
+        s->desc.nslots != s0->desc.nslots) {
+      set_error("batched sessions must share device, patterns, states, categories and slots");
+      return GEMS_ERR_BAD_ARG;
+    }
+    if (!s->model_set || !s->tips_ok) {
+      set_error(!s->model_set ? "model not set" : "tip states invalid (last upload was rejected)");
+      return GEMS_ERR_STATE;
+    }
+    for (int j = 0; j < i; j++)
+      if (ss[j] == s) {
+        set_error("a session appears twice in the batch");
+        return GEMS_ERR_BAD_ARG;
+      }
+    tc = tc && tc61_supported(s);
+  }
+  GEMS_CUDA(cudaSetDevice(s0->desc.device));
+  if (!tc) {  // no batched kernel for this form: one traversal per session, on its own stream
+    for (int i = 0; i < nsess; i++)
+      if (int st = run_ops(ss[i], ops, nops)) return st;
+    for (int i = 0; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
+    return GEMS_OK;
+  }
+  for (int i = 0; i < nsess; i++) {
+    if (int st = upload_ops(ss[i], ops, nops)) return st;
+    if (int st = launch_prep_ops_tc61(ss[i], nops)) return st;
+  }
+  // the batched launch runs on the first session's stream after every session's tables
+  for (int i = 1; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
+  std::vector<Session *> v(ss, ss + nsess);
+  if (int st = launch_traverse_tc61_batch(v.data(), nsess, nops)) return st;
+  for (int i = 0; i < nsess; i++) invalidate_theta(ss[i], ops, nops);
+  return GEMS_OK;
+}
+
+int gems_branch_lnl_batch(gems_session *const *ss, int nsess, const gems_op *ops, int nops,
+                          const gems_branch *br, double *lnl) {
+  if (!lnl) return GEMS_ERR_BAD_ARG;
+  if (int st = gems_traverse_batch(ss, nsess, ops, nops)) return st;
+  for (int i = 0; i < nsess; i++)
+    if (int st = gems_branch_lnl(ss[i], nullptr, 0, br, &lnl[i], nullptr)) return st;
+  return GEMS_OK;
+}
+
 int gems_branch_lnl(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
                     double *lnl, double *pattern_lh) {
   if (!s || !lnl || (nops > 0 && !ops)) return GEMS_ERR_BAD_ARG;
@@ -684,8 +758,10 @@ int gems_get_partial(gems_session *s, int slot, double *partial, uint16_t *scale
       for (long p = 0; p < s->desc.nptn; p++)
         for (int cc = 0; cc < s->desc.ncat; cc++) {
           for (int x = 0; x < nst; x++) {
-            const size_t o = s->tiled ? mix_off<20>(c, p, cc) + (size_t)(x / 4) * mix_cs<20>() + x % 4
-                                      : (size_t)p * blk + (size_t)cc * nst + x;
+            const size_t o =
+                !s->tiled ? (size_t)p * blk + (size_t)cc * nst + x
+                : nst == 20 ? mix_off<20>(c, p, cc) + (size_t)(x / 4) * mix_cs<20>() + x % 4
+                            : mix_off<61>(c, p, cc) + (size_t)(x / 4) * mix_cs<61>() + x % 4;
             partial[(size_t)p * blk + (size_t)cc * nst + x] = tmp[o];
           }
         }

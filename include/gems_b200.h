@@ -127,6 +127,17 @@ int gems_get_eigensystem(gems_session *s, double *eval, double *evec, double *in
 /* Postorder list of node updates (computePartialLikelihood over all patterns for each
  * entry of traversal_info; tree/phylokernelnew.h:1293-2043). */
 int gems_traverse(gems_session *s, const gems_op *ops, int nops);
+/* Batched traversal over sessions that share one tree (the same op list and lengths) but hold
+ * different models -- ModelFinder's candidate models on one alignment (modelfactory.cpp:1558,
+ * main/phylotesting.cpp) -- so that many small sessions fill the GPU.  All sessions must have the
+ * same device, nptn, nstates, ncat and nslots, at most 128 per call.  61-state mixed SAFE
+ * sessions (with tensor cores on) run as one launch over every (session, pattern tile); other
+ * forms run one traversal per session.  No counterpart in the reference (it evaluates models
+ * one after the other). */
+int gems_traverse_batch(gems_session *const *sessions, int nsess, const gems_op *ops, int nops);
+/* gems_traverse_batch, then the branch lnL of each session (lnl[nsess]). */
+int gems_branch_lnl_batch(gems_session *const *sessions, int nsess, const gems_op *ops, int nops,
+                          const gems_branch *br, double *lnl);
 /* Branch log-likelihood (computeLikelihoodBranchSIMD, tree/phylokernelnew.h:2658-3275),
  * after running ops (may be 0).  pattern_lh[nptn] optional (log-likelihood per pattern
  * including the scaling correction). */
