@@ -15,9 +15,11 @@ the FP64 lnL of the same run (reported as `lnl_rel_err_mixed`), else the FP64 fo
 weights up, pattern lnL down).  Timing uses CUDA events on the session's stream; the partial
 buffers (65 GB FP64, 33 GB mixed) exceed L2 many times over, so no flush is needed.
 
-Also reported (same run): one Newton branch optimisation (optimizeOneBranch) per branch, and
-the 20-state protein +G4 configuration (128 taxa, 100,000 sites) FP64 vs mixed (tcgen05
-split-TF32) with its lnL error.
+Also reported (same run): one Newton branch optimisation (optimizeOneBranch) per branch; the
+20-state protein +G4 configuration (128 taxa, 100,000 sites) FP64 vs mixed (tcgen05 split-TF32)
+with its lnL error; 256 RELL reweightings; 64 candidate codon models (+G4 and +R8) on one
+200-taxon, 4,000-site alignment in one batched tcgen05 launch; the serving loop on a seeded
+request stream; the measured compute peaks.  `--block NAME` runs one of these alone.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gems|reference]
 
@@ -394,6 +396,63 @@ def rell_block(gt, aln, stream, R=256, reps=5):
                          "unit": "GB/s", "frac": byts / (ms * 1e-3) / 1e9 / hbm_peak}}
 
 
+def codon_batch_block(local, nmodels=64, reps=3):
+    """64 candidate codon models (61 states, kappa ~ U[1,5], omega ~ U[0.1,1], Dirichlet
+    frequencies; +G4 and +R8) on one 200-taxon, 4,000-site alignment: one batched tcgen05
+    traversal over every (model, pattern tile) plus each model's branch lnL, against one model
+    in the plain FP64 form (timed alone, as the reference evaluates candidates one by one)."""
+    import torch
+    from gems_b200 import PhyloTree, Session, branch_lnl_batch, full_traversal, traverse_batch
+    out = {}
+    for freerate in (False, True):
+        tree, model, aln = synth.config_codon200(nsites=4000, freerate=freerate)
+        C = model.ncat
+        nops = sum(op_kinds(tree))
+        rng = np.random.default_rng(17 + C)
+        models = [model] + [synth.codon_gy(rng, C, float(rng.uniform(0.3, 1.5)), freerate=freerate)
+                            for _ in range(nmodels - 1)]
+        sessions = []
+        for m in models:
+            s = Session(tree.ntaxa, aln.npat, 61, C, tree.ntaxa - 2, "mixed", "safe", local)
+            s.upload_tips(aln.patterns)
+            s.upload_patterns(aln.weights)
+            s.set_model(m.eval, m.evec, m.inv_evec, m.rates, m.props)
+            sessions.append(s)
+        ops, br = full_traversal(tree)
+        lnl = branch_lnl_batch(sessions, ops, br)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            lnl = branch_lnl_batch(sessions, ops, br)
+        wall = (time.perf_counter() - t0) / reps
+        s0 = sessions[0]
+        s0.profile(True)
+        s0.profile_read(0)
+        traverse_batch(sessions, ops)
+        kms, kn = s0.profile_read(0)
+        s0.profile(False)
+        for s in sessions:
+            s.close()
+        # model 0 in FP64, alone
+        g64 = PhyloTree.from_case(tree, model, aln, precision="fp64", scaling="safe", device=local)
+        l64 = g64.computeLikelihood()
+        stream = torch.cuda.ExternalStream(g64.session.stream_handle(), device=local)
+        lnl_buf = torch.zeros(1, dtype=torch.float64, device=f"cuda:{local}")
+        ms64, _, _, _ = time_lnl(g64, 3, 1, stream, None, lnl_buf)
+        g64.close()
+        g64.session.close()
+        out[f"C{C}"] = {
+            "model": "codon GY 61 states " + ("+R8" if freerate else "+G4"), "npat": aln.npat,
+            "models": nmodels, "batched_wall_ms": wall * 1e3,
+            "batched_traversal_kernel_ms": kms / max(kn, 1),
+            "models_per_s": nmodels / wall,
+            "site_partial_updates_per_s": nmodels * nops * aln.npat / wall,
+            "fp64_one_model_ms": ms64,
+            "speedup_vs_fp64_one_by_one": nmodels * ms64 / (wall * 1e3),
+            "lnl_rel_err_model0_vs_fp64": abs(lnl[0] - l64) / abs(l64)}
+    return out
+
+
 def serving_block(local, nsess=48, nreq=800, rate=250.0):
     """The serving loop on a seeded stream: sessions of 8-256 taxa and 500-50,000 sites
     (log-uniform), 4/20/61 states, 1/4/8 categories, FP64/mixed; NNI + 5-branch Newton + lnL
@@ -423,6 +482,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the Newton timing and the protein comparison")
+    ap.add_argument("--block", choices=["protein20", "codon64", "serving"], default=None,
+                    help="run only this block of the line and print it (profiling runs)")
     ap.add_argument("--no-tc", action="store_true",
                     help="20-state mixed traversal on CUDA cores instead of tcgen05")
     args = ap.parse_args()
@@ -435,6 +496,13 @@ def main():
     from gems_b200 import PhyloTree
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
+    if args.block is not None:
+        from gems_b200 import measure_peaks
+        fn = {"protein20": lambda: protein_comparison(args, local, measure_peaks(local)),
+              "codon64": lambda: codon_batch_block(local),
+              "serving": lambda: serving_block(local)}[args.block]
+        print(json.dumps({args.block: fn()}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -546,6 +614,7 @@ def main():
         line["rell"] = rell
     if rank == 0 and not args.no_extras and args.config == "dna512":
         line["protein20"] = protein_comparison(args, local, peaks)
+        line["codon64"] = codon_batch_block(local)
         line["serving"] = serving_block(local)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tree, model, aln)
