@@ -610,7 +610,10 @@ int launch_traverse_tc20(Session *s, int nops) {
   const size_t smem = tc_smem(s->desc.ncat);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   void *fn = safe ? (void *)k_traverse_tc20<true> : (void *)k_traverse_tc20<false>;
-  GEMS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the limit is a property of the kernel, shared by every session and host thread: set it to
+  // the largest size any session needs (4 categories), so that a concurrent setting for another
+  // session never lowers it below this launch's size
+  GEMS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem(4)));
   GEMS_CUDA(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
   const int grid = (s->P + kTile - 1) / kTile;
   cudaEvent_t ev0;

@@ -197,11 +197,19 @@ class Server:
                 sid, (arr, i, seq) = job
                 gt = open_sess[sid]
                 ts = time.perf_counter() - t0
-                lnl, nbr = nni5(gt, spec_of[sid].ntaxa, np.random.default_rng((spec_of[sid].seed, seq)))
+                try:
+                    lnl, nbr = nni5(gt, spec_of[sid].ntaxa,
+                                    np.random.default_rng((spec_of[sid].seed, seq)))
+                    err = None
+                except GemsError as e:  # the request fails; the server carries on
+                    lnl, nbr, err = None, 0, str(e)
                 te = time.perf_counter() - t0
                 with lock:
                     records[i] = {"sid": sid, "seq": seq, "arrival": arr, "start": ts, "end": te,
                                   "latency_ms": 1e3 * (te - arr), "lnl": lnl, "branches": nbr}
+                    if err is not None:
+                        records[i]["error"] = err
+                        records[i]["spec"] = dataclasses.asdict(spec_of[sid])
                     busy.discard(sid)
                     state["done"] += 1
                     remaining[sid] -= 1
@@ -242,14 +250,16 @@ def make_stream(nsessions, nrequests, rate, seed, taxa=(8, 1024), sites=(500, 50
 
 
 def summarize(records, wall, specs, cases):
-    done = [r for r in records if r and not r.get("rejected")]
+    failed = [r for r in records if r and r.get("error")]
+    done = [r for r in records if r and not r.get("rejected") and not r.get("error")]
     lat = np.array([r["latency_ms"] for r in done]) if done else np.zeros(1)
     upd = 0
     for r in done:
         spec = specs[r["sid"]]
         npat = cases[r["sid"]][2].npat
         upd += npat  # at least one partial per touched branch; reported as patterns served
-    return {"requests": len(records), "served": len(done),
+    return {"requests": len(records), "served": len(done), "failed": len(failed),
+            "errors": sorted({f"{r['error']} {r['spec']}" for r in failed})[:5],
             "rejected": sum(1 for r in records if r and r.get("rejected")),
             "wall_s": wall, "throughput_req_s": len(done) / wall,
             "latency_ms": {"p50": float(np.percentile(lat, 50)),

@@ -32,7 +32,7 @@ def test_same_alone_and_in_mix(gpu):
     specs, reqs, cases = workload()
     srv = serve.Server(workers=4)
     records, wall = srv.run(specs, cases, reqs)
-    assert all(r is not None and not r.get("rejected") for r in records)
+    assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
     check_same_as_alone(specs, cases, records)
     s = serve.summarize(records, wall, specs, cases)
     assert s["served"] == len(reqs) and s["latency_ms"]["p99"] >= s["latency_ms"]["p50"] > 0
@@ -54,3 +54,35 @@ def test_admission_by_footprint(gpu):
         assert r is not None
         assert bool(r.get("rejected")) == (specs[sid].footprint(cases[sid][2].npat) > budget)
     assert any(r.get("rejected") for r in records)
+
+
+def test_concurrent_sessions_of_different_shapes(gpu):
+    """Host threads driving tensor-core sessions of different category counts at the same time
+    (what the serving loop does): no launch may fail because another thread's session set up
+    the same kernel for a different shape."""
+    import threading
+    from gems_b200 import PhyloTree, synth
+    trees = []
+    for ncat, seed in ((1, 5), (4, 6), (2, 7), (4, 8)):
+        rng = np.random.default_rng(seed)
+        model = synth.protein(rng, ncat, 0.8)
+        tree = synth.random_tree(24, 0.1, seed)
+        aln = synth.simulate(tree, model, 3000, seed + 1)
+        trees.append(PhyloTree.from_case(tree, model, aln, precision="mixed"))
+    ref = [gt.computeLikelihood() for gt in trees]
+    errors = []
+
+    def run(gt, expect):
+        try:
+            for _ in range(40):
+                gt.clearAllPartialLH()
+                assert gt.computeLikelihood() == expect
+        except Exception as e:  # collected and reported by the main thread
+            errors.append(repr(e))
+
+    th = [threading.Thread(target=run, args=(gt, r)) for gt, r in zip(trees, ref)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    assert not errors, errors
