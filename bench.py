@@ -484,6 +484,8 @@ def main():
                     help="skip the Newton timing and the protein comparison")
     ap.add_argument("--block", choices=["protein20", "codon64", "serving"], default=None,
                     help="run only this block of the line and print it (profiling runs)")
+    ap.add_argument("--codon-models", type=int, default=64,
+                    help="candidate codon models in the batched block (small for profiling)")
     ap.add_argument("--no-tc", action="store_true",
                     help="20-state mixed traversal on CUDA cores instead of tcgen05")
     args = ap.parse_args()
@@ -499,7 +501,7 @@ def main():
     if args.block is not None:
         from gems_b200 import measure_peaks
         fn = {"protein20": lambda: protein_comparison(args, local, measure_peaks(local)),
-              "codon64": lambda: codon_batch_block(local),
+              "codon64": lambda: codon_batch_block(local, args.codon_models),
               "serving": lambda: serving_block(local)}[args.block]
         print(json.dumps({args.block: fn()}), flush=True)
         return
@@ -614,7 +616,7 @@ def main():
         line["rell"] = rell
     if rank == 0 and not args.no_extras and args.config == "dna512":
         line["protein20"] = protein_comparison(args, local, peaks)
-        line["codon64"] = codon_batch_block(local)
+        line["codon64"] = codon_batch_block(local, args.codon_models)
         line["serving"] = serving_block(local)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tree, model, aln)
