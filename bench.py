@@ -441,8 +441,23 @@ def codon_batch_block(local, nmodels=64, reps=3):
         ms64, _, _, _ = time_lnl(g64, 3, 1, stream, None, lnl_buf)
         g64.close()
         g64.session.close()
+        kinds = op_kinds(tree)
+        b_ii, b_ti, b_tt = update_bytes(4, 61, C, safe=True)
+        alg = nmodels * aln.npat * (kinds[0] * b_ii + kinds[1] * b_ti + kinds[2] * b_tt)
+        flops = nmodels * aln.npat * nops * update_flops(61, C)
+        kt = kms / max(kn, 1) * 1e-3
+        hbm_peak, _, peak_src = read_peaks()
         out[f"C{C}"] = {
             "model": "codon GY 61 states " + ("+R8" if freerate else "+G4"), "npat": aln.npat,
+            "roofline": {"bound": "hbm", "kernel": "batched tcgen05 traversal",
+                         "achieved": alg / kt / 1e9, "peak": hbm_peak, "peak_source": peak_src,
+                         "unit": "GB/s", "frac": alg / kt / 1e9 / hbm_peak,
+                         "algorithmic_bytes_per_launch": alg,
+                         "traffic": read_traffic("traverse_tc61_codon200.md")
+                         if (C == 4 and nmodels == 64) else None},
+            "compute": {"unit_used": "tcgen05 TF32 (3 products issued per credited one)",
+                        "achieved_tflops": flops / kt / 1e12,
+                        "algorithmic_flops_per_launch": flops},
             "models": nmodels, "batched_wall_ms": wall * 1e3,
             "batched_traversal_kernel_ms": kms / max(kn, 1),
             "models_per_s": nmodels / wall,
