@@ -74,6 +74,26 @@ def measure_peaks(device=0):
     return {"fp64_tflops": a.value, "fp32_tflops": b.value, "tf32_tflops": c.value}
 
 
+def compress_alignment(seqs, nstates, encoded=False, device=0):
+    """Encode and compress an alignment on the device (gems_compress_alignment).
+    seqs: [ntaxa][nsites] uint8 (characters, or state codes when encoded).  Returns
+    (patterns [ntaxa][npat] uint8, weights [npat], site_pattern [nsites], const_char [npat])."""
+    a = np.ascontiguousarray(seqs, dtype=np.uint8)
+    ntaxa, nsites = a.shape
+    pat = np.empty(ntaxa * nsites, np.uint8)
+    w = np.empty(nsites, np.float64)
+    sp = np.empty(nsites, np.int32)
+    cc = np.empty(nsites, np.uint8)
+    npat = c_longlong()
+    lib = _lib.gems()
+    _check(lib.gems_compress_alignment(device, ntaxa, c_longlong(nsites), nstates, _dptr(a),
+                                       int(encoded), _dptr(pat), _dptr(w), _dptr(sp), _dptr(cc),
+                                       byref(npat)), "gems_compress_alignment")
+    k = npat.value
+    return (np.ascontiguousarray(pat[: ntaxa * k].reshape(ntaxa, k)), w[:k].copy(), sp,
+            cc[:k].copy())
+
+
 def full_traversal(tree):
     """Ops of a from-scratch traversal with one slot per internal node (slot = node - ntaxa),
     rooted at the branch between leaf 0 and its neighbour, and that branch: (ops, branch)."""

@@ -207,6 +207,17 @@ int gems_launch_count(gems_session *s, long long *count);
  * summed device time in ms and the number of timed launches, then resets the counters. */
 int gems_profile_enable(gems_session *s, int on);
 int gems_profile_read(gems_session *s, int kernel_id, double *total_ms, long long *launches);
+/* Alignment ingest on the device: state encoding and pattern compression in the reference's
+ * first-appearance order (Alignment::buildPattern / addPatternLazy, alignment.cpp:1240-1268 and
+ * :1511-1543; convertState :1856-1958; computeConst :1321-1420).  seqs: host [ntaxa][nsites]
+ * characters (encoded = 0; DNA or protein letters as the reference reads them, either case) or
+ * state codes (encoded = 1; any state count).  Outputs (host, caller-sized for npat <= nsites):
+ * patterns [ntaxa][npat] (row stride npat), weights[npat] (site counts), site_pattern[nsites]
+ * and const_char[npat] (may be NULL).  An unrecognised character returns GEMS_ERR_BAD_ARG and
+ * names its sequence and site. */
+int gems_compress_alignment(int device, int ntaxa, long long nsites, int nstates,
+                            const uint8_t *seqs, int encoded, uint8_t *patterns, double *weights,
+                            int *site_pattern, uint8_t *const_char, long long *npat);
 /* Measured compute peaks of a device (no counterpart in the reference: the denominators of the
  * compute rooflines): FP64 and FP32 FMA throughput of the CUDA cores and the dense TF32 rate of
  * the tcgen05 tensor cores, in TFLOP/s.  Takes a few tens of milliseconds. */

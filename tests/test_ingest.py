@@ -1,0 +1,101 @@
+"""Alignment ingest: the device pattern compression (gems_compress_alignment) against the
+reference's pattern building restated in oracle/ingest.py -- same patterns in the same
+first-appearance order, weights, site -> pattern map and constant states -- for DNA and protein
+characters (ambiguity codes, gaps, lower case) and pre-encoded codon states; and at a larger size
+against the host compressor."""
+import numpy as np
+import pytest
+
+from gems_b200 import GemsError, compress_alignment, synth
+from oracle import ingest
+
+DNA = "ACGTURYWSMKBHDVNXO-?.~acgtn"
+PROT = "ARNDCQEGHILKMFPSTWYVBZJX*UO-?arndcq"
+
+
+def random_chars(rng, ntaxa, nsites, alphabet, common, p_common=0.9):
+    """Columns drawn from a small set so that patterns repeat, with random noise."""
+    base = rng.choice(list(common), size=(ntaxa, 8))
+    cols = base[:, rng.integers(8, size=nsites)]
+    noise = rng.random((ntaxa, nsites)) > p_common
+    cols[noise] = rng.choice(list(alphabet), size=int(noise.sum()))
+    return ["".join(r) for r in cols]
+
+
+def shuffled_columns(seed, ntaxa, nsites, gap=0.05):
+    """Simulated DNA columns in a seeded random site order (so that first appearances are not
+    grouped by pattern)."""
+    rng = np.random.default_rng(seed)
+    tree = synth.random_tree(ntaxa, 0.05, seed + 1)
+    aln = synth.simulate(tree, synth.dna_gtr(rng), nsites, seed + 2, gap_frac=gap)
+    cols = synth.expand_patterns(aln)
+    return np.ascontiguousarray(cols[:, rng.permutation(cols.shape[1])])
+
+
+def test_restatement_matches_host_compressor():
+    """The restatement and the host compressor (synth.c) agree on encoded data."""
+    codes = shuffled_columns(1, 12, 3000)
+    host = synth.compress(codes, 4)
+    pat, w, sp, cc = ingest.build_patterns(codes, 4)
+    np.testing.assert_array_equal(host.patterns, pat)
+    np.testing.assert_array_equal(host.weights, w)
+    np.testing.assert_array_equal(pat[:, sp], codes)
+
+
+def test_const_char_cases():
+    # all unknown; one state with ambiguity around it; DNA ambiguity set; protein B; none
+    assert ingest.const_char([18, 18], 4) == 18
+    assert ingest.const_char([0, 8, 18], 4) == 0        # A, R = {A, G}, N
+    assert ingest.const_char([8, 8], 4) == 8            # R, R -> R
+    assert ingest.const_char([20, 23], 20) == 20        # B, X -> B
+    assert ingest.const_char([0, 1], 4) == 19
+    assert ingest.const_char([60, 61], 61) == 60
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,alphabet,common", [(4, DNA, "ACGT-RN"), (20, PROT, "ARNDCQ-BX")])
+def test_device_ingest_characters(gpu, n, alphabet, common):
+    rng = np.random.default_rng(7 + n)
+    seqs = random_chars(rng, 17, 5000, alphabet, common)
+    raw = np.array([np.frombuffer(s.encode(), np.uint8) for s in seqs])
+    pat, w, sp, cc = compress_alignment(raw, n)
+    rp, rw, rsp, rcc = ingest.build_patterns(ingest.encode(seqs, n), n)
+    np.testing.assert_array_equal(pat, rp)
+    np.testing.assert_array_equal(w, rw)
+    np.testing.assert_array_equal(sp, rsp)
+    np.testing.assert_array_equal(cc, rcc)
+
+
+@pytest.mark.gpu
+def test_device_ingest_codon_states(gpu):
+    rng = np.random.default_rng(9)
+    codes = rng.integers(0, 62, size=(9, 800)).astype(np.uint8)
+    codes[:, 400:] = codes[:, :400]          # every column appears twice
+    codes[:, 10] = 61                        # all unknown
+    codes[:, 11] = 5                         # constant
+    pat, w, sp, cc = compress_alignment(codes, 61, encoded=True)
+    rp, rw, rsp, rcc = ingest.build_patterns(codes, 61)
+    np.testing.assert_array_equal(pat, rp)
+    np.testing.assert_array_equal(w, rw)
+    np.testing.assert_array_equal(sp, rsp)
+    np.testing.assert_array_equal(cc, rcc)
+
+
+@pytest.mark.gpu
+def test_device_ingest_large_matches_host(gpu):
+    """512 taxa x 200,000 sites with 5% gaps: same patterns and weights as the host compressor,
+    and the site map reproduces the alignment."""
+    codes = shuffled_columns(3, 512, 200_000)
+    host = synth.compress(codes, 4)
+    pat, w, sp, cc = compress_alignment(codes, 4, encoded=True)
+    np.testing.assert_array_equal(pat, host.patterns)
+    np.testing.assert_array_equal(w, host.weights)
+    np.testing.assert_array_equal(pat[:, sp], codes)
+
+
+@pytest.mark.gpu
+def test_device_ingest_rejects_bad_character(gpu):
+    raw = np.frombuffer(b"ACGTACGT" + b"ACGJACGT", np.uint8).reshape(2, 8)
+    with pytest.raises(GemsError) as e:
+        compress_alignment(raw, 4)
+    assert e.value.status == 5
