@@ -94,6 +94,49 @@ def compress_alignment(seqs, nstates, encoded=False, device=0):
             cc[:k].copy())
 
 
+class Ingest:
+    """A compressed alignment kept on the device (gems_ingest_*): build it from sequences once,
+    read results back or load them straight into a session."""
+
+    def __init__(self, seqs, nstates, encoded=False, device=0):
+        a = np.ascontiguousarray(seqs, dtype=np.uint8)
+        self.ntaxa, self.nsites = a.shape
+        self.nstates = nstates
+        self.lib = _lib.gems()
+        self.handle = c_void_p()
+        npat = c_longlong()
+        _check(self.lib.gems_ingest_create(device, self.ntaxa, c_longlong(self.nsites), nstates,
+                                           _dptr(a), int(encoded), byref(self.handle),
+                                           byref(npat)), "gems_ingest_create")
+        self.npat = npat.value
+
+    def read(self):
+        """(patterns [ntaxa][npat], weights [npat], site_pattern [nsites], const_char [npat])."""
+        pat = np.empty((self.ntaxa, self.npat), np.uint8)
+        w = np.empty(self.npat, np.float64)
+        sp = np.empty(self.nsites, np.int32)
+        cc = np.empty(self.npat, np.uint8)
+        _check(self.lib.gems_ingest_read(self.handle, _dptr(pat), _dptr(w), _dptr(sp), _dptr(cc)),
+               "gems_ingest_read")
+        return pat, w, sp, cc
+
+    def to_session(self, session, p_invar=0.0, state_freq=None):
+        f = None if state_freq is None else _f64(state_freq)
+        _check(self.lib.gems_ingest_to_session(self.handle, session.handle, c_double(p_invar),
+                                               _dptr(f)), "gems_ingest_to_session")
+
+    def close(self):
+        if self.handle:
+            self.lib.gems_ingest_destroy(self.handle)
+            self.handle = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def full_traversal(tree):
     """Ops of a from-scratch traversal with one slot per internal node (slot = node - ntaxa),
     rooted at the branch between leaf 0 and its neighbour, and that branch: (ops, branch)."""

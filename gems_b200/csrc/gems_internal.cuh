@@ -160,6 +160,9 @@ struct Session {
   DevCtx ctx() const;
 };
 
+// tip bytes into a session (host or device source), checked on the device (session.cu)
+int load_tips(Session *s, const uint8_t *src, size_t src_pitch, cudaMemcpyKind kind);
+
 // brackets a launch with timing events when profiling is on
 int prof_begin(Session *s, int kernel, cudaEvent_t *a);
 int prof_end(Session *s, int kernel, cudaEvent_t a);

@@ -208,20 +208,73 @@ void build_lut(int n, uint8_t *lut) {
 }
 
 }  // namespace
+
+// ptn_invar of each pattern from its constant state (computePtnInvar,
+// tree/phylotreesse.cpp:549-612): p_invar times the frequency of the states it stands for
+struct FreqPack {
+  double f[64];
+};
+__global__ void k_ptn_invar(const uint8_t *cc, long long npat, int n, double p_invar,
+                            FreqPack fr, double *invar) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npat) return;
+  const int unk = n == 4 ? 18 : (n == 20 ? 23 : n);
+  const int c = cc[p];
+  double v = 0.0;
+  if (p_invar != 0.0 && c <= unk) {
+    if (c == unk) {
+      v = p_invar;
+    } else if (c < n) {
+      v = p_invar * fr.f[c];
+    } else {
+      const unsigned long long app = appearance(c, n);
+      double acc = 0.0;
+      for (int x = 0; x < n; x++)
+        if (app & (1ULL << x)) acc += fr.f[x];
+      v = acc * p_invar;
+    }
+  }
+  invar[p] = v;
+}
+__global__ void k_counts(const unsigned int *count, long long npat, double *w) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < npat) w[p] = (double)count[p];
+}
+
 }  // namespace gems
 
 using namespace gems;
 
-extern "C" int gems_compress_alignment(int device, int ntaxa, long long nsites, int nstates,
-                                       const uint8_t *seqs, int encoded, uint8_t *patterns,
-                                       double *weights, int *site_pattern, uint8_t *const_char,
-                                       long long *npat_out) {
-  if (ntaxa < 1 || nsites < 1 || nsites > 0x7FFFFFFFLL || !seqs || !patterns || !weights ||
-      !npat_out || (nstates != 4 && nstates != 20 && nstates != 61) ||
-      (!encoded && nstates == 61)) {
-    set_error("compress_alignment: bad arguments (characters are read for 4 and 20 states)");
+// compressed alignment kept on the device
+struct gems_ingest {
+  int device = 0, ntaxa = 0, nstates = 0;
+  long long nsites = 0, npat = 0;
+  uint8_t *d_pat = nullptr, *d_cc = nullptr;
+  unsigned int *d_count = nullptr;
+  int *d_sp = nullptr;
+  cudaStream_t st = nullptr;
+};
+
+extern "C" void gems_ingest_destroy(gems_ingest *g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  cudaFree(g->d_pat);
+  cudaFree(g->d_cc);
+  cudaFree(g->d_count);
+  cudaFree(g->d_sp);
+  if (g->st) cudaStreamDestroy(g->st);
+  delete g;
+}
+
+extern "C" int gems_ingest_create(int device, int ntaxa, long long nsites, int nstates,
+                                  const uint8_t *seqs, int encoded, gems_ingest **out,
+                                  long long *npat_out) {
+  if (!out || !npat_out || ntaxa < 1 || nsites < 1 || nsites > 0x7FFFFFFFLL || !seqs ||
+      (nstates != 4 && nstates != 20 && nstates != 61) || (!encoded && nstates == 61)) {
+    set_error("ingest: bad arguments (characters are read for 4 and 20 states)");
     return GEMS_ERR_BAD_ARG;
   }
+  *out = nullptr;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
     cudaGetLastError();
@@ -229,27 +282,29 @@ extern "C" int gems_compress_alignment(int device, int ntaxa, long long nsites, 
     return GEMS_ERR_NO_DEVICE;
   }
   GEMS_CUDA(cudaSetDevice(device));
+  gems_ingest *g = new gems_ingest();
+  g->device = device;
+  g->ntaxa = ntaxa;
+  g->nstates = nstates;
+  g->nsites = nsites;
   const size_t cells = (size_t)ntaxa * nsites;
   unsigned long long cap = 1;
   while (cap < 2ULL * (unsigned long long)nsites) cap <<= 1;
   const long long nblk = (nsites + 1023) / 1024;
-  uint8_t *d_raw = nullptr, *d_codes = nullptr, *d_lut = nullptr, *d_pat = nullptr,
-          *d_cc = nullptr;
+  // working buffers, freed before returning
+  uint8_t *d_raw = nullptr, *d_codes = nullptr, *d_lut = nullptr;
   unsigned long long *d_h = nullptr, *d_tab = nullptr, *d_min = nullptr, *d_bad = nullptr;
   long long *d_grp = nullptr, *d_pid = nullptr, *d_bsum = nullptr, *d_rep = nullptr;
-  unsigned int *d_flag = nullptr, *d_count = nullptr;
-  int *d_sp = nullptr;
-  cudaStream_t st = nullptr;
-  auto cleanup = [&]() {
-    cudaFree(d_raw); cudaFree(d_codes); cudaFree(d_lut); cudaFree(d_pat); cudaFree(d_cc);
-    cudaFree(d_h); cudaFree(d_tab); cudaFree(d_min); cudaFree(d_bad); cudaFree(d_grp);
-    cudaFree(d_pid); cudaFree(d_bsum); cudaFree(d_rep); cudaFree(d_flag); cudaFree(d_count);
-    cudaFree(d_sp);
-    if (st) cudaStreamDestroy(st);
+  unsigned int *d_flag = nullptr;
+  auto release = [&]() {
+    cudaFree(d_raw); cudaFree(d_codes); cudaFree(d_lut); cudaFree(d_h); cudaFree(d_tab);
+    cudaFree(d_min); cudaFree(d_bad); cudaFree(d_grp); cudaFree(d_pid); cudaFree(d_bsum);
+    cudaFree(d_rep); cudaFree(d_flag);
   };
   auto fail = [&](cudaError_t e, const char *what) {
     const int code = cuda_status(e, what);
-    cleanup();
+    release();
+    gems_ingest_destroy(g);
     return code;
   };
   cudaError_t e;
@@ -269,11 +324,12 @@ extern "C" int gems_compress_alignment(int device, int ntaxa, long long nsites, 
   ALLOC(d_bsum, sizeof(long long) * (nblk + 1));
   ALLOC(d_rep, sizeof(long long) * nsites);
   ALLOC(d_flag, sizeof(unsigned int) * nsites);
-  ALLOC(d_count, sizeof(unsigned int) * nsites);
-  ALLOC(d_sp, sizeof(int) * nsites);
+  ALLOC(g->d_count, sizeof(unsigned int) * nsites);
+  ALLOC(g->d_sp, sizeof(int) * nsites);
 #undef ALLOC
-  if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess)
+  if ((e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking)) != cudaSuccess)
     return fail(e, "cudaStreamCreate");
+  cudaStream_t st = g->st;
   const int T = 256;
   const unsigned gs = (unsigned)((nsites + T - 1) / T);
   unsigned long long bad = kEmpty;
@@ -290,9 +346,10 @@ extern "C" int gems_compress_alignment(int device, int ntaxa, long long nsites, 
         (e = cudaStreamSynchronize(st)))
       return fail(e, "ingest encode");
     if (bad != kEmpty) {
-      cleanup();
-      set_error("compress_alignment: unrecognised character in sequence " +
-                std::to_string(bad / nsites) + " at site " + std::to_string(bad % nsites + 1));
+      release();
+      gems_ingest_destroy(g);
+      set_error("ingest: unrecognised character in sequence " + std::to_string(bad / nsites) +
+                " at site " + std::to_string(bad % nsites + 1));
       return GEMS_ERR_BAD_ARG;
     }
   } else {
@@ -302,7 +359,7 @@ extern "C" int gems_compress_alignment(int device, int ntaxa, long long nsites, 
   if ((e = cudaMemsetAsync(d_tab, 0xFF, sizeof(unsigned long long) * cap, st)) ||
       (e = cudaMemsetAsync(d_grp, 0xFF, sizeof(long long) * nsites, st)) ||
       (e = cudaMemsetAsync(d_min, 0xFF, sizeof(unsigned long long) * cap, st)) ||
-      (e = cudaMemsetAsync(d_count, 0, sizeof(unsigned int) * nsites, st)))
+      (e = cudaMemsetAsync(g->d_count, 0, sizeof(unsigned int) * nsites, st)))
     return fail(e, "ingest memset");
   k_hash<<<gs, T, 0, st>>>(d_codes, ntaxa, nsites, d_h);
   k_insert<<<gs, T, 0, st>>>(d_codes, ntaxa, nsites, d_h, d_tab, d_min, cap - 1, d_grp);
@@ -310,31 +367,82 @@ extern "C" int gems_compress_alignment(int device, int ntaxa, long long nsites, 
   k_scan_block<<<(unsigned)nblk, 1024, 0, st>>>(d_flag, nsites, d_pid, d_bsum);
   k_scan_sums<<<1, 32, 0, st>>>(d_bsum, nblk, d_bsum + nblk);
   k_scan_add<<<(unsigned)nblk, 1024, 0, st>>>(d_pid, nsites, d_bsum);
-  k_assign<<<gs, T, 0, st>>>(d_grp, d_min, d_pid, nsites, d_sp, d_count, d_rep);
+  k_assign<<<gs, T, 0, st>>>(d_grp, d_min, d_pid, nsites, g->d_sp, g->d_count, d_rep);
   long long npat = 0;
   if ((e = cudaGetLastError()) ||
       (e = cudaMemcpyAsync(&npat, d_bsum + nblk, sizeof(npat), cudaMemcpyDeviceToHost, st)) ||
       (e = cudaStreamSynchronize(st)))
     return fail(e, "ingest compress");
-  if ((e = cudaMalloc((void **)&d_pat, (size_t)ntaxa * npat)) != cudaSuccess ||
-      (e = cudaMalloc((void **)&d_cc, (size_t)npat)) != cudaSuccess)
+  g->npat = npat;
+  if ((e = cudaMalloc((void **)&g->d_pat, (size_t)ntaxa * npat)) != cudaSuccess ||
+      (e = cudaMalloc((void **)&g->d_cc, (size_t)npat)) != cudaSuccess)
     return fail(e, "cudaMalloc patterns");
   const unsigned gp = (unsigned)((npat + T - 1) / T);
-  k_gather<<<gp, T, 0, st>>>(d_codes, ntaxa, nsites, npat, d_rep, d_pat);
-  k_const<<<gp, T, 0, st>>>(d_pat, ntaxa, npat, nstates, d_cc);
-  std::vector<unsigned int> cnt((size_t)npat);
-  if ((e = cudaGetLastError()) ||
-      (e = cudaMemcpyAsync(patterns, d_pat, (size_t)ntaxa * npat, cudaMemcpyDeviceToHost, st)) ||
-      (e = cudaMemcpyAsync(cnt.data(), d_count, sizeof(unsigned int) * npat,
-                           cudaMemcpyDeviceToHost, st)) ||
-      (site_pattern && (e = cudaMemcpyAsync(site_pattern, d_sp, sizeof(int) * nsites,
-                                            cudaMemcpyDeviceToHost, st))) ||
-      (const_char && (e = cudaMemcpyAsync(const_char, d_cc, (size_t)npat,
-                                          cudaMemcpyDeviceToHost, st))) ||
-      (e = cudaStreamSynchronize(st)))
-    return fail(e, "ingest download");
-  for (long long p = 0; p < npat; p++) weights[p] = (double)cnt[(size_t)p];
+  k_gather<<<gp, T, 0, st>>>(d_codes, ntaxa, nsites, npat, d_rep, g->d_pat);
+  k_const<<<gp, T, 0, st>>>(g->d_pat, ntaxa, npat, nstates, g->d_cc);
+  if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(st))) return fail(e, "ingest gather");
+  release();
+  *out = g;
   *npat_out = npat;
-  cleanup();
   return GEMS_OK;
+}
+
+extern "C" int gems_ingest_read(gems_ingest *g, uint8_t *patterns, double *weights,
+                                int *site_pattern, uint8_t *const_char) {
+  if (!g) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(g->device));
+  std::vector<unsigned int> cnt((size_t)g->npat);
+  if (patterns)
+    GEMS_CUDA(cudaMemcpyAsync(patterns, g->d_pat, (size_t)g->ntaxa * g->npat,
+                              cudaMemcpyDeviceToHost, g->st));
+  if (weights)
+    GEMS_CUDA(cudaMemcpyAsync(cnt.data(), g->d_count, sizeof(unsigned int) * g->npat,
+                              cudaMemcpyDeviceToHost, g->st));
+  if (site_pattern)
+    GEMS_CUDA(cudaMemcpyAsync(site_pattern, g->d_sp, sizeof(int) * g->nsites,
+                              cudaMemcpyDeviceToHost, g->st));
+  if (const_char)
+    GEMS_CUDA(cudaMemcpyAsync(const_char, g->d_cc, (size_t)g->npat, cudaMemcpyDeviceToHost,
+                              g->st));
+  GEMS_CUDA(cudaStreamSynchronize(g->st));
+  if (weights)
+    for (long long p = 0; p < g->npat; p++) weights[p] = (double)cnt[(size_t)p];
+  return GEMS_OK;
+}
+
+extern "C" int gems_ingest_to_session(gems_ingest *g, gems_session *s, double p_invar,
+                                      const double *state_freq) {
+  if (!g || !s || (p_invar != 0.0 && !state_freq) || p_invar < 0.0 || p_invar >= 1.0)
+    return GEMS_ERR_BAD_ARG;
+  if (s->desc.device != g->device || s->desc.ntaxa != g->ntaxa || s->desc.nptn != g->npat ||
+      s->desc.nstates != g->nstates) {
+    set_error("ingest_to_session: the session's device, taxa, patterns or states differ");
+    return GEMS_ERR_BAD_ARG;
+  }
+  GEMS_CUDA(cudaSetDevice(g->device));
+  GEMS_CUDA(cudaStreamSynchronize(g->st));  // the ingest's kernels have finished
+  FreqPack fr{};
+  for (int x = 0; x < g->nstates && state_freq; x++) fr.f[x] = state_freq[x];
+  const unsigned gp = (unsigned)((g->npat + 255) / 256);
+  k_counts<<<gp, 256, 0, s->stream>>>(g->d_count, g->npat, s->d_freq);
+  k_ptn_invar<<<gp, 256, 0, s->stream>>>(g->d_cc, g->npat, g->nstates, p_invar, fr, s->d_invar);
+  s->launches += 2;
+  GEMS_CUDA(cudaGetLastError());
+  s->theta_valid = false;
+  return load_tips(s, g->d_pat, (size_t)g->npat, cudaMemcpyDeviceToDevice);
+}
+
+extern "C" int gems_compress_alignment(int device, int ntaxa, long long nsites, int nstates,
+                                       const uint8_t *seqs, int encoded, uint8_t *patterns,
+                                       double *weights, int *site_pattern, uint8_t *const_char,
+                                       long long *npat_out) {
+  if (!patterns || !weights || !npat_out) return GEMS_ERR_BAD_ARG;
+  gems_ingest *g = nullptr;
+  long long npat = 0;
+  if (int st = gems_ingest_create(device, ntaxa, nsites, nstates, seqs, encoded, &g, &npat))
+    return st;
+  const int st = gems_ingest_read(g, patterns, weights, site_pattern, const_char);
+  gems_ingest_destroy(g);
+  if (!st) *npat_out = npat;
+  return st;
 }

@@ -292,6 +292,53 @@ static void copy_pattern_lh(Session *s, double *pattern_lh, double lnl_raw_finit
     if (!std::isfinite(pattern_lh[p])) pattern_lh[p] = 4.0 * kLogScaleThr;
 }
 
+// largest state byte of the uploaded tips (rows of P bytes, P a multiple of 64, the first nptn
+// of each row valid): a grid-stride loop over 16-byte words, per-byte maxima with __vmaxu4
+__global__ void k_tips_max(const uint8_t *__restrict__ tips, int P, int nptn, int ntaxa,
+                           unsigned int *out) {
+  const long long words_per_row = P / 16, total = words_per_row * ntaxa;
+  unsigned int m4 = 0;
+  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+       w += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(w % words_per_row) * 16;
+    uint4 v = reinterpret_cast<const uint4 *>(tips)[w];
+    if (col + 16 > nptn) {  // the row's padding bytes do not count
+      unsigned int b[4] = {v.x, v.y, v.z, v.w};
+      for (int j = 0; j < 16; j++)
+        if (col + j >= nptn) b[j / 4] &= ~(0xFFu << (8 * (j % 4)));
+      v = make_uint4(b[0], b[1], b[2], b[3]);
+    }
+    m4 = __vmaxu4(m4, __vmaxu4(__vmaxu4(v.x, v.y), __vmaxu4(v.z, v.w)));
+  }
+  unsigned int m = max(max(m4 & 0xFFu, (m4 >> 8) & 0xFFu), max((m4 >> 16) & 0xFFu, m4 >> 24));
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+// copies rows of nptn tip bytes (host or device, row stride src_pitch) into the session and
+// checks them on the device: on a bad byte the tips of the session are invalid (traversals are
+// refused) until the next successful load
+int load_tips(Session *s, const uint8_t *src, size_t src_pitch, cudaMemcpyKind kind) {
+  unsigned int *d_max = reinterpret_cast<unsigned int *>(s->d_flag) + 8;
+  GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), s->stream));
+  GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips, s->P, src, src_pitch, s->desc.nptn, s->desc.ntaxa, kind,
+                              s->stream));
+  k_tips_max<<<148 * 8, 256, 0, s->stream>>>(s->d_tips, s->P, s->desc.nptn, s->desc.ntaxa, d_max);
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  unsigned int mx = 0;
+  GEMS_CUDA(cudaMemcpyAsync(&mx, d_max, sizeof(mx), cudaMemcpyDeviceToHost, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  s->theta_valid = false;
+  if ((int)mx > s->unknown) {
+    s->tips_ok = false;
+    set_error("tip state byte out of range");
+    return GEMS_ERR_BAD_ARG;
+  }
+  s->tips_ok = true;
+  return GEMS_OK;
+}
+
 }  // namespace gems
 
 using namespace gems;
@@ -444,48 +491,10 @@ int gems_session_stream(gems_session *s, void **stream) {
   return GEMS_OK;
 }
 
-// largest state byte of the uploaded tips (rows of P bytes, the first nptn of each valid)
-__global__ void k_tips_max(const uint8_t *__restrict__ tips, int P, int nptn, int ntaxa,
-                           unsigned int *out) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;  // 4-byte word of a row
-  unsigned int m = 0;
-  for (int row = blockIdx.y; row < ntaxa; row += gridDim.y) {
-    if (4 * q < nptn) {
-      const uint32_t w = reinterpret_cast<const uint32_t *>(tips + (size_t)row * P)[q];
-#pragma unroll
-      for (int b = 0; b < 4; b++)
-        if (4 * q + b < nptn) m = max(m, (w >> (8 * b)) & 0xFFu);
-    }
-  }
-  m = __reduce_max_sync(0xffffffffu, m);
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
-}
-
 int gems_upload_tips(gems_session *s, const uint8_t *states) {
   if (!s || !states) return GEMS_ERR_BAD_ARG;
   GEMS_CUDA(cudaSetDevice(s->desc.device));
-  // the bytes are checked on the device after the copy: on a bad byte the tips of the session
-  // are invalid (traversals are refused) until the next successful upload
-  unsigned int *d_max = reinterpret_cast<unsigned int *>(s->d_flag) + 8;
-  GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), s->stream));
-  GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips, s->P, states, s->desc.nptn, s->desc.nptn,
-                              s->desc.ntaxa, cudaMemcpyHostToDevice, s->stream));
-  const int words = (s->desc.nptn + 3) / 4;
-  const dim3 grid((words + 255) / 256, s->desc.ntaxa < 65535 ? s->desc.ntaxa : 65535);
-  k_tips_max<<<grid, 256, 0, s->stream>>>(s->d_tips, s->P, s->desc.nptn, s->desc.ntaxa, d_max);
-  s->launches++;
-  GEMS_CUDA(cudaGetLastError());
-  unsigned int mx = 0;
-  GEMS_CUDA(cudaMemcpyAsync(&mx, d_max, sizeof(mx), cudaMemcpyDeviceToHost, s->stream));
-  GEMS_CUDA(cudaStreamSynchronize(s->stream));
-  s->theta_valid = false;
-  if ((int)mx > s->unknown) {
-    s->tips_ok = false;
-    set_error("tip state byte out of range");
-    return GEMS_ERR_BAD_ARG;
-  }
-  s->tips_ok = true;
-  return GEMS_OK;
+  return load_tips(s, states, s->desc.nptn, cudaMemcpyHostToDevice);
 }
 
 int gems_upload_patterns(gems_session *s, const double *ptn_freq, const double *ptn_invar) {

@@ -218,6 +218,20 @@ int gems_profile_read(gems_session *s, int kernel_id, double *total_ms, long lon
 int gems_compress_alignment(int device, int ntaxa, long long nsites, int nstates,
                             const uint8_t *seqs, int encoded, uint8_t *patterns, double *weights,
                             int *site_pattern, uint8_t *const_char, long long *npat);
+/* The same ingest kept on the device: gems_ingest_create encodes and compresses (the
+ * sequences cross to the GPU once), gems_ingest_read copies any of the results back (NULL to
+ * skip), gems_ingest_to_session loads the patterns into a session created with nptn = npat
+ * (tips copied on the device and checked as gems_upload_tips does, weights, and ptn_invar from
+ * the constant states: computePtnInvar, tree/phylotreesse.cpp:549-612, with p_invar and the
+ * model's state frequencies; p_invar = 0 for no +I). */
+typedef struct gems_ingest gems_ingest;
+int gems_ingest_create(int device, int ntaxa, long long nsites, int nstates, const uint8_t *seqs,
+                       int encoded, gems_ingest **out, long long *npat);
+int gems_ingest_read(gems_ingest *g, uint8_t *patterns, double *weights, int *site_pattern,
+                     uint8_t *const_char);
+int gems_ingest_to_session(gems_ingest *g, gems_session *s, double p_invar,
+                           const double *state_freq);
+void gems_ingest_destroy(gems_ingest *g);
 /* Measured compute peaks of a device (no counterpart in the reference: the denominators of the
  * compute rooflines): FP64 and FP32 FMA throughput of the CUDA cores and the dense TF32 rate of
  * the tcgen05 tensor cores, in TFLOP/s.  Takes a few tens of milliseconds. */

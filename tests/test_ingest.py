@@ -99,3 +99,30 @@ def test_device_ingest_rejects_bad_character(gpu):
     with pytest.raises(GemsError) as e:
         compress_alignment(raw, 4)
     assert e.value.status == 5
+
+
+@pytest.mark.gpu
+def test_ingest_to_session_lnl_matches_oracle(gpu):
+    """Sequences -> device patterns -> session (tips, weights and +I terms loaded on the device):
+    the lnL equals the oracle's on the same patterns, constant states and p_invar."""
+    from gems_b200 import Ingest, PhyloTree, Session
+    from oracle import oracle as orc
+    codes = shuffled_columns(21, 20, 6000)
+    rng = np.random.default_rng(22)
+    amb = rng.random(codes.shape) < 0.02
+    codes[amb] = rng.choice([8, 13, 7], size=int(amb.sum()))  # R, Y, M
+    rng = np.random.default_rng(23)
+    model = synth.dna_gtr(rng, 4, 0.5)
+    model.p_invar = 0.2
+    tree = synth.random_tree(20, 0.1, 24)
+    ing = Ingest(codes, 4, encoded=True)
+    pat, w, sp, cc = ing.read()
+    s = Session(20, ing.npat, 4, 4, 18)
+    ing.to_session(s, model.p_invar, model.freq)
+    s.set_model(model.eval, model.evec, model.inv_evec, model.rates, model.props)
+    gt = PhyloTree(s, tree.eu, tree.ev, tree.length)
+    aln = synth.Alignment(20, 4, int(w.sum()), pat, w)
+    ot = orc.OracleTree(tree, model, aln, const_char=cc, p_invar=model.p_invar)
+    lo, lg = ot.computeLikelihood(), gt.computeLikelihood()
+    assert abs(lg - lo) <= 1e-9 * abs(lo), (lg, lo)
+    ing.close()
