@@ -468,6 +468,53 @@ def codon_batch_block(local, nmodels=64, reps=3):
     return out
 
 
+def ingest_block(aln, local, reps=3):
+    """Alignment ingest of the headline alignment (512 taxa x 1,000,000 sites): from host
+    sequences to a session ready to evaluate, by the device path (sequences cross once; encoding,
+    compression, tips, weights and +I terms on the GPU) and by the host path (host compressor, C
+    with OpenMP hashing, then the uploads).  Both must produce the same patterns and weights."""
+    from gems_b200 import Ingest, Session
+    cols = synth.expand_patterns(aln)
+    ntaxa, n = cols.shape[0], aln.nstates
+
+    def host_path():
+        h = synth.compress(cols, n)
+        s = Session(ntaxa, h.npat, n, 4, 1, "mixed", "norm", local)  # loading only
+        s.upload_tips(h.patterns)
+        s.upload_patterns(h.weights)
+        return h, s
+
+    def device_path():
+        g = Ingest(cols, n, encoded=True, device=local)
+        s = Session(ntaxa, g.npat, n, 4, 1, "mixed", "norm", local)
+        g.to_session(s)
+        return g, s
+
+    h, s = host_path()  # warm-up
+    s.close()
+    g, s = device_path()
+    pat, w, _, _ = g.read()
+    same = bool(np.array_equal(pat, h.patterns) and np.array_equal(w, h.weights))
+    g.close()
+    s.close()
+    t = {}
+    for name, fn in (("host", host_path), ("device", device_path)):
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            a, sess = fn()
+            sess.sync()
+            sess.close()
+            if name == "device":
+                a.close()
+        t[name] = (time.perf_counter() - t0) / reps
+    return {"ntaxa": int(ntaxa), "sites": int(cols.shape[1]), "npat": int(len(w)),
+            "device_path_ms": t["device"] * 1e3, "host_path_ms": t["host"] * 1e3,
+            "host_threads": os.cpu_count(), "speedup_vs_host": t["host"] / t["device"],
+            "identical_to_host": same,
+            "path": "host sequences -> session with tips, weights and +I terms loaded "
+                    "(creation of a one-slot session included in both)"}
+
+
 def serving_block(local, nsess=48, nreq=800, rate=250.0):
     """The serving loop on a seeded stream: sessions of 8-256 taxa and 500-50,000 sites
     (log-uniform), 4/20/61 states, 1/4/8 categories, FP64/mixed; NNI + 5-branch Newton + lnL
@@ -632,6 +679,7 @@ def main():
     if rank == 0 and not args.no_extras and args.config == "dna512":
         line["protein20"] = protein_comparison(args, local, peaks)
         line["codon64"] = codon_batch_block(local, args.codon_models)
+        line["ingest"] = ingest_block(aln, local)
         line["serving"] = serving_block(local)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tree, model, aln)
