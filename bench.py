@@ -515,20 +515,33 @@ def ingest_block(aln, local, reps=3):
                     "(creation of a one-slot session included in both)"}
 
 
-def serving_block(local, nsess=48, nreq=800, rate=250.0):
+def serving_block(local, nsess=48, nreq=800, load=0.7):
     """The serving loop on a seeded stream: sessions of 8-256 taxa and 500-50,000 sites
     (log-uniform), 4/20/61 states, 1/4/8 categories, FP64/mixed; NNI + 5-branch Newton + lnL
-    per request; Poisson arrivals at `rate` requests/s."""
+    per request.  Two passes over the same stream, sessions opened before each: every request
+    queued at once gives the capacity; Poisson arrivals at `load` x capacity give the request
+    latency.  Session open times (create, upload, first full lnL) are reported apart."""
     from gems_b200 import serve
-    specs, reqs = serve.make_stream(nsess, nreq, rate, seed=5, taxa=(8, 256), sites=(500, 50_000))
+    kw = dict(seed=5, taxa=(8, 256), sites=(500, 50_000))
+    specs, reqs = serve.make_stream(nsess, nreq, 1.0, **kw)
     cases = {sp.sid: serve.build_case(sp) for sp in specs}
     srv = serve.Server(device=local, workers=16)
-    records, wall = srv.run(specs, cases, reqs)
+    records, wall = srv.run(specs, cases, [(0.0, sid) for _, sid in reqs], preopen=True)
+    cap = serve.summarize(records, wall, specs, cases)
+    opened = np.array(srv.open_ms)
+    rate = load * cap["throughput_req_s"]
+    _, reqs = serve.make_stream(nsess, nreq, rate, **kw)
+    records, wall = srv.run(specs, cases, reqs, preopen=True)
     out = serve.summarize(records, wall, specs, cases)
-    out.update({"sessions": nsess, "offered_rate_req_s": rate, "workers": 16,
+    out.update({"capacity_req_s": cap["throughput_req_s"], "capacity_failed": cap["failed"],
+                "offered_rate_req_s": rate, "load": load,
+                "session_open_ms": {"p50": float(np.percentile(opened, 50)),
+                                    "p99": float(np.percentile(opened, 99)),
+                                    "max": float(opened.max())},
+                "sessions": nsess, "workers": 16,
                 "stream": "seeded; taxa 8-256, sites 500-50,000 (log-uniform), states {4,20,61}, "
                           "categories {1,4,8}, fp64/mixed; request = NNI + Newton on the 5 "
-                          "branches around it + lnL"})
+                          "branches around it + lnL; latency at Poisson arrivals, sessions open"})
     return out
 
 

@@ -441,10 +441,10 @@ class PhyloTree:
         return out.value
 
     def getBranchLength(self, u, v):
-        for i, (a, b) in enumerate(zip(self.eu, self.ev)):
-            if (a == u and b == v) or (a == v and b == u):
-                return float(self.getBranchLengths()[i])
-        raise KeyError((u, v))
+        i = np.nonzero(((self.eu == u) & (self.ev == v)) | ((self.eu == v) & (self.ev == u)))[0]
+        if len(i) == 0:
+            raise KeyError((u, v))
+        return float(self.getBranchLengths()[i[0]])
 
     def doNNI(self, u, v, a, b):
         """Swap subtree a (at u) with subtree b (at v) across the internal branch (u, v)."""
@@ -453,13 +453,9 @@ class PhyloTree:
                "get_edges")
 
     def neighbors(self, u):
-        out = []
-        for a, b in zip(self.eu, self.ev):
-            if a == u:
-                out.append(int(b))
-            elif b == u:
-                out.append(int(a))
-        return out
+        """Nodes adjacent to u, in edge order."""
+        i = np.nonzero((self.eu == u) | (self.ev == u))[0]
+        return np.where(self.eu[i] == u, self.ev[i], self.eu[i]).tolist()
 
     def computeFuncDerv(self, node1, node2, value, new_branch=False):
         f, df = c_double(), c_double()

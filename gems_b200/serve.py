@@ -74,7 +74,8 @@ def open_session(spec, case, device=0):
 def nni5(gt: PhyloTree, ntaxa: int, rng: np.random.Generator):
     """One request: a random NNI on an internal branch, Newton on the 5 branches around it,
     then lnL.  Returns (lnL, branches optimised)."""
-    internal = [(int(a), int(b)) for a, b in zip(gt.eu, gt.ev) if a >= ntaxa and b >= ntaxa]
+    mask = (gt.eu >= ntaxa) & (gt.ev >= ntaxa)
+    internal = list(zip(gt.eu[mask].tolist(), gt.ev[mask].tolist()))
     u, v = internal[int(rng.integers(len(internal)))]
     nu = [x for x in gt.neighbors(u) if x != v]
     nv = [x for x in gt.neighbors(v) if x != u]
@@ -107,9 +108,12 @@ class Server:
         self.budget = int(0.85 * free) if budget_bytes is None else int(budget_bytes)
         self.workers = workers
 
-    def run(self, specs, cases, requests):
-        """requests: list of (arrival_s, sid) in arrival order.  Returns per-request records
-        and counters."""
+    def run(self, specs, cases, requests, preopen=False):
+        """requests: list of (arrival_s, sid) in arrival order, arrival times counted from the
+        start of the request stream.  A session opens when its first request arrives; with
+        `preopen`, the sessions that fit the budget are opened (in first-arrival order) before
+        the stream starts, as a server does with the datasets it holds.  Session open times are
+        kept in self.open_ms.  Returns the per-request records and the stream's wall time."""
         lock = threading.Condition()
         npat = {s.sid: cases[s.sid][2].npat for s in specs}
         fp = {s.sid: s.footprint(npat[s.sid]) for s in specs}
@@ -122,10 +126,52 @@ class Server:
         busy = set()
         waiting_admit = collections.deque()
         records = [None] * len(requests)
-        t0 = time.perf_counter()
+        self.open_ms = []
         for sid in fp:
             if fp[sid] > self.budget:
                 state["rejected"].add(sid)
+
+        def open_one(sid):
+            t = time.perf_counter()
+            try:
+                gt = open_session(spec_of[sid], cases[sid], self.device)
+                gt.computeLikelihood()
+            except GemsError:
+                return None
+            with lock:
+                self.open_ms.append(1e3 * (time.perf_counter() - t))
+            return gt
+
+        if preopen:
+            queue = collections.deque()
+            for sid in dict.fromkeys(sid for _, sid in requests):
+                if sid in state["rejected"]:
+                    continue
+                if state["used"] + fp[sid] > self.budget:
+                    break
+                state["used"] += fp[sid]
+                queue.append(sid)
+
+            def opener():
+                while True:
+                    with lock:
+                        if not queue:
+                            return
+                        sid = queue.popleft()
+                    gt = open_one(sid)
+                    with lock:
+                        if gt is None:
+                            state["rejected"].add(sid)
+                            state["used"] -= fp[sid]
+                        else:
+                            open_sess[sid] = gt
+
+            openers = [threading.Thread(target=opener) for _ in range(self.workers)]
+            for th in openers:
+                th.start()
+            for th in openers:
+                th.join()
+        t0 = time.perf_counter()
 
         def admit_locked():
             # admit waiting sessions in arrival order while they fit
@@ -177,11 +223,7 @@ class Server:
                             break
                         lock.wait(0.05)
                 if to_open is not None:
-                    try:
-                        gt = open_session(spec_of[to_open], cases[to_open], self.device)
-                        gt.computeLikelihood()
-                    except GemsError:
-                        gt = None
+                    gt = open_one(to_open)
                     with lock:
                         if gt is None:
                             state["rejected"].add(to_open)
