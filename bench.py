@@ -12,7 +12,8 @@ pattern-weighted sum.  Both precision forms are timed in the same run:
 `value` is the mixed form's site-partial updates/s when its lnL is within 1e-6 relative of
 the FP64 lnL of the same run (reported as `lnl_rel_err_mixed`), else the FP64 form's.
 `e2e` runs the same step through the public PhyloTree API from pinned host buffers (tips and
-weights up, pattern lnL down).  Timing uses CUDA events on the session's stream; the partial
+weights up, pattern lnL down; computeLikelihoodFromHost, the tip upload overlapped with the
+traversal in pattern chunks).  Timing uses CUDA events on the session's stream; the partial
 buffers (65 GB FP64, 33 GB mixed) exceed L2 many times over, so no flush is needed.
 
 Also reported (same run): one Newton branch optimisation (optimizeOneBranch) per branch; the
@@ -561,6 +562,8 @@ def main():
                     help="run only this block of the line and print it (profiling runs)")
     ap.add_argument("--codon-models", type=int, default=64,
                     help="candidate codon models in the batched block (small for profiling)")
+    ap.add_argument("--e2e-chunks", type=int, default=16,
+                    help="pattern chunks of the overlapped tip upload in the e2e measurement")
     ap.add_argument("--no-tc", action="store_true",
                     help="20-state mixed traversal on CUDA cores instead of tcgen05")
     args = ap.parse_args()
@@ -645,7 +648,8 @@ def main():
     s = gt.session
     pin_pat = torch.empty(aln.patterns.shape, dtype=torch.uint8, pin_memory=True)
     pin_w = torch.empty(aln.weights.shape, dtype=torch.float64, pin_memory=True)
-    pat_host, w_host = pin_pat.numpy(), pin_w.numpy()
+    pin_plh = torch.empty(P, dtype=torch.float64, pin_memory=True)
+    pat_host, w_host, plh_host = pin_pat.numpy(), pin_w.numpy(), pin_plh.numpy()
     pat_host[:] = aln.patterns
     w_host[:] = aln.weights
     h2d = pat_host.nbytes + w_host.nbytes
@@ -655,10 +659,7 @@ def main():
     torch.cuda.synchronize()
     e2.record(stream)
     for _ in range(args.steps):
-        s.upload_tips(pat_host)
-        s.upload_patterns(w_host)
-        gt.clearAllPartialLH()
-        gt.computeLikelihood(pattern_lh=True)
+        gt.computeLikelihoodFromHost(pat_host, w_host, chunks=args.e2e_chunks, pattern_lh=plh_host)
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3) / args.steps
@@ -681,7 +682,8 @@ def main():
         "lnl_evals_per_s": 1.0 / (H["ms_per_step"] * 1e-3), "lnl": H["lnl"],
         "gpu_launches": H["gpu_launches"],
         "e2e": {"value": world * nops * P / (ms_e2e * 1e-3), "unit": "site-partial updates/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
+                "upload_chunks": args.e2e_chunks},
         "roofline": H["roofline"],
         "forms": forms,
         "clocks": clk.summary(),

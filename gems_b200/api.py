@@ -409,6 +409,28 @@ class PhyloTree:
                "computeLikelihood")
         return (out.value, plh) if pattern_lh else out.value
 
+    def computeLikelihoodFromHost(self, states, ptn_freq, ptn_invar=None, chunks=16,
+                                  pattern_lh=False):
+        """computeLikelihood on new tip states [ntaxa][nptn], pattern weights and +I terms:
+        the tip upload overlaps the traversal in up to `chunks` pattern chunks (pinned host
+        arrays needed for the overlap).  pattern_lh: False, True, or a float64 array [nptn]
+        to fill (pinned for the fastest copy)."""
+        st = np.ascontiguousarray(states, dtype=np.uint8)
+        assert st.shape == (self.session.ntaxa, self.session.nptn)
+        f = _f64(ptn_freq)
+        iv = None if ptn_invar is None else _f64(ptn_invar)
+        out = c_double()
+        if isinstance(pattern_lh, np.ndarray):
+            assert pattern_lh.dtype == np.float64 and pattern_lh.shape == (self.session.nptn,)
+            assert pattern_lh.flags.c_contiguous
+            plh = pattern_lh
+        else:
+            plh = np.zeros(self.session.nptn) if pattern_lh else None
+        _check(self.lib.gems_tree_compute_likelihood_from_host(
+            self.handle, _dptr(st), _dptr(f), _dptr(iv), int(chunks), byref(out), _dptr(plh)),
+            "computeLikelihoodFromHost")
+        return (out.value, plh) if plh is not None else out.value
+
     def computeLikelihoodBranch(self, node, dad, pattern_lh=False):
         out = c_double()
         plh = np.zeros(self.session.nptn) if pattern_lh else None

@@ -135,6 +135,13 @@ struct Session {
   static constexpr int kMaxBatch = 128;
   TcJob *d_jobs = nullptr;
   TcJob *h_jobs = nullptr;
+  // streamed evaluation from host data (gems_branch_lnl_from_host): a copy stream, one event
+  // per pattern chunk and a pinned word for the tip check, created on first use
+  static constexpr int kMaxChunks = 64;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t start_ev = nullptr;
+  cudaEvent_t chunk_ev[kMaxChunks] = {};
+  unsigned int *h_tipmax = nullptr;
   // pinned host staging
   DevOp *h_ops = nullptr;
   double *h_result = nullptr;
@@ -197,7 +204,10 @@ int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool st
 // factored whole-traversal kernels for 4 and 20 states (kernels_traverse.cu)
 bool traverse_v2_supported(const Session *s);
 int launch_prep_ops_v2(Session *s, int nops);
-int launch_traverse_v2(Session *s, int nops);
+// patterns [p0, p1) of the traversal (p1 <= P); tip state bytes are clamped to STATE_UNKNOWN
+int launch_traverse_v2(Session *s, int nops, int p0, int p1);
+// patterns that one wave of resident blocks of the traversal kernel covers (0 if unknown)
+int traverse_v2_wave_patterns(const Session *s);
 // tcgen05 split-TF32 traversal for 20 states (kernels_tc.cu)
 size_t tc20_op_floats(int ncat, int unknown);
 bool tc20_supported(const Session *s);

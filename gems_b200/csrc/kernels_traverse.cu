@@ -105,7 +105,7 @@ __device__ __forceinline__ void msg_f64(const DevCtx &c, const EigPack<N> &E, in
                                         double (&v)[N], int &s) {
   const int C = c.C;
   if (kind == GEMS_CHILD_TIP) {
-    const int st = c.tips[(size_t)id * c.P + p];
+    const int st = min((int)c.tips[(size_t)id * c.P + p], c.unknown);
     const double *lt = leaf + (size_t)st * c.block + gl;
 #pragma unroll
     for (int x = 0; x < N; x++) v[x] = __ldg(lt + x * C);
@@ -144,11 +144,12 @@ template <int N, bool SAFE>
 __global__ void __launch_bounds__(kThreads) k_traverse_f64(DevCtx c, const DevOp *__restrict__ ops,
                                                            int nops,
                                                            const double *__restrict__ tab,
-                                                           size_t stride, const EigPack<N> E) {
+                                                           size_t stride, const EigPack<N> E,
+                                                           int p0, int p1) {
   const int G = c.G;
   const int gl = threadIdx.x & (G - 1);
-  const long p = ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const bool act = p < c.P && gl < c.C;
+  const long p = p0 + ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool act = p < p1 && gl < c.C;
   const int C = c.C, blk = c.block;
   double *part = static_cast<double *>(c.partials);
   __shared__ int4 s_ops[kOpChunk];
@@ -250,7 +251,7 @@ __device__ __forceinline__ void msg_mix(const DevCtx &c, int kind, int id,
                                         float (&v)[N], int &s) {
   const int C = c.C;
   if (kind == GEMS_CHILD_TIP) {
-    const int st = c.tips[(size_t)id * c.P + p];
+    const int st = min((int)c.tips[(size_t)id * c.P + p], c.unknown);
     const float *lt = leaf + (size_t)st * c.block + gl;
 #pragma unroll
     for (int x = 0; x < N; x++) v[x] = __ldg(lt + x * C);
@@ -305,11 +306,11 @@ __device__ __forceinline__ void msg_mix(const DevCtx &c, int kind, int id,
 template <int N, bool SAFE>
 __global__ void __launch_bounds__(kThreads, N == 4 ? 8 : 1) k_traverse_mix(DevCtx c, const DevOp *__restrict__ ops,
                                                            int nops, const float *__restrict__ tab,
-                                                           size_t stride_f) {
+                                                           size_t stride_f, int p0, int p1) {
   const int G = c.G;
   const int gl = threadIdx.x & (G - 1);
-  const long p = ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const bool act = p < c.P && gl < c.C;
+  const long p = p0 + ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool act = p < p1 && gl < c.C;
   const int C = c.C;
   const size_t nnC = (size_t)N * N * C;
   float *part = static_cast<float *>(c.partials);
@@ -362,13 +363,13 @@ __global__ void __launch_bounds__(kThreads, N == 4 ? 8 : 1) k_traverse_mix(DevCt
   }
 }
 
-inline int grid_for(const Session *s) {
-  const long threads = (long)s->P * s->G;
+inline int grid_for(const Session *s, int p0, int p1) {
+  const long threads = (long)(p1 - p0) * s->G;
   return (int)((threads + kThreads - 1) / kThreads);
 }
 
 template <int N>
-int launch_f64(Session *s, int nops) {
+int launch_f64(Session *s, int nops, int p0, int p1) {
   DevCtx c = s->ctx();
   EigPack<N> E;
   if (s->h_evec.size() != (size_t)N * N || s->h_inv.size() != (size_t)N * N) {
@@ -379,14 +380,14 @@ int launch_f64(Session *s, int nops) {
     E.evec[i] = s->h_evec[i];
     E.inv[i] = s->h_inv[i];
   }
-  const int grid = grid_for(s);
+  const int grid = grid_for(s, p0, p1);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   if (safe)
     k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                               s->op_stride, E);
+                                                               s->op_stride, E, p0, p1);
   else
     k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                                s->op_stride, E);
+                                                                s->op_stride, E, p0, p1);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   return GEMS_OK;
@@ -415,27 +416,45 @@ int launch_prep_ops_v2(Session *s, int nops) {
   return GEMS_OK;
 }
 
-int launch_traverse_v2(Session *s, int nops) {
-  if (nops <= 0) return GEMS_OK;
+int traverse_v2_wave_patterns(const Session *s) {
+  const bool mixed = s->desc.precision == GEMS_PREC_MIXED;
+  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  const bool four = s->desc.nstates == 4;
+  const void *fn =
+      mixed ? (four ? (safe ? (const void *)k_traverse_mix<4, true> : (const void *)k_traverse_mix<4, false>)
+                    : (safe ? (const void *)k_traverse_mix<20, true> : (const void *)k_traverse_mix<20, false>))
+            : (four ? (safe ? (const void *)k_traverse_f64<4, true> : (const void *)k_traverse_f64<4, false>)
+                    : (safe ? (const void *)k_traverse_f64<20, true> : (const void *)k_traverse_f64<20, false>));
+  int nsm = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->desc.device) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * nsm * (kThreads / s->G);
+}
+
+int launch_traverse_v2(Session *s, int nops, int p0, int p1) {
+  if (nops <= 0 || p1 <= p0) return GEMS_OK;
   cudaEvent_t ev0;
   if (int st = prof_begin(s, 0, &ev0)) return st;
   int st = GEMS_OK;
   if (s->desc.precision == GEMS_PREC_MIXED) {
     DevCtx c = s->ctx();
-    const int grid = grid_for(s);
+    const int grid = grid_for(s, p0, p1);
     const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
     const float *tab = reinterpret_cast<const float *>(s->d_opmats);
     if (s->desc.nstates == 4) {
-      if (safe) k_traverse_mix<4, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
-      else k_traverse_mix<4, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+      if (safe) k_traverse_mix<4, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
+      else k_traverse_mix<4, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
     } else {
-      if (safe) k_traverse_mix<20, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
-      else k_traverse_mix<20, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride);
+      if (safe) k_traverse_mix<20, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
+      else k_traverse_mix<20, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
     }
     s->launches++;
     GEMS_CUDA(cudaGetLastError());
   } else {
-    st = s->desc.nstates == 4 ? launch_f64<4>(s, nops) : launch_f64<20>(s, nops);
+    st = s->desc.nstates == 4 ? launch_f64<4>(s, nops, p0, p1) : launch_f64<20>(s, nops, p0, p1);
   }
   if (st) return st;
   return prof_end(s, 0, ev0);

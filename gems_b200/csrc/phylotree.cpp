@@ -2,6 +2,7 @@
 // kernel set of gems_b200.h.  The tree owns topology, branch lengths and cache flags; the
 // device session owns every buffer.  Each method names the reference member it restates
 // (paths relative to the IQ-TREE 3 source tree).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -302,6 +303,26 @@ struct Tree {
     const int v = adj[cur_u * 3 + cur_k];
     return lh_branch(v, cur_u, lnl, pattern_lh);
   }
+
+  // computeLikelihood on new data: every partial is stale, the session's tips, weights and +I
+  // terms are replaced, and the upload overlaps the traversal (gems_branch_lnl_from_host)
+  int compute_likelihood_from_host(const uint8_t *states, const double *ptn_freq,
+                                   const double *ptn_invar, int nchunks, double *lnl,
+                                   double *pattern_lh) {
+    std::fill(computed.begin(), computed.end(), 0);
+    theta_computed = false;
+    if (cur_u < 0) {
+      std::vector<int> h(nnode, 0);
+      cur_u = far_leaf(0, -1, h);
+      cur_k = 0;
+    }
+    int node = adj[cur_u * 3 + cur_k], dad = cur_u;
+    gems_branch br = branch(node, dad);
+    const int st = gems_branch_lnl_from_host(s, states, ptn_freq, ptn_invar, ops.data(),
+                                             (int)ops.size(), &br, nchunks, lnl, pattern_lh);
+    if (st) std::fill(computed.begin(), computed.end(), 0);
+    return st;
+  }
 };
 
 }  // namespace
@@ -411,6 +432,13 @@ int gems_tree_clear_all_partial_lh(gems_tree *t) {
 int gems_tree_compute_likelihood(gems_tree *t, double *lnl, double *pattern_lh) {
   if (!t || !lnl) return GEMS_ERR_BAD_ARG;
   return t->compute_likelihood(lnl, pattern_lh);
+}
+
+int gems_tree_compute_likelihood_from_host(gems_tree *t, const uint8_t *states,
+                                           const double *ptn_freq, const double *ptn_invar,
+                                           int nchunks, double *lnl, double *pattern_lh) {
+  if (!t || !states || !ptn_freq || !lnl || nchunks < 1) return GEMS_ERR_BAD_ARG;
+  return t->compute_likelihood_from_host(states, ptn_freq, ptn_invar, nchunks, lnl, pattern_lh);
 }
 
 int gems_tree_compute_likelihood_branch(gems_tree *t, int node, int dad, double *lnl,

@@ -1,4 +1,5 @@
 // session.cu -- C-ABI of the kernel set: device sessions, uploads, model, kernel calls.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -190,6 +191,14 @@ static void free_session(Session *s) {
   cudaFree(s->d_jobs);
   cudaFreeHost(s->h_jobs);
   cudaFreeHost(s->h_result);
+  if (s->copy_stream) {
+    cudaStreamSynchronize(s->copy_stream);
+    cudaStreamDestroy(s->copy_stream);
+  }
+  if (s->start_ev) cudaEventDestroy(s->start_ev);
+  for (cudaEvent_t e : s->chunk_ev)
+    if (e) cudaEventDestroy(e);
+  cudaFreeHost(s->h_tipmax);
   if (s->stream) {
     cudaStreamSynchronize(s->stream);
     prof_collect(s);
@@ -270,7 +279,7 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
     if ((st = launch_traverse_tc61(s, nops))) return st;
   } else if (traverse_v2_supported(s)) {
     if ((st = launch_prep_ops_v2(s, nops))) return st;
-    if ((st = launch_traverse_v2(s, nops))) return st;
+    if ((st = launch_traverse_v2(s, nops, 0, s->P))) return st;
   } else if (s->desc.precision == GEMS_PREC_MIXED) {
     if ((st = launch_prep_ops_mixed(s, nops))) return st;
     if ((st = launch_traverse_mixed(s, nops))) return st;
@@ -292,16 +301,18 @@ static void copy_pattern_lh(Session *s, double *pattern_lh, double lnl_raw_finit
     if (!std::isfinite(pattern_lh[p])) pattern_lh[p] = 4.0 * kLogScaleThr;
 }
 
-// largest state byte of the uploaded tips (rows of P bytes, P a multiple of 64, the first nptn
-// of each row valid): a grid-stride loop over 16-byte words, per-byte maxima with __vmaxu4
-__global__ void k_tips_max(const uint8_t *__restrict__ tips, int P, int nptn, int ntaxa,
-                           unsigned int *out) {
-  const long long words_per_row = P / 16, total = words_per_row * ntaxa;
+// largest state byte of the uploaded tips in columns [c0, c1) (rows of P bytes, P a multiple of
+// 64, the first nptn of each row valid; c0 and c1 multiples of 16): a grid-stride loop over
+// 16-byte words, per-byte maxima with __vmaxu4
+__global__ void k_tips_max(const uint8_t *__restrict__ tips, int P, int nptn, int ntaxa, int c0,
+                           int c1, unsigned int *out) {
+  const long long words_per_row = (c1 - c0) / 16, total = words_per_row * ntaxa;
   unsigned int m4 = 0;
   for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
        w += (long long)gridDim.x * blockDim.x) {
-    const int col = (int)(w % words_per_row) * 16;
-    uint4 v = reinterpret_cast<const uint4 *>(tips)[w];
+    const long long row = w / words_per_row;
+    const int col = c0 + (int)(w - row * words_per_row) * 16;
+    uint4 v = *reinterpret_cast<const uint4 *>(tips + row * P + col);
     if (col + 16 > nptn) {  // the row's padding bytes do not count
       unsigned int b[4] = {v.x, v.y, v.z, v.w};
       for (int j = 0; j < 16; j++)
@@ -323,7 +334,8 @@ int load_tips(Session *s, const uint8_t *src, size_t src_pitch, cudaMemcpyKind k
   GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), s->stream));
   GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips, s->P, src, src_pitch, s->desc.nptn, s->desc.ntaxa, kind,
                               s->stream));
-  k_tips_max<<<148 * 8, 256, 0, s->stream>>>(s->d_tips, s->P, s->desc.nptn, s->desc.ntaxa, d_max);
+  k_tips_max<<<148 * 8, 256, 0, s->stream>>>(s->d_tips, s->P, s->desc.nptn, s->desc.ntaxa, 0,
+                                             s->P, d_max);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   unsigned int mx = 0;
@@ -677,6 +689,95 @@ int gems_branch_lnl(gems_session *s, const gems_op *ops, int nops, const gems_br
     st = launch_theta_mixed(s, br, true, false, lnl);
   else
     st = launch_branch_lnl(s, br, lnl);
+  if (st) return st;
+  copy_pattern_lh(s, pattern_lh, *lnl);
+  return GEMS_OK;
+}
+
+// New tips, pattern weights and +I terms from the host, then the lnL of one branch, with the
+// upload overlapped with the traversal: the tip rows go up in `nchunks` pattern chunks on a
+// copy stream, each checked there (k_tips_max over its columns), and the traversal of a chunk
+// starts on the session stream as soon as its copy is done.  The check is read on the host once
+// the last copy is done, while the traversal still runs; the traversal clamps state bytes, so a
+// bad byte makes the call fail and the tips invalid, as gems_upload_tips does.  Sessions whose
+// traversal kernel does not take a pattern range (tcgen05, 61 states, generic n) load first and
+// evaluate after.
+int gems_branch_lnl_from_host(gems_session *s, const uint8_t *states, const double *ptn_freq,
+                              const double *ptn_invar, const gems_op *ops, int nops,
+                              const gems_branch *br, int nchunks, double *lnl,
+                              double *pattern_lh) {
+  if (!s || !states || !ptn_freq || !lnl || (nops > 0 && !ops) || nchunks < 1 ||
+      nchunks > Session::kMaxChunks)
+    return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  int st = check_branch(s, br);
+  if (st) return st;
+  if (!s->model_set) {
+    set_error("model not set");
+    return GEMS_ERR_STATE;
+  }
+  const bool ranged = traverse_v2_supported(s) && !tc20_supported(s) && !tc61_supported(s);
+  if (!ranged || nchunks == 1 || nops == 0) {
+    if ((st = gems_upload_tips(s, states))) return st;
+    if ((st = gems_upload_patterns(s, ptn_freq, ptn_invar))) return st;
+    return gems_branch_lnl(s, ops, nops, br, lnl, pattern_lh);
+  }
+  if (!s->copy_stream)
+    GEMS_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+  if (!s->start_ev) GEMS_CUDA(cudaEventCreateWithFlags(&s->start_ev, cudaEventDisableTiming));
+  for (cudaEvent_t &e : s->chunk_ev)
+    if (!e) GEMS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (!s->h_tipmax) GEMS_CUDA(cudaHostAlloc((void **)&s->h_tipmax, sizeof(unsigned int), 0));
+  const int n = s->desc.nptn, ntaxa = s->desc.ntaxa;
+  unsigned int *d_max = reinterpret_cast<unsigned int *>(s->d_flag) + 8;
+  cudaStream_t cs = s->copy_stream;
+  // nothing queued on the session stream may still read the old tips, weights or +I terms
+  GEMS_CUDA(cudaEventRecord(s->start_ev, s->stream));
+  GEMS_CUDA(cudaStreamWaitEvent(cs, s->start_ev, 0));
+  GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), cs));
+  GEMS_CUDA(cudaMemcpyAsync(s->d_freq, ptn_freq, n * sizeof(double), cudaMemcpyHostToDevice, cs));
+  if (ptn_invar)
+    GEMS_CUDA(
+        cudaMemcpyAsync(s->d_invar, ptn_invar, n * sizeof(double), cudaMemcpyHostToDevice, cs));
+  else
+    GEMS_CUDA(cudaMemsetAsync(s->d_invar, 0, n * sizeof(double), cs));
+  s->theta_valid = false;
+  // the op tables do not depend on the data: prepared while the first chunk goes up
+  if ((st = upload_ops(s, ops, nops))) return st;
+  if ((st = launch_prep_ops_v2(s, nops))) return st;
+  // chunks of whole waves of resident blocks, so that no chunk's launch ends on a partly filled
+  // wave, rounded to 128 patterns (P is a multiple of 64: every bound is a multiple of 16)
+  const int wave = std::max(128, traverse_v2_wave_patterns(s));
+  const int waves = (s->P + wave - 1) / wave;
+  const long long per = (long long)((waves + nchunks - 1) / nchunks) * wave;
+  const int chunk = (int)std::min<long long>((per + 127) / 128 * 128, (s->P + 127) / 128 * 128);
+  for (int c = 0, p0 = 0; p0 < s->P; c++, p0 += chunk) {
+    const int p1 = std::min(s->P, p0 + chunk);
+    const int w = std::min(p1, n) - p0;
+    if (w > 0)
+      GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips + p0, s->P, states + p0, n, w, ntaxa,
+                                  cudaMemcpyHostToDevice, cs));
+    const long long words = (long long)(p1 - p0) / 16 * ntaxa;
+    const int grid = (int)std::min<long long>(148 * 8, (words + 255) / 256);
+    k_tips_max<<<grid, 256, 0, cs>>>(s->d_tips, s->P, n, ntaxa, p0, p1, d_max);
+    s->launches++;
+    GEMS_CUDA(cudaGetLastError());
+    GEMS_CUDA(cudaEventRecord(s->chunk_ev[c], cs));
+    GEMS_CUDA(cudaStreamWaitEvent(s->stream, s->chunk_ev[c], 0));
+    if ((st = launch_traverse_v2(s, nops, p0, p1))) return st;
+  }
+  GEMS_CUDA(cudaMemcpyAsync(s->h_tipmax, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost, cs));
+  GEMS_CUDA(cudaStreamSynchronize(cs));
+  if ((int)*s->h_tipmax > s->unknown) {
+    s->tips_ok = false;
+    GEMS_CUDA(cudaStreamSynchronize(s->stream));
+    set_error("tip state byte out of range");
+    return GEMS_ERR_BAD_ARG;
+  }
+  s->tips_ok = true;
+  invalidate_theta(s, ops, nops);
+  st = s->desc.precision == GEMS_PREC_MIXED ? launch_theta_mixed(s, br, true, false, lnl)
+                                            : launch_branch_lnl(s, br, lnl);
   if (st) return st;
   copy_pattern_lh(s, pattern_lh, *lnl);
   return GEMS_OK;

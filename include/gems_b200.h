@@ -143,6 +143,17 @@ int gems_branch_lnl_batch(gems_session *const *sessions, int nsess, const gems_o
  * including the scaling correction). */
 int gems_branch_lnl(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
                     double *lnl, double *pattern_lh);
+/* gems_upload_tips + gems_upload_patterns + gems_branch_lnl in one call, with the tip upload
+ * overlapped with the traversal: the rows go up in nchunks (1..64) pattern chunks on a second
+ * stream and each chunk's traversal starts when its copy is done (4-state sessions, and 20-state
+ * sessions with tensor cores off; other forms load first, then evaluate).  Overlap needs pinned
+ * host buffers.  A tip byte above STATE_UNKNOWN fails the call with GEMS_ERR_BAD_ARG and leaves
+ * the tips invalid, as gems_upload_tips does.  No counterpart in the reference (its alignment is
+ * loaded once); replaces reloading the alignment and calling computeLikelihood. */
+int gems_branch_lnl_from_host(gems_session *s, const uint8_t *states, const double *ptn_freq,
+                              const double *ptn_invar, const gems_op *ops, int nops,
+                              const gems_branch *br, int nchunks, double *lnl,
+                              double *pattern_lh);
 /* Derivatives of lnL w.r.t. the branch length (computeLikelihoodDervSIMD,
  * tree/phylokernelnew.h:2238-2650).  When compute_theta != 0 the ops run first and theta is
  * rebuilt from the two partials (computeLikelihoodBufferSIMD, :2053-2235); otherwise the
@@ -253,6 +264,11 @@ int gems_tree_clear_all_partial_lh(gems_tree *t);
 /* PhyloTree::computeLikelihood (tree/phylotree.cpp:1258) */
 int gems_tree_compute_likelihood(gems_tree *t, double *lnl, double *pattern_lh);
 /* computeLikelihoodBranch(dad->findNeighbor(node), dad) */
+/* computeLikelihood on new tips, weights and +I terms (every partial recomputed), through
+ * gems_branch_lnl_from_host. */
+int gems_tree_compute_likelihood_from_host(gems_tree *t, const uint8_t *states,
+                                           const double *ptn_freq, const double *ptn_invar,
+                                           int nchunks, double *lnl, double *pattern_lh);
 int gems_tree_compute_likelihood_branch(gems_tree *t, int node, int dad, double *lnl,
                                         double *pattern_lh);
 /* computeLikelihoodDerv(dad->findNeighbor(node), dad) */
