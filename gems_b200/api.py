@@ -326,6 +326,10 @@ class Session:
         cores."""
         _check(self.lib.gems_session_set_option(self.handle, 1, int(on)), "set_option")
 
+    def set_tiled_fp64(self, on=True):
+        """61-state FP64 traversal as register-tiled GEMMs (default) or the per-row kernel."""
+        _check(self.lib.gems_session_set_option(self.handle, 2, int(on)), "set_option")
+
     def stream_handle(self):
         p = c_void_p()
         _check(self.lib.gems_session_stream(self.handle, byref(p)), "gems_session_stream")

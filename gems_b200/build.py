@@ -25,7 +25,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                   "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
 CUDA_SOURCES = ["session.cu", "kernels_fp64.cu", "kernels_mixed.cu", "kernels_traverse.cu",
-                "kernels_tc20.cu", "kernels_tc61.cu", "kernels_rell.cu", "eigen.cu", "noalloc.cu", "peaks.cu", "ingest.cu",
+                "kernels_tc20.cu", "kernels_tc61.cu", "kernels_g61.cu", "kernels_rell.cu", "eigen.cu", "noalloc.cu", "peaks.cu", "ingest.cu",
                 "phylotree.cpp"]
 HEADERS = ["gems_internal.cuh", "tc_common.cuh"]
 

@@ -149,6 +149,8 @@ struct Session {
   std::vector<double> h_evec, h_inv;  // host copy of the eigenvectors in use
   // tensor-core path (20 states, mixed): per-op table stride in floats
   bool tc_enabled = true;
+  // FP64 61-state traversal as register-tiled GEMMs (else the per-row kernel)
+  bool g61_enabled = true;
   size_t op_stride_tc = 0;
   // FP32 partials stored tile-major (20- and 61-state mixed forms); elements per slot
   bool tiled = false;
@@ -219,6 +221,11 @@ bool tc61_supported(const Session *s);
 int launch_prep_ops_tc61(Session *s, int nops);
 int launch_traverse_tc61(Session *s, int nops);
 int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops);
+// FP64 61-state traversal as register-tiled GEMMs, C in {1, 2, 4, 8} (kernels_g61.cu)
+size_t g61_op_doubles(int ncat, int unknown);
+bool g61_supported(const Session *s);
+int launch_prep_ops_g61(Session *s, int nops);
+int launch_traverse_g61(Session *s, int nops);
 // bootstrap reweighting (kernels_rell.cu)
 int launch_rell_lnl(Session *s, double *d_out);
 int launch_rell_derv(Session *s, double *d_out);

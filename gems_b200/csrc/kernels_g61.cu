@@ -1,0 +1,315 @@
+// kernels_g61.cu -- FP64 traversal for 61 states (codon models) as register-tiled GEMMs.
+//
+// The node update of the reference (tree/phylokernelnew.h:1911-2035) per (pattern, category)
+// row is
+//     out = inv_evec . ((E_L,c . L) * (E_R,c . R)),   E_c = evec . diag(exp(eval r_c t)).
+// Over a tile of rows each product is a GEMM: V = L . E_c^T (K = N = 61) for the rows of
+// category c, and out = T . inv_evec^T for all rows.  The products and their summation order
+// are those of the per-row form (fma over the contraction index in ascending order), so the
+// values are the generic kernel's bit for bit.  (The factored form evec . (d (*) L) of the 4- and
+// 20-state kernels was tried here: with 61 states the eigen-space sums cancel heavily, and on
+// a 160-taxon tree with long branches it moved partials by up to 2.5e-8 of their pattern's
+// largest value, measured in plain FP64 numpy as well.)
+//
+// One CTA per tile of up to 128 rows = tp patterns x C categories (tp = 128 / C rounded down to
+// a multiple of 8), stored category-major in the tile (row = c * tp + pattern), 256 threads as
+// 16 x 16: thread (ty, tx) owns rows ty*8..ty*8+7 -- all of one category -- and columns tx,
+// tx+16, tx+32, tx+48 (32 FP64 accumulators).  The A operand of a child (its 128 partial rows) is staged
+// k-major in shared memory (sA[k][row]: a thread reads its 8 rows as 4 double2 per k);
+// inv_evec^T stays in shared memory for the whole traversal; E_c^T is read through L1 from the
+// op table, stored [side][c][k][64 columns] by the prep kernel.  A tip child's V is a row of the
+// op's leaf table (E_c . tip vector), gathered by state.  Scaling: SAFE per row (max over the
+// row's 61 values: own columns, then a shuffle over the 16 tx lanes of the half-warp); NORM per
+// pattern (row maxima through shared memory).
+#include <string>
+
+#include "gems_internal.cuh"
+
+namespace gems {
+
+namespace {
+
+constexpr int kN = 61;
+constexpr int kK = 62;       // padded contraction length (even: double2 steps)
+constexpr int kNC = 64;      // padded output columns
+constexpr int kRows = 128;   // rows per tile
+constexpr int kSaLd = kRows + 2;
+constexpr int kMaxCatG = 8;
+constexpr int kThreadsG = 256;
+constexpr size_t kSmemG = sizeof(double) * ((size_t)kK * kNC + (size_t)kK * kSaLd + kRows);
+
+// patterns per tile: 128 / C rounded down to a multiple of 8, so that the 8 rows of a thread
+// (category-major rows) belong to one category
+__host__ __device__ constexpr int tile_patterns(int C) { return kRows / C / 8 * 8; }
+
+// per-op table (doubles): Et[2][C][kK][kNC] (Et[side][c][i][x] = E_c[x][i], zero padded), then
+// leaf[2][unknown + 1][C][61]
+__host__ __device__ constexpr size_t et_doubles(int C) { return (size_t)C * kK * kNC; }
+
+__global__ void k_prep_ops_g61(DevCtx c, const DevOp *ops, double *tab, size_t stride) {
+  __shared__ double dsh[kMaxCatG * kN];
+  const int k = blockIdx.x, side = blockIdx.y;
+  const DevOp op = ops[k];
+  const int kind = side ? op.r_kind : op.l_kind;
+  const double len = side ? op.r_len : op.l_len;
+  const int C = c.C, blk = C * kN;
+  for (int idx = threadIdx.x; idx < blk; idx += blockDim.x) {
+    const int cc = idx / kN, i = idx - cc * kN;
+    dsh[idx] = exp(c.eval[i] * (c.rates[cc] * len));
+  }
+  __syncthreads();
+  double *et = tab + (size_t)k * stride + (size_t)side * et_doubles(C);
+  for (int idx = threadIdx.x; idx < (int)et_doubles(C); idx += blockDim.x) {
+    const int cc = idx / (kK * kNC), r = idx - cc * (kK * kNC), i = r / kNC, x = r - i * kNC;
+    et[idx] = (i < kN && x < kN) ? c.evec[x * kN + i] * dsh[cc * kN + i] : 0.0;
+  }
+  if (kind != GEMS_CHILD_TIP) return;
+  double *leaf = tab + (size_t)k * stride + 2 * et_doubles(C) + (size_t)side * (c.unknown + 1) * blk;
+  const int rows = c.unknown * blk;
+  for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
+    const int s = idx / blk, r = idx - s * blk, cc = r / kN, x = r - cc * kN;
+    const double *t = c.tip + (size_t)s * kN;
+    double acc = 0.0;
+    for (int i = 0; i < kN; i++) acc = fma(c.evec[x * kN + i] * dsh[cc * kN + i], t[i], acc);
+    leaf[idx] = acc;
+  }
+  for (int idx = threadIdx.x; idx < blk; idx += blockDim.x) leaf[rows + idx] = 1.0;
+}
+
+// acc[j][q] = sum_k sA[k][ty*8 + j] * B[k][tx + 16 q], k ascending; B in global memory (read
+// through L1) or shared memory
+template <bool GLOBAL_B>
+__device__ __forceinline__ void gemm_tile(const double *__restrict__ sA,
+                                          const double *__restrict__ B, int ty, int tx,
+                                          double (&acc)[8][4]) {
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[j][q] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < kK; k++) {
+    double b[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = GLOBAL_B ? __ldg(B + k * kNC + tx + 16 * q) : B[k * kNC + tx + 16 * q];
+    const double2 *a2 = reinterpret_cast<const double2 *>(sA + k * kSaLd + ty * 8);
+    double a[8];
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const double2 t = a2[h];
+      a[2 * h] = t.x;
+      a[2 * h + 1] = t.y;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[j][q] = fma(a[j], b[q], acc[j][q]);
+  }
+}
+
+// tile row -> (category, pattern within the tile) and back to the slot's pattern-major rows
+struct TileMap {
+  int C, tp, nrow;
+  long p0, P;
+  __device__ int cat(int r) const { return r / tp; }
+  __device__ long pattern(int r) const { return p0 + (r - (r / tp) * tp); }
+  __device__ bool valid(int r) const { return r < nrow && pattern(r) < P; }
+  // offset of the row's first state in the slot
+  __device__ size_t off(int r) const { return ((size_t)pattern(r) * C + cat(r)) * kN; }
+};
+
+// V of one child for the thread's rows and columns, and its scale counts (per row: SAFE; the
+// pattern's: NORM).  A partial child's GEMM leaves sA in use: the caller synchronises before
+// the next write of sA.
+template <bool SAFE>
+__device__ __forceinline__ void child_v(const DevCtx &c, const TileMap &tm, int kind, int id,
+                                        const double *et, const double *leaf, double *sA, int ty,
+                                        int tx, double (&v)[8][4], int (&s)[8]) {
+  if (kind == GEMS_CHILD_TIP) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int r = ty * 8 + j;
+      const bool ok = tm.valid(r);
+      const int st = ok ? min((int)c.tips[(size_t)id * c.P + tm.pattern(r)], c.unknown) : 0;
+      const double *row = leaf + ((size_t)st * tm.C + tm.cat(r)) * kN;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int col = tx + 16 * q;
+        v[j][q] = ok && col < kN ? __ldg(row + col) : 0.0;
+      }
+      s[j] = 0;
+    }
+    return;
+  }
+  // sA[k][r] = L[r][k] for k < 61, zero elsewhere.  idx runs over (pattern, category, k) in
+  // the slot's order, so consecutive threads read consecutive doubles.
+  const double *src = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
+  for (int idx = threadIdx.x; idx < kRows * kK; idx += blockDim.x) {
+    const int g = idx / kK, k = idx - g * kK;  // g = pattern-major row within the tile
+    const int lp = g / tm.C, cc = g - lp * tm.C;
+    const int r = cc * tm.tp + lp;
+    double a = 0.0;
+    if (g < tm.nrow && tm.p0 + lp < tm.P && k < kN)
+      a = __ldcg(src + ((size_t)(tm.p0 + lp) * tm.C + cc) * kN + k);
+    if (g < tm.nrow) sA[k * kSaLd + r] = a;
+  }
+  const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int r = ty * 8 + j;
+    const long p = tm.pattern(r);
+    s[j] = tm.valid(r) ? (SAFE ? sc[(size_t)p * tm.C + tm.cat(r)] : sc[p]) : 0;
+  }
+  __syncthreads();
+  // rows past the tile's (128 % C) have no category: any table will do, their A rows are zero
+  const int cat = min(tm.cat(ty * 8), tm.C - 1);
+  gemm_tile<true>(sA, et + (size_t)cat * kK * kNC, ty, tx, v);
+}
+
+template <bool SAFE>
+__global__ void __launch_bounds__(kThreadsG, 1)
+    k_traverse_g61(DevCtx c, const DevOp *__restrict__ ops, int nops,
+                   const double *__restrict__ tab, size_t stride) {
+  extern __shared__ __align__(16) double smem[];
+  double *sIv = smem;                  // [kK][kNC]: inv_evec[j][x] at [x][j]
+  double *sA = sIv + kK * kNC;         // [kK][kSaLd]
+  double *sMax = sA + kK * kSaLd;      // [kRows] row maxima (NORM)
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  TileMap tm;
+  tm.C = c.C;
+  tm.tp = tile_patterns(c.C);
+  tm.nrow = tm.tp * c.C;
+  tm.p0 = (long)blockIdx.x * tm.tp;
+  tm.P = c.P;
+  for (int idx = tid; idx < kK * kNC; idx += blockDim.x) {
+    const int k = idx / kNC, x = idx - k * kNC;
+    sIv[idx] = (k < kN && x < kN) ? c.inv_evec[x * kN + k] : 0.0;
+  }
+  // rows of sA past the tile's rows (128 % C) are never written: zero them once
+  for (int idx = tid; idx < kK * kSaLd; idx += blockDim.x) sA[idx] = 0.0;
+  double *part = static_cast<double *>(c.partials);
+  const int blk = c.C * kN;
+  for (int kop = 0; kop < nops; kop++) {
+    const DevOp op = ops[kop];
+    const double *tk = tab + (size_t)kop * stride;
+    const double *leafL = tk + 2 * et_doubles(c.C);
+    const double *leafR = leafL + (size_t)(c.unknown + 1) * blk;
+    const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
+    double vl[8][4], o[8][4];
+    int sl[8], sr[8];
+    __syncthreads();  // sA free (previous op's last GEMM, or the set-up)
+    child_v<SAFE>(c, tm, op.l_kind, op.l_id, tk, leafL, sA, ty, tx, vl, sl);
+    __syncthreads();
+    child_v<SAFE>(c, tm, op.r_kind, op.r_id, tk + et_doubles(c.C), leafR, sA, ty, tx, o, sr);
+    __syncthreads();
+    // T = V_L (*) V_R into sA (k-major); columns >= 61 of V are zero, so row 61 of T is zero
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int x = tx + 16 * q;
+      if (x < kK) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) sA[x * kSaLd + ty * 8 + j] = vl[j][q] * o[j][q];
+      }
+    }
+    __syncthreads();
+    gemm_tile<false>(sA, sIv, ty, tx, o);
+    double m[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      double x = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) x = fmax(x, fabs(o[j][q]));
+      for (int off = 1; off < 16; off <<= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, off));
+      m[j] = x;
+    }
+    if (!SAFE) {
+      // the pattern's maximum over its C rows (rows c * tp + lp, in other threads)
+      if (tx == 0) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) sMax[ty * 8 + j] = m[j];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int lp = (ty * 8 + j) % tm.tp;
+        double x = 0.0;
+        for (int u = 0; u < tm.C; u++) x = fmax(x, sMax[u * tm.tp + lp]);
+        m[j] = x;
+      }
+    }
+    uint16_t *scd = c.scale + (size_t)op.dst_slot * c.slot_scale;
+    double *dst = part + (size_t)op.dst_slot * c.slot_elems;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int r = ty * 8 + j;
+      if (!tm.valid(r)) continue;
+      const long p = tm.pattern(r);
+      const int cat = tm.cat(r);
+      int s_out = sl[j] + sr[j];
+      if (!tiptip && m[j] < kScaleThr && c.invar[p] == 0.0) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) o[j][q] = ldexp(o[j][q], kScaleExp);
+        s_out += 1;
+      }
+      double *row = dst + tm.off(r);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int col = tx + 16 * q;
+        if (col < kN) row[col] = o[j][q];
+      }
+      if (tx == 0) {
+        if (SAFE)
+          scd[(size_t)p * tm.C + cat] = (uint16_t)s_out;
+        else if (cat == 0)
+          scd[p] = (uint16_t)s_out;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+size_t g61_op_doubles(int ncat, int unknown) {
+  return 2 * et_doubles(ncat) + 2 * (size_t)(unknown + 1) * ncat * kN;
+}
+
+bool g61_supported(const Session *s) {
+  const int C = s->desc.ncat;
+  return s->g61_enabled && s->desc.precision == GEMS_PREC_FP64 && s->desc.nstates == kN &&
+         C >= 1 && C <= kMaxCatG;
+}
+
+int launch_prep_ops_g61(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  k_prep_ops_g61<<<dim3(nops, 2), 256, 0, s->stream>>>(s->ctx(), s->d_ops, s->d_opmats,
+                                                        s->op_stride);
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  return GEMS_OK;
+}
+
+int launch_traverse_g61(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  cudaEvent_t ev0;
+  if (int st = prof_begin(s, 0, &ev0)) return st;
+  const int tp = tile_patterns(s->desc.ncat);
+  const int grid = (s->P + tp - 1) / tp;
+  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  // the limit is a per-kernel attribute shared by every thread of the process: always the same
+  // value
+  if (safe) {
+    GEMS_CUDA(cudaFuncSetAttribute(k_traverse_g61<true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemG));
+    k_traverse_g61<true><<<grid, kThreadsG, kSmemG, s->stream>>>(s->ctx(), s->d_ops, nops,
+                                                                  s->d_opmats, s->op_stride);
+  } else {
+    GEMS_CUDA(cudaFuncSetAttribute(k_traverse_g61<false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemG));
+    k_traverse_g61<false><<<grid, kThreadsG, kSmemG, s->stream>>>(s->ctx(), s->d_ops, nops,
+                                                                   s->d_opmats, s->op_stride);
+  }
+  s->launches++;
+  GEMS_CUDA(cudaGetLastError());
+  return prof_end(s, 0, ev0);
+}
+
+}  // namespace gems

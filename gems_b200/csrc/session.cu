@@ -143,6 +143,10 @@ static Sizes compute_sizes(const gems_session_desc &d) {
     const size_t need = (tc61_op_floats(d.ncat) + 1) / 2;
     if (z.op_stride < need) z.op_stride = need;
   }
+  if (d.nstates == 61 && d.precision == GEMS_PREC_FP64) {
+    const size_t need = g61_op_doubles(d.ncat, unk);
+    if (z.op_stride < need) z.op_stride = need;
+  }
   z.op_stride = (z.op_stride + 7) & ~(size_t)7;  // 64-byte aligned op tables
   z.opmats_bytes = (size_t)z.nops_max * z.op_stride * sizeof(double);
   z.branch_bytes = (3 * blk + (size_t)(unk + 1) * blk) * sizeof(double);
@@ -280,6 +284,9 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
   } else if (traverse_v2_supported(s)) {
     if ((st = launch_prep_ops_v2(s, nops))) return st;
     if ((st = launch_traverse_v2(s, nops, 0, s->P))) return st;
+  } else if (g61_supported(s)) {
+    if ((st = launch_prep_ops_g61(s, nops))) return st;
+    if ((st = launch_traverse_g61(s, nops))) return st;
   } else if (s->desc.precision == GEMS_PREC_MIXED) {
     if ((st = launch_prep_ops_mixed(s, nops))) return st;
     if ((st = launch_traverse_mixed(s, nops))) return st;
@@ -491,6 +498,9 @@ int gems_session_set_option(gems_session *s, int option, int value) {
   switch (option) {
     case GEMS_OPT_TENSOR_CORES:
       s->tc_enabled = value != 0;
+      return GEMS_OK;
+    case GEMS_OPT_TILED_FP64:
+      s->g61_enabled = value != 0;
       return GEMS_OK;
     default:
       return GEMS_ERR_BAD_ARG;

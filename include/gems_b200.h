@@ -98,8 +98,11 @@ int gems_session_info(gems_session *s, gems_session_desc *desc);
 /* the CUDA stream (cudaStream_t) the session launches on, for event timing by the caller */
 int gems_session_stream(gems_session *s, void **stream);
 /* Session options.  GEMS_OPT_TENSOR_CORES (default 1): the mixed-precision 20-state traversal
- * runs on tcgen05 split-TF32 products; 0 selects the FP32 CUDA-core kernel. */
-enum { GEMS_OPT_TENSOR_CORES = 1 };
+ * runs on tcgen05 split-TF32 products; 0 selects the FP32 CUDA-core kernel.
+ * GEMS_OPT_TILED_FP64 (default 1): the FP64 61-state traversal (1 to 8 categories) runs as
+ * register-tiled GEMMs over 128-row tiles; 0 selects the per-row kernel (same values, bit for
+ * bit). */
+enum { GEMS_OPT_TENSOR_CORES = 1, GEMS_OPT_TILED_FP64 = 2 };
 int gems_session_set_option(gems_session *s, int option, int value);
 
 /* Tip state bytes [ntaxa][nptn] (PhyloTree::getConvertedSequenceByNumber rows,
