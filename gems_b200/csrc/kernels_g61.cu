@@ -11,10 +11,12 @@
 // a 160-taxon tree with long branches it moved partials by up to 2.5e-8 of their pattern's
 // largest value, measured in plain FP64 numpy as well.)
 //
-// One CTA per tile of up to 128 rows = tp patterns x C categories (tp = 128 / C rounded down to
-// a multiple of 8), stored category-major in the tile (row = c * tp + pattern), 256 threads as
-// 16 x 16: thread (ty, tx) owns rows ty*8..ty*8+7 -- all of one category -- and columns tx,
-// tx+16, tx+32, tx+48 (32 FP64 accumulators).  The A operand of a child (its 128 partial rows) is staged
+// One CTA per tile of up to 64 rows = tp patterns x C categories (tp = 64 / C rounded down to a
+// multiple of 8), stored category-major in the tile (row = c * tp + pattern), 128 threads as
+// 8 x 16: thread (ty, tx) owns rows ty*8..ty*8+7 -- all of one category -- and columns tx,
+// tx+16, tx+32, tx+48 (32 FP64 accumulators); two CTAs per SM, so that one's loads overlap the
+// other's GEMMs (measured against 128-row tiles of 256 threads: 7.0 -> 6.2 ms on one 200-taxon
+// codon model).  The A operand of a child (its partial rows) is staged
 // k-major in shared memory (sA[k][row]: a thread reads its 8 rows as 4 double2 per k);
 // inv_evec^T stays in shared memory for the whole traversal; E_c^T is read through L1 from the
 // op table, stored [side][c][k][64 columns] by the prep kernel.  A tip child's V is a row of the
@@ -32,13 +34,13 @@ namespace {
 constexpr int kN = 61;
 constexpr int kK = 62;       // padded contraction length (even: double2 steps)
 constexpr int kNC = 64;      // padded output columns
-constexpr int kRows = 128;   // rows per tile
+constexpr int kRows = 64;    // rows per tile
 constexpr int kSaLd = kRows + 2;
 constexpr int kMaxCatG = 8;
-constexpr int kThreadsG = 256;
+constexpr int kThreadsG = 2 * kRows;  // 8 rows x 4 columns per thread
 constexpr size_t kSmemG = sizeof(double) * ((size_t)kK * kNC + (size_t)kK * kSaLd + kRows);
 
-// patterns per tile: 128 / C rounded down to a multiple of 8, so that the 8 rows of a thread
+// patterns per tile: 64 / C rounded down to a multiple of 8, so that the 8 rows of a thread
 // (category-major rows) belong to one category
 __host__ __device__ constexpr int tile_patterns(int C) { return kRows / C / 8 * 8; }
 
@@ -140,17 +142,36 @@ __device__ __forceinline__ void child_v(const DevCtx &c, const TileMap &tm, int 
     }
     return;
   }
+  // the rows of E_c^T this CTA will read, pulled into L1 while the child's rows load (the
+  // GEMM's first touch of each row otherwise waits on L2: 7.0 -> 5.9 ms with 128-row tiles)
+  {
+    const char *e0 = reinterpret_cast<const char *>(et);
+    const int lines = (int)(et_doubles(tm.C) * sizeof(double) / 128);
+    for (int l = threadIdx.x; l < lines; l += blockDim.x)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(e0 + (size_t)l * 128));
+  }
   // sA[k][r] = L[r][k] for k < 61, zero elsewhere.  idx runs over (pattern, category, k) in
-  // the slot's order, so consecutive threads read consecutive doubles.
+  // the slot's order, so consecutive threads read consecutive doubles; every load of a thread
+  // is issued before the first store.
   const double *src = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
-  for (int idx = threadIdx.x; idx < kRows * kK; idx += blockDim.x) {
+  constexpr int kPer = kRows * kK / kThreadsG;
+  static_assert(kRows * kK % kThreadsG == 0, "whole loads per thread");
+  double a[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int idx = threadIdx.x + u * kThreadsG;
     const int g = idx / kK, k = idx - g * kK;  // g = pattern-major row within the tile
     const int lp = g / tm.C, cc = g - lp * tm.C;
-    const int r = cc * tm.tp + lp;
-    double a = 0.0;
-    if (g < tm.nrow && tm.p0 + lp < tm.P && k < kN)
-      a = __ldcg(src + ((size_t)(tm.p0 + lp) * tm.C + cc) * kN + k);
-    if (g < tm.nrow) sA[k * kSaLd + r] = a;
+    a[u] = (g < tm.nrow && tm.p0 + lp < tm.P && k < kN)
+               ? __ldcg(src + ((size_t)(tm.p0 + lp) * tm.C + cc) * kN + k)
+               : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int idx = threadIdx.x + u * kThreadsG;
+    const int g = idx / kK, k = idx - g * kK;
+    const int lp = g / tm.C, cc = g - lp * tm.C;
+    if (g < tm.nrow) sA[k * kSaLd + cc * tm.tp + lp] = a[u];
   }
   const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
 #pragma unroll
@@ -160,13 +181,13 @@ __device__ __forceinline__ void child_v(const DevCtx &c, const TileMap &tm, int 
     s[j] = tm.valid(r) ? (SAFE ? sc[(size_t)p * tm.C + tm.cat(r)] : sc[p]) : 0;
   }
   __syncthreads();
-  // rows past the tile's (128 % C) have no category: any table will do, their A rows are zero
+  // rows past the tile's (64 % C) have no category: any table will do, their A rows are zero
   const int cat = min(tm.cat(ty * 8), tm.C - 1);
   gemm_tile<true>(sA, et + (size_t)cat * kK * kNC, ty, tx, v);
 }
 
 template <bool SAFE>
-__global__ void __launch_bounds__(kThreadsG, 1)
+__global__ void __launch_bounds__(kThreadsG, 2)
     k_traverse_g61(DevCtx c, const DevOp *__restrict__ ops, int nops,
                    const double *__restrict__ tab, size_t stride) {
   extern __shared__ __align__(16) double smem[];
@@ -184,7 +205,7 @@ __global__ void __launch_bounds__(kThreadsG, 1)
     const int k = idx / kNC, x = idx - k * kNC;
     sIv[idx] = (k < kN && x < kN) ? c.inv_evec[x * kN + k] : 0.0;
   }
-  // rows of sA past the tile's rows (128 % C) are never written: zero them once
+  // rows of sA past the tile's rows (64 % C) are never written: zero them once
   for (int idx = tid; idx < kK * kSaLd; idx += blockDim.x) sA[idx] = 0.0;
   double *part = static_cast<double *>(c.partials);
   const int blk = c.C * kN;
