@@ -301,10 +301,9 @@ __device__ __forceinline__ void msg_mix(const DevCtx &c, int kind, int id,
   }
 }
 
-// 4 states: the kernel is latency-bound on its child loads, and the most warps per SM win
-// (measured: 8 resident blocks at 32 registers beat 5 at 46 by 18% on the 512-taxon case)
+// 20 states on CUDA cores (4 states run k_traverse_mix4)
 template <int N, bool SAFE>
-__global__ void __launch_bounds__(kThreads, N == 4 ? 8 : 1) k_traverse_mix(DevCtx c, const DevOp *__restrict__ ops,
+__global__ void __launch_bounds__(kThreads, 1) k_traverse_mix(DevCtx c, const DevOp *__restrict__ ops,
                                                            int nops, const float *__restrict__ tab,
                                                            size_t stride_f, int p0, int p1) {
   const int G = c.G;
@@ -358,6 +357,112 @@ __global__ void __launch_bounds__(kThreads, N == 4 ? 8 : 1) k_traverse_mix(DevCt
         sc[(size_t)p * C + gl] = (uint16_t)s_out;
       else if (gl == 0)
         sc[p] = (uint16_t)s_out;
+    }
+    __syncwarp();
+  }
+}
+
+// 4 states: the kernel is latency-bound on its child loads.  Each lane group handles kMix4PP
+// patterns, kThreads / G apart, so that a warp has the child loads of all of them in flight at
+// once and loads each P row once for all of them; same arithmetic, in the same order, as
+// msg_mix / k_traverse_mix.  Measured on the 512-taxon, 1M-pattern case: one pattern per group
+// at 8 blocks per SM (32 registers) 14.8 ms; two at 5 blocks (48 registers) 12.6 ms; two at 4
+// or 6 blocks 14.8 / 12.7 ms; four at 3 blocks 12.8 ms.
+constexpr int kMix4PP = 2;
+constexpr int kMix4Blocks = 5;
+
+template <bool SAFE>
+__device__ __forceinline__ void msg_mix4(const DevCtx &c, int kind, int id,
+                                         const float *__restrict__ Pm,
+                                         const float *__restrict__ leaf,
+                                         const long (&p)[kMix4PP], int gq,
+                                         float (&v)[kMix4PP][4], int (&s)[kMix4PP]) {
+  const int C = c.C;
+  if (kind == GEMS_CHILD_TIP) {
+    int st[kMix4PP];
+#pragma unroll
+    for (int u = 0; u < kMix4PP; u++) st[u] = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
+#pragma unroll
+    for (int u = 0; u < kMix4PP; u++) {
+      const float *lt = leaf + (size_t)st[u] * c.block + gq;
+#pragma unroll
+      for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
+      s[u] = 0;
+    }
+  } else {
+    const float *base = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems;
+    float4 L[kMix4PP];
+#pragma unroll
+    for (int u = 0; u < kMix4PP; u++)
+      L[u] = __ldcg(reinterpret_cast<const float4 *>(base + mix_off<4>(c, p[u], gq)));
+    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+#pragma unroll
+    for (int u = 0; u < kMix4PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const float4 r = __ldg(reinterpret_cast<const float4 *>(Pm + ((size_t)x * C + gq) * 4));
+#pragma unroll
+      for (int u = 0; u < kMix4PP; u++)
+        v[u][x] = fmaf(r.w, L[u].w, fmaf(r.z, L[u].z, fmaf(r.y, L[u].y, fmaf(r.x, L[u].x, 0.f))));
+    }
+  }
+}
+
+template <bool SAFE>
+__global__ void __launch_bounds__(kThreads, kMix4Blocks)
+    k_traverse_mix4(DevCtx c, const DevOp *__restrict__ ops, int nops,
+                    const float *__restrict__ tab, size_t stride_f, int p0, int p1) {
+  const int G = c.G, C = c.C;
+  const int gl = threadIdx.x & (G - 1);
+  const int gq = gl < C ? gl : 0;  // loads of idle lanes stay inside the tables
+  const int per = kThreads / G;
+  const long pb = p0 + (long)blockIdx.x * per * kMix4PP + threadIdx.x / G;
+  long p[kMix4PP];
+  bool act[kMix4PP];
+#pragma unroll
+  for (int u = 0; u < kMix4PP; u++) {
+    const long q = pb + (long)u * per;
+    act[u] = q < p1 && gl < C;
+    p[u] = q < p1 ? q : p0;
+  }
+  const size_t nnC = (size_t)16 * C;
+  float *part = static_cast<float *>(c.partials);
+  __shared__ int4 s_ops[kOpChunk];
+  for (int k = 0; k < nops; k++) {
+    if ((k & (kOpChunk - 1)) == 0) stage_ops(ops, k, nops, s_ops);
+    const OpIds op = staged_op(s_ops, k & (kOpChunk - 1));
+    const float *tk = tab + (size_t)k * stride_f;
+    const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
+    float vl[kMix4PP][4], vr[kMix4PP][4];
+    int sl[kMix4PP], sr[kMix4PP];
+    msg_mix4<SAFE>(c, op.l_kind, op.l_id, tk, tk + 2 * nnC, p, gq, vl, sl);
+    msg_mix4<SAFE>(c, op.r_kind, op.r_id, tk + nnC, tk + 2 * nnC + (size_t)(c.unknown + 1) * c.block,
+                   p, gq, vr, sr);
+#pragma unroll
+    for (int u = 0; u < kMix4PP; u++) {
+      float lh_max = 0.f;
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        vl[u][x] *= vr[u][x];
+        lh_max = fmaxf(lh_max, vl[u][x]);
+      }
+      if (!act[u]) lh_max = 0.f;
+      if (!SAFE) lh_max = group_maxf(lh_max, G);
+      if (act[u]) {
+        int s_out = sl[u] + sr[u];
+        if (!tiptip && lh_max < kScaleThrF && c.invar[p[u]] == 0.0) {
+#pragma unroll
+          for (int x = 0; x < 4; x++) vl[u][x] *= 18446744073709551616.0f;  // 2^64
+          s_out += 1;
+        }
+        *reinterpret_cast<float4 *>(part + (size_t)op.dst_slot * c.slot_elems + mix_off<4>(c, p[u], gl)) =
+            make_float4(vl[u][0], vl[u][1], vl[u][2], vl[u][3]);
+        uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
+        if (SAFE)
+          sc[(size_t)p[u] * C + gl] = (uint16_t)s_out;
+        else if (gl == 0)
+          sc[p[u]] = (uint16_t)s_out;
+      }
     }
     __syncwarp();
   }
@@ -421,7 +526,7 @@ int traverse_v2_wave_patterns(const Session *s) {
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   const bool four = s->desc.nstates == 4;
   const void *fn =
-      mixed ? (four ? (safe ? (const void *)k_traverse_mix<4, true> : (const void *)k_traverse_mix<4, false>)
+      mixed ? (four ? (safe ? (const void *)k_traverse_mix4<true> : (const void *)k_traverse_mix4<false>)
                     : (safe ? (const void *)k_traverse_mix<20, true> : (const void *)k_traverse_mix<20, false>))
             : (four ? (safe ? (const void *)k_traverse_f64<4, true> : (const void *)k_traverse_f64<4, false>)
                     : (safe ? (const void *)k_traverse_f64<20, true> : (const void *)k_traverse_f64<20, false>));
@@ -431,7 +536,7 @@ int traverse_v2_wave_patterns(const Session *s) {
     cudaGetLastError();
     return 0;
   }
-  return per_sm * nsm * (kThreads / s->G);
+  return per_sm * nsm * (kThreads / s->G) * (mixed && four ? kMix4PP : 1);
 }
 
 int launch_traverse_v2(Session *s, int nops, int p0, int p1) {
@@ -445,8 +550,10 @@ int launch_traverse_v2(Session *s, int nops, int p0, int p1) {
     const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
     const float *tab = reinterpret_cast<const float *>(s->d_opmats);
     if (s->desc.nstates == 4) {
-      if (safe) k_traverse_mix<4, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
-      else k_traverse_mix<4, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
+      const long per = (long)(kThreads / s->G) * kMix4PP;
+      const int g4 = (int)((p1 - p0 + per - 1) / per);
+      if (safe) k_traverse_mix4<true><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
+      else k_traverse_mix4<false><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
     } else {
       if (safe) k_traverse_mix<20, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
       else k_traverse_mix<20, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
