@@ -207,6 +207,132 @@ __global__ void __launch_bounds__(kThreads) k_traverse_f64(DevCtx c, const DevOp
   }
 }
 
+// FP64, 4 states: kF64PP patterns per lane group (as k_traverse_mix4), same arithmetic in the
+// same order as msg_f64 / k_traverse_f64.  Measured on the 512-taxon, 1M-pattern case: one
+// pattern per group (40 registers) 23.6 ms; two at 4 blocks per SM 22.5 ms, at 3 or 5 blocks
+// 23.7 / 24.5 ms.
+constexpr int kF64PP = 2;
+constexpr int kF64Blocks = 4;
+
+template <bool SAFE>
+__device__ __forceinline__ void msg_f64_4(const DevCtx &c, const EigPack<4> &E, int kind, int id,
+                                          const double *__restrict__ d,
+                                          const double *__restrict__ leaf,
+                                          const long (&p)[kF64PP], int gq,
+                                          double (&v)[kF64PP][4], int (&s)[kF64PP]) {
+  const int C = c.C;
+  if (kind == GEMS_CHILD_TIP) {
+    int st[kF64PP];
+#pragma unroll
+    for (int u = 0; u < kF64PP; u++) st[u] = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
+#pragma unroll
+    for (int u = 0; u < kF64PP; u++) {
+      const double *lt = leaf + (size_t)st[u] * c.block + gq;
+#pragma unroll
+      for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
+      s[u] = 0;
+    }
+  } else {
+    const double *base = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
+    double L[kF64PP][4];
+#pragma unroll
+    for (int u = 0; u < kF64PP; u++) {
+      const double2 *s2 = reinterpret_cast<const double2 *>(base + (size_t)p[u] * c.block + gq * 4);
+      const double2 a = __ldcg(s2), b = __ldcg(s2 + 1);
+      L[u][0] = a.x;
+      L[u][1] = a.y;
+      L[u][2] = b.x;
+      L[u][3] = b.y;
+    }
+    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+#pragma unroll
+    for (int u = 0; u < kF64PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const double di = __ldg(d + i * C + gq);
+#pragma unroll
+      for (int u = 0; u < kF64PP; u++) L[u][i] *= di;
+    }
+#pragma unroll
+    for (int u = 0; u < kF64PP; u++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc = fma(E.evec[x * 4 + i], L[u][i], acc);
+        v[u][x] = acc;
+      }
+  }
+}
+
+template <bool SAFE>
+__global__ void __launch_bounds__(kThreads, kF64Blocks)
+    k_traverse_f64x(DevCtx c, const DevOp *__restrict__ ops, int nops,
+                    const double *__restrict__ tab, size_t stride, const EigPack<4> E, int p0,
+                    int p1) {
+  const int G = c.G, C = c.C, blk = c.block;
+  const int gl = threadIdx.x & (G - 1);
+  const int gq = gl < C ? gl : 0;  // loads of idle lanes stay inside the tables
+  const int per = kThreads / G;
+  const long pb = p0 + (long)blockIdx.x * per * kF64PP + threadIdx.x / G;
+  long p[kF64PP];
+  bool act[kF64PP];
+#pragma unroll
+  for (int u = 0; u < kF64PP; u++) {
+    const long q = pb + (long)u * per;
+    act[u] = q < p1 && gl < C;
+    p[u] = q < p1 ? q : p0;
+  }
+  double *part = static_cast<double *>(c.partials);
+  __shared__ int4 s_ops[kOpChunk];
+  for (int k = 0; k < nops; k++) {
+    if ((k & (kOpChunk - 1)) == 0) stage_ops(ops, k, nops, s_ops);
+    const OpIds op = staged_op(s_ops, k & (kOpChunk - 1));
+    const double *tk = tab + (size_t)k * stride;
+    const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
+    double vl[kF64PP][4], vr[kF64PP][4];
+    int sl[kF64PP], sr[kF64PP];
+    msg_f64_4<SAFE>(c, E, op.l_kind, op.l_id, tk, tk + 2 * blk, p, gq, vl, sl);
+    msg_f64_4<SAFE>(c, E, op.r_kind, op.r_id, tk + blk, tk + 2 * blk + (size_t)(c.unknown + 1) * blk,
+                    p, gq, vr, sr);
+#pragma unroll
+    for (int u = 0; u < kF64PP; u++) {
+      double tmp[4], out[4];
+#pragma unroll
+      for (int x = 0; x < 4; x++) tmp[x] = vl[u][x] * vr[u][x];
+      double lh_max = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int x = 0; x < 4; x++) acc = fma(E.inv[j * 4 + x], tmp[x], acc);
+        out[j] = acc;
+        lh_max = fmax(lh_max, fabs(acc));
+      }
+      if (!act[u]) lh_max = 0.0;
+      if (!SAFE) lh_max = group_max(lh_max, G);
+      if (act[u]) {
+        int s_out = sl[u] + sr[u];
+        if (!tiptip && lh_max < kScaleThr && c.invar[p[u]] == 0.0) {
+#pragma unroll
+          for (int j = 0; j < 4; j++) out[j] = ldexp(out[j], kScaleExp);
+          s_out += 1;
+        }
+        double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)op.dst_slot * c.slot_elems +
+                                                  (size_t)p[u] * blk + gl * 4);
+        d2[0] = make_double2(out[0], out[1]);
+        d2[1] = make_double2(out[2], out[3]);
+        uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
+        if (SAFE)
+          sc[(size_t)p[u] * C + gl] = (uint16_t)s_out;
+        else if (gl == 0)
+          sc[p[u]] = (uint16_t)s_out;
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // Mixed: P_c(t) = evec diag(exp(eval r_c t)) inv_evec in FP64, rounded to FP32, stored
 // [side][x][y][c]; tip tables [side][s][x][c] = P_c . indicator(s).
@@ -485,8 +611,21 @@ int launch_f64(Session *s, int nops, int p0, int p1) {
     E.evec[i] = s->h_evec[i];
     E.inv[i] = s->h_inv[i];
   }
-  const int grid = grid_for(s, p0, p1);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  if constexpr (N == 4) {
+    const long per = (long)(kThreads / s->G) * kF64PP;
+    const int g4 = (int)((p1 - p0 + per - 1) / per);
+    if (safe)
+      k_traverse_f64x<true><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                            s->op_stride, E, p0, p1);
+    else
+      k_traverse_f64x<false><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                             s->op_stride, E, p0, p1);
+    s->launches++;
+    GEMS_CUDA(cudaGetLastError());
+    return GEMS_OK;
+  }
+  const int grid = grid_for(s, p0, p1);
   if (safe)
     k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
                                                                s->op_stride, E, p0, p1);
@@ -528,7 +667,7 @@ int traverse_v2_wave_patterns(const Session *s) {
   const void *fn =
       mixed ? (four ? (safe ? (const void *)k_traverse_mix4<true> : (const void *)k_traverse_mix4<false>)
                     : (safe ? (const void *)k_traverse_mix<20, true> : (const void *)k_traverse_mix<20, false>))
-            : (four ? (safe ? (const void *)k_traverse_f64<4, true> : (const void *)k_traverse_f64<4, false>)
+            : (four ? (safe ? (const void *)k_traverse_f64x<true> : (const void *)k_traverse_f64x<false>)
                     : (safe ? (const void *)k_traverse_f64<20, true> : (const void *)k_traverse_f64<20, false>));
   int nsm = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->desc.device) != cudaSuccess ||
@@ -536,7 +675,7 @@ int traverse_v2_wave_patterns(const Session *s) {
     cudaGetLastError();
     return 0;
   }
-  return per_sm * nsm * (kThreads / s->G) * (mixed && four ? kMix4PP : 1);
+  return per_sm * nsm * (kThreads / s->G) * (four ? (mixed ? kMix4PP : kF64PP) : 1);
 }
 
 int launch_traverse_v2(Session *s, int nops, int p0, int p1) {
