@@ -516,14 +516,14 @@ def ingest_block(aln, local, reps=3):
                     "(creation of a one-slot session included in both)"}
 
 
-def serving_block(local, nsess=48, nreq=800, load=0.7):
+def serving_block(local, nsess=48, nreq=800, load=0.7, taxa=(8, 256), sites=(500, 50_000)):
     """The serving loop on a seeded stream: sessions of 8-256 taxa and 500-50,000 sites
     (log-uniform), 4/20/61 states, 1/4/8 categories, FP64/mixed; NNI + 5-branch Newton + lnL
     per request.  Two passes over the same stream, sessions opened before each: every request
     queued at once gives the capacity; Poisson arrivals at `load` x capacity give the request
     latency.  Session open times (create, upload, first full lnL) are reported apart."""
     from gems_b200 import serve
-    kw = dict(seed=5, taxa=(8, 256), sites=(500, 50_000))
+    kw = dict(seed=5, taxa=taxa, sites=sites)
     specs, reqs = serve.make_stream(nsess, nreq, 1.0, **kw)
     cases = {sp.sid: serve.build_case(sp) for sp in specs}
     srv = serve.Server(device=local, workers=16)
@@ -535,14 +535,17 @@ def serving_block(local, nsess=48, nreq=800, load=0.7):
     records, wall = srv.run(specs, cases, reqs, preopen=True)
     out = serve.summarize(records, wall, specs, cases)
     out.update({"capacity_req_s": cap["throughput_req_s"], "capacity_failed": cap["failed"],
+                "capacity_rejected": cap["rejected"], "capacity_wall_s": cap["wall_s"],
                 "offered_rate_req_s": rate, "load": load,
                 "session_open_ms": {"p50": float(np.percentile(opened, 50)),
                                     "p99": float(np.percentile(opened, 99)),
                                     "max": float(opened.max())},
                 "sessions": nsess, "workers": 16,
-                "stream": "seeded; taxa 8-256, sites 500-50,000 (log-uniform), states {4,20,61}, "
-                          "categories {1,4,8}, fp64/mixed; request = NNI + Newton on the 5 "
-                          "branches around it + lnL; latency at Poisson arrivals, sessions open"})
+                "stream": f"seeded; taxa {taxa[0]}-{taxa[1]}, sites {sites[0]:,}-{sites[1]:,} "
+                          "(log-uniform), states {4,20,61}, categories {1,4,8}, fp64/mixed; "
+                          "request = NNI + Newton on the 5 branches around it + lnL; latency at "
+                          "Poisson arrivals; sessions that fit the HBM budget opened first, the "
+                          "others admitted as memory frees"})
     return out
 
 
@@ -558,7 +561,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the Newton timing and the protein comparison")
-    ap.add_argument("--block", choices=["protein20", "codon64", "serving"], default=None,
+    ap.add_argument("--block", choices=["protein20", "codon64", "serving", "serving_full"],
+                    default=None,
                     help="run only this block of the line and print it (profiling runs)")
     ap.add_argument("--codon-models", type=int, default=64,
                     help="candidate codon models in the batched block (small for profiling)")
@@ -580,7 +584,11 @@ def main():
         from gems_b200 import measure_peaks
         fn = {"protein20": lambda: protein_comparison(args, local, measure_peaks(local)),
               "codon64": lambda: codon_batch_block(local, args.codon_models),
-              "serving": lambda: serving_block(local)}[args.block]
+              "serving": lambda: serving_block(local),
+              # the full serving stream: 200 sessions, 20,000 requests, up to 1024 taxa and
+              # 500,000 sites (minutes; not part of the default line)
+              "serving_full": lambda: serving_block(local, 200, 20_000, taxa=(8, 1024),
+                                                    sites=(500, 500_000))}[args.block]
         print(json.dumps({args.block: fn()}), flush=True)
         return
     dist = None

@@ -10,7 +10,11 @@ partials on the affected paths are recomputed.
 Scheduling:
   * admission by HBM footprint: a session is created on the GPU when its footprint
     (gems_session_footprint) fits the remaining budget; it is released after its last
-    request, which admits the next waiting ones;
+    request, which admits the next waiting ones.  When the session at the head of the
+    admission queue does not fit, idle sessions (no request running or queued) are evicted,
+    least recently used first: the evolved tree (topology and branch lengths) is kept on the
+    host and the session is rebuilt from it at its next request -- partials are a function of
+    the tree, so its results are the same as if it had stayed;
   * continuous batching: requests arrive over time (Poisson); a pool of worker threads takes
     the oldest runnable request of any admitted session whose previous request has finished.
     Each session has its own CUDA stream and the C-ABI calls release the GIL, so the work of
@@ -28,6 +32,7 @@ import dataclasses
 import json
 import threading
 import time
+import types
 
 import numpy as np
 
@@ -65,10 +70,18 @@ def build_case(spec: SessionSpec):
     return tree, model, aln
 
 
-def open_session(spec, case, device=0):
-    tree, model, aln = case
-    return PhyloTree.from_case(tree, model, aln, precision=spec.precision,
+def open_session(spec, case, device=0, tree=None):
+    """The session of a case, on the case's tree or on `tree` (an evicted session's)."""
+    t0, model, aln = case
+    return PhyloTree.from_case(tree if tree is not None else t0, model, aln,
+                               precision=spec.precision,
                                scaling="safe" if spec.nstates == 61 else "norm", device=device)
+
+
+def saved_tree(gt: PhyloTree, ntaxa: int):
+    """Topology and branch lengths of a session's tree, to rebuild it after an eviction."""
+    return types.SimpleNamespace(ntaxa=ntaxa, eu=gt.eu.copy(), ev=gt.ev.copy(),
+                                 length=gt.getBranchLengths())
 
 
 def nni5(gt: PhyloTree, ntaxa: int, rng: np.random.Generator):
@@ -101,12 +114,13 @@ def run_alone(spec, case, nreq, device=0):
 
 
 class Server:
-    def __init__(self, device=0, budget_bytes=None, workers=8):
+    def __init__(self, device=0, budget_bytes=None, workers=8, evict=True):
         import torch
         free, _ = torch.cuda.mem_get_info(device)
         self.device = device
         self.budget = int(0.85 * free) if budget_bytes is None else int(budget_bytes)
         self.workers = workers
+        self.evict = evict
 
     def run(self, specs, cases, requests, preopen=False):
         """requests: list of (arrival_s, sid) in arrival order, arrival times counted from the
@@ -127,6 +141,10 @@ class Server:
         waiting_admit = collections.deque()
         records = [None] * len(requests)
         self.open_ms = []
+        self.evictions = 0
+        saved = {}       # sid -> tree of an evicted session
+        open_fail = collections.Counter()
+        last_used = {}   # sid -> end of its last request
         for sid in fp:
             if fp[sid] > self.budget:
                 state["rejected"].add(sid)
@@ -134,7 +152,7 @@ class Server:
         def open_one(sid):
             t = time.perf_counter()
             try:
-                gt = open_session(spec_of[sid], cases[sid], self.device)
+                gt = open_session(spec_of[sid], cases[sid], self.device, saved.get(sid))
                 gt.computeLikelihood()
             except GemsError:
                 return None
@@ -174,16 +192,35 @@ class Server:
         t0 = time.perf_counter()
 
         def admit_locked():
-            # admit waiting sessions in arrival order while they fit
-            while waiting_admit:
-                sid = waiting_admit[0]
-                if state["used"] + fp[sid] > self.budget:
-                    break
-                waiting_admit.popleft()
-                state["used"] += fp[sid]
-                open_sess[sid] = "opening"
-                return sid
-            return None
+            """The next waiting session to open (arrival order) and the idle sessions to evict
+            first to make room for it, or (None, [])."""
+            if not waiting_admit:
+                return None, []
+            sid = waiting_admit[0]
+            need = state["used"] + fp[sid] - self.budget
+            victims = []
+            if need > 0:
+                if not self.evict:
+                    return None, []
+                idle = sorted((last_used.get(s, 0.0), s) for s, g in open_sess.items()
+                              if isinstance(g, PhyloTree) and s not in busy and not pending[s])
+                freed = 0
+                for _, s in idle:
+                    if freed >= need:
+                        break
+                    victims.append((s, open_sess.pop(s)))
+                    freed += fp[s]
+                if freed < need:  # not enough idle memory: put them back and wait
+                    for s, g in victims:
+                        open_sess[s] = g
+                    return None, []
+                for s, g in victims:  # their memory counts as used until they are closed
+                    saved[s] = saved_tree(g, spec_of[s].ntaxa)  # before any reopen can read it
+                    self.evictions += 1
+            waiting_admit.popleft()
+            state["used"] += fp[sid]
+            open_sess[sid] = "opening"
+            return sid, victims
 
         def dispatcher():
             for i, (arr, sid) in enumerate(requests):
@@ -205,11 +242,12 @@ class Server:
             while True:
                 job = None
                 to_open = None
+                victims = []
                 with lock:
                     while True:
                         if state["done"] >= len(requests):
                             return
-                        to_open = admit_locked()
+                        to_open, victims = admit_locked()
                         if to_open is not None:
                             break
                         best = None
@@ -223,8 +261,22 @@ class Server:
                             break
                         lock.wait(0.05)
                 if to_open is not None:
+                    for s, g in victims:  # evicted (tree saved): free the device memory
+                        g.close()
+                        g.session.close()
+                        with lock:
+                            state["used"] -= fp[s]
+                            lock.notify_all()
                     gt = open_one(to_open)
                     with lock:
+                        if gt is None and open_fail[to_open] < 3:
+                            # out of memory while the budget said it fits: try again later
+                            open_fail[to_open] += 1
+                            state["used"] -= fp[to_open]
+                            del open_sess[to_open]
+                            waiting_admit.append(to_open)
+                            lock.notify_all()
+                            continue
                         if gt is None:
                             state["rejected"].add(to_open)
                             state["used"] -= fp[to_open]
@@ -253,6 +305,7 @@ class Server:
                         records[i]["error"] = err
                         records[i]["spec"] = dataclasses.asdict(spec_of[sid])
                     busy.discard(sid)
+                    last_used[sid] = te
                     state["done"] += 1
                     remaining[sid] -= 1
                     if remaining[sid] == 0:

@@ -56,6 +56,19 @@ def test_admission_by_footprint(gpu):
     assert any(r.get("rejected") for r in records)
 
 
+def test_eviction_keeps_results(gpu):
+    """A budget that holds the largest session and little more: idle sessions are evicted while
+    they still have requests to come, rebuilt from their saved trees, and every session's
+    results stay bit-identical to running it alone."""
+    specs, reqs, cases = workload(nsess=6, nreq=40, seed=6)
+    fps = sorted(s.footprint(cases[s.sid][2].npat) for s in specs)
+    srv = serve.Server(workers=3, budget_bytes=fps[-1] + fps[0])
+    records, _ = srv.run(specs, cases, reqs)
+    assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
+    assert srv.evictions > 0
+    check_same_as_alone(specs, cases, records)
+
+
 def test_concurrent_sessions_of_different_shapes(gpu):
     """Host threads driving tensor-core sessions of different category counts at the same time
     (what the serving loop does): no launch may fail because another thread's session set up
