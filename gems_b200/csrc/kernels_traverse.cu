@@ -621,17 +621,15 @@ int launch_f64(Session *s, int nops, int p0, int p1) {
     else
       k_traverse_f64x<false><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
                                                              s->op_stride, E, p0, p1);
-    s->launches++;
-    GEMS_CUDA(cudaGetLastError());
-    return GEMS_OK;
+  } else {
+    const int grid = grid_for(s, p0, p1);
+    if (safe)
+      k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                                 s->op_stride, E, p0, p1);
+    else
+      k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
+                                                                  s->op_stride, E, p0, p1);
   }
-  const int grid = grid_for(s, p0, p1);
-  if (safe)
-    k_traverse_f64<N, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                               s->op_stride, E, p0, p1);
-  else
-    k_traverse_f64<N, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                                s->op_stride, E, p0, p1);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   return GEMS_OK;
