@@ -745,7 +745,8 @@ int gems_branch_lnl_from_host(gems_session *s, const uint8_t *states, const doub
   GEMS_CUDA(cudaEventRecord(s->start_ev, s->stream));
   GEMS_CUDA(cudaStreamWaitEvent(cs, s->start_ev, 0));
   GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), cs));
-  GEMS_CUDA(cudaMemcpyAsync(s->d_freq, ptn_freq, n * sizeof(double), cudaMemcpyHostToDevice, cs));
+  // +I terms first (the traversal's scaling rule reads them); the weights, which only the branch
+  // terms read, go up after the last tip chunk
   if (ptn_invar)
     GEMS_CUDA(
         cudaMemcpyAsync(s->d_invar, ptn_invar, n * sizeof(double), cudaMemcpyHostToDevice, cs));
@@ -776,6 +777,7 @@ int gems_branch_lnl_from_host(gems_session *s, const uint8_t *states, const doub
     GEMS_CUDA(cudaStreamWaitEvent(s->stream, s->chunk_ev[c], 0));
     if ((st = launch_traverse_v2(s, nops, p0, p1))) return st;
   }
+  GEMS_CUDA(cudaMemcpyAsync(s->d_freq, ptn_freq, n * sizeof(double), cudaMemcpyHostToDevice, cs));
   GEMS_CUDA(cudaMemcpyAsync(s->h_tipmax, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost, cs));
   GEMS_CUDA(cudaStreamSynchronize(cs));
   if ((int)*s->h_tipmax > s->unknown) {
