@@ -700,12 +700,14 @@ def main():
     }
     if rell is not None:
         line["rell"] = rell
-    if rank == 0 and not args.no_extras and args.config == "dna512":
+    # single-GPU blocks and the CPU baseline: one GPU only (under torchrun the other ranks would
+    # wait for them at the closing barrier)
+    if world == 1 and not args.no_extras and args.config == "dna512":
         line["protein20"] = protein_comparison(args, local, peaks)
         line["codon64"] = codon_batch_block(local, args.codon_models)
         line["ingest"] = ingest_block(aln, local)
         line["serving"] = serving_block(local)
-    if rank == 0 and not args.no_cpu:
+    if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tree, model, aln)
     if rank == 0:
         print(json.dumps(line), flush=True)
