@@ -6,9 +6,11 @@ this package only binds it.  There is no CPU fallback: when the library or a CUD
 missing, the calls raise.
 """
 from .api import (GemsError, PhyloTree, Session, STATUS, op_array, branch_struct,
-                  measure_peaks, compress_alignment, Ingest, full_traversal, traverse_batch, branch_lnl_batch,
+                  measure_peaks, check_barrier_timeout, compress_alignment, Ingest, full_traversal,
+                  traverse_batch, branch_lnl_batch,
                   GEMS_CHILD_PARTIAL, GEMS_CHILD_TIP)
 
 __all__ = ["GemsError", "PhyloTree", "Session", "STATUS", "op_array", "branch_struct",
-           "measure_peaks", "compress_alignment", "Ingest", "full_traversal", "traverse_batch", "branch_lnl_batch",
+           "measure_peaks", "check_barrier_timeout", "compress_alignment", "Ingest", "full_traversal",
+           "traverse_batch", "branch_lnl_batch",
            "GEMS_CHILD_PARTIAL", "GEMS_CHILD_TIP"]

@@ -74,6 +74,13 @@ def measure_peaks(device=0):
     return {"fp64_tflops": a.value, "fp32_tflops": b.value, "tf32_tflops": c.value}
 
 
+def check_barrier_timeout(device=0):
+    """Status the grid barrier reports when a wait cannot complete (GEMS_ERR_TIMEOUT = 4)."""
+    st = c_int()
+    _check(_lib.gems().gems_check_barrier_timeout(device, byref(st)), "check_barrier_timeout")
+    return st.value
+
+
 def compress_alignment(seqs, nstates, encoded=False, device=0):
     """Encode and compress an alignment on the device (gems_compress_alignment).
     seqs: [ntaxa][nsites] uint8 (characters, or state codes when encoded).  Returns

@@ -226,6 +226,8 @@ size_t g61_op_doubles(int ncat, int unknown);
 bool g61_supported(const Session *s);
 int launch_prep_ops_g61(Session *s, int nops);
 int launch_traverse_g61(Session *s, int nops);
+// the grid barrier's time-out path, run on purpose (kernels_fp64.cu)
+int check_barrier_timeout(int device, int *status);
 // bootstrap reweighting (kernels_rell.cu)
 int launch_rell_lnl(Session *s, double *d_out);
 int launch_rell_derv(Session *s, double *d_out);

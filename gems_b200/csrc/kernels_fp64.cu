@@ -509,6 +509,12 @@ __device__ bool grid_barrier(unsigned int *bar, unsigned int nblk, int *flag) {
   return ok_sh != 0;
 }
 
+// The barrier's time-out path on purpose: the grid waits for one more block than it has, so
+// every block gives up after kBarrierSpins (about a second) and the flag reads GEMS_ERR_TIMEOUT.
+__global__ void k_barrier_probe(unsigned int *bar, int *flag) {
+  if (grid_barrier(bar, gridDim.x + 1, flag) && threadIdx.x == 0) atomicExch(flag, GEMS_OK);
+}
+
 template <int N>
 __global__ void __launch_bounds__(kThreads) k_newton(DevCtx c, double guess, double x1, double x2,
                                                      double xacc, int maxstep,
@@ -776,6 +782,28 @@ int launch_newton(Session *s, double guess, double min_len, double max_len, doub
   *opt_len = s->h_result[0];
   *nevals = (int)s->h_result[1];
   return (int)s->h_result[2];
+}
+
+int check_barrier_timeout(int device, int *status) {
+  GEMS_CUDA(cudaSetDevice(device));
+  unsigned int *bar = nullptr;
+  int *flag = nullptr;
+  GEMS_CUDA(cudaMalloc((void **)&bar, 2 * sizeof(unsigned int)));
+  cudaError_t e = cudaMalloc((void **)&flag, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(bar, 0, 2 * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    void *args[] = {&bar, &flag};
+    e = cudaLaunchCooperativeKernel((void *)k_barrier_probe, dim3(2), dim3(32), args, 0, nullptr);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int h = -1;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(bar);
+  cudaFree(flag);
+  if (e != cudaSuccess) return cuda_status(e, "barrier probe");
+  *status = h;
+  return GEMS_OK;
 }
 
 int launch_unpack_partial(Session *s, int slot, double *d_out) {

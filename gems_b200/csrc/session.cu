@@ -481,6 +481,11 @@ int gems_session_destroy(gems_session *s) {
   return GEMS_OK;
 }
 
+int gems_check_barrier_timeout(int device, int *status) {
+  if (!status) return GEMS_ERR_BAD_ARG;
+  return check_barrier_timeout(device, status);
+}
+
 int gems_session_sync(gems_session *s) {
   if (!s) return GEMS_ERR_BAD_ARG;
   GEMS_CUDA(cudaStreamSynchronize(s->stream));

@@ -250,6 +250,11 @@ void gems_ingest_destroy(gems_ingest *g);
  * compute rooflines): FP64 and FP32 FMA throughput of the CUDA cores and the dense TF32 rate of
  * the tcgen05 tensor cores, in TFLOP/s.  Takes a few tens of milliseconds. */
 int gems_measure_peaks(int device, double *fp64_tflops, double *fp32_tflops, double *tf32_tflops);
+/* Runs the time-out path of the bounded grid barrier that the device Newton loop uses (no
+ * counterpart in the reference): a two-block cooperative launch waits for a third block that
+ * never comes, gives up after about a second and reports GEMS_ERR_TIMEOUT in *status; the
+ * device stays usable.  Allocates a few bytes.  For failure-handling tests. */
+int gems_check_barrier_timeout(int device, int *status);
 
 /* ---- tree mirror (PhyloTree calls on the path) ---- */
 typedef struct gems_tree gems_tree;
