@@ -11,18 +11,24 @@
 // a 160-taxon tree with long branches it moved partials by up to 2.5e-8 of their pattern's
 // largest value, measured in plain FP64 numpy as well.)
 //
-// One CTA per tile of up to 64 rows = tp patterns x C categories (tp = 64 / C rounded down to a
-// multiple of 8), stored category-major in the tile (row = c * tp + pattern), 128 threads as
-// 8 x 16: thread (ty, tx) owns rows ty*8..ty*8+7 -- all of one category -- and columns tx,
-// tx+16, tx+32, tx+48 (32 FP64 accumulators); two CTAs per SM, so that one's loads overlap the
-// other's GEMMs (measured against 128-row tiles of 256 threads: 7.0 -> 6.2 ms on one 200-taxon
-// codon model).  The A operand of a child (its partial rows) is staged
-// k-major in shared memory (sA[k][row]: a thread reads its 8 rows as 4 double2 per k);
-// inv_evec^T stays in shared memory for the whole traversal; E_c^T is read through L1 from the
-// op table, stored [side][c][k][64 columns] by the prep kernel.  A tip child's V is a row of the
-// op's leaf table (E_c . tip vector), gathered by state.  Scaling: SAFE per row (max over the
-// row's 61 values: own columns, then a shuffle over the 16 tx lanes of the half-warp); NORM per
-// pattern (row maxima through shared memory).
+// Two kernels share the per-op tables (prep) and the row layout of the partial slots:
+// - k_traverse_g61m (SAFE scaling): the GEMMs on the FP64 tensor cores (mma.sync m8n8k4 f64),
+//   one CTA per tile of 64 patterns of ONE category -- categories are independent under SAFE
+//   scaling -- so that a CTA reads one E table per side and op (32 KB) instead of C of them;
+// - k_traverse_g61 (NORM scaling, whose per-pattern maximum spans the categories): FP64 FMA,
+//   one CTA per tile of up to 64 rows = tp patterns x C categories (tp = 64 / C rounded down to
+//   a multiple of 8), stored category-major (row = c * tp + pattern), 128 threads as 8 x 16:
+//   thread (ty, tx) owns rows ty*8..ty*8+7 -- all of one category -- and columns tx, tx+16,
+//   tx+32, tx+48 (32 FP64 accumulators).
+// Both: two CTAs per SM, so that one's loads overlap the other's GEMMs; the A operand of a child
+// (its partial rows) staged k-major in shared memory; inv_evec^T in shared memory for the whole
+// traversal; E_c^T read through L1 from the op table (stored [side][c][k][64 columns] by the
+// prep kernel) and prefetched into L1 while the child's rows load.  A tip child's V is a row of
+// the op's leaf table (E_c . tip vector), gathered by state.  The tensor-core products come out
+// bit-identical to the FMA ones (the tests compare every partial).  Measured on one 200-taxon
+// codon model (3,780 patterns): per-row kernel 26.6 ms (+G4); FMA tiles of 128 rows 7.0 ms, with
+// the L1 prefetch 5.9 ms, 64-row tiles at two CTAs per SM 5.3 ms; tensor cores with mixed
+// categories per tile 5.9 ms (spills), one category per tile 4.7 ms (+R8: 11.9 -> 9.6 ms).
 #include <string>
 
 #include "gems_internal.cuh"
@@ -32,7 +38,7 @@ namespace gems {
 namespace {
 
 constexpr int kN = 61;
-constexpr int kK = 62;       // padded contraction length (even: double2 steps)
+constexpr int kK = 64;       // padded contraction length (MMA k-steps of 4)
 constexpr int kNC = 64;      // padded output columns
 constexpr int kRows = 64;    // rows per tile
 constexpr int kSaLd = kRows + 2;
@@ -117,6 +123,20 @@ struct TileMap {
   __device__ bool valid(int r) const { return r < nrow && pattern(r) < P; }
   // offset of the row's first state in the slot
   __device__ size_t off(int r) const { return ((size_t)pattern(r) * C + cat(r)) * kN; }
+};
+
+// SAFE only: a tile of 64 patterns of one category (categories are independent under SAFE
+// scaling), so a CTA reads one E table per side instead of C
+struct TileMap1 {
+  int C, tp, nrow, c0;
+  long p0, P;
+  __device__ int cat(int) const { return c0; }
+  __device__ long pattern(int r) const { return p0 + r; }
+  __device__ bool valid(int r) const { return p0 + r < P; }
+  __device__ size_t off(int r) const { return ((size_t)(p0 + r) * C + c0) * kN; }
+  __device__ int tile_row(int g) const { return g < kRows ? g : -1; }
+  __device__ bool row_ok(int g) const { return g < kRows && p0 + g < P; }
+  __device__ size_t slot_row(int g) const { return (size_t)(p0 + g) * C + c0; }
 };
 
 // V of one child for the thread's rows and columns, and its scale counts (per row: SAFE; the
@@ -287,6 +307,196 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// The same traversal with the GEMMs on the FP64 tensor cores (mma.sync m8n8k4 f64: one warp
+// instruction does 8 x 8 x 4 multiply-adds).  Warp w owns rows 16w..16w+15 as two 8-row blocks
+// (each of one category, tp being a multiple of 8) and all 64 columns as eight 8-column blocks;
+// lane l holds rows l/4 and columns 2(l%4), 2(l%4)+1 of each 8 x 8 block (the instruction's
+// accumulator layout).  Operand rows in shared memory are 72 doubles apart, so that the four
+// k-rows of a fragment load fall in two bank halves.
+// ---------------------------------------------------------------------------------------
+constexpr int kLdM = 72;
+constexpr size_t kSmemM = sizeof(double) * 2 * (size_t)kK * kLdM;
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// acc[rb][cb] = A[rows of row block rb][k] . B_rb[k][columns of block cb] over k < kK, with
+// A k-major in shared memory (row stride kLdM) and B_rb = B0 or B1 (row stride ldb)
+template <bool GLOBAL_B>
+__device__ __forceinline__ void gemm_mma(const double *__restrict__ sA,
+                                         const double *__restrict__ B0,
+                                         const double *__restrict__ B1, int ldb, int w, int lane,
+                                         double (&acc)[2][8][2]) {
+#pragma unroll
+  for (int rb = 0; rb < 2; rb++)
+#pragma unroll
+    for (int cb = 0; cb < 8; cb++) acc[rb][cb][0] = acc[rb][cb][1] = 0.0;
+  const int kr = lane & 3, rc = lane >> 2;
+  const bool same = B0 == B1;
+#pragma unroll 2
+  for (int k0 = 0; k0 < kK; k0 += 4) {
+    const double *ar = sA + (k0 + kr) * kLdM + 16 * w + rc;
+    const double a0 = ar[0], a1 = ar[8];
+    const double *b0 = B0 + (size_t)(k0 + kr) * ldb + rc;
+    double bv[8];
+#pragma unroll
+    for (int cb = 0; cb < 8; cb++) bv[cb] = GLOBAL_B ? __ldg(b0 + 8 * cb) : b0[8 * cb];
+#pragma unroll
+    for (int cb = 0; cb < 8; cb++) dmma(acc[0][cb], a0, bv[cb]);
+    if (same) {
+#pragma unroll
+      for (int cb = 0; cb < 8; cb++) dmma(acc[1][cb], a1, bv[cb]);
+    } else {
+      const double *b1 = B1 + (size_t)(k0 + kr) * ldb + rc;
+#pragma unroll
+      for (int cb = 0; cb < 8; cb++) bv[cb] = GLOBAL_B ? __ldg(b1 + 8 * cb) : b1[8 * cb];
+#pragma unroll
+      for (int cb = 0; cb < 8; cb++) dmma(acc[1][cb], a1, bv[cb]);
+    }
+  }
+}
+
+template <bool SAFE>
+__device__ __forceinline__ void child_v_mma(const DevCtx &c, const TileMap1 &tm, int kind, int id,
+                                            const double *et, const double *leaf, double *sA,
+                                            int w, int lane, double (&v)[2][8][2], int (&s)[2]) {
+  const int kr = lane & 3, rc = lane >> 2;
+  if (kind == GEMS_CHILD_TIP) {
+#pragma unroll
+    for (int rb = 0; rb < 2; rb++) {
+      const int r = 16 * w + 8 * rb + rc;
+      const bool ok = tm.valid(r);
+      const int st = ok ? min((int)c.tips[(size_t)id * c.P + tm.pattern(r)], c.unknown) : 0;
+      const double *row = leaf + ((size_t)st * tm.C + tm.cat(r)) * kN;
+#pragma unroll
+      for (int cb = 0; cb < 8; cb++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int col = 8 * cb + 2 * kr + e;
+          v[rb][cb][e] = ok && col < kN ? __ldg(row + col) : 0.0;
+        }
+      s[rb] = 0;
+    }
+    return;
+  }
+  {
+    const char *e0 = reinterpret_cast<const char *>(et);
+    const int lines = (int)(et_doubles(tm.C) * sizeof(double) / 128);
+    for (int l = threadIdx.x; l < lines; l += blockDim.x)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(e0 + (size_t)l * 128));
+  }
+  const double *src = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
+  constexpr int kPer = kRows * kK / kThreadsG;
+  static_assert(kRows * kK % kThreadsG == 0, "whole loads per thread");
+  double a[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int idx = threadIdx.x + u * kThreadsG;
+    const int g = idx / kK, k = idx - g * kK;
+    a[u] = (tm.row_ok(g) && k < kN) ? __ldcg(src + tm.slot_row(g) * kN + k) : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int idx = threadIdx.x + u * kThreadsG;
+    const int g = idx / kK, k = idx - g * kK;
+    const int r = tm.tile_row(g);
+    if (r >= 0) sA[k * kLdM + r] = a[u];
+  }
+  const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+#pragma unroll
+  for (int rb = 0; rb < 2; rb++) {
+    const int r = 16 * w + 8 * rb + rc;
+    const long p = tm.pattern(r);
+    s[rb] = tm.valid(r) ? (SAFE ? sc[(size_t)p * tm.C + tm.cat(r)] : sc[p]) : 0;
+  }
+  __syncthreads();
+  const double *b = et + (size_t)tm.c0 * kK * kNC;
+  gemm_mma<true>(sA, b, b, kNC, w, lane, v);
+}
+
+template <bool SAFE>
+__global__ void __launch_bounds__(kThreadsG, 2)
+    k_traverse_g61m(DevCtx c, const DevOp *__restrict__ ops, int nops,
+                    const double *__restrict__ tab, size_t stride) {
+  static_assert(SAFE, "one category per tile: SAFE scaling only");
+  extern __shared__ __align__(16) double smem[];
+  double *sIv = smem;                  // [kK][kLdM]: inv_evec[j][x] at [x][j]
+  double *sA = sIv + kK * kLdM;        // [kK][kLdM]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, kr = lane & 3, rc = lane >> 2;
+  TileMap1 tm;
+  tm.C = c.C;
+  tm.tp = kRows;
+  tm.nrow = kRows;
+  tm.c0 = blockIdx.x % c.C;
+  tm.p0 = (long)(blockIdx.x / c.C) * kRows;
+  tm.P = c.P;
+  for (int idx = threadIdx.x; idx < kK * kLdM; idx += blockDim.x) {
+    const int k = idx / kLdM, x = idx - k * kLdM;
+    sIv[idx] = (k < kN && x < kN) ? c.inv_evec[x * kN + k] : 0.0;
+    sA[idx] = 0.0;  // rows past the tile's rows (64 % C) are never written
+  }
+  double *part = static_cast<double *>(c.partials);
+  const int blk = c.C * kN;
+  for (int kop = 0; kop < nops; kop++) {
+    const DevOp op = ops[kop];
+    const double *tk = tab + (size_t)kop * stride;
+    const double *leafL = tk + 2 * et_doubles(c.C);
+    const double *leafR = leafL + (size_t)(c.unknown + 1) * blk;
+    const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
+    double vl[2][8][2], o[2][8][2];
+    int sl[2], sr[2];
+    __syncthreads();
+    child_v_mma<SAFE>(c, tm, op.l_kind, op.l_id, tk, leafL, sA, w, lane, vl, sl);
+    __syncthreads();
+    child_v_mma<SAFE>(c, tm, op.r_kind, op.r_id, tk + et_doubles(c.C), leafR, sA, w, lane, o, sr);
+    __syncthreads();
+#pragma unroll
+    for (int rb = 0; rb < 2; rb++)
+#pragma unroll
+      for (int cb = 0; cb < 8; cb++)
+#pragma unroll
+        for (int e = 0; e < 2; e++)
+          sA[(8 * cb + 2 * kr + e) * kLdM + 16 * w + 8 * rb + rc] = vl[rb][cb][e] * o[rb][cb][e];
+    __syncthreads();
+    gemm_mma<false>(sA, sIv, sIv, kLdM, w, lane, o);
+    double m[2];
+#pragma unroll
+    for (int rb = 0; rb < 2; rb++) {
+      double x = 0.0;
+#pragma unroll
+      for (int cb = 0; cb < 8; cb++) x = fmax(x, fmax(fabs(o[rb][cb][0]), fabs(o[rb][cb][1])));
+      x = fmax(x, __shfl_xor_sync(0xffffffffu, x, 1));
+      x = fmax(x, __shfl_xor_sync(0xffffffffu, x, 2));
+      m[rb] = x;
+    }
+    uint16_t *scd = c.scale + (size_t)op.dst_slot * c.slot_scale;
+    double *dst = part + (size_t)op.dst_slot * c.slot_elems;
+#pragma unroll
+    for (int rb = 0; rb < 2; rb++) {
+      const int r = 16 * w + 8 * rb + rc;
+      if (!tm.valid(r)) continue;
+      const long p = tm.pattern(r);
+      const int cat = tm.cat(r);
+      int s_out = sl[rb] + sr[rb];
+      const bool scale = !tiptip && m[rb] < kScaleThr && c.invar[p] == 0.0;
+      if (scale) s_out += 1;
+      double *row = dst + tm.off(r);
+#pragma unroll
+      for (int cb = 0; cb < 8; cb++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int col = 8 * cb + 2 * kr + e;
+          if (col < kN) row[col] = scale ? ldexp(o[rb][cb][e], kScaleExp) : o[rb][cb][e];
+        }
+      if (kr == 0) scd[(size_t)p * tm.C + cat] = (uint16_t)s_out;
+    }
+  }
+}
+
 }  // namespace
 
 size_t g61_op_doubles(int ncat, int unknown) {
@@ -317,12 +527,13 @@ int launch_traverse_g61(Session *s, int nops) {
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   // the limit is a per-kernel attribute shared by every thread of the process: always the same
   // value
-  if (safe) {
-    GEMS_CUDA(cudaFuncSetAttribute(k_traverse_g61<true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemG));
-    k_traverse_g61<true><<<grid, kThreadsG, kSmemG, s->stream>>>(s->ctx(), s->d_ops, nops,
-                                                                  s->d_opmats, s->op_stride);
-  } else {
+  if (safe) {  // FP64 tensor cores, one category per tile
+    const int g = (s->P + kRows - 1) / kRows * s->desc.ncat;
+    GEMS_CUDA(cudaFuncSetAttribute(k_traverse_g61m<true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemM));
+    k_traverse_g61m<true><<<g, kThreadsG, kSmemM, s->stream>>>(s->ctx(), s->d_ops, nops,
+                                                                s->d_opmats, s->op_stride);
+  } else {  // NORM: a pattern's categories in one tile, FP64 FMA
     GEMS_CUDA(cudaFuncSetAttribute(k_traverse_g61<false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemG));
     k_traverse_g61<false><<<grid, kThreadsG, kSmemG, s->stream>>>(s->ctx(), s->d_ops, nops,
