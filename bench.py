@@ -38,6 +38,7 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -143,7 +144,7 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"clocks_bench_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
