@@ -629,6 +629,9 @@ def main():
                              "algorithmic_bytes_per_launch": alg, "avg_launch_ms": kms,
                              "traffic": read_traffic(f"traverse_{prec}_{args.config}.md")},
             }
+            pp, blocks, tuned = gt.session.traversal_shape()
+            forms[prec]["launch_shape"] = {"patterns_per_lane_group": pp, "blocks_per_sm": blocks,
+                                           "tuned": tuned}
             if not args.no_extras and rank == 0:
                 forms[prec]["newton"] = time_newton(gt, tree, stream)
             if keep is not None:

@@ -333,6 +333,19 @@ class Session:
         cores."""
         _check(self.lib.gems_session_set_option(self.handle, 1, int(on)), "set_option")
 
+    def set_autotune(self, on=True, force_shape=None):
+        """Tune the 4-state traversal's launch shape on its first large traversal (default), or
+        force shape k of the kernel's list (comparisons)."""
+        v = 2 + int(force_shape) if force_shape is not None else int(on)
+        _check(self.lib.gems_session_set_option(self.handle, 3, v), "set_option")
+
+    def traversal_shape(self):
+        """(patterns per lane group, blocks per SM, tuned) of the 4-state traversal in use."""
+        a, b, t = c_int(), c_int(), c_int()
+        _check(self.lib.gems_session_traversal_shape(self.handle, byref(a), byref(b), byref(t)),
+               "traversal_shape")
+        return a.value, b.value, bool(t.value)
+
     def set_tiled_fp64(self, on=True):
         """61-state FP64 traversal as register-tiled GEMMs (default) or the per-row kernel."""
         _check(self.lib.gems_session_set_option(self.handle, 2, int(on)), "set_option")

@@ -151,6 +151,9 @@ struct Session {
   bool tc_enabled = true;
   // FP64 61-state traversal as register-tiled GEMMs (else the per-row kernel)
   bool g61_enabled = true;
+  // 4-state traversal: launch shape chosen by timing the variants on the first large traversal
+  bool autotune = true;
+  int force_shape = -1;  // >= 0: that launch shape, no tuning (comparisons)
   size_t op_stride_tc = 0;
   // FP32 partials stored tile-major (20- and 61-state mixed forms); elements per slot
   bool tiled = false;
@@ -210,6 +213,9 @@ int launch_prep_ops_v2(Session *s, int nops);
 int launch_traverse_v2(Session *s, int nops, int p0, int p1);
 // patterns that one wave of resident blocks of the traversal kernel covers (0 if unknown)
 int traverse_v2_wave_patterns(const Session *s);
+// launch shape of the 4-state traversal in use for this session's class (patterns per lane
+// group, blocks per SM); returns 1 while the tuner has not chosen yet, else 0
+int traverse_v2_shape(const Session *s, int *patterns_per_group, int *blocks_per_sm);
 // tcgen05 split-TF32 traversal for 20 states (kernels_tc.cu)
 size_t tc20_op_floats(int ncat, int unknown);
 bool tc20_supported(const Session *s);

@@ -17,7 +17,10 @@
 //
 // Mixed form (FP32 real space): the transition matrices P_c(t) are op-dependent; they are
 // stored [x][c][y], so lane c reads its row x of P_c as contiguous float4s.
+#include <array>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "gems_internal.cuh"
@@ -207,26 +210,24 @@ __global__ void __launch_bounds__(kThreads) k_traverse_f64(DevCtx c, const DevOp
   }
 }
 
-// FP64, 4 states: kF64PP patterns per lane group (as k_traverse_mix4), same arithmetic in the
-// same order as msg_f64 / k_traverse_f64.  Measured on the 512-taxon, 1M-pattern case: one
-// pattern per group (40 registers) 23.6 ms; two at 4 blocks per SM 22.5 ms, at 3 or 5 blocks
-// 23.7 / 24.5 ms.
-constexpr int kF64PP = 2;
-constexpr int kF64Blocks = 4;
-
-template <bool SAFE>
+// FP64, 4 states: PP patterns per lane group at B blocks per SM (as k_traverse_mix4), same
+// arithmetic in the same order as msg_f64 / k_traverse_f64, so every (PP, B) gives the same
+// values.  Measured on the 512-taxon, 1M-pattern case: one pattern per group (40 registers)
+// 23.6 ms; two at 4 blocks per SM 22.5 ms, at 3 or 5 blocks 23.7 / 24.5 ms; three at 3 blocks
+// 22.4 ms; four at 2 blocks 24.7 ms.  The variant in use is picked by the tuner below.
+template <bool SAFE, int PP>
 __device__ __forceinline__ void msg_f64_4(const DevCtx &c, const EigPack<4> &E, int kind, int id,
                                           const double *__restrict__ d,
                                           const double *__restrict__ leaf,
-                                          const long (&p)[kF64PP], int gq,
-                                          double (&v)[kF64PP][4], int (&s)[kF64PP]) {
+                                          const long (&p)[PP], int gq,
+                                          double (&v)[PP][4], int (&s)[PP]) {
   const int C = c.C;
   if (kind == GEMS_CHILD_TIP) {
-    int st[kF64PP];
+    int st[PP];
 #pragma unroll
-    for (int u = 0; u < kF64PP; u++) st[u] = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
+    for (int u = 0; u < PP; u++) st[u] = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
 #pragma unroll
-    for (int u = 0; u < kF64PP; u++) {
+    for (int u = 0; u < PP; u++) {
       const double *lt = leaf + (size_t)st[u] * c.block + gq;
 #pragma unroll
       for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
@@ -234,9 +235,9 @@ __device__ __forceinline__ void msg_f64_4(const DevCtx &c, const EigPack<4> &E, 
     }
   } else {
     const double *base = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
-    double L[kF64PP][4];
+    double L[PP][4];
 #pragma unroll
-    for (int u = 0; u < kF64PP; u++) {
+    for (int u = 0; u < PP; u++) {
       const double2 *s2 = reinterpret_cast<const double2 *>(base + (size_t)p[u] * c.block + gq * 4);
       const double2 a = __ldcg(s2), b = __ldcg(s2 + 1);
       L[u][0] = a.x;
@@ -246,15 +247,15 @@ __device__ __forceinline__ void msg_f64_4(const DevCtx &c, const EigPack<4> &E, 
     }
     const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
 #pragma unroll
-    for (int u = 0; u < kF64PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
+    for (int u = 0; u < PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const double di = __ldg(d + i * C + gq);
 #pragma unroll
-      for (int u = 0; u < kF64PP; u++) L[u][i] *= di;
+      for (int u = 0; u < PP; u++) L[u][i] *= di;
     }
 #pragma unroll
-    for (int u = 0; u < kF64PP; u++)
+    for (int u = 0; u < PP; u++)
 #pragma unroll
       for (int x = 0; x < 4; x++) {
         double acc = 0.0;
@@ -265,8 +266,8 @@ __device__ __forceinline__ void msg_f64_4(const DevCtx &c, const EigPack<4> &E, 
   }
 }
 
-template <bool SAFE>
-__global__ void __launch_bounds__(kThreads, kF64Blocks)
+template <bool SAFE, int PP, int B>
+__global__ void __launch_bounds__(kThreads, B)
     k_traverse_f64x(DevCtx c, const DevOp *__restrict__ ops, int nops,
                     const double *__restrict__ tab, size_t stride, const EigPack<4> E, int p0,
                     int p1) {
@@ -274,11 +275,11 @@ __global__ void __launch_bounds__(kThreads, kF64Blocks)
   const int gl = threadIdx.x & (G - 1);
   const int gq = gl < C ? gl : 0;  // loads of idle lanes stay inside the tables
   const int per = kThreads / G;
-  const long pb = p0 + (long)blockIdx.x * per * kF64PP + threadIdx.x / G;
-  long p[kF64PP];
-  bool act[kF64PP];
+  const long pb = p0 + (long)blockIdx.x * per * PP + threadIdx.x / G;
+  long p[PP];
+  bool act[PP];
 #pragma unroll
-  for (int u = 0; u < kF64PP; u++) {
+  for (int u = 0; u < PP; u++) {
     const long q = pb + (long)u * per;
     act[u] = q < p1 && gl < C;
     p[u] = q < p1 ? q : p0;
@@ -290,13 +291,13 @@ __global__ void __launch_bounds__(kThreads, kF64Blocks)
     const OpIds op = staged_op(s_ops, k & (kOpChunk - 1));
     const double *tk = tab + (size_t)k * stride;
     const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
-    double vl[kF64PP][4], vr[kF64PP][4];
-    int sl[kF64PP], sr[kF64PP];
-    msg_f64_4<SAFE>(c, E, op.l_kind, op.l_id, tk, tk + 2 * blk, p, gq, vl, sl);
-    msg_f64_4<SAFE>(c, E, op.r_kind, op.r_id, tk + blk, tk + 2 * blk + (size_t)(c.unknown + 1) * blk,
+    double vl[PP][4], vr[PP][4];
+    int sl[PP], sr[PP];
+    msg_f64_4<SAFE, PP>(c, E, op.l_kind, op.l_id, tk, tk + 2 * blk, p, gq, vl, sl);
+    msg_f64_4<SAFE, PP>(c, E, op.r_kind, op.r_id, tk + blk, tk + 2 * blk + (size_t)(c.unknown + 1) * blk,
                     p, gq, vr, sr);
 #pragma unroll
-    for (int u = 0; u < kF64PP; u++) {
+    for (int u = 0; u < PP; u++) {
       double tmp[4], out[4];
 #pragma unroll
       for (int x = 0; x < 4; x++) tmp[x] = vl[u][x] * vr[u][x];
@@ -488,28 +489,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_traverse_mix(DevCtx c, const De
   }
 }
 
-// 4 states: the kernel is latency-bound on its child loads.  Each lane group handles kMix4PP
-// patterns, kThreads / G apart, so that a warp has the child loads of all of them in flight at
+// 4 states: the kernel is latency-bound on its child loads.  Each lane group handles PP
+// patterns (at B blocks per SM), kThreads / G apart, so that a warp has the child loads of all of them in flight at
 // once and loads each P row once for all of them; same arithmetic, in the same order, as
 // msg_mix / k_traverse_mix.  Measured on the 512-taxon, 1M-pattern case: one pattern per group
 // at 8 blocks per SM (32 registers) 14.8 ms; two at 5 blocks (48 registers) 12.6 ms; two at 4
-// or 6 blocks 14.8 / 12.7 ms; four at 3 blocks 12.8 ms.
-constexpr int kMix4PP = 2;
-constexpr int kMix4Blocks = 5;
-
-template <bool SAFE>
+// or 6 blocks 14.8 / 12.7 ms; four at 3 blocks 12.8 ms.  The variant in use is picked by the
+// tuner below; every (PP, B) gives the same values.
+template <bool SAFE, int PP>
 __device__ __forceinline__ void msg_mix4(const DevCtx &c, int kind, int id,
                                          const float *__restrict__ Pm,
                                          const float *__restrict__ leaf,
-                                         const long (&p)[kMix4PP], int gq,
-                                         float (&v)[kMix4PP][4], int (&s)[kMix4PP]) {
+                                         const long (&p)[PP], int gq,
+                                         float (&v)[PP][4], int (&s)[PP]) {
   const int C = c.C;
   if (kind == GEMS_CHILD_TIP) {
-    int st[kMix4PP];
+    int st[PP];
 #pragma unroll
-    for (int u = 0; u < kMix4PP; u++) st[u] = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
+    for (int u = 0; u < PP; u++) st[u] = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
 #pragma unroll
-    for (int u = 0; u < kMix4PP; u++) {
+    for (int u = 0; u < PP; u++) {
       const float *lt = leaf + (size_t)st[u] * c.block + gq;
 #pragma unroll
       for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
@@ -517,36 +516,36 @@ __device__ __forceinline__ void msg_mix4(const DevCtx &c, int kind, int id,
     }
   } else {
     const float *base = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems;
-    float4 L[kMix4PP];
+    float4 L[PP];
 #pragma unroll
-    for (int u = 0; u < kMix4PP; u++)
+    for (int u = 0; u < PP; u++)
       L[u] = __ldcg(reinterpret_cast<const float4 *>(base + mix_off<4>(c, p[u], gq)));
     const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
 #pragma unroll
-    for (int u = 0; u < kMix4PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
+    for (int u = 0; u < PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
 #pragma unroll
     for (int x = 0; x < 4; x++) {
       const float4 r = __ldg(reinterpret_cast<const float4 *>(Pm + ((size_t)x * C + gq) * 4));
 #pragma unroll
-      for (int u = 0; u < kMix4PP; u++)
+      for (int u = 0; u < PP; u++)
         v[u][x] = fmaf(r.w, L[u].w, fmaf(r.z, L[u].z, fmaf(r.y, L[u].y, fmaf(r.x, L[u].x, 0.f))));
     }
   }
 }
 
-template <bool SAFE>
-__global__ void __launch_bounds__(kThreads, kMix4Blocks)
+template <bool SAFE, int PP, int B>
+__global__ void __launch_bounds__(kThreads, B)
     k_traverse_mix4(DevCtx c, const DevOp *__restrict__ ops, int nops,
                     const float *__restrict__ tab, size_t stride_f, int p0, int p1) {
   const int G = c.G, C = c.C;
   const int gl = threadIdx.x & (G - 1);
   const int gq = gl < C ? gl : 0;  // loads of idle lanes stay inside the tables
   const int per = kThreads / G;
-  const long pb = p0 + (long)blockIdx.x * per * kMix4PP + threadIdx.x / G;
-  long p[kMix4PP];
-  bool act[kMix4PP];
+  const long pb = p0 + (long)blockIdx.x * per * PP + threadIdx.x / G;
+  long p[PP];
+  bool act[PP];
 #pragma unroll
-  for (int u = 0; u < kMix4PP; u++) {
+  for (int u = 0; u < PP; u++) {
     const long q = pb + (long)u * per;
     act[u] = q < p1 && gl < C;
     p[u] = q < p1 ? q : p0;
@@ -559,13 +558,13 @@ __global__ void __launch_bounds__(kThreads, kMix4Blocks)
     const OpIds op = staged_op(s_ops, k & (kOpChunk - 1));
     const float *tk = tab + (size_t)k * stride_f;
     const bool tiptip = op.l_kind == GEMS_CHILD_TIP && op.r_kind == GEMS_CHILD_TIP;
-    float vl[kMix4PP][4], vr[kMix4PP][4];
-    int sl[kMix4PP], sr[kMix4PP];
-    msg_mix4<SAFE>(c, op.l_kind, op.l_id, tk, tk + 2 * nnC, p, gq, vl, sl);
-    msg_mix4<SAFE>(c, op.r_kind, op.r_id, tk + nnC, tk + 2 * nnC + (size_t)(c.unknown + 1) * c.block,
+    float vl[PP][4], vr[PP][4];
+    int sl[PP], sr[PP];
+    msg_mix4<SAFE, PP>(c, op.l_kind, op.l_id, tk, tk + 2 * nnC, p, gq, vl, sl);
+    msg_mix4<SAFE, PP>(c, op.r_kind, op.r_id, tk + nnC, tk + 2 * nnC + (size_t)(c.unknown + 1) * c.block,
                    p, gq, vr, sr);
 #pragma unroll
-    for (int u = 0; u < kMix4PP; u++) {
+    for (int u = 0; u < PP; u++) {
       float lh_max = 0.f;
 #pragma unroll
       for (int x = 0; x < 4; x++) {
@@ -599,6 +598,112 @@ inline int grid_for(const Session *s, int p0, int p1) {
   return (int)((threads + kThreads - 1) / kThreads);
 }
 
+// ---------------------------------------------------------------------------------------
+// Launch shapes of the 4-state kernels and their tuner.  A variant is (patterns per lane
+// group, blocks per SM); all give the same values, so the choice only moves the time.  The
+// first full traversal of a session class (precision, scaling, categories, pattern count to
+// the power of two) with enough work times every variant once on its own op list and keeps
+// the fastest for the process; smaller traversals and pattern ranges use the cached choice or
+// the first variant (the measured best on the 512-taxon case).
+// ---------------------------------------------------------------------------------------
+struct Variant4 {
+  int pp, blocks;
+  const void *fn[2];  // [safe]
+};
+template <int PP, int B>
+Variant4 mix_variant() {
+  return {PP, B, {(const void *)k_traverse_mix4<false, PP, B>, (const void *)k_traverse_mix4<true, PP, B>}};
+}
+template <int PP, int B>
+Variant4 f64_variant() {
+  return {PP, B, {(const void *)k_traverse_f64x<false, PP, B>, (const void *)k_traverse_f64x<true, PP, B>}};
+}
+const Variant4 *variants4(bool mixed, int *n) {
+  static const Variant4 mix[] = {mix_variant<2, 5>(), mix_variant<2, 6>(), mix_variant<4, 3>(),
+                                 mix_variant<1, 8>()};
+  static const Variant4 f64[] = {f64_variant<2, 4>(), f64_variant<3, 3>(), f64_variant<1, 6>()};
+  *n = mixed ? 4 : 3;
+  return mixed ? mix : f64;
+}
+constexpr long long kTuneMinWork = 1ll << 22;  // patterns x ops below which no tuning is done
+
+std::mutex g_tune_mu;
+std::map<std::array<int, 4>, int> g_tune;
+
+std::array<int, 4> tune_key(const Session *s, bool mixed) {
+  int b = 0;
+  while (b < 30 && (1 << (b + 1)) <= s->P) b++;
+  return {mixed ? 1 : 0, s->desc.scaling == GEMS_SCALE_SAFE ? 1 : 0, s->desc.ncat, b};
+}
+int tuned4(const Session *s, bool mixed) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto it = g_tune.find(tune_key(s, mixed));
+  return it == g_tune.end() ? -1 : it->second;
+}
+
+int launch4(Session *s, bool mixed, int v, int nops, int p0, int p1, const EigPack<4> *E) {
+  int nv = 0;
+  const Variant4 &var = variants4(mixed, &nv)[v];
+  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  const long per = (long)(kThreads / s->G) * var.pp;
+  const int grid = (int)((p1 - p0 + per - 1) / per);
+  DevCtx c = s->ctx();
+  const DevOp *ops = s->d_ops;
+  size_t stride = s->op_stride;
+  if (mixed) {
+    const float *tab = reinterpret_cast<const float *>(s->d_opmats);
+    void *args[] = {&c, &ops, &nops, &tab, &stride, &p0, &p1};
+    GEMS_CUDA(cudaLaunchKernel(var.fn[safe], dim3(grid), dim3(kThreads), args, 0, s->stream));
+  } else {
+    const double *tab = s->d_opmats;
+    EigPack<4> e = *E;
+    void *args[] = {&c, &ops, &nops, &tab, &stride, &e, &p0, &p1};
+    GEMS_CUDA(cudaLaunchKernel(var.fn[safe], dim3(grid), dim3(kThreads), args, 0, s->stream));
+  }
+  s->launches++;
+  return GEMS_OK;
+}
+
+int shape4(const Session *s, bool mixed) {  // forced, tuned (-1: not yet), for this session
+  int nv = 0;
+  variants4(mixed, &nv);
+  return s->force_shape >= 0 ? (s->force_shape < nv ? s->force_shape : nv - 1) : tuned4(s, mixed);
+}
+
+int traverse4(Session *s, bool mixed, int nops, int p0, int p1, const EigPack<4> *E) {
+  int nv = 0;
+  variants4(mixed, &nv);
+  const int v = shape4(s, mixed);
+  const bool tune = v < 0 && s->autotune && p0 == 0 && p1 == s->P &&
+                    (long long)s->P * nops >= kTuneMinWork;
+  if (!tune) return launch4(s, mixed, v < 0 ? 0 : v, nops, p0, p1, E);
+  cudaEvent_t ev[2];
+  GEMS_CUDA(cudaEventCreate(&ev[0]));
+  if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return cuda_status(cudaErrorUnknown, "tuner events");
+  }
+  int best = 0, st = GEMS_OK;
+  float best_ms = 0.f;
+  for (int i = 0; i < nv && st == GEMS_OK; i++) {  // every variant writes the same partials
+    cudaEventRecord(ev[0], s->stream);
+    st = launch4(s, mixed, i, nops, p0, p1, E);
+    cudaEventRecord(ev[1], s->stream);
+    float ms = 0.f;
+    if (st == GEMS_OK && cudaEventSynchronize(ev[1]) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess && (i == 0 || ms < best_ms)) {
+      best = i;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (st) return st;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune[tune_key(s, mixed)] = best;
+  return GEMS_OK;
+}
+
 template <int N>
 int launch_f64(Session *s, int nops, int p0, int p1) {
   DevCtx c = s->ctx();
@@ -613,14 +718,7 @@ int launch_f64(Session *s, int nops, int p0, int p1) {
   }
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   if constexpr (N == 4) {
-    const long per = (long)(kThreads / s->G) * kF64PP;
-    const int g4 = (int)((p1 - p0 + per - 1) / per);
-    if (safe)
-      k_traverse_f64x<true><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                            s->op_stride, E, p0, p1);
-    else
-      k_traverse_f64x<false><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats,
-                                                             s->op_stride, E, p0, p1);
+    return traverse4(s, false, nops, p0, p1, &E);
   } else {
     const int grid = grid_for(s, p0, p1);
     if (safe)
@@ -662,18 +760,36 @@ int traverse_v2_wave_patterns(const Session *s) {
   const bool mixed = s->desc.precision == GEMS_PREC_MIXED;
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   const bool four = s->desc.nstates == 4;
-  const void *fn =
-      mixed ? (four ? (safe ? (const void *)k_traverse_mix4<true> : (const void *)k_traverse_mix4<false>)
-                    : (safe ? (const void *)k_traverse_mix<20, true> : (const void *)k_traverse_mix<20, false>))
-            : (four ? (safe ? (const void *)k_traverse_f64x<true> : (const void *)k_traverse_f64x<false>)
-                    : (safe ? (const void *)k_traverse_f64<20, true> : (const void *)k_traverse_f64<20, false>));
+  int pp = 1;
+  const void *fn = nullptr;
+  if (four) {
+    int nv = 0, v = shape4(s, mixed);
+    const Variant4 &var = variants4(mixed, &nv)[v < 0 ? 0 : v];
+    fn = var.fn[safe];
+    pp = var.pp;
+  } else {
+    fn = mixed ? (safe ? (const void *)k_traverse_mix<20, true> : (const void *)k_traverse_mix<20, false>)
+               : (safe ? (const void *)k_traverse_f64<20, true> : (const void *)k_traverse_f64<20, false>);
+  }
   int nsm = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->desc.device) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  return per_sm * nsm * (kThreads / s->G) * (four ? (mixed ? kMix4PP : kF64PP) : 1);
+  return per_sm * nsm * (kThreads / s->G) * pp;
+}
+
+int traverse_v2_shape(const Session *s, int *patterns_per_group, int *blocks_per_sm) {
+  *patterns_per_group = 1;
+  *blocks_per_sm = 0;
+  if (s->desc.nstates != 4) return GEMS_OK;
+  const bool mixed = s->desc.precision == GEMS_PREC_MIXED;
+  int nv = 0, v = shape4(s, mixed);
+  const Variant4 &var = variants4(mixed, &nv)[v < 0 ? 0 : v];
+  *patterns_per_group = var.pp;
+  *blocks_per_sm = var.blocks;
+  return v < 0 ? 1 : GEMS_OK;
 }
 
 int launch_traverse_v2(Session *s, int nops, int p0, int p1) {
@@ -687,16 +803,13 @@ int launch_traverse_v2(Session *s, int nops, int p0, int p1) {
     const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
     const float *tab = reinterpret_cast<const float *>(s->d_opmats);
     if (s->desc.nstates == 4) {
-      const long per = (long)(kThreads / s->G) * kMix4PP;
-      const int g4 = (int)((p1 - p0 + per - 1) / per);
-      if (safe) k_traverse_mix4<true><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
-      else k_traverse_mix4<false><<<g4, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
+      st = traverse4(s, true, nops, p0, p1, nullptr);
     } else {
       if (safe) k_traverse_mix<20, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
       else k_traverse_mix<20, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, tab, s->op_stride, p0, p1);
+      s->launches++;
+      GEMS_CUDA(cudaGetLastError());
     }
-    s->launches++;
-    GEMS_CUDA(cudaGetLastError());
   } else {
     st = s->desc.nstates == 4 ? launch_f64<4>(s, nops, p0, p1) : launch_f64<20>(s, nops, p0, p1);
   }

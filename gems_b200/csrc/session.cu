@@ -481,6 +481,13 @@ int gems_session_destroy(gems_session *s) {
   return GEMS_OK;
 }
 
+int gems_session_traversal_shape(gems_session *s, int *patterns_per_group, int *blocks_per_sm,
+                                 int *tuned) {
+  if (!s || !patterns_per_group || !blocks_per_sm || !tuned) return GEMS_ERR_BAD_ARG;
+  *tuned = traverse_v2_shape(s, patterns_per_group, blocks_per_sm) == 0 && s->desc.nstates == 4;
+  return GEMS_OK;
+}
+
 int gems_check_barrier_timeout(int device, int *status) {
   if (!status) return GEMS_ERR_BAD_ARG;
   return check_barrier_timeout(device, status);
@@ -506,6 +513,11 @@ int gems_session_set_option(gems_session *s, int option, int value) {
       return GEMS_OK;
     case GEMS_OPT_TILED_FP64:
       s->g61_enabled = value != 0;
+      return GEMS_OK;
+    case GEMS_OPT_AUTOTUNE:
+      if (value < 0) return GEMS_ERR_BAD_ARG;
+      s->autotune = value == 1;
+      s->force_shape = value >= 2 ? value - 2 : -1;
       return GEMS_OK;
     default:
       return GEMS_ERR_BAD_ARG;

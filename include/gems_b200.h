@@ -102,7 +102,16 @@ int gems_session_stream(gems_session *s, void **stream);
  * GEMS_OPT_TILED_FP64 (default 1): the FP64 61-state traversal (1 to 8 categories) runs as
  * register-tiled GEMMs over 128-row tiles; 0 selects the per-row kernel (same values, bit for
  * bit). */
-enum { GEMS_OPT_TENSOR_CORES = 1, GEMS_OPT_TILED_FP64 = 2 };
+enum { GEMS_OPT_TENSOR_CORES = 1, GEMS_OPT_TILED_FP64 = 2, GEMS_OPT_AUTOTUNE = 3 };
+/* GEMS_OPT_AUTOTUNE (default 1): the first traversal of a 4-state session class (precision,
+ * scaling, categories, pattern count to the power of two) with at least 2^22 pattern-updates
+ * times every launch shape of the traversal kernel (patterns per lane group x blocks per SM; all
+ * give the same values) and keeps the fastest for the process; 0 keeps the default shape (or
+ * the one already chosen for the class); 2 + k forces shape k (for comparisons).  No
+ * counterpart in the reference.  gems_session_traversal_shape reports the shape in use and
+ * whether it was tuned (0 0 0 for the forms that have one shape). */
+int gems_session_traversal_shape(gems_session *s, int *patterns_per_group, int *blocks_per_sm,
+                                 int *tuned);
 int gems_session_set_option(gems_session *s, int option, int value);
 
 /* Tip state bytes [ntaxa][nptn] (PhyloTree::getConvertedSequenceByNumber rows,
