@@ -101,9 +101,9 @@ def nni5(gt: PhyloTree, ntaxa: int, rng: np.random.Generator):
     return gt.computeLikelihoodFromBuffer(), len(branches)
 
 
-def run_alone(spec, case, nreq, device=0):
+def run_alone(spec, case, nreq, device=0, opener=open_session):
     """The session's requests in order, nothing else on the GPU."""
-    gt = open_session(spec, case, device)
+    gt = opener(spec, case, device)
     gt.computeLikelihood()
     out = []
     for k in range(nreq):
@@ -114,13 +114,18 @@ def run_alone(spec, case, nreq, device=0):
 
 
 class Server:
-    def __init__(self, device=0, budget_bytes=None, workers=8, evict=True):
-        import torch
-        free, _ = torch.cuda.mem_get_info(device)
+    def __init__(self, device=0, budget_bytes=None, workers=8, evict=True, opener=open_session):
+        """opener(spec, case, device, tree) builds a session's tree object (open_session: a
+        PhyloTree on the GPU); budget_bytes defaults to 85% of the device's free memory."""
+        if budget_bytes is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info(device)
+            budget_bytes = int(0.85 * free)
         self.device = device
-        self.budget = int(0.85 * free) if budget_bytes is None else int(budget_bytes)
+        self.budget = int(budget_bytes)
         self.workers = workers
         self.evict = evict
+        self.opener = opener
 
     def run(self, specs, cases, requests, preopen=False):
         """requests: list of (arrival_s, sid) in arrival order, arrival times counted from the
@@ -152,7 +157,7 @@ class Server:
         def open_one(sid):
             t = time.perf_counter()
             try:
-                gt = open_session(spec_of[sid], cases[sid], self.device, saved.get(sid))
+                gt = self.opener(spec_of[sid], cases[sid], self.device, saved.get(sid))
                 gt.computeLikelihood()
             except GemsError:
                 return None
@@ -203,7 +208,7 @@ class Server:
                 if not self.evict:
                     return None, []
                 idle = sorted((last_used.get(s, 0.0), s) for s, g in open_sess.items()
-                              if isinstance(g, PhyloTree) and s not in busy and not pending[s])
+                              if not isinstance(g, str) and s not in busy and not pending[s])
                 freed = 0
                 for _, s in idle:
                     if freed >= need:
@@ -252,7 +257,8 @@ class Server:
                             break
                         best = None
                         for sid, dq in pending.items():
-                            if dq and sid not in busy and isinstance(open_sess.get(sid), PhyloTree):
+                            if dq and sid not in busy and sid in open_sess and \
+                                    not isinstance(open_sess[sid], str):
                                 if best is None or dq[0][0] < pending[best][0][0]:
                                     best = sid
                         if best is not None:

@@ -1,0 +1,66 @@
+"""The serving loop's scheduler on the CPU: sessions are oracle trees in the place of device
+sessions, so admission by footprint, continuous batching over worker threads, eviction of idle
+sessions and their rebuild from saved trees run without a GPU.  Every session's results must be
+the same as running it alone, and a session that can never fit must have its requests
+rejected."""
+import types
+
+import numpy as np
+
+from gems_b200 import serve
+from oracle import oracle as orc
+
+
+class OracleSession:
+    """An oracle tree in the role of a session's tree object (same method names)."""
+
+    def __init__(self, spec, case, device=0, tree=None):
+        t0, model, aln = case
+        self.t = orc.OracleTree(tree if tree is not None else t0, model, aln,
+                                safe=spec.nstates == 61)
+        self.session = types.SimpleNamespace(close=lambda: None)
+
+    def __getattr__(self, name):
+        return getattr(self.t, name)
+
+    def close(self):
+        pass
+
+
+def stream(nsess, nreq, seed, rate=5000.0):
+    specs, reqs = serve.make_stream(nsess, nreq, rate=rate, seed=seed, taxa=(6, 14),
+                                    sites=(60, 300), states=(4, 20), cats=(1, 4))
+    cases = {s.sid: serve.build_case(s) for s in specs}
+    return specs, reqs, cases
+
+
+def same_as_alone(specs, cases, records):
+    by_sid = {}
+    for r in records:
+        by_sid.setdefault(r["sid"], []).append(r)
+    for sid, rs in by_sid.items():
+        rs.sort(key=lambda r: r["seq"])
+        alone = serve.run_alone(specs[sid], cases[sid], len(rs), opener=OracleSession)
+        assert [r["lnl"] for r in rs] == alone, sid
+
+
+def test_admission_batching_and_eviction_keep_results():
+    # arrivals spread out, so that sessions sit idle with requests still to come
+    specs, reqs, cases = stream(5, 40, seed=8, rate=300.0)
+    fps = sorted(s.footprint(cases[s.sid][2].npat) for s in specs)
+    srv = serve.Server(budget_bytes=fps[-1] + fps[0], workers=3, opener=OracleSession)
+    records, _ = srv.run(specs, cases, reqs)
+    assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
+    assert srv.evictions > 0
+    same_as_alone(specs, cases, records)
+
+
+def test_session_that_cannot_fit_is_rejected():
+    specs, reqs, cases = stream(4, 24, seed=9)
+    fps = {s.sid: s.footprint(cases[s.sid][2].npat) for s in specs}
+    budget = sorted(fps.values())[-1] - 1
+    srv = serve.Server(budget_bytes=budget, workers=2, opener=OracleSession)
+    records, _ = srv.run(specs, cases, reqs)
+    for r, (_, sid) in zip(records, reqs):
+        assert bool(r.get("rejected")) == (fps[sid] > budget)
+    same_as_alone(specs, cases, [r for r in records if not r.get("rejected")])
