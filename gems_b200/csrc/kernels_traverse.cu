@@ -690,8 +690,11 @@ int traverse4(Session *s, bool mixed, int nops, int p0, int p1, const EigPack<4>
     st = launch4(s, mixed, i, nops, p0, p1, E);
     cudaEventRecord(ev[1], s->stream);
     float ms = 0.f;
+    // another shape replaces the first (default) one only when it is more than 2% faster, so
+    // that timing noise does not move the choice
     if (st == GEMS_OK && cudaEventSynchronize(ev[1]) == cudaSuccess &&
-        cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess && (i == 0 || ms < best_ms)) {
+        cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess &&
+        (i == 0 || ms < best_ms * (best == 0 ? 0.98f : 1.0f))) {
       best = i;
       best_ms = ms;
     }
