@@ -56,14 +56,20 @@ constexpr int kAhi61 = 128;
 __host__ __device__ constexpr size_t op_floats61(int C) { return (size_t)2 * C * (kBSide / 4); }
 
 __global__ void k_prep_ops_tc61(DevCtx c, const DevOp *ops, float *tab, size_t stride_f) {
-  extern __shared__ double ex[];  // [C][n] exp terms
+  // exp terms [C][n], then evec and inv_evec [n][n]: every product below reads shared memory
+  extern __shared__ double ex[];
   const int k = blockIdx.x, side = blockIdx.y;
   const DevOp op = ops[k];
   const double len = side ? op.r_len : op.l_len;
   const int C = c.C, n = kN;
+  double *ev = ex + C * n, *iv = ev + n * n;
   for (int idx = threadIdx.x; idx < C * n; idx += blockDim.x) {
     const int cc = idx / n, i = idx - cc * n;
     ex[idx] = exp(c.eval[i] * (c.rates[cc] * len));
+  }
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    ev[idx] = c.evec[idx];
+    iv[idx] = c.inv_evec[idx];
   }
   __syncthreads();
   float *img = tab + (size_t)k * stride_f + (size_t)side * C * (kBSide / 4);
@@ -74,7 +80,7 @@ __global__ void k_prep_ops_tc61(DevCtx c, const DevOp *ops, float *tab, size_t s
     float v = 0.f;
     if (x < n && y < n) {
       double acc = 0.0;
-      for (int i = 0; i < n; i++) acc = fma(c.evec[x * n + i] * ex[cc * n + i], c.inv_evec[i * n + y], acc);
+      for (int i = 0; i < n; i++) acc = fma(ev[x * n + i] * ex[cc * n + i], iv[i * n + y], acc);
       v = (float)fmax(acc, 0.0);
     }
     const float hi = tf32_rna(v);
@@ -399,7 +405,11 @@ bool tc61_supported(const Session *s) {
 int launch_prep_ops_tc61(Session *s, int nops) {
   if (nops <= 0) return GEMS_OK;
   DevCtx c = s->ctx();
-  const size_t smem = sizeof(double) * s->desc.ncat * kN;
+  const size_t smem = sizeof(double) * ((size_t)s->desc.ncat * kN + 2 * kN * kN);
+  // the limit is a per-kernel attribute shared by every thread of the process: always set to
+  // the largest size (kMaxCat categories)
+  GEMS_CUDA(cudaFuncSetAttribute(k_prep_ops_tc61, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * ((size_t)kMaxCat * kN + 2 * kN * kN))));
   k_prep_ops_tc61<<<dim3(nops, 2), 256, smem, s->stream>>>(
       c, s->d_ops, reinterpret_cast<float *>(s->d_opmats), s->op_stride_tc);
   s->launches++;
