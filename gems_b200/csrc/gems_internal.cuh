@@ -204,6 +204,10 @@ int launch_unpack_partial(Session *s, int slot, double *d_out);
 // mixed precision (kernels_mixed.cu)
 int launch_prep_ops_mixed(Session *s, int nops);
 int launch_traverse_mixed(Session *s, int nops);
+// the same without waiting: with want_lnl the result is copied to s->h_result, read by
+// theta_mixed_lnl once the session's stream has completed
+int enqueue_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta);
+double theta_mixed_lnl(const Session *s);
 int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta,
                        double *lnl);
 // factored whole-traversal kernels for 4 and 20 states (kernels_traverse.cu)

@@ -373,8 +373,7 @@ int launch_traverse_mixed(Session *s, int nops) {
 }
 
 // theta (and optionally the branch lnL) from the two FP32 partials of br
-int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta,
-                       double *lnl) {
+int enqueue_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta) {
   DevCtx c = s->ctx();
   const int grid = grid_for(s);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
@@ -398,8 +397,19 @@ int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool st
   GEMS_CUDA(cudaGetLastError());
   GEMS_CUDA(cudaMemcpyAsync(s->h_result, s->d_result, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                             s->stream));
+  return GEMS_OK;
+}
+
+double theta_mixed_lnl(const Session *s) {
+  return std::isfinite(s->h_result[0]) ? s->h_result[0] : s->h_result[1];
+}
+
+int launch_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta,
+                       double *lnl) {
+  if (int st = enqueue_theta_mixed(s, br, want_lnl, store_theta)) return st;
+  if (!want_lnl) return GEMS_OK;
   GEMS_CUDA(cudaStreamSynchronize(s->stream));
-  *lnl = std::isfinite(s->h_result[0]) ? s->h_result[0] : s->h_result[1];
+  *lnl = theta_mixed_lnl(s);
   return GEMS_OK;
 }
 

@@ -700,8 +700,22 @@ int gems_branch_lnl_batch(gems_session *const *ss, int nsess, const gems_op *ops
                           const gems_branch *br, double *lnl) {
   if (!lnl) return GEMS_ERR_BAD_ARG;
   if (int st = gems_traverse_batch(ss, nsess, ops, nops)) return st;
-  for (int i = 0; i < nsess; i++)
-    if (int st = gems_branch_lnl(ss[i], nullptr, 0, br, &lnl[i], nullptr)) return st;
+  bool mixed = true;
+  for (int i = 0; i < nsess; i++) mixed = mixed && ss[i]->desc.precision == GEMS_PREC_MIXED;
+  if (!mixed) {
+    for (int i = 0; i < nsess; i++)
+      if (int st = gems_branch_lnl(ss[i], nullptr, 0, br, &lnl[i], nullptr)) return st;
+    return GEMS_OK;
+  }
+  // every session's branch terms enqueued on its own stream first, then the results read
+  for (int i = 0; i < nsess; i++) {
+    if (int st = check_branch(ss[i], br)) return st;
+    if (int st = enqueue_theta_mixed(ss[i], br, true, false)) return st;
+  }
+  for (int i = 0; i < nsess; i++) {
+    GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
+    lnl[i] = theta_mixed_lnl(ss[i]);
+  }
   return GEMS_OK;
 }
 
