@@ -69,6 +69,87 @@ def update_bytes(s, n=4, C=4, safe=False):
     return 3 * C * n * s + 3 * sig, 2 * C * n * s + 1 + 2 * sig, C * n * s + 2 + sig
 
 
+def required_bytes(P, nops, ntaxa, s, n=4, C=4, safe=False):
+    """DRAM bytes a from-scratch traversal cannot avoid: every internal partial and its scale
+    counters written once (they are the stored result later calls read), every tip byte read
+    once.  Child partials read back by the op that consumes them are not counted: a kernel
+    that keeps them on chip never reads them from DRAM."""
+    sig = 2 * C if safe else 2
+    return P * (nops * (C * n * s + sig) + ntaxa)
+
+
+def _r(x, d=4):
+    return float(f"{x:.{d}g}") if isinstance(x, (int, float)) and x is not None else x
+
+
+def compact_line(line):
+    """The bench line the driver parses: the contract's keys and a short summary of every
+    block, small enough to stay whole in a 3,000-character output tail."""
+    keep = ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+            "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "gpu_launches",
+            "clocks")
+    out = {k: line[k] for k in keep if k in line}
+    cfg = line["config"]
+    out["config"] = {"workload": cfg["workload"], "npat_per_rank": cfg["npat_per_rank"],
+                     "parallelism": cfg["parallelism"], "precision": cfg.get("precision"),
+                     "l2": "inputs > L2, no flush"}
+    rf = line["roofline"]
+    out["roofline"] = {k: _r(rf[k]) for k in ("bound", "achieved", "peak", "unit", "frac",
+                                               "traffic", "frac_required_bytes")}
+    e = line["e2e"]
+    out["e2e"] = {k: _r(e[k]) for k in ("value", "unit", "h2d_bytes_per_step",
+                                        "d2h_bytes_per_step", "ms_per_step")}
+    forms = {}
+    for k, f in line.get("forms", {}).items():
+        forms[k] = {"ms": _r(f["ms_per_step"]), "frac": _r(f["roofline"]["frac"]),
+                    "frac_req": _r(f["roofline"]["frac_required_bytes"])}
+        if "newton" in f:
+            forms[k]["newton_ms_per_branch"] = _r(f["newton"]["ms_per_branch"])
+        if "lnl_rel_err_vs_fp64" in f:
+            forms[k]["lnl_rel_err_vs_fp64"] = _r(f["lnl_rel_err_vs_fp64"], 2)
+    out["forms"] = forms
+    if "parity" in line:
+        p = line["parity"]
+        out["parity_vs_oracle"] = {"patterns": p["patterns"], **{
+            k: {"lnl": _r(p[k]["lnl_rel_err_vs_oracle"], 2),
+                "df/ddf": _r(p[k]["df_err_over_ddf"], 2), "ddf": _r(p[k]["ddf_rel_err"], 2)}
+            for k in ("fp64", "mixed")}}
+    if "protein20" in line:
+        p = line["protein20"]
+        out["protein20"] = {"fp64_ms": _r(p["fp64"]["ms_per_step"]),
+                            "tcgen05_ms": _r(p["mixed_tcgen05"]["ms_per_step"]),
+                            "speedup_vs_fp64": _r(p["mixed_tcgen05"]["speedup_vs_fp64"]),
+                            "lnl_rel_err_vs_fp64": _r(p["mixed_tcgen05"]["lnl_rel_err_vs_fp64"], 2),
+                            "tensor_frac": _r(p["mixed_tcgen05"]["compute"]["frac"], 3),
+                            "hbm_frac": _r(p["mixed_tcgen05"]["roofline"]["frac"], 3)}
+    if "codon64" in line:
+        out["codon64"] = {k: {"batched_ms": _r(c["batched_wall_ms"]),
+                              "kernel_ms": _r(c["batched_traversal_kernel_ms"]),
+                              "fp64_one_ms": _r(c["fp64_one_model_ms"]),
+                              "speedup": _r(c["speedup_vs_fp64_one_by_one"], 3),
+                              "err": _r(c["lnl_rel_err_model0_vs_fp64"], 2)}
+                          for k, c in line["codon64"].items()}
+    if "rell" in line:
+        r = line["rell"]
+        out["rell"] = {"ms": _r(r["ms_per_call"]), "frac": _r(r["roofline"]["frac"], 3),
+                       "err": _r(r["max_rel_err_vs_fp64_dot"], 2)}
+    if "serving" in line:
+        sv = line["serving"]
+        out["serving"] = {"req_s": _r(sv["throughput_req_s"]),
+                          "capacity_req_s": _r(sv["capacity_req_s"]),
+                          "p50_ms": _r(sv["latency_ms"]["p50"]),
+                          "p99_ms": _r(sv["latency_ms"]["p99"]), "load": sv["load"]}
+    if "ingest" in line:
+        g = line["ingest"]
+        out["ingest"] = {"device_ms": _r(g["device_path_ms"]), "host_ms": _r(g["host_path_ms"]),
+                         "identical": g["identical_to_host"]}
+    if "cpu_baseline" in line:
+        c = line["cpu_baseline"]
+        out["cpu_baseline"] = {"value": _r(c["value"]), "unit": c["unit"], "cores": c["cores"],
+                               "kind": c["kind"], "sample": c["sample"]}
+    return out
+
+
 def update_flops(n=4, C=4):
     """Algorithmic flops of one site-partial update (eigen-space form): 6*C*n^2 + C*n."""
     return 6 * C * n * n + C * n
@@ -205,14 +286,20 @@ def config_block(args, aln, nops):
             "l2": "inputs larger than L2 (partials 33-65 GB), no flush needed"}
 
 
-def cpu_baseline(tree, model, aln, target_s=12.0):
+def cpu_sample(model, aln, nsamp=40_000):
+    """The first nsamp patterns of the workload, as an alignment of their own."""
+    nsamp = min(aln.npat, nsamp)
+    return synth.Alignment(aln.ntaxa, model.nstates, int(aln.weights[:nsamp].sum()),
+                           np.ascontiguousarray(aln.patterns[:, :nsamp]), aln.weights[:nsamp])
+
+
+def cpu_baseline(tree, model, aln, target_s=12.0, sub=None):
     """The oracle (CPU restatement of the reference kernels) on a bounded pattern sample."""
     from oracle import oracle as orc
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
-    nsamp = min(aln.npat, 40_000)
-    sub = synth.Alignment(aln.ntaxa, model.nstates, int(aln.weights[:nsamp].sum()),
-                          np.ascontiguousarray(aln.patterns[:, :nsamp]), aln.weights[:nsamp])
+    sub = sub if sub is not None else cpu_sample(model, aln)
+    nsamp = sub.npat
     ot = orc.OracleTree(tree, model, sub)
     nops = sum(op_kinds(tree))
     ot.computeLikelihood()  # warm-up (allocation of the oracle's buffers)
@@ -228,8 +315,41 @@ def cpu_baseline(tree, model, aln, target_s=12.0):
     ups = k * nops * nsamp / el
     return {"value": ups, "unit": "site-partial updates/s", "cores": threads, "kind": "port",
             "sample": f"{nsamp} of {aln.npat} patterns, {k} from-scratch lnL evaluations "
-                      f"({nops} node updates each), oracle FP64, {threads} threads",
+                      f"({nops} node updates each), oracle FP64 (scalar C, -O3, no FMA "
+                      f"contraction), {threads} threads",
             "lnl_evals_per_s": k / el}
+
+
+def slice_parity(tree, model, sub, local, nbranch=8):
+    """Parity at the bench's own tree and model on the CPU sample: the oracle's lnL, pattern
+    lnL and derivatives on `nbranch` branches against the FP64 and mixed GPU forms evaluated on
+    the same patterns (a session over the sample)."""
+    from gems_b200 import PhyloTree
+    from oracle import oracle as orc
+    ot = orc.OracleTree(tree, model, sub)
+    lo, plo = ot.computeLikelihood(pattern_lh=True)
+    edges = list(range(0, tree.nedges, max(1, tree.nedges // nbranch)))[:nbranch]
+    dref = []
+    for e in edges:
+        u, v = int(tree.eu[e]), int(tree.ev[e])
+        f, df = ot.computeFuncDerv(u, v, float(tree.length[e]), new_branch=True)
+        dref.append((-f, -df))
+    out = {"patterns": sub.npat, "oracle_lnl": lo, "branches_with_derivatives": len(edges)}
+    for prec in ("fp64", "mixed"):
+        gt = PhyloTree.from_case(tree, model, sub, precision=prec, device=local)
+        lg, plg = gt.computeLikelihood(pattern_lh=True)
+        d1e = d2e = 0.0
+        for e, (r1, r2) in zip(edges, dref):
+            u, v = int(tree.eu[e]), int(tree.ev[e])
+            f, df = gt.computeFuncDerv(u, v, float(tree.length[e]), new_branch=True)
+            d1e = max(d1e, abs(-f - r1) / abs(r2))
+            d2e = max(d2e, abs(-df - r2) / abs(r2))
+        out[prec] = {"lnl_rel_err_vs_oracle": abs(lg - lo) / abs(lo),
+                     "pattern_lnl_max_abs_err": float(np.max(np.abs(plg - plo))),
+                     "df_err_over_ddf": d1e, "ddf_rel_err": d2e}
+        gt.close()
+        gt.session.close()
+    return out
 
 
 def run_reference(args):
@@ -620,6 +740,7 @@ def main():
             b_ii, b_ti, b_tt = update_bytes(s_bytes, model.nstates, model.ncat)
             alg = P * (kinds[0] * b_ii + kinds[1] * b_ti + kinds[2] * b_tt)
             ach = alg / (kms * 1e-3) / 1e9
+            req = required_bytes(P, nops, tree.ntaxa, s_bytes, model.nstates, model.ncat)
             forms[prec] = {
                 "ms_per_step": ms, "value": world * nops * P / (ms * 1e-3), "lnl": lnl,
                 "gpu_launches": launches,
@@ -627,7 +748,9 @@ def main():
                              "achieved": ach, "peak": hbm_peak,
                              "peak_source": peak_src, "unit": "GB/s", "frac": ach / hbm_peak,
                              "algorithmic_bytes_per_launch": alg, "avg_launch_ms": kms,
-                             "traffic": read_traffic(f"traverse_{prec}_{args.config}.md")},
+                             "traffic": read_traffic(f"traverse_{prec}_{args.config}.md"),
+                             "required_bytes_per_launch": req,
+                             "frac_required_bytes": req / (kms * 1e-3) / 1e9 / hbm_peak},
             }
             pp, blocks, tuned = gt.session.traversal_shape()
             forms[prec]["launch_shape"] = {"patterns_per_lane_group": pp, "blocks_per_sm": blocks,
@@ -712,9 +835,13 @@ def main():
         line["ingest"] = ingest_block(aln, local)
         line["serving"] = serving_block(local)
     if world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(tree, model, aln)
+        sub = cpu_sample(model, aln)
+        line["parity"] = slice_parity(tree, model, sub, local)
+        line["cpu_baseline"] = cpu_baseline(tree, model, aln, sub=sub)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        # the full record first (stderr), then the one compact line the driver parses (stdout)
+        print(json.dumps({"detail": line}), file=sys.stderr, flush=True)
+        print(json.dumps(compact_line(line)), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

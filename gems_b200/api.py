@@ -258,6 +258,20 @@ class Session:
         arr, n = op_array(ops)
         _check(self.lib.gems_traverse(self.handle, arr, n), "gems_traverse")
 
+    def compute_partial(self, op, ptn_lower, ptn_upper):
+        """One node update over patterns [ptn_lower, ptn_upper) (computePartialLikelihood of
+        one TraversalInfo entry for one packet); op = (dst, lkind, lid, rkind, rid, llen, rlen)."""
+        arr, _ = op_array([op])
+        _check(self.lib.gems_compute_partial(self.handle, arr, int(ptn_lower), int(ptn_upper)),
+               "gems_compute_partial")
+
+    def pattern_granule(self):
+        """Alignment that the pattern ranges of compute_partial must respect."""
+        g = c_int()
+        _check(self.lib.gems_session_pattern_granule(self.handle, byref(g)),
+               "gems_session_pattern_granule")
+        return g.value
+
     def branch_lnl(self, ops, br, pattern_lh=False):
         arr, n = op_array(ops)
         out = c_double()

@@ -58,7 +58,7 @@ def build_synth(force=False):
 def build_cuda(force=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "gems_b200.h")]
-    objs = []
+    objs, jobs = [], []
     for src in CUDA_SOURCES:
         path = os.path.join(CSRC, src)
         if not os.path.exists(path):
@@ -66,8 +66,12 @@ def build_cuda(force=False, verbose=False):
         obj = os.path.join(BUILD, src + ".o")
         objs.append(obj)
         if force or _newer(obj, [path] + hdrs):
-            cmd = [NVCC] + NVFLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", path, "-o", obj]
-            r = _run(cmd)
+            jobs.append([NVCC] + NVFLAGS + (["-Xptxas", "-v"] if verbose else []) +
+                        ["-c", path, "-o", obj])
+    # translation units compile independently: one nvcc per source, in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for r in ex.map(_run, jobs):
             if verbose:
                 sys.stderr.write(r.stderr)
     if force or _newer(LIB, objs):

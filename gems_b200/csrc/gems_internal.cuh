@@ -192,7 +192,8 @@ int cuda_status(cudaError_t e, const char *what);
 
 // launch helpers implemented in kernels.cu
 int launch_prep_ops(Session *s, int nops);
-int launch_traverse(Session *s, int nops);
+// patterns [p0, p1) of the traversal, p1 <= P (every launch_traverse* below alike)
+int launch_traverse(Session *s, int nops, int p0, int p1);
 int launch_branch_lnl(Session *s, const gems_branch *br, double *lnl);
 int launch_theta(Session *s, const gems_branch *br);
 int launch_derv(Session *s, double length, double *df, double *ddf);
@@ -203,7 +204,7 @@ int launch_eigen(Session *s, const double *exch_upper, const double *freq);
 int launch_unpack_partial(Session *s, int slot, double *d_out);
 // mixed precision (kernels_mixed.cu)
 int launch_prep_ops_mixed(Session *s, int nops);
-int launch_traverse_mixed(Session *s, int nops);
+int launch_traverse_mixed(Session *s, int nops, int p0, int p1);
 // the same without waiting: with want_lnl the result is copied to s->h_result, read by
 // theta_mixed_lnl once the session's stream has completed
 int enqueue_theta_mixed(Session *s, const gems_branch *br, bool want_lnl, bool store_theta);
@@ -224,18 +225,22 @@ int traverse_v2_shape(const Session *s, int *patterns_per_group, int *blocks_per
 size_t tc20_op_floats(int ncat, int unknown);
 bool tc20_supported(const Session *s);
 int launch_prep_ops_tc20(Session *s, int nops);
-int launch_traverse_tc20(Session *s, int nops);
+// p0 a multiple of 128, p1 a multiple of 128 or P
+int launch_traverse_tc20(Session *s, int nops, int p0, int p1);
 // tcgen05 split-TF32 traversal for 61 states, SAFE (kernels_tc61.cu)
 size_t tc61_op_floats(int ncat);
 bool tc61_supported(const Session *s);
 int launch_prep_ops_tc61(Session *s, int nops);
-int launch_traverse_tc61(Session *s, int nops);
-int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops);
+// p0 a multiple of 128, p1 a multiple of 128 or P
+int launch_traverse_tc61(Session *s, int nops, int p0, int p1);
+int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, int p1);
 // FP64 61-state traversal as register-tiled GEMMs, C in {1, 2, 4, 8} (kernels_g61.cu)
 size_t g61_op_doubles(int ncat, int unknown);
 bool g61_supported(const Session *s);
 int launch_prep_ops_g61(Session *s, int nops);
-int launch_traverse_g61(Session *s, int nops);
+// p0 and p1 multiples of g61_pattern_granule (p1 may be P)
+int g61_pattern_granule(const Session *s);
+int launch_traverse_g61(Session *s, int nops, int p0, int p1);
 // the grid barrier's time-out path, run on purpose (kernels_fp64.cu)
 int check_barrier_timeout(int device, int *status);
 // bootstrap reweighting (kernels_rell.cu)

@@ -155,17 +155,17 @@ __device__ __forceinline__ void child_msg(const DevCtx &c, int kind, int id, con
   }
 }
 
-// Whole traversal for the patterns of this CTA: every op in postorder.  A pattern is always
-// handled by the same lane group, so children written by an earlier op are read back by the
-// same warp (ordered by __syncwarp); no inter-CTA dependency exists.
+// Whole traversal for the patterns [p0, p1) of this launch, p1 <= P: every op in postorder.
+// A pattern is always handled by the same lane group, so children written by an earlier op are
+// read back by the same warp (ordered by __syncwarp); no inter-CTA dependency exists.
 template <int N, bool SAFE>
 __global__ void __launch_bounds__(kThreads) k_traverse(DevCtx c, const DevOp *__restrict__ ops,
                                                        int nops, const double *__restrict__ opmats,
-                                                       size_t stride) {
+                                                       size_t stride, int p0, int p1) {
   const int G = c.G;
   const int gl = threadIdx.x & (G - 1);
-  const long p = ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const bool act = p < c.P && gl < c.C;
+  const long p = p0 + ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool act = p < p1 && gl < c.C;
   const int C = c.C;
   const size_t nnC = (size_t)C * N * N;
   double *part = static_cast<double *>(c.partials);
@@ -645,16 +645,16 @@ int launch_prep_ops(Session *s, int nops) {
   return GEMS_OK;
 }
 
-int launch_traverse(Session *s, int nops) {
-  if (nops <= 0) return GEMS_OK;
+int launch_traverse(Session *s, int nops, int p0, int p1) {
+  if (nops <= 0 || p1 <= p0) return GEMS_OK;
   DevCtx c = s->ctx();
-  const int grid = grid_for(s);
+  const int grid = (int)(((long)(p1 - p0) * s->G + kThreads - 1) / kThreads);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   cudaEvent_t ev0;
   if (int st = prof_begin(s, 0, &ev0)) return st;
   GEMS_DISPATCH_N(s->desc.nstates, "traverse",
-    if (safe) k_traverse<NS, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats, s->op_stride);
-    else k_traverse<NS, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats, s->op_stride));
+    if (safe) k_traverse<NS, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats, s->op_stride, p0, p1);
+    else k_traverse<NS, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, s->d_opmats, s->op_stride, p0, p1));
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   return prof_end(s, 0, ev0);

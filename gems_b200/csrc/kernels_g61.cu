@@ -209,7 +209,7 @@ __device__ __forceinline__ void child_v(const DevCtx &c, const TileMap &tm, int 
 template <bool SAFE>
 __global__ void __launch_bounds__(kThreadsG, 2)
     k_traverse_g61(DevCtx c, const DevOp *__restrict__ ops, int nops,
-                   const double *__restrict__ tab, size_t stride) {
+                   const double *__restrict__ tab, size_t stride, int tile0) {
   extern __shared__ __align__(16) double smem[];
   double *sIv = smem;                  // [kK][kNC]: inv_evec[j][x] at [x][j]
   double *sA = sIv + kK * kNC;         // [kK][kSaLd]
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   tm.C = c.C;
   tm.tp = tile_patterns(c.C);
   tm.nrow = tm.tp * c.C;
-  tm.p0 = (long)blockIdx.x * tm.tp;
+  tm.p0 = (long)(tile0 + blockIdx.x) * tm.tp;
   tm.P = c.P;
   for (int idx = tid; idx < kK * kNC; idx += blockDim.x) {
     const int k = idx / kNC, x = idx - k * kNC;
@@ -421,7 +421,7 @@ __device__ __forceinline__ void child_v_mma(const DevCtx &c, const TileMap1 &tm,
 template <bool SAFE>
 __global__ void __launch_bounds__(kThreadsG, 2)
     k_traverse_g61m(DevCtx c, const DevOp *__restrict__ ops, int nops,
-                    const double *__restrict__ tab, size_t stride) {
+                    const double *__restrict__ tab, size_t stride, int tile0) {
   static_assert(SAFE, "one category per tile: SAFE scaling only");
   extern __shared__ __align__(16) double smem[];
   double *sIv = smem;                  // [kK][kLdM]: inv_evec[j][x] at [x][j]
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kThreadsG, 2)
   tm.tp = kRows;
   tm.nrow = kRows;
   tm.c0 = blockIdx.x % c.C;
-  tm.p0 = (long)(blockIdx.x / c.C) * kRows;
+  tm.p0 = (long)(tile0 + blockIdx.x / c.C) * kRows;
   tm.P = c.P;
   for (int idx = threadIdx.x; idx < kK * kLdM; idx += blockDim.x) {
     const int k = idx / kLdM, x = idx - k * kLdM;
@@ -518,26 +518,38 @@ int launch_prep_ops_g61(Session *s, int nops) {
   return GEMS_OK;
 }
 
-int launch_traverse_g61(Session *s, int nops) {
-  if (nops <= 0) return GEMS_OK;
+int g61_pattern_granule(const Session *s) {
+  return s->desc.scaling == GEMS_SCALE_SAFE ? kRows : tile_patterns(s->desc.ncat);
+}
+
+int launch_traverse_g61(Session *s, int nops, int p0, int p1) {
+  if (nops <= 0 || p1 <= p0) return GEMS_OK;
+  const int tp = tile_patterns(s->desc.ncat);
+  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  const int gran = safe ? kRows : tp;
+  if (p0 % gran != 0 || (p1 % gran != 0 && p1 != s->P)) {
+    set_error("FP64 61-state traversal: pattern range not aligned to its pattern tiles");
+    return GEMS_ERR_BAD_ARG;
+  }
   cudaEvent_t ev0;
   if (int st = prof_begin(s, 0, &ev0)) return st;
-  const int tp = tile_patterns(s->desc.ncat);
-  const int grid = (s->P + tp - 1) / tp;
-  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  const int tile0 = p0 / gran;
+  const int grid = (p1 + tp - 1) / tp - tile0;
   // the limit is a per-kernel attribute shared by every thread of the process: always the same
   // value
   if (safe) {  // FP64 tensor cores, one category per tile
-    const int g = (s->P + kRows - 1) / kRows * s->desc.ncat;
+    const int g = ((p1 + kRows - 1) / kRows - tile0) * s->desc.ncat;
     GEMS_CUDA(cudaFuncSetAttribute(k_traverse_g61m<true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemM));
     k_traverse_g61m<true><<<g, kThreadsG, kSmemM, s->stream>>>(s->ctx(), s->d_ops, nops,
-                                                                s->d_opmats, s->op_stride);
+                                                                s->d_opmats, s->op_stride,
+                                                                tile0);
   } else {  // NORM: a pattern's categories in one tile, FP64 FMA
     GEMS_CUDA(cudaFuncSetAttribute(k_traverse_g61<false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemG));
     k_traverse_g61<false><<<grid, kThreadsG, kSmemG, s->stream>>>(s->ctx(), s->d_ops, nops,
-                                                                   s->d_opmats, s->op_stride);
+                                                                   s->d_opmats, s->op_stride,
+                                                                   tile0);
   }
   s->launches++;
   GEMS_CUDA(cudaGetLastError());

@@ -169,11 +169,11 @@ __device__ __forceinline__ void child_msg_f(const DevCtx &c, int kind, int id, c
 template <int N, bool SAFE>
 __global__ void __launch_bounds__(kThreads) k_traverse_mixed(DevCtx c, const DevOp *__restrict__ ops,
                                                              int nops, const float *__restrict__ opm,
-                                                             size_t stride_f) {
+                                                             size_t stride_f, int p0, int p1) {
   const int G = c.G;
   const int gl = threadIdx.x & (G - 1);
-  const long p = ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const bool act = p < c.P && gl < c.C;
+  const long p = p0 + ((long)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool act = p < p1 && gl < c.C;
   const int C = c.C;
   const size_t nnC = (size_t)C * N * N;
   float *part = static_cast<float *>(c.partials);
@@ -356,17 +356,17 @@ int launch_prep_ops_mixed(Session *s, int nops) {
   return GEMS_OK;
 }
 
-int launch_traverse_mixed(Session *s, int nops) {
-  if (nops <= 0) return GEMS_OK;
+int launch_traverse_mixed(Session *s, int nops, int p0, int p1) {
+  if (nops <= 0 || p1 <= p0) return GEMS_OK;
   DevCtx c = s->ctx();
-  const int grid = grid_for(s);
+  const int grid = (int)(((long)(p1 - p0) * s->G + kThreads - 1) / kThreads);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   const float *opm = reinterpret_cast<const float *>(s->d_opmats);
   cudaEvent_t ev0;
   if (int st = prof_begin(s, 0, &ev0)) return st;
   GEMS_DISPATCH_NM(s->desc.nstates, "traverse_mixed",
-    if (safe) k_traverse_mixed<NS, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, opm, s->op_stride);
-    else k_traverse_mixed<NS, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, opm, s->op_stride));
+    if (safe) k_traverse_mixed<NS, true><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, opm, s->op_stride, p0, p1);
+    else k_traverse_mixed<NS, false><<<grid, kThreads, 0, s->stream>>>(c, s->d_ops, nops, opm, s->op_stride, p0, p1));
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   return prof_end(s, 0, ev0);

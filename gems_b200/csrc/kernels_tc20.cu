@@ -291,7 +291,7 @@ __device__ __forceinline__ void load_op_inputs(const DevCtx &c, const DevOp &op,
 template <bool SAFE>
 __global__ void __launch_bounds__(kThreadsTc, 1)
     k_traverse_tc20(DevCtx c, const DevOp *__restrict__ ops, int nops,
-                    const float *__restrict__ tab, size_t stride_f, int *flag) {
+                    const float *__restrict__ tab, size_t stride_f, int *flag, int tile0) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = smem_raw;
   float *A[2], *Alo[2];
@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   const int t = threadIdx.x, warp = t >> 5;
   const int row = ((warp & 3) << 5) | (t & 31);  // TMEM lane = pattern row of the tile
   const int half = warp >> 2;                    // categories {2h, 2h+1}
-  const int p0 = blockIdx.x * kTile;
+  const int tile = tile0 + blockIdx.x;  // pattern tile of this CTA
+  const int p0 = tile * kTile;
   const long p = p0 + row;
   const bool act = p < c.P;
   const uint32_t bar_tile = sptr(&ctl->bar_tile), bar_tab = sptr(&ctl->bar_tab);
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   DevOp nxt = nops > 1 ? ops[1] : cur;
   int cur_mask = tma_mask(cur, -1);
   if (warp == 0 && elect_one()) {
-    issue_tiles(c, cur, cur_mask, sA0, sA1, blockIdx.x, bar_tile);
+    issue_tiles(c, cur, cur_mask, sA0, sA1, tile, bar_tile);
     issue_tables(c, cur, tab, Bbase, bar_tab);
   }
   tile_pending = tab_pending = true;
@@ -388,7 +389,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         if (cur_mask == 0) {
           mma_commit(bar_mma);
           // nothing to split: the landing buffers are free for the next op's tiles
-          if (has_next) issue_tiles(c, nxt, nxt_mask, sA0, sA1, blockIdx.x, bar_tile);
+          if (has_next) issue_tiles(c, nxt, nxt_mask, sA0, sA1, tile, bar_tile);
         }
       }
       if (cur_mask) {
@@ -423,7 +424,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           if (cur_mask & 2) issue_side_mmas(1, C, tmem, dB0, dL0[1]);
           mma_commit(bar_mma);
           // the split has read the landing buffers: the next op's tiles can come in
-          if (has_next) issue_tiles(c, nxt, nxt_mask, sA0, sA1, blockIdx.x, bar_tile);
+          if (has_next) issue_tiles(c, nxt, nxt_mask, sA0, sA1, tile, bar_tile);
         }
       }
       tile_pending = has_next;
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       tc_fence_after();
     } else {
       if (has_next && warp == 0 && elect_one())
-        issue_tiles(c, nxt, nxt_mask, sA0, sA1, blockIdx.x, bar_tile);
+        issue_tiles(c, nxt, nxt_mask, sA0, sA1, tile, bar_tile);
       tile_pending = has_next;
     }
     // ---- epilogue, part 1: messages and products into registers (the tip tables of this op
@@ -526,7 +527,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     // writes 32 consecutive rows, 512 contiguous bytes.  When the next op consumes this output
     // the split rows also go into its operand buffers.
     float *dtile = static_cast<float *>(c.partials) + (size_t)cur.dst_slot * c.slot_elems +
-                   (size_t)blockIdx.x * (5 * C * kAChunk / 4);
+                   (size_t)tile * (5 * C * kAChunk / 4);
     float *fl = nxt_fwd == 1 ? Alo[1] : Alo[0];
     {
       uint16_t *sd = c.scale + (size_t)cur.dst_slot * c.slot_scale;
@@ -604,8 +605,12 @@ int launch_prep_ops_tc20(Session *s, int nops) {
   return GEMS_OK;
 }
 
-int launch_traverse_tc20(Session *s, int nops) {
-  if (nops <= 0) return GEMS_OK;
+int launch_traverse_tc20(Session *s, int nops, int p0, int p1) {
+  if (nops <= 0 || p1 <= p0) return GEMS_OK;
+  if (p0 % kTile != 0 || (p1 % kTile != 0 && p1 != s->P)) {
+    set_error("tcgen05 20-state traversal: pattern range not aligned to its 128-pattern tiles");
+    return GEMS_ERR_BAD_ARG;
+  }
   DevCtx c = s->ctx();
   const size_t smem = tc_smem(s->desc.ncat);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
@@ -615,16 +620,19 @@ int launch_traverse_tc20(Session *s, int nops) {
   // session never lowers it below this launch's size
   GEMS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem(4)));
   GEMS_CUDA(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
-  const int grid = (s->P + kTile - 1) / kTile;
+  const int tile0 = p0 / kTile;
+  const int grid = (p1 + kTile - 1) / kTile - tile0;
   cudaEvent_t ev0;
   if (int st = prof_begin(s, 0, &ev0)) return st;
   const float *tab = reinterpret_cast<const float *>(s->d_opmats);
   if (safe)
     k_traverse_tc20<true><<<grid, kThreadsTc, smem, s->stream>>>(c, s->d_ops, nops, tab,
-                                                                  s->op_stride_tc, s->d_flag);
+                                                                  s->op_stride_tc, s->d_flag,
+                                                                  tile0);
   else
     k_traverse_tc20<false><<<grid, kThreadsTc, smem, s->stream>>>(c, s->d_ops, nops, tab,
-                                                                   s->op_stride_tc, s->d_flag);
+                                                                   s->op_stride_tc, s->d_flag,
+                                                                   tile0);
   s->launches++;
   GEMS_CUDA(cudaGetLastError());
   if (int st = prof_end(s, 0, ev0)) return st;

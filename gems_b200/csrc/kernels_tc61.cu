@@ -177,7 +177,8 @@ __device__ __forceinline__ void issue_b(const float *tab_op, int C, int cat, uns
 }
 
 __global__ void __launch_bounds__(kThreads61, 1)
-    k_traverse_tc61(const TcJob *__restrict__ jobs, int nops, size_t stride_f, int *flag) {
+    k_traverse_tc61(const TcJob *__restrict__ jobs, int nops, size_t stride_f, int *flag,
+                    int tile0) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ TcJob sj;
   unsigned char *land = smem_raw;                     // [2][32 KB] raw operand tiles
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(kThreads61, 1)
   const DevOp *ops = sj.ops;
   const float *tab = sj.tab;
   const int C = c.C;
-  const int tile = blockIdx.x;
+  const int tile = tile0 + blockIdx.x;
   const long p = (long)tile * kTile + row;
   const bool act = p < c.P;
   const bool inv0 = act ? c.invar[p] == 0.0 : false;
@@ -419,9 +420,13 @@ int launch_prep_ops_tc61(Session *s, int nops) {
 
 // one launch over the tiles of every session in `ss` (all with the same op list, pattern
 // count, categories and device), on the stream of ss[0]
-int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops) {
-  if (nops <= 0 || nsess <= 0) return GEMS_OK;
+int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, int p1) {
+  if (nops <= 0 || nsess <= 0 || p1 <= p0) return GEMS_OK;
   Session *s0 = ss[0];
+  if (p0 % kTile != 0 || (p1 % kTile != 0 && p1 != s0->P)) {
+    set_error("tcgen05 61-state traversal: pattern range not aligned to its 128-pattern tiles");
+    return GEMS_ERR_BAD_ARG;
+  }
   if (nsess > Session::kMaxBatch) {
     set_error("too many sessions in one batched launch");
     return GEMS_ERR_BAD_ARG;
@@ -441,11 +446,12 @@ int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops) {
   GEMS_CUDA(cudaFuncSetAttribute(k_traverse_tc61, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
   GEMS_CUDA(cudaMemsetAsync(s0->d_flag, 0, sizeof(int), s0->stream));
-  const dim3 grid((s0->P + kTile - 1) / kTile, nsess);
+  const int tile0 = p0 / kTile;
+  const dim3 grid((p1 + kTile - 1) / kTile - tile0, nsess);
   cudaEvent_t ev0;
   if (int st = prof_begin(s0, 0, &ev0)) return st;
   k_traverse_tc61<<<grid, kThreads61, smem, s0->stream>>>(
-      reinterpret_cast<const TcJob *>(s0->d_jobs), nops, s0->op_stride_tc, s0->d_flag);
+      reinterpret_cast<const TcJob *>(s0->d_jobs), nops, s0->op_stride_tc, s0->d_flag, tile0);
   s0->launches++;
   GEMS_CUDA(cudaGetLastError());
   if (int st = prof_end(s0, 0, ev0)) return st;
@@ -459,9 +465,9 @@ int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops) {
   return GEMS_OK;
 }
 
-int launch_traverse_tc61(Session *s, int nops) {
+int launch_traverse_tc61(Session *s, int nops, int p0, int p1) {
   Session *one[1] = {s};
-  return launch_traverse_tc61_batch(one, 1, nops);
+  return launch_traverse_tc61_batch(one, 1, nops, p0, p1);
 }
 
 }  // namespace gems

@@ -1,20 +1,25 @@
 // noalloc.cu -- log-likelihood from a caller-owned theta buffer, without any allocation.
 //
-// Some callers cannot allocate device memory at the point they need a likelihood: code that
-// runs while a CUDA graph is being captured, hosts whose memory pool owns the whole device
-// and forbids outside cudaMalloc, or a driver loop that must not hit the allocator (and its
-// implicit synchronisation) on every evaluation.  gems_lnl_from_theta_noalloc serves them: it
-// evaluates the same sum as gems_lnl_from_buffer (theta . exp(eval r_c t) prop_c per pattern,
-// |.| + invar, log, + scale, weighted by the pattern counts) over buffers the caller already
-// owns, and keeps its only scratch -- the per-CTA partial sums of the deterministic two-level
-// reduction -- in a fixed file-scope device array instead of allocating it.
+// Some callers cannot allocate device memory at the point they need a likelihood:
+//  * a host application whose own memory pool has reserved (nearly) all of the device, so a
+//    library cudaMalloc either fails or steals from the pool's budget behind its back;
+//  * an embedding that accounts every device byte itself (a serving process with a fixed
+//    per-tenant budget) and forbids libraries from allocating outside that accounting;
+//  * a tight evaluation loop that must not touch the allocator, because cudaMalloc and
+//    cudaFree synchronise the device and would stall the other streams on every evaluation.
+// gems_lnl_from_theta_noalloc serves them: it evaluates the same sum as gems_lnl_from_buffer
+// (theta . exp(eval r_c t) prop_c per pattern, |.| + invar, log, + scale, weighted by the
+// pattern counts) over buffers the caller already owns, and keeps its only scratch -- the
+// per-CTA partial sums of the deterministic two-level reduction -- in a fixed file-scope device
+// array instead of allocating it.  The call is synchronous: it waits for its stream and returns
+// the lnL on the host.
 //
 // The scratch array holds kNoAllocMaxBlocks pairs of doubles plus the two final sums
 // (256 KiB + 16 B).  Every GPU that loads this library holds it until the process exits.  A
 // call needs one pair per CTA of 256 threads, and a CTA covers 256 / G patterns
 // (G = the smallest power of two >= ncat), so nptn is limited to kNoAllocMaxBlocks * 256 / G
 // (4,194,304 patterns for 1 category, 1,048,576 for 4, 524,288 for 8); larger calls are
-// rejected with GEMS_ERR_BAD_ARG.
+// rejected with GEMS_ERR_BAD_ARG before anything is launched.
 //
 // Every call shares the one array and it keeps the last call's contents.  Each call writes
 // every slot it reads before reading it (one pair per CTA of this call, then the final pair),
@@ -25,6 +30,9 @@
 // Host code does not use the array's name as a device address: on the first call on a device
 // (with that device current) the address is looked up once with cudaGetSymbolAddress and cached
 // per device.  That first call should therefore come before any stream capture on that device.
+// The cached address belongs to the device's primary context: after cudaDeviceReset the
+// library's device state (sessions and this address alike) is gone and the library must not be
+// used again in that process.
 #include <cmath>
 #include <mutex>
 

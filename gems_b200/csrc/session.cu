@@ -264,7 +264,29 @@ static void invalidate_theta(Session *s, const gems_op *ops, int nops) {
       s->theta_valid = false;
 }
 
-static int run_ops(Session *s, const gems_op *ops, int nops) {
+// The traversal kernel family a session uses, and the pattern granule a pattern range of it
+// must respect (lower bound a multiple of it; upper bound a multiple of it or the end).
+enum class Form { kTc20, kTc61, kV2, kG61, kMixed, kFp64 };
+
+static Form traversal_form(const Session *s) {
+  if (tc20_supported(s)) return Form::kTc20;
+  if (tc61_supported(s)) return Form::kTc61;
+  if (traverse_v2_supported(s)) return Form::kV2;
+  if (g61_supported(s)) return Form::kG61;
+  return s->desc.precision == GEMS_PREC_MIXED ? Form::kMixed : Form::kFp64;
+}
+
+static int pattern_granule(const Session *s) {
+  switch (traversal_form(s)) {
+    case Form::kTc20:
+    case Form::kTc61: return 128;
+    case Form::kG61: return g61_pattern_granule(s);
+    default: return 1;
+  }
+}
+
+// the op tables of `nops` uploaded ops, then their traversal over patterns [p0, p1)
+static int run_ops_range(Session *s, const gems_op *ops, int nops, int p0, int p1) {
   if (!s->model_set) {
     set_error("model not set");
     return GEMS_ERR_STATE;
@@ -275,27 +297,38 @@ static int run_ops(Session *s, const gems_op *ops, int nops) {
   }
   int st = upload_ops(s, ops, nops);
   if (st) return st;
-  if (tc20_supported(s)) {
-    if ((st = launch_prep_ops_tc20(s, nops))) return st;
-    if ((st = launch_traverse_tc20(s, nops))) return st;
-  } else if (tc61_supported(s)) {
-    if ((st = launch_prep_ops_tc61(s, nops))) return st;
-    if ((st = launch_traverse_tc61(s, nops))) return st;
-  } else if (traverse_v2_supported(s)) {
-    if ((st = launch_prep_ops_v2(s, nops))) return st;
-    if ((st = launch_traverse_v2(s, nops, 0, s->P))) return st;
-  } else if (g61_supported(s)) {
-    if ((st = launch_prep_ops_g61(s, nops))) return st;
-    if ((st = launch_traverse_g61(s, nops))) return st;
-  } else if (s->desc.precision == GEMS_PREC_MIXED) {
-    if ((st = launch_prep_ops_mixed(s, nops))) return st;
-    if ((st = launch_traverse_mixed(s, nops))) return st;
-  } else {
-    if ((st = launch_prep_ops(s, nops))) return st;
-    if ((st = launch_traverse(s, nops))) return st;
+  switch (traversal_form(s)) {
+    case Form::kTc20:
+      if ((st = launch_prep_ops_tc20(s, nops))) return st;
+      if ((st = launch_traverse_tc20(s, nops, p0, p1))) return st;
+      break;
+    case Form::kTc61:
+      if ((st = launch_prep_ops_tc61(s, nops))) return st;
+      if ((st = launch_traverse_tc61(s, nops, p0, p1))) return st;
+      break;
+    case Form::kV2:
+      if ((st = launch_prep_ops_v2(s, nops))) return st;
+      if ((st = launch_traverse_v2(s, nops, p0, p1))) return st;
+      break;
+    case Form::kG61:
+      if ((st = launch_prep_ops_g61(s, nops))) return st;
+      if ((st = launch_traverse_g61(s, nops, p0, p1))) return st;
+      break;
+    case Form::kMixed:
+      if ((st = launch_prep_ops_mixed(s, nops))) return st;
+      if ((st = launch_traverse_mixed(s, nops, p0, p1))) return st;
+      break;
+    case Form::kFp64:
+      if ((st = launch_prep_ops(s, nops))) return st;
+      if ((st = launch_traverse(s, nops, p0, p1))) return st;
+      break;
   }
   invalidate_theta(s, ops, nops);
   return GEMS_OK;
+}
+
+static int run_ops(Session *s, const gems_op *ops, int nops) {
+  return run_ops_range(s, ops, nops, 0, s->P);
 }
 
 static void copy_pattern_lh(Session *s, double *pattern_lh, double lnl_raw_finite) {
@@ -652,6 +685,31 @@ int gems_traverse(gems_session *s, const gems_op *ops, int nops) {
   return GEMS_OK;
 }
 
+int gems_session_pattern_granule(gems_session *s, int *granule) {
+  if (!s || !granule) return GEMS_ERR_BAD_ARG;
+  *granule = pattern_granule(s);
+  return GEMS_OK;
+}
+
+int gems_compute_partial(gems_session *s, const gems_op *op, int ptn_lower, int ptn_upper) {
+  if (!s || !op) return GEMS_ERR_BAD_ARG;
+  const int n = s->desc.nptn, g = pattern_granule(s);
+  if (ptn_lower < 0 || ptn_upper > n || ptn_lower >= ptn_upper || ptn_lower % g != 0 ||
+      (ptn_upper % g != 0 && ptn_upper != n)) {
+    set_error("gems_compute_partial: pattern range out of bounds or not aligned to the "
+              "session's pattern granule (gems_session_pattern_granule)");
+    return GEMS_ERR_BAD_ARG;
+  }
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  // the last range of a traversal also covers the padding patterns, as a whole-list traversal
+  // does, so that the slot holds the same bytes either way
+  const int p1 = ptn_upper == n ? s->P : ptn_upper;
+  int st = run_ops_range(s, op, 1, ptn_lower, p1);
+  if (st) return st;
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  return GEMS_OK;
+}
+
 int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, int nops) {
   if (!ss || nsess <= 0 || nsess > Session::kMaxBatch || (nops > 0 && !ops))
     return GEMS_ERR_BAD_ARG;
@@ -691,7 +749,7 @@ int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, 
   // the batched launch runs on the first session's stream after every session's tables
   for (int i = 1; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
   std::vector<Session *> v(ss, ss + nsess);
-  if (int st = launch_traverse_tc61_batch(v.data(), nsess, nops)) return st;
+  if (int st = launch_traverse_tc61_batch(v.data(), nsess, nops, 0, s0->P)) return st;
   for (int i = 0; i < nsess; i++) invalidate_theta(ss[i], ops, nops);
   return GEMS_OK;
 }

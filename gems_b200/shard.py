@@ -63,7 +63,8 @@ class ShardedTree:
 
     def optimizeOneBranch(self, node1, node2, min_bl=1e-6, max_bl=10.0, max_nr_step=100):
         """Newton on -lnL(t) of the whole (sharded) alignment; every rank takes the same
-        steps.  Returns the optimal length (also set on the engine)."""
+        steps, then the reference's divergence check.  Returns the optimal length (also set on
+        the engine)."""
         eng = self.engine
         t0 = eng.getBranchLength(node1, node2)
         first = [True]
@@ -118,5 +119,15 @@ class ShardedTree:
                     xl = rts
                 elif f > 0.0:
                     xh = rts
+        if res > max_bl * 0.95:
+            # Newton diverged towards the upper bound: keep the old length if its lnL is
+            # higher (optimizeOneBranch, phylotree.cpp:2640-2650); both lnL values are sums
+            # over ranks from the resident theta, and every rank takes the same decision
+            eng.computeFuncDerv(node1, node2, res, False)
+            opt_lh = self._sum(eng.computeLikelihoodFromBuffer())[0]
+            eng.computeFuncDerv(node1, node2, t0, False)
+            orig_lh = self._sum(eng.computeLikelihoodFromBuffer())[0]
+            if orig_lh > opt_lh:
+                res = t0
         eng.setLength(node1, node2, res)  # also invalidates the partials across the branch
         return res

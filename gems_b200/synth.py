@@ -176,14 +176,12 @@ def codon_sense():
     return cods, aas
 
 
-def codon_gy(rng: np.random.Generator, ncat=4, alpha=0.5, freerate=False) -> Model:
-    """Goldman-Yang style codon model: exchangeability kappa for a transition, omega for a
-    non-synonymous change, 0 for codons differing at more than one position."""
+def gy_exchangeabilities(omega: float, kappa: float) -> np.ndarray:
+    """Goldman-Yang exchangeabilities over the 61 sense codons (upper triangle, row-major):
+    kappa for a transition, times omega for a non-synonymous change, 0 for codons differing
+    at more than one position (model/modelcodon.cpp:366, GY with fixed kappa and omega)."""
     cods, aas = codon_sense()
     n = len(cods)
-    omega = rng.uniform(0.1, 1.0)
-    kappa = rng.uniform(1.0, 5.0)
-    freq = rng.dirichlet(np.ones(n))
     purine = set("AG")
     exch = []
     for i in range(n):
@@ -197,7 +195,17 @@ def codon_gy(rng: np.random.Generator, ncat=4, alpha=0.5, freerate=False) -> Mod
             if aas[i] != aas[j]:
                 r *= omega
             exch.append(r)
-    exch = np.array(exch)
+    return np.array(exch)
+
+
+def codon_gy(rng: np.random.Generator, ncat=4, alpha=0.5, freerate=False) -> Model:
+    """Goldman-Yang style codon model: omega ~ U[0.1,1], kappa ~ U[1,5], frequencies
+    ~ Dirichlet(1^61); +G (mean rates) or a free-rate model with ncat categories."""
+    n = len(codon_sense()[0])
+    omega = rng.uniform(0.1, 1.0)
+    kappa = rng.uniform(1.0, 5.0)
+    freq = rng.dirichlet(np.ones(n))
+    exch = gy_exchangeabilities(omega, kappa)
     if freerate:
         props = rng.dirichlet(np.ones(ncat))
         rates = np.sort(rng.gamma(1.0, 1.0, ncat))

@@ -8,7 +8,8 @@
  *     likelihood buffer, scale counter, theta buffer and tip byte; the caller keeps topology
  *     and cache flags and names buffers by slot id.  Replaces the pointer targets that
  *     PhyloTree::setLikelihoodKernel installs (tree/phylotreesse.cpp:91-199):
- *        computePartialLikelihoodPointer   (tree/phylotree.h:902-903)   -> gems_traverse
+ *        computePartialLikelihoodPointer   (tree/phylotree.h:902-903)   -> gems_compute_partial
+ *                                        (one entry, one packet; gems_traverse: the whole list)
  *        computeLikelihoodBranchPointer    (tree/phylotree.h:948-950)   -> gems_branch_lnl
  *        computeLikelihoodDervPointer      (tree/phylotree.h:1343-1345) -> gems_branch_derv
  *        computeLikelihoodFromBufferPointer(tree/phylotree.h:1002-1003) -> gems_lnl_from_buffer
@@ -139,6 +140,21 @@ int gems_get_eigensystem(gems_session *s, double *eval, double *evec, double *in
 /* Postorder list of node updates (computePartialLikelihood over all patterns for each
  * entry of traversal_info; tree/phylokernelnew.h:1293-2043). */
 int gems_traverse(gems_session *s, const gems_op *ops, int nops);
+/* One node update over the patterns [ptn_lower, ptn_upper): the partial of op->dst_slot from
+ * its two children, for those patterns only -- PhyloTree::computePartialLikelihood
+ * (TraversalInfo &info, size_t ptn_lower, size_t ptn_upper, int packet_id)
+ * (tree/phylotree.h:900-903, tree/phylotreesse.cpp:212), which the reference's drivers call
+ * once per (packet, traversal entry) (tree/phylokernelnew.h:1274-1281).  Patterns outside the
+ * range are left as they are.  ptn_lower must be a multiple of the session's pattern granule,
+ * ptn_upper a multiple of it or nptn; the range must be non-empty and inside [0, nptn).
+ * Packets that cover [0, nptn) give the same slot contents, bit for bit, as gems_traverse of
+ * the same ops. */
+int gems_compute_partial(gems_session *s, const gems_op *op, int ptn_lower, int ptn_upper);
+/* The pattern granule of gems_compute_partial for this session: 1 for the CUDA-core forms of
+ * 4 and 20 states and the generic forms, 128 for the tcgen05 forms (their pattern tiles), the
+ * pattern tile of the FP64 61-state GEMM form (the reference's packets are aligned to its
+ * vector width in the same way, computeBounds, tree/phylokernelnew.h:1118). */
+int gems_session_pattern_granule(gems_session *s, int *granule);
 /* Batched traversal over sessions that share one tree (the same op list and lengths) but hold
  * different models -- ModelFinder's candidate models on one alignment (modelfactory.cpp:1558,
  * main/phylotesting.cpp) -- so that many small sessions fill the GPU.  All sessions must have the
@@ -185,18 +201,20 @@ int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems
 
 /* ---- allocation-free evaluation ---- */
 /* No counterpart in the reference.  lnL at branch length `length` from a theta buffer the
- * caller owns, for callers that cannot allocate device memory when they evaluate (inside a
- * stream capture, under a memory pool that owns the device, or in a loop that must not touch
- * the allocator).  It computes what gems_lnl_from_buffer computes, over caller-owned device
- * arrays: theta[nptn][ncat][nstates] and scale_all[nptn] (the layout gems_get_theta returns),
+ * caller owns, for callers that cannot allocate device memory when they evaluate: a host whose
+ * own memory pool has reserved the device, an embedding that accounts every device byte itself,
+ * or a loop that must not hit cudaMalloc/cudaFree (they synchronise the device).  It computes
+ * what gems_lnl_from_buffer computes, over caller-owned device arrays:
+ * theta[nptn][ncat][nstates] and scale_all[nptn] (the layout gems_get_theta returns),
  * freq[nptn] and invar[nptn] (invar may be NULL); eval[nstates], rates[ncat], props[ncat]
- * are host arrays.  stream is a cudaStream_t (NULL: the default stream); lnl (host) receives
- * the result after the stream synchronises.  No cudaMalloc, cudaFree or allocating library
- * call is made: the reduction scratch is a fixed device array of this library (256 KiB per
- * GPU, held until exit), which limits nptn to 4194304 / G (G = smallest power of two >=
- * ncat); larger calls return GEMS_ERR_BAD_ARG.  The first call on a device looks up the
- * array's device address, so make it before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * are host arrays.  stream is a cudaStream_t (NULL: the default stream).  The call is
+ * synchronous: it waits for its stream and writes the result to lnl (host).  No cudaMalloc,
+ * cudaFree or allocating library call is made: the reduction scratch is a fixed device array
+ * of this library (256 KiB per GPU, held until exit), which limits nptn to 4194304 / G
+ * (G = smallest power of two >= ncat); larger calls return GEMS_ERR_BAD_ARG.  The first call
+ * on a device looks up the array's device address, so make it before any stream capture on
+ * that device.  All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 int gems_lnl_from_theta_noalloc(const double *theta, const double *scale_all,
                                 const double *freq, const double *invar, int nptn,
                                 int nstates, int ncat, const double *eval,

@@ -5,7 +5,10 @@ of gems_compress_alignment; never used by the product path).
   sequences upper-cased first (:2451);
 - build_patterns: one site after another, a new column becomes the next pattern, a repeated
   one adds to its pattern's frequency (buildPattern :1240-1268, addPatternLazy :1511-1543);
-- const_char: computeConst :1321-1420 with getAppearance :5567-5600.
+- const_char: computeConst :1321-1420 with getAppearance :5567-5600;
+- site_stat / site_summary: the pattern flags of computeConst (:1365-1371, :1410-1451), the
+  per-site statistic of printSiteInfo (:1455-1477) and the counts of countConstSite
+  (:4822-4843) that the program's report prints.
 """
 from __future__ import annotations
 
@@ -89,3 +92,38 @@ def build_patterns(codes: np.ndarray, n: int):
     pat = np.stack(cols, axis=1)
     cc = np.array([const_char(pat[:, p], n) for p in range(pat.shape[1])], dtype=np.uint8)
     return pat, np.array(weights, np.float64), np.array(site_pattern, np.int32), cc
+
+
+# per-site statistic codes, in printSiteInfo's letters: I, C, c, U, -
+STAT_INFORMATIVE, STAT_CONST, STAT_CONST_AMBIG, STAT_UNINFORMATIVE, STAT_ALL_GAP = range(5)
+
+
+def pattern_flags(column, n: int):
+    """(is_const, is_informative, const_char) of one pattern: const when some state is
+    compatible with every character (is_const and is_invariant coincide there); informative
+    when at least two unambiguous states appear at least twice each."""
+    cc = const_char(column, n)
+    counts = np.bincount(np.asarray([c for c in column if c < n], np.int64), minlength=n)
+    informative = int((counts >= 2).sum()) >= 2
+    return cc <= _unknown(n), informative, cc
+
+
+def site_stat(column, n: int) -> int:
+    is_const, informative, cc = pattern_flags(column, n)
+    if informative:
+        return STAT_INFORMATIVE
+    if is_const:
+        if cc == _unknown(n):
+            return STAT_ALL_GAP
+        return STAT_CONST if cc < n else STAT_CONST_AMBIG
+    return STAT_UNINFORMATIVE
+
+
+def site_summary(patterns: np.ndarray, weights: np.ndarray, n: int):
+    """(constant, invariant, informative, distinct) site counts as countConstSite forms them."""
+    const = inform = 0
+    for p in range(patterns.shape[1]):
+        is_const, informative, _ = pattern_flags(patterns[:, p], n)
+        const += int(weights[p]) if is_const else 0
+        inform += int(weights[p]) if informative else 0
+    return const, const, inform, patterns.shape[1]

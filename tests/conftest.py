@@ -19,6 +19,11 @@ def golden_files():
     return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
 
 
+def golden_opt_files():
+    """Golden cases that carry the program's optimised branch lengths."""
+    return [p for p in golden_files() if "ref_lnl_opt" in np.load(p).files]
+
+
 def load_golden(path):
     """Inputs of a golden case as (tree, model, aln, z) with the oracle's eigensystem."""
     from gems_b200 import synth

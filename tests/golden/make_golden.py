@@ -13,11 +13,21 @@ and `-prec 12` so the report prints 12 decimals:
   * `-safe`       : the same with the SAFE (per-category) scaling kernel.
 
 Each case is saved as <name>.npz holding the inputs (compressed patterns, tree, model
-parameters) and the program's outputs.  Re-run with
+parameters) and the program's outputs.  A 61-state codon case (GY with omega and kappa fixed,
+`-st CODON`) pins the codon model and the 61-state kernels the same way.
 
-    python tests/golden/make_golden.py [--ref /path/to/iqtree-source]
+The ingest fixtures under ingest/ pin the alignment reading and pattern compression on the
+reference's own test alignments (turtle.fa, turtle_aa.fasta, example.phy): the raw
+characters, the program's distinct-pattern count and site summary counts, its per-site
+statistic (`-alninfo`: informative / constant / ambiguous-constant / uninformative / all-gap)
+and its per-site log-likelihoods at a fixed model and tree.
 
-This script needs the reference tree; the committed .npz fixtures do not.
+Re-run with
+
+    python tests/golden/make_golden.py --ref <iqtree source tree> [--only name ...]
+
+or with the source tree in the IQTREE_SOURCE environment variable.  This script needs the
+reference tree; the committed .npz fixtures do not.
 """
 from __future__ import annotations
 
@@ -163,10 +173,11 @@ def run_iqtree(binary, aln_path, tree_path, model, workdir, prefix, extra=()):
     if r.returncode != 0:
         raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
     rep = open(os.path.join(workdir, prefix + ".iqtree")).read()
+    log = r.stdout
     lnl = float(re.search(r"Log-likelihood of the tree: (-?[0-9.]+)", rep).group(1))
     rates = [float(x) for x in re.findall(r"^\s+\d+\s+([0-9.eE+-]+)\s+[0-9.eE+-]+\s*$", rep,
                                           re.M)]
-    out = {"lnl": lnl, "rates": rates}
+    out = {"lnl": lnl, "rates": rates, "log": log, "report": rep}
     sl = os.path.join(workdir, prefix + ".sitelh")
     if os.path.exists(sl):
         lines = open(sl).read().split("\n")
@@ -186,6 +197,162 @@ def paml_file(path, model):
         for i in range(1, n):
             f.write(" ".join(f"{s[i, j]:.17g}" for j in range(i)) + "\n")
         f.write("\n" + " ".join(f"{x:.17g}" for x in model.freq) + "\n")
+
+
+def codon_case(binary, workdir, name="codon12_g4"):
+    """GY codon model with omega, kappa, the 61 frequencies and the Gamma shape fixed; 12 taxa,
+    1,500 codon sites with 3% gap codons; the program runs it with -st CODON."""
+    rng = np.random.default_rng(606)
+    omega, kappa = rng.uniform(0.1, 1.0), rng.uniform(1.0, 5.0)
+    cods, _ = synth.codon_sense()
+    freq = rng.dirichlet(np.ones(len(cods)))
+    alpha, ncat = 0.6, 4
+    model = synth.Model(61, synth.gy_exchangeabilities(omega, kappa), freq,
+                        orc.gamma_rates(alpha, ncat), np.full(ncat, 1.0 / ncat),
+                        gamma_shape=alpha)
+    tree = synth.random_tree(12, 0.15, 611)
+    aln = synth.simulate(tree, model, 1500, 623, gap_frac=0.03)
+    names = [f"T{i}" for i in range(tree.ntaxa)]
+    cols = synth.expand_patterns(aln)
+    fa = os.path.join(workdir, name + ".fa")
+    with open(fa, "w") as f:
+        for i, row in enumerate(cols):
+            f.write(f">{names[i]}\n" + "".join(cods[x] if x < 61 else "---" for x in row) + "\n")
+    nwk = os.path.join(workdir, name + ".nwk")
+    open(nwk, "w").write(tree.newick(names))
+    # the program orders codons by nucleotides A < C < G < T
+    order = sorted(range(61), key=lambda i: ["ACGT".index(c) for c in cods[i]])
+    mstr = (f"GY{{{omega:.17g},{kappa:.17g}}}+F{{" +
+            ",".join(f"{freq[i]:.17g}" for i in order) + f"}}+G{ncat}{{{alpha:.17g}}}")
+    extra = ["-st", "CODON", "-safe"]
+    fixed = run_iqtree(binary, fa, nwk, mstr, workdir, name + "_fix", ["-blfix", "-wsl"] + extra)
+    if "not present" in fixed["log"]:
+        raise RuntimeError("a codon state is absent: the program would drop it from the model")
+    # With every model parameter fixed the program does not re-optimise the branch lengths of
+    # a codon model given by -te (its report shows one round and the input lengths), so this
+    # case carries no optimised lengths.
+    reps = aln.weights.astype(np.int64)
+    first = np.concatenate([[0], np.cumsum(reps)[:-1]])
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        nstates=61, ntaxa=tree.ntaxa, eu=tree.eu, ev=tree.ev, length=tree.length,
+        exch_upper=model.exch_upper, freq=freq, alpha=alpha, ncat=ncat, p_invar=0.0,
+        rates=model.rates, props=model.props, patterns=aln.patterns, weights=aln.weights,
+        const_char=aln.const_char(), safe=1, omega=omega, kappa=kappa,
+        ref_lnl_fixed=fixed["lnl"], ref_rates=np.array(fixed["rates"]),
+        ref_pattern_lnl_6sig=fixed["site_lnl"][first], model_string=mstr)
+    print(f"{name}: npat={aln.npat} lnl_fixed={fixed['lnl']!r}")
+
+
+def read_phylip(path):
+    """Sequential PHYLIP: a header 'ntaxa nsites', then a name and its sequence per taxon."""
+    lines = [ln.rstrip("\n") for ln in open(path)]
+    ntaxa, nsites = (int(x) for x in lines[0].split()[:2])
+    names, seqs = [], []
+    for ln in lines[1:]:
+        if not ln.strip():
+            continue
+        if len(names) < ntaxa and (not seqs or len(seqs[-1]) >= nsites):
+            parts = ln.split()
+            names.append(parts[0])
+            seqs.append("".join(parts[1:]))
+        else:
+            seqs[-1] += "".join(ln.split())
+    assert len(names) == ntaxa and all(len(x) == nsites for x in seqs)
+    return names, seqs
+
+
+def tree_from_treefile(treefile, names):
+    """A program-written Newick tree as a synth.Tree with leaves numbered in sequence order."""
+    nd, ed = parse_newick(treefile)
+    leaf_idx = {nm: i for i, nm in enumerate(names)}
+    ntaxa = len(names)
+    mp, nxt = {}, ntaxa
+    for i, nm in enumerate(nd):
+        if nm is not None:
+            mp[i] = leaf_idx[nm]
+        else:
+            mp[i] = nxt
+            nxt += 1
+    eu = np.array([mp[p] for p, c, ln in ed], np.int32)
+    ev = np.array([mp[c] for p, c, ln in ed], np.int32)
+    ln = np.array([l for p, c, l in ed])
+    return synth.Tree(ntaxa, eu, ev, ln)
+
+
+STAT_CODE = {"I": 0, "C": 1, "c": 2, "U": 3, "-": 4}
+
+
+def ingest_case(binary, ref, workdir, fname, nstates, seed):
+    """One of the reference's test alignments: raw characters, the program's pattern and site
+    statistics, and its per-site lnL at a fixed seeded model on the tree the program builds
+    for the file (`-n 0`)."""
+    path = os.path.join(ref, "test_scripts", "test_data", fname)
+    names, seqs = read_phylip(path) if fname.endswith(".phy") else read_fasta_raw(path)
+    start = run_iqtree_plain(binary, path, "JC" if nstates == 4 else "LG", workdir,
+                             "start_" + fname, ["-n", "0"])
+    tree = tree_from_treefile(start["treefile"], names)
+    tree_path = os.path.join(workdir, "tree_" + fname + ".nwk")
+    open(tree_path, "w").write(start["treefile"])
+    rng = np.random.default_rng(seed)
+    alpha, ncat = 0.7, 4
+    if nstates == 4:
+        m = synth.dna_gtr(rng, ncat, alpha)
+        ex = m.exch_upper / m.exch_upper[5]
+        mstr = ("GTR{" + ",".join(f"{x:.17g}" for x in ex[:5]) + "}+F{" +
+                ",".join(f"{x:.17g}" for x in m.freq) + "}")
+    else:
+        m = synth.protein(rng, ncat, alpha)
+        pf = os.path.join(workdir, fname + ".paml")
+        paml_file(pf, m)
+        mstr = pf
+    mstr += f"+G{ncat}{{{alpha:.17g}}}"
+    out = run_iqtree(binary, path, tree_path, mstr, workdir, "fix_" + fname,
+                     ["-blfix", "-wsl", "-alninfo"])
+    rep = out["report"]
+
+    def count(label):
+        return int(re.search(label + r": (\d+)", rep).group(1))
+
+    stat_lines = open(os.path.join(workdir, "fix_" + fname + ".alninfo")).read().split("\n")
+    stats = [ln.split("\t") for ln in stat_lines if ln and not ln.startswith("#")][1:]
+    site_stat = np.array([STAT_CODE[st] for _, st in stats], np.uint8)
+    raw = np.array([np.frombuffer(s.encode(), np.uint8) for s in seqs])
+    key = os.path.splitext(fname)[0]
+    np.savez_compressed(
+        os.path.join(HERE, "ingest", key + ".npz"),
+        source=fname, nstates=nstates, chars=raw, ntaxa=len(names), eu=tree.eu, ev=tree.ev,
+        length=tree.length, exch_upper=m.exch_upper, freq=m.freq, alpha=alpha,
+        rates=orc.gamma_rates(alpha, ncat), props=np.full(ncat, 1.0 / ncat),
+        ref_lnl=out["lnl"], ref_site_lnl_6sig=out["site_lnl"], ref_site_stat=site_stat,
+        ref_distinct=count("Number of distinct site patterns"),
+        ref_const=count("Number of constant sites"),
+        ref_invariant=count(r"Number of invariant \(constant or ambiguous constant\) sites"),
+        ref_informative=count("Number of parsimony informative sites"), model_string=mstr)
+    print(f"ingest/{key}: sites={raw.shape[1]} distinct={count('Number of distinct site patterns')}"
+          f" lnl={out['lnl']!r}")
+
+
+def read_fasta_raw(path):
+    """FASTA with the characters as written (no case change)."""
+    names, seqs = [], []
+    for line in open(path):
+        line = line.strip()
+        if line.startswith(">"):
+            names.append(line[1:].split()[0])
+            seqs.append([])
+        elif line:
+            seqs[-1].append(line)
+    return names, ["".join(s) for s in seqs]
+
+
+def run_iqtree_plain(binary, aln_path, model, workdir, prefix, extra=()):
+    cmd = [binary, "-s", aln_path, "-m", model, "-T", "1", "-prec", "12", "-redo", "-pre",
+           os.path.join(workdir, prefix), "-seed", "1"] + list(extra)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stdout[-2000:] + r.stderr[-2000:])
+    return {"treefile": open(os.path.join(workdir, prefix + ".treefile")).read().strip()}
 
 
 def model_arrays(model, alpha, ncat, pinv=0.0):
@@ -306,58 +473,81 @@ def turtle_case(binary, ref, workdir):
     print(f"turtle_ref: npat={aln.npat} lnl_fixed={fixed['lnl']!r}")
 
 
+CASES = ("dna16_g4", "dna24_gaps_amb", "dna160_deep", "dna12_inv_g4", "prot12_g4", "turtle_ref",
+         "codon12_g4", "ingest")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("IQTREE_SOURCE"),
+                    help="IQ-TREE source tree holding test_scripts/ (or set IQTREE_SOURCE)")
+    ap.add_argument("--only", nargs="*", choices=CASES, default=list(CASES),
+                    help="regenerate only these cases")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref or set IQTREE_SOURCE")
     binary = os.path.join(args.ref, "test_scripts", "iqtree2", "Linux-intel", "iqtree2")
+    only = set(args.only)
     with tempfile.TemporaryDirectory() as wd:
-        # DNA GTR+G4, 16 taxa (the small FP64 configuration, 2,000 sites)
-        rng = np.random.default_rng(101)
-        m = synth.dna_gtr(rng, 4, 0.5)
-        m = synth.Model(4, m.exch_upper, m.freq, orc.gamma_rates(0.5, 4), np.full(4, 0.25),
-                        gamma_shape=0.5)
-        t = synth.random_tree(16, 0.1, 111)
-        a = synth.simulate(t, m, 2000, 123)
-        make_case(binary, "dna16_g4", t, m, a, wd)
-        make_case(binary, "dna16_g4_safe", t, m, a, wd, safe=True)
-        # gaps and IUPAC ambiguity codes, 24 taxa
-        rng = np.random.default_rng(202)
-        m = synth.dna_gtr(rng, 4, 0.7)
-        m = synth.Model(4, m.exch_upper, m.freq, orc.gamma_rates(0.7, 4), np.full(4, 0.25),
-                        gamma_shape=0.7)
-        t = synth.random_tree(24, 0.08, 211)
-        a = synth.simulate(t, m, 1500, 223, gap_frac=0.05)
-        cols = synth.expand_patterns(a)
-        amb = np.random.default_rng(5).random(cols.shape) < 0.03
-        cols[amb] = np.random.default_rng(6).integers(4, 18, amb.sum())
-        cols[:, 0] = 18  # an all-gap column
-        a = synth.compress(cols, 4)
-        make_case(binary, "dna24_gaps_amb", t, m, a, wd)
-        # deep tree: underflow scaling events (NORM and SAFE)
-        rng = np.random.default_rng(303)
-        m = synth.dna_gtr(rng, 4, 0.5)
-        m = synth.Model(4, m.exch_upper, m.freq, orc.gamma_rates(0.5, 4), np.full(4, 0.25),
-                        gamma_shape=0.5)
-        t = synth.random_tree(160, 0.3, 311)
-        a = synth.simulate(t, m, 400, 323)
-        make_case(binary, "dna160_deep", t, m, a, wd)
-        make_case(binary, "dna160_deep_safe", t, m, a, wd, safe=True)
-        # +I+G4 (invariant sites)
-        rng = np.random.default_rng(404)
-        m = synth.dna_gtr(rng, 4, 0.6)
-        t = synth.random_tree(12, 0.1, 411)
-        a = synth.simulate(t, m, 1200, 423)
-        make_case(binary, "dna12_inv_g4", t, m, a, wd, pinv=0.25)
-        # 20-state protein +G4 with a user exchangeability matrix (PAML format)
-        rng = np.random.default_rng(505)
-        m = synth.protein(rng, 4, 0.8)
-        m = synth.Model(20, m.exch_upper, m.freq, orc.gamma_rates(0.8, 4), np.full(4, 0.25),
-                        gamma_shape=0.8)
-        t = synth.random_tree(12, 0.15, 511)
-        a = synth.simulate(t, m, 800, 523)
-        make_case(binary, "prot12_g4", t, m, a, wd, protein=True)
-        turtle_case(binary, args.ref, wd)
+        if "dna16_g4" in only:
+            # DNA GTR+G4, 16 taxa (the small FP64 configuration, 2,000 sites)
+            rng = np.random.default_rng(101)
+            m = synth.dna_gtr(rng, 4, 0.5)
+            m = synth.Model(4, m.exch_upper, m.freq, orc.gamma_rates(0.5, 4), np.full(4, 0.25),
+                            gamma_shape=0.5)
+            t = synth.random_tree(16, 0.1, 111)
+            a = synth.simulate(t, m, 2000, 123)
+            make_case(binary, "dna16_g4", t, m, a, wd)
+            make_case(binary, "dna16_g4_safe", t, m, a, wd, safe=True)
+        if "dna24_gaps_amb" in only:
+            # gaps and IUPAC ambiguity codes, 24 taxa
+            rng = np.random.default_rng(202)
+            m = synth.dna_gtr(rng, 4, 0.7)
+            m = synth.Model(4, m.exch_upper, m.freq, orc.gamma_rates(0.7, 4), np.full(4, 0.25),
+                            gamma_shape=0.7)
+            t = synth.random_tree(24, 0.08, 211)
+            a = synth.simulate(t, m, 1500, 223, gap_frac=0.05)
+            cols = synth.expand_patterns(a)
+            amb = np.random.default_rng(5).random(cols.shape) < 0.03
+            cols[amb] = np.random.default_rng(6).integers(4, 18, amb.sum())
+            cols[:, 0] = 18  # an all-gap column
+            a = synth.compress(cols, 4)
+            make_case(binary, "dna24_gaps_amb", t, m, a, wd)
+        if "dna160_deep" in only:
+            # deep tree: underflow scaling events (NORM and SAFE)
+            rng = np.random.default_rng(303)
+            m = synth.dna_gtr(rng, 4, 0.5)
+            m = synth.Model(4, m.exch_upper, m.freq, orc.gamma_rates(0.5, 4), np.full(4, 0.25),
+                            gamma_shape=0.5)
+            t = synth.random_tree(160, 0.3, 311)
+            a = synth.simulate(t, m, 400, 323)
+            make_case(binary, "dna160_deep", t, m, a, wd)
+            make_case(binary, "dna160_deep_safe", t, m, a, wd, safe=True)
+        if "dna12_inv_g4" in only:
+            # +I+G4 (invariant sites)
+            rng = np.random.default_rng(404)
+            m = synth.dna_gtr(rng, 4, 0.6)
+            t = synth.random_tree(12, 0.1, 411)
+            a = synth.simulate(t, m, 1200, 423)
+            make_case(binary, "dna12_inv_g4", t, m, a, wd, pinv=0.25)
+        if "prot12_g4" in only:
+            # 20-state protein +G4 with a user exchangeability matrix (PAML format)
+            rng = np.random.default_rng(505)
+            m = synth.protein(rng, 4, 0.8)
+            m = synth.Model(20, m.exch_upper, m.freq, orc.gamma_rates(0.8, 4), np.full(4, 0.25),
+                            gamma_shape=0.8)
+            t = synth.random_tree(12, 0.15, 511)
+            a = synth.simulate(t, m, 800, 523)
+            make_case(binary, "prot12_g4", t, m, a, wd, protein=True)
+        if "turtle_ref" in only:
+            turtle_case(binary, args.ref, wd)
+        if "codon12_g4" in only:
+            codon_case(binary, wd)
+        if "ingest" in only:
+            os.makedirs(os.path.join(HERE, "ingest"), exist_ok=True)
+            ingest_case(binary, args.ref, wd, "turtle.fa", 4, 701)
+            ingest_case(binary, args.ref, wd, "turtle_aa.fasta", 20, 702)
+            ingest_case(binary, args.ref, wd, "example.phy", 4, 703)
 
 
 if __name__ == "__main__":

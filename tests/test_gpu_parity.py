@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import golden_files, load_golden, ptn_invar
+from conftest import golden_files, golden_opt_files, load_golden, ptn_invar
 from gems_b200 import GemsError, PhyloTree, Session, synth
 from oracle import oracle as orc
 
@@ -83,8 +83,10 @@ def test_lnl_on_every_branch_and_derivatives(gpu, path):
         assert abs(ddfg - ddfo) <= RTOL * max(1.0, abs(ddfo))
 
 
-@pytest.mark.parametrize("path", [p for p in CASES if "turtle" not in p],
-                         ids=[i for i in IDS if "turtle" not in i])
+OPT = golden_opt_files()
+
+
+@pytest.mark.parametrize("path", OPT, ids=[os.path.basename(p)[:-4] for p in OPT])
 def test_optimize_all_branches(gpu, path):
     tree, model, aln, z = load_golden(path)
     safe = bool(z["safe"])

@@ -3,6 +3,9 @@ reference's pattern building restated in oracle/ingest.py -- same patterns in th
 first-appearance order, weights, site -> pattern map and constant states -- for DNA and protein
 characters (ambiguity codes, gaps, lower case) and pre-encoded codon states; and at a larger size
 against the host compressor."""
+import glob
+import os
+
 import numpy as np
 import pytest
 
@@ -125,4 +128,88 @@ def test_ingest_to_session_lnl_matches_oracle(gpu):
     ot = orc.OracleTree(tree, model, aln, const_char=cc, p_invar=model.p_invar)
     lo, lg = ot.computeLikelihood(), gt.computeLikelihood()
     assert abs(lg - lo) <= 1e-9 * abs(lo), (lg, lo)
+    ing.close()
+
+
+# ---- pinned to the reference program on the reference's own test alignments ----
+INGEST_GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ingest",
+                                              "*.npz")))
+INGEST_IDS = [os.path.basename(p)[:-4] for p in INGEST_GOLDEN]
+
+
+def _ingest_fixture(path):
+    z = np.load(path)
+    seqs = [bytes(r).decode() for r in z["chars"]]
+    return z, seqs, int(z["nstates"])
+
+
+@pytest.mark.parametrize("path", INGEST_GOLDEN, ids=INGEST_IDS)
+def test_restatement_pattern_statistics_match_program(path):
+    """Distinct patterns, constant / invariant / informative site counts and the per-site
+    statistic (-alninfo) of the restatement equal the program's on the raw file characters."""
+    z, seqs, n = _ingest_fixture(path)
+    pat, w, sp, cc = ingest.build_patterns(ingest.encode(seqs, n), n)
+    const, invar, inform, distinct = ingest.site_summary(pat, w, n)
+    assert distinct == int(z["ref_distinct"])
+    assert const == int(z["ref_const"])
+    assert invar == int(z["ref_invariant"])
+    assert inform == int(z["ref_informative"])
+    stat = np.array([ingest.site_stat(pat[:, p], n) for p in range(pat.shape[1])])
+    np.testing.assert_array_equal(stat[sp], z["ref_site_stat"])
+
+
+def _fixture_case(z, pat, w):
+    n = int(z["nstates"])
+    tree = synth.Tree(int(z["ntaxa"]), z["eu"], z["ev"], z["length"])
+    from oracle import oracle as orc
+    ev, v, iv = orc.eigensystem(z["exch_upper"], z["freq"])
+    model = synth.Model(n, z["exch_upper"], z["freq"], z["rates"], z["props"], ev, v, iv,
+                        gamma_shape=float(z["alpha"]))
+    aln = synth.Alignment(int(z["ntaxa"]), n, int(w.sum()), pat, w)
+    return tree, model, aln
+
+
+@pytest.mark.parametrize("path", INGEST_GOLDEN, ids=INGEST_IDS)
+def test_restatement_site_lnl_matches_program(path):
+    """Each site's log-likelihood, read through the restatement's site -> pattern map, equals
+    the program's per-site value (printed to 6 significant digits) at a fixed model and tree;
+    the total to the program's 12 decimals.  This pins the character encoding (ambiguity codes,
+    gaps, case) and the site map together."""
+    from oracle import oracle as orc
+    z, seqs, n = _ingest_fixture(path)
+    pat, w, sp, cc = ingest.build_patterns(ingest.encode(seqs, n), n)
+    tree, model, aln = _fixture_case(z, pat, w)
+    ot = orc.OracleTree(tree, model, aln, const_char=cc)
+    lnl, plh = ot.computeLikelihood(pattern_lh=True)
+    ref = float(z["ref_lnl"])
+    assert abs(lnl - ref) <= 1e-11 * abs(ref), (lnl, ref)
+    site = plh[sp]
+    r = z["ref_site_lnl_6sig"]
+    assert np.all(np.abs(site - r) <= 1e-5 * np.abs(r) + 1e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", INGEST_GOLDEN, ids=INGEST_IDS)
+def test_device_ingest_on_reference_files(gpu, path):
+    """The device ingest of the raw file characters gives the restatement's patterns, weights,
+    site map and constant states, and a session loaded from it on the device reproduces the
+    program's log-likelihood."""
+    from gems_b200 import Ingest, PhyloTree, Session
+    z, seqs, n = _ingest_fixture(path)
+    raw = np.ascontiguousarray(z["chars"], np.uint8)
+    ing = Ingest(raw, n)
+    pat, w, sp, cc = ing.read()
+    rp, rw, rsp, rcc = ingest.build_patterns(ingest.encode(seqs, n), n)
+    np.testing.assert_array_equal(pat, rp)
+    np.testing.assert_array_equal(w, rw)
+    np.testing.assert_array_equal(sp, rsp)
+    np.testing.assert_array_equal(cc, rcc)
+    tree, model, aln = _fixture_case(z, pat, w)
+    s = Session(tree.ntaxa, ing.npat, n, model.ncat, tree.ntaxa - 2)
+    ing.to_session(s, 0.0, model.freq)
+    s.set_model(model.eval, model.evec, model.inv_evec, model.rates, model.props)
+    gt = PhyloTree(s, tree.eu, tree.ev, tree.length)
+    lg = gt.computeLikelihood()
+    ref = float(z["ref_lnl"])
+    assert abs(lg - ref) <= 1e-11 * abs(ref), (lg, ref)
     ing.close()

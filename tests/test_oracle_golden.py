@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import golden_files, load_golden
+from conftest import golden_files, golden_opt_files, load_golden
 from oracle import oracle as orc
 
 CASES = golden_files()
@@ -32,8 +32,10 @@ def test_lnl_at_fixed_lengths(path):
     assert np.allclose(rates, rr, rtol=1e-10, atol=0)
 
 
-@pytest.mark.parametrize("path", [p for p in CASES if "turtle" not in p],
-                         ids=[os.path.basename(p)[:-4] for p in CASES if "turtle" not in p])
+OPT = golden_opt_files()
+
+
+@pytest.mark.parametrize("path", OPT, ids=[os.path.basename(p)[:-4] for p in OPT])
 def test_branch_optimisation_reaches_reference_optimum(path):
     tree, model, aln, z = load_golden(path)
     ot = orc.OracleTree(tree, model, aln, safe=bool(z["safe"]), const_char=z["const_char"])

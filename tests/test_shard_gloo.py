@@ -83,3 +83,39 @@ def test_two_rank_gloo_matches_unsharded(tmp_path):
         assert abs(r["opt"] - opt) <= 1e-8
         assert abs(r["lnl_after"] - lnl_after) <= 1e-10 * abs(lnl_after)
     assert res[0] == res[1]
+
+
+class _FakeEngine:
+    """An engine whose -lnL has its minimum at the upper bound and whose lnL at the old
+    length is higher than at that minimum: optimizeOneBranch's divergence check must keep
+    the old length."""
+
+    def __init__(self):
+        self.t = 0.3
+        self.lengths = {}
+
+    def getBranchLength(self, u, v):
+        return 0.3
+
+    def computeFuncDerv(self, u, v, x, new_branch=False):
+        self.t = x
+        return -1.0, 1.0  # f < 0 everywhere: Newton walks to the upper bound
+
+    def computeLikelihoodFromBuffer(self):
+        return -10.0 if abs(self.t - 0.3) < 1e-12 else -20.0
+
+    def setLength(self, u, v, x):
+        self.lengths[(u, v)] = x
+
+
+class _NoDist:
+    @staticmethod
+    def all_reduce(buf, group=None):
+        return None
+
+
+def test_divergence_check_keeps_old_length():
+    eng = _FakeEngine()
+    st = ShardedTree(eng, _NoDist)
+    assert st.optimizeOneBranch(0, 1) == 0.3
+    assert eng.lengths[(0, 1)] == 0.3
