@@ -27,7 +27,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 CUDA_SOURCES = ["session.cu", "kernels_fp64.cu", "kernels_mixed.cu", "kernels_traverse.cu",
                 "kernels_tc20.cu", "kernels_tc61.cu", "kernels_g61.cu", "kernels_rell.cu", "eigen.cu", "noalloc.cu", "peaks.cu", "ingest.cu",
                 "phylotree.cpp"]
-HEADERS = ["gems_internal.cuh", "tc_common.cuh"]
+HEADERS = ["gems_internal.cuh", "tc_common.cuh", "plan.h"]
 
 LIB = os.path.join(HERE, "libgems_b200.so")
 SYNTH = os.path.join(HERE, "libgems_synth.so")

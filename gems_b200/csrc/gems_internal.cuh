@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/gems_b200.h"
+#include "plan.h"
 
 namespace gems {
 
@@ -105,6 +106,7 @@ struct Session {
   int block = 0;
   int G = 1;
   int nops_max = 0;
+  int plan_depth = 0;    // stack positions the uploaded op list's plan uses
   size_t op_stride = 0;  // doubles per op in opmats
   cudaStream_t stream = nullptr;
   bool model_set = false;
@@ -120,7 +122,8 @@ struct Session {
   double *d_theta = nullptr, *d_scale_all = nullptr, *d_pattern_lh = nullptr, *d_df_frac = nullptr;
   double *d_ddf_term = nullptr;
   // bootstrap reweightings (RELL): R rows of P pattern counts
-  float *d_rell_w = nullptr;
+  float *d_rell_w = nullptr;       // [R][P] counts, then the partial-sum scratch
+  double *d_rell_part = nullptr;
   int rell_R = 0;
   size_t rell_ld = 0;
   double *d_model = nullptr;  // eval | evec | inv_evec | rates | props | tip | tip_real
@@ -244,6 +247,8 @@ int launch_traverse_g61(Session *s, int nops, int p0, int p1);
 // the grid barrier's time-out path, run on purpose (kernels_fp64.cu)
 int check_barrier_timeout(int device, int *status);
 // bootstrap reweighting (kernels_rell.cu)
+// scratch of the tiled reductions (per replicate row and pattern chunk), in doubles
+size_t rell_scratch_doubles(int R, int P);
 int launch_rell_lnl(Session *s, double *d_out);
 int launch_rell_derv(Session *s, double *d_out);
 

@@ -543,8 +543,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           float4 l;
           split4(v, h[i], l);
           const int idx = (cc * 5 + i) * kTile + row;
-          reinterpret_cast<float4 *>(dtile)[idx] = join4(h[i], l);
-          if (nxt_fwd >= 0) reinterpret_cast<float4 *>(fl)[idx] = l;
+          const float4 stored = join4(h[i], l);
+          reinterpret_cast<float4 *>(dtile)[idx] = stored;
+          if (nxt_fwd >= 0) {
+            // forward the split of the stored value, which is what a copy of this row splits
+            // into: when lo rounded to exactly half a TF32 ulp of hi, that split moves the ulp
+            // from lo to hi (same sum, other products)
+            split4(stored, h[i], l);
+            reinterpret_cast<float4 *>(fl)[idx] = l;
+          }
         }
         if (nxt_fwd >= 0)
           tmem_st_row(tmem + lane_off + (uint32_t)(kAhiCol + (nxt_fwd * 4 + cc) * kKP), h);

@@ -17,6 +17,7 @@
 //
 // Mixed form (FP32 real space): the transition matrices P_c(t) are op-dependent; they are
 // stored [x][c][y], so lane c reads its row x of P_c as contiguous float4s.
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <map>
@@ -593,6 +594,279 @@ __global__ void __launch_bounds__(kThreads, B)
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// 4 states with the traversal plan (plan.h): a child produced earlier in the same launch comes
+// from registers (forwarded: its consumer is the next op) or from a per-thread stack in shared
+// memory, not from a dependent global load; every output is still stored to its slot, with a
+// streaming store.  DRAM then carries what a traversal must move: the partial writes, the tip
+// bytes, children computed before the launch.  Same arithmetic in the same order as
+// msg_mix4 / k_traverse_mix4 (R = float) and msg_f64_4 / k_traverse_f64x (R = double), so the
+// values are bit-identical to theirs.  Shared memory: depth positions x PP patterns x
+// kThreads threads of 4 values (FP32 as one float4, FP64 as two double2 planes) and a uint16
+// scale counter.
+// ---------------------------------------------------------------------------------------
+template <typename R, int PP>
+struct Stack4 {
+  unsigned char *base;
+  int depth;
+  static constexpr size_t kVal = 4 * sizeof(R);  // bytes of one thread's entry
+  __device__ __forceinline__ size_t vidx(int pos, int u) const {
+    return ((size_t)pos * PP + u) * kThreads + threadIdx.x;
+  }
+  __device__ __forceinline__ void put(int pos, int u, const R (&v)[4], int sc) const {
+    if constexpr (sizeof(R) == 4) {
+      reinterpret_cast<float4 *>(base)[vidx(pos, u)] = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+      double2 *d = reinterpret_cast<double2 *>(base);
+      const size_t plane = (size_t)depth * PP * kThreads;
+      d[vidx(pos, u)] = make_double2(v[0], v[1]);
+      d[plane + vidx(pos, u)] = make_double2(v[2], v[3]);
+    }
+    scales()[vidx(pos, u)] = (uint16_t)sc;
+  }
+  __device__ __forceinline__ void get(int pos, int u, R (&v)[4], int &sc) const {
+    if constexpr (sizeof(R) == 4) {
+      const float4 t = reinterpret_cast<const float4 *>(base)[vidx(pos, u)];
+      v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+    } else {
+      const double2 *d = reinterpret_cast<const double2 *>(base);
+      const size_t plane = (size_t)depth * PP * kThreads;
+      const double2 a = d[vidx(pos, u)], b = d[plane + vidx(pos, u)];
+      v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+    }
+    sc = scales()[vidx(pos, u)];
+  }
+  __device__ __forceinline__ uint16_t *scales() const {
+    return reinterpret_cast<uint16_t *>(base + (size_t)depth * PP * kThreads * kVal);
+  }
+  static size_t bytes(int depth) { return (size_t)depth * PP * kThreads * (kVal + 2); }
+};
+
+// one child's message: L from the plan's source, then the op's transition applied
+template <typename R, bool SAFE, int PP>
+__device__ __forceinline__ void msg4s(const DevCtx &c, const EigPack<4> &E, int kind, int id,
+                                      int src, int pos, const Stack4<R, PP> &stk,
+                                      const R (&fwd)[PP][4], const int (&fwd_s)[PP],
+                                      const R *__restrict__ tabk, int side, const long (&p)[PP],
+                                      int gq, R (&v)[PP][4], int (&s)[PP]) {
+  const int C = c.C;
+  if constexpr (sizeof(R) == 4) {
+    const size_t nnC = (size_t)16 * C;
+    const float *Pm = tabk + side * nnC;
+    const float *leaf = tabk + 2 * nnC + (size_t)side * (c.unknown + 1) * c.block;
+    if (kind == GEMS_CHILD_TIP) {
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+        const int st = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
+        const float *lt = leaf + (size_t)st * c.block + gq;
+#pragma unroll
+        for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
+        s[u] = 0;
+      }
+      return;
+    }
+    float L[PP][4];
+    if (src == kSrcFwd) {
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+#pragma unroll
+        for (int x = 0; x < 4; x++) L[u][x] = fwd[u][x];
+        s[u] = fwd_s[u];
+      }
+    } else if (src == kSrcStack) {
+#pragma unroll
+      for (int u = 0; u < PP; u++) stk.get(min(pos, stk.depth - 1), u, L[u], s[u]);
+    } else {
+      const float *base = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems;
+      const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+        const float4 t = __ldcg(reinterpret_cast<const float4 *>(base + mix_off<4>(c, p[u], gq)));
+        L[u][0] = t.x, L[u][1] = t.y, L[u][2] = t.z, L[u][3] = t.w;
+      }
+#pragma unroll
+      for (int u = 0; u < PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const float4 r = __ldg(reinterpret_cast<const float4 *>(Pm + ((size_t)x * C + gq) * 4));
+#pragma unroll
+      for (int u = 0; u < PP; u++)
+        v[u][x] = fmaf(r.w, L[u][3], fmaf(r.z, L[u][2], fmaf(r.y, L[u][1], fmaf(r.x, L[u][0], 0.f))));
+    }
+  } else {
+    const int blk = c.block;
+    const double *d = tabk + side * blk;
+    const double *leaf = tabk + 2 * blk + (size_t)side * (c.unknown + 1) * blk;
+    if (kind == GEMS_CHILD_TIP) {
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+        const int st = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
+        const double *lt = leaf + (size_t)st * blk + gq;
+#pragma unroll
+        for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
+        s[u] = 0;
+      }
+      return;
+    }
+    double L[PP][4];
+    if (src == kSrcFwd) {
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+#pragma unroll
+        for (int x = 0; x < 4; x++) L[u][x] = fwd[u][x];
+        s[u] = fwd_s[u];
+      }
+    } else if (src == kSrcStack) {
+#pragma unroll
+      for (int u = 0; u < PP; u++) stk.get(min(pos, stk.depth - 1), u, L[u], s[u]);
+    } else {
+      const double *base = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
+      const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+        const double2 *s2 = reinterpret_cast<const double2 *>(base + (size_t)p[u] * blk + gq * 4);
+        const double2 a = __ldcg(s2), b = __ldcg(s2 + 1);
+        L[u][0] = a.x, L[u][1] = a.y, L[u][2] = b.x, L[u][3] = b.y;
+      }
+#pragma unroll
+      for (int u = 0; u < PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const double di = __ldg(d + i * C + gq);
+#pragma unroll
+      for (int u = 0; u < PP; u++) L[u][i] *= di;
+    }
+#pragma unroll
+    for (int u = 0; u < PP; u++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc = fma(E.evec[x * 4 + i], L[u][i], acc);
+        v[u][x] = acc;
+      }
+  }
+}
+
+template <typename R, bool SAFE, int PP, int B>
+__global__ void __launch_bounds__(kThreads, B)
+    k_traverse4s(DevCtx c, const DevOp *__restrict__ ops, int nops, const R *__restrict__ tab,
+                 size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
+  extern __shared__ __align__(16) unsigned char stk_raw[];
+  const int G = c.G, C = c.C;
+  const int gl = threadIdx.x & (G - 1);
+  const int gq = gl < C ? gl : 0;  // loads of idle lanes stay inside the tables
+  const int per = kThreads / G;
+  const long pb = p0 + (long)blockIdx.x * per * PP + threadIdx.x / G;
+  long p[PP];
+  bool act[PP];
+#pragma unroll
+  for (int u = 0; u < PP; u++) {
+    const long q = pb + (long)u * per;
+    act[u] = q < p1 && gl < C;
+    p[u] = q < p1 ? q : p0;
+  }
+  const Stack4<R, PP> stk{stk_raw, depth};
+  R fwd[PP][4];
+  int fwd_s[PP];
+#pragma unroll
+  for (int u = 0; u < PP; u++) {
+    fwd_s[u] = 0;
+#pragma unroll
+    for (int x = 0; x < 4; x++) fwd[u][x] = R(0);
+  }
+  R *part = static_cast<R *>(c.partials);
+  __shared__ int4 s_ops[kOpChunk];
+  for (int k = 0; k < nops; k++) {
+    if ((k & (kOpChunk - 1)) == 0) {
+      const int nk = min(kOpChunk, nops - k);
+      __syncthreads();  // the previous chunk is no longer read
+      for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+        const DevOp o = ops[k + i];
+        s_ops[i] = make_int4(o.dst_slot, o.l_id, o.r_id, o.pad_);
+      }
+      __syncthreads();
+    }
+    const int4 od = s_ops[k & (kOpChunk - 1)];
+    const int w = od.w;
+    const R *tk = tab + (size_t)k * stride;
+    const int lkind = plan_lkind(w), rkind = plan_rkind(w);
+    const bool tiptip = lkind == GEMS_CHILD_TIP && rkind == GEMS_CHILD_TIP;
+    R vl[PP][4], vr[PP][4];
+    int sl[PP], sr[PP];
+    msg4s<R, SAFE, PP>(c, E, lkind, od.y, plan_lsrc(w), plan_lpos(w), stk, fwd, fwd_s, tk, 0, p,
+                       gq, vl, sl);
+    msg4s<R, SAFE, PP>(c, E, rkind, od.z, plan_rsrc(w), plan_rpos(w), stk, fwd, fwd_s, tk, 1, p,
+                       gq, vr, sr);
+    const int outk = plan_out(w), opos = min(plan_opos(w), max(depth - 1, 0));
+#pragma unroll
+    for (int u = 0; u < PP; u++) {
+      R out[4];
+      R lh_max = R(0);
+      if constexpr (sizeof(R) == 4) {
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+          out[x] = vl[u][x] * vr[u][x];
+          lh_max = fmaxf(lh_max, out[x]);
+        }
+      } else {
+        double tmp[4];
+#pragma unroll
+        for (int x = 0; x < 4; x++) tmp[x] = vl[u][x] * vr[u][x];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          double acc = 0.0;
+#pragma unroll
+          for (int x = 0; x < 4; x++) acc = fma(E.inv[j * 4 + x], tmp[x], acc);
+          out[j] = acc;
+          lh_max = fmax(lh_max, fabs(acc));
+        }
+      }
+      if (!act[u]) lh_max = R(0);
+      if constexpr (!SAFE) {
+        if constexpr (sizeof(R) == 4) lh_max = group_maxf(lh_max, G);
+        else lh_max = group_max(lh_max, G);
+      }
+      int s_out = sl[u] + sr[u];
+      bool thr;
+      if constexpr (sizeof(R) == 4) thr = lh_max < kScaleThrF;
+      else thr = lh_max < kScaleThr;
+      if (act[u] && !tiptip && thr && c.invar[p[u]] == 0.0) {
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+          if constexpr (sizeof(R) == 4) out[x] *= 18446744073709551616.0f;  // 2^64
+          else out[x] = ldexp(out[x], kScaleExp);
+        }
+        s_out += 1;
+      }
+      if (act[u]) {
+        if constexpr (sizeof(R) == 4) {
+          __stcs(reinterpret_cast<float4 *>(part + (size_t)od.x * c.slot_elems +
+                                            mix_off<4>(c, p[u], gl)),
+                 make_float4(out[0], out[1], out[2], out[3]));
+        } else {
+          double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)od.x * c.slot_elems +
+                                                    (size_t)p[u] * c.block + gl * 4);
+          __stcs(d2, make_double2(out[0], out[1]));
+          __stcs(d2 + 1, make_double2(out[2], out[3]));
+        }
+        uint16_t *sc = c.scale + (size_t)od.x * c.slot_scale;
+        if (SAFE)
+          sc[(size_t)p[u] * C + gl] = (uint16_t)s_out;
+        else if (gl == 0)
+          sc[p[u]] = (uint16_t)s_out;
+      }
+      if (outk == kSrcStack) stk.put(opos, u, out, s_out);
+#pragma unroll
+      for (int x = 0; x < 4; x++) fwd[u][x] = out[x];
+      fwd_s[u] = s_out;
+    }
+    __syncwarp();
+  }
+}
+
 inline int grid_for(const Session *s, int p0, int p1) {
   const long threads = (long)(p1 - p0) * s->G;
   return (int)((threads + kThreads - 1) / kThreads);
@@ -609,20 +883,32 @@ inline int grid_for(const Session *s, int p0, int p1) {
 struct Variant4 {
   int pp, blocks;
   const void *fn[2];  // [safe]
+  bool stack;         // plan-driven kernel (k_traverse4s): takes the plan depth, dynamic smem
+  size_t (*smem)(int depth);
 };
 template <int PP, int B>
 Variant4 mix_variant() {
-  return {PP, B, {(const void *)k_traverse_mix4<false, PP, B>, (const void *)k_traverse_mix4<true, PP, B>}};
+  return {PP, B, {(const void *)k_traverse_mix4<false, PP, B>, (const void *)k_traverse_mix4<true, PP, B>},
+          false, nullptr};
 }
 template <int PP, int B>
 Variant4 f64_variant() {
-  return {PP, B, {(const void *)k_traverse_f64x<false, PP, B>, (const void *)k_traverse_f64x<true, PP, B>}};
+  return {PP, B, {(const void *)k_traverse_f64x<false, PP, B>, (const void *)k_traverse_f64x<true, PP, B>},
+          false, nullptr};
+}
+template <typename R, int PP, int B>
+Variant4 stack_variant() {
+  return {PP, B,
+          {(const void *)k_traverse4s<R, false, PP, B>, (const void *)k_traverse4s<R, true, PP, B>},
+          true, &Stack4<R, PP>::bytes};
 }
 const Variant4 *variants4(bool mixed, int *n) {
-  static const Variant4 mix[] = {mix_variant<2, 5>(), mix_variant<2, 6>(), mix_variant<4, 3>(),
-                                 mix_variant<1, 8>()};
-  static const Variant4 f64[] = {f64_variant<2, 4>(), f64_variant<3, 3>(), f64_variant<1, 6>()};
-  *n = mixed ? 4 : 3;
+  static const Variant4 mix[] = {stack_variant<float, 2, 4>(), stack_variant<float, 1, 6>(),
+                                 stack_variant<float, 4, 2>(), mix_variant<2, 5>(),
+                                 mix_variant<2, 6>(), mix_variant<4, 3>(), mix_variant<1, 8>()};
+  static const Variant4 f64[] = {stack_variant<double, 1, 4>(), stack_variant<double, 2, 3>(),
+                                 f64_variant<2, 4>(), f64_variant<3, 3>(), f64_variant<1, 6>()};
+  *n = mixed ? 7 : 5;
   return mixed ? mix : f64;
 }
 constexpr long long kTuneMinWork = 1ll << 22;  // patterns x ops below which no tuning is done
@@ -641,16 +927,36 @@ int tuned4(const Session *s, bool mixed) {
   return it == g_tune.end() ? -1 : it->second;
 }
 
+constexpr size_t kMaxDynSmem = 227 * 1024;
+
 int launch4(Session *s, bool mixed, int v, int nops, int p0, int p1, const EigPack<4> *E) {
   int nv = 0;
-  const Variant4 &var = variants4(mixed, &nv)[v];
+  const Variant4 *all = variants4(mixed, &nv);
+  if (all[v].stack && all[v].smem(s->plan_depth) > kMaxDynSmem) {
+    // a plan deeper than this variant's shared memory holds: the first variant without a stack
+    v = 0;
+    while (v < nv && all[v].stack) v++;
+  }
+  const Variant4 &var = all[v];
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   const long per = (long)(kThreads / s->G) * var.pp;
   const int grid = (int)((p1 - p0 + per - 1) / per);
   DevCtx c = s->ctx();
   const DevOp *ops = s->d_ops;
   size_t stride = s->op_stride;
-  if (mixed) {
+  if (var.stack) {
+    int depth = s->plan_depth;
+    const size_t smem = var.smem(depth);
+    // the limit is a per-kernel attribute shared by every thread of the process: always set to
+    // the largest size a plan may need
+    GEMS_CUDA(cudaFuncSetAttribute(var.fn[safe], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)std::min(var.smem(kPlanMaxPos), kMaxDynSmem)));
+    EigPack<4> e{};
+    if (E) e = *E;
+    void *args[] = {&c, &ops, &nops, mixed ? (void *)&s->d_opmats : (void *)&s->d_opmats,
+                    &stride, &e, &p0, &p1, &depth};
+    GEMS_CUDA(cudaLaunchKernel(var.fn[safe], dim3(grid), dim3(kThreads), args, smem, s->stream));
+  } else if (mixed) {
     const float *tab = reinterpret_cast<const float *>(s->d_opmats);
     void *args[] = {&c, &ops, &nops, &tab, &stride, &p0, &p1};
     GEMS_CUDA(cudaLaunchKernel(var.fn[safe], dim3(grid), dim3(kThreads), args, 0, s->stream));

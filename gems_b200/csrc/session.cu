@@ -233,7 +233,7 @@ static int upload_ops(Session *s, const gems_op *ops, int nops) {
   }
   // host staging: wait for any kernel still reading the previous op table
   GEMS_CUDA(cudaStreamSynchronize(s->stream));
-  std::memcpy(s->h_ops, ops, sizeof(gems_op) * nops);
+  s->plan_depth = plan_ops(ops, nops, s->desc.nslots, reinterpret_cast<gems_op *>(s->h_ops));
   GEMS_CUDA(cudaMemcpyAsync(s->d_ops, s->h_ops, sizeof(DevOp) * nops, cudaMemcpyHostToDevice,
                             s->stream));
   return GEMS_OK;
@@ -1006,18 +1006,24 @@ int gems_upload_reweightings(gems_session *s, const float *weights, int R) {
   if (s->d_rell_w && s->rell_R != R) {
     cudaFree(s->d_rell_w);
     s->d_rell_w = nullptr;
+    s->d_rell_part = nullptr;
     s->rell_R = 0;
   }
   const size_t ld = (size_t)s->P;
   if (!s->d_rell_w) {
+    // the counts (rows of P floats, P a multiple of 64: every row 256-byte aligned), then the
+    // scratch of the tiled reductions
+    const size_t wbytes = (size_t)R * ld * sizeof(float);
+    const size_t bytes = wbytes + rell_scratch_doubles(R, s->P) * sizeof(double);
     size_t free_b = 0, total_b = 0;
     GEMS_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    if ((size_t)R * ld * sizeof(float) > free_b) {
+    if (bytes > free_b) {
       set_error("reweightings exceed free device memory");
       return GEMS_ERR_ADMISSION;
     }
-    GEMS_CUDA(cudaMalloc((void **)&s->d_rell_w, (size_t)R * ld * sizeof(float)));
-    GEMS_CUDA(cudaMemsetAsync(s->d_rell_w, 0, (size_t)R * ld * sizeof(float), s->stream));
+    GEMS_CUDA(cudaMalloc((void **)&s->d_rell_w, bytes));
+    GEMS_CUDA(cudaMemsetAsync(s->d_rell_w, 0, wbytes, s->stream));
+    s->d_rell_part = reinterpret_cast<double *>(reinterpret_cast<char *>(s->d_rell_w) + wbytes);
   }
   s->rell_R = R;
   s->rell_ld = ld;

@@ -29,16 +29,19 @@ def computed_partials(gt, tree):
     return out
 
 
-@pytest.mark.parametrize("precision,nshapes", [("fp64", 3), ("mixed", 4)])
-def test_every_shape_gives_the_same_values(gpu, precision, nshapes):
+# shapes: the plan-driven stack kernels first (FP64: 2, mixed: 3), then the kernels that read
+# every child from global memory
+@pytest.mark.parametrize("scaling", ["norm", "safe"])
+@pytest.mark.parametrize("precision,nshapes", [("fp64", 5), ("mixed", 7)])
+def test_every_shape_gives_the_same_values(gpu, precision, nshapes, scaling):
     tree, model, aln = case(11, 40, 5001)
     ref = None
     seen = set()
     for k in range(nshapes):
-        gt = PhyloTree.from_case(tree, model, aln, precision=precision)
+        gt = PhyloTree.from_case(tree, model, aln, precision=precision, scaling=scaling)
         gt.session.set_autotune(force_shape=k)
         lnl, plh = gt.computeLikelihood(pattern_lh=True)
-        part = computed_partials(gt, tree) if precision == "fp64" else None
+        part = computed_partials(gt, tree)
         pp, blocks, _ = gt.session.traversal_shape()
         seen.add((pp, blocks))
         if ref is None:
