@@ -867,6 +867,429 @@ __global__ void __launch_bounds__(kThreads, B)
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// 4 states, one thread per pattern (all C categories in registers), with the traversal plan.
+// Every per-op input a thread needs sits in shared memory before the op starts: the op
+// descriptors, the op tables and the tip bytes of the CTA's 128 patterns are copied with
+// cp.async one chunk of kChunkP ops ahead (double-buffered), and children produced in the
+// launch come from registers (forwarded) or the per-thread stack.  Per op a warp then does
+// shared-memory reads, FMAs and one coalesced 32 x (C*4 values) store: no load on its critical
+// path.  Mixed form: the tip messages are taken from the staged P_c(t) (a tip's value for
+// state set S is the sum of the P columns in S, added in state order as the table of
+// k_prep_ops_mix forms it, so the bits are the same).  FP64 form: the staged tables hold the
+// exp factors and the leaf rows of the four bases and of the unknown state; ambiguity codes
+// read their row from global memory.  Values are bit-identical to k_traverse_mix4 /
+// k_traverse_f64x.
+// ---------------------------------------------------------------------------------------
+constexpr int kThreadsP = 128;  // patterns per CTA
+constexpr int kChunkP = 8;      // ops staged together
+
+template <typename R, int C>
+struct Tab4P {
+  static constexpr int kP = 2 * 16 * C;    // mixed: P_c(t) floats, [side][x][c][y]
+  static constexpr int kD = 2 * 4 * C;     // FP64: exp factors, [side][i][c]
+  static constexpr int kLeaf = 5 * 4 * C;  // FP64: leaf rows {A, C, G, T, unknown}, [5][x][c]
+  static constexpr int kBytes = sizeof(R) == 4 ? kP * 4 : (kD + 2 * kLeaf) * 8;
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+// 8-byte copy (the op descriptors are 40 bytes, 8-byte aligned)
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait1() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
+template <typename R, int C>
+struct StageP {
+  DevOp desc[2][kChunkP];
+  alignas(16) unsigned char tab[2][kChunkP][Tab4P<R, C>::kBytes];
+  alignas(16) uint8_t tips[2][kChunkP][2][kThreadsP];
+};
+// every 16-byte copy target inside StageP, and the stack placed after it, stay 16-byte aligned
+static_assert(Tab4P<float, 1>::kBytes % 16 == 0 && Tab4P<double, 1>::kBytes % 16 == 0 &&
+                  sizeof(StageP<float, 1>) % 16 == 0 && sizeof(StageP<double, 8>) % 16 == 0,
+              "16-byte pieces");
+
+// copies the descriptors, tables and tip bytes of ops [k0, k0 + nk) into buffer b (every thread
+// takes a share of the 16-byte pieces); tip bytes of a side are copied only for a tip child, and
+// only when the CTA's first pattern is 16-byte aligned (tips_async), else read directly
+template <typename R, int C>
+__device__ __forceinline__ void stage4p(StageP<R, C> &st, int b, const DevCtx &c,
+                                        const DevOp *__restrict__ ops, const R *__restrict__ tab,
+                                        size_t stride, int k0, int nk, long pbase,
+                                        bool tips_async) {
+  using T = Tab4P<R, C>;
+  const int tid = threadIdx.x;
+  // descriptors: sizeof(DevOp) / 8 pieces of 8 bytes each
+  constexpr int kDescPieces = sizeof(DevOp) / 8;
+  static_assert(sizeof(DevOp) % 8 == 0 && alignof(DevOp) >= 8, "8-byte pieces of a DevOp");
+  for (int q = tid; q < kDescPieces * nk; q += kThreadsP) {
+    const int i = q / kDescPieces, r = q - i * kDescPieces;
+    cp_async8(reinterpret_cast<char *>(&st.desc[b][i]) + 8 * r,
+              reinterpret_cast<const char *>(ops + k0 + i) + 8 * r);
+  }
+  constexpr int kPieces = T::kBytes / 16;
+  for (int q = tid; q < nk * kPieces; q += kThreadsP) {
+    const int i = q / kPieces, r = q - i * kPieces;
+    const R *tk = tab + (size_t)(k0 + i) * stride;
+    const char *src;
+    if constexpr (sizeof(R) == 4) {
+      src = reinterpret_cast<const char *>(tk) + 16 * r;
+    } else {
+      const int blk = 4 * C, u1 = c.unknown + 1;
+      const int off = 16 * r;  // byte offset inside the staged table
+      constexpr int dB = T::kD * 8, rowsB = 16 * C * 8, rowB = 4 * C * 8;
+      if (off < dB) {
+        src = reinterpret_cast<const char *>(tk) + off;
+      } else {
+        const int o = off - dB, side = o / (rowsB + rowB), w = o - side * (rowsB + rowB);
+        const double *leaf = tk + 2 * blk + (size_t)side * u1 * blk;
+        src = w < rowsB ? reinterpret_cast<const char *>(leaf) + w
+                        : reinterpret_cast<const char *>(leaf + (size_t)c.unknown * blk) + (w - rowsB);
+      }
+    }
+    cp_async16(st.tab[b][i] + 16 * r, src);
+  }
+  if (tips_async) {
+    // 8 pieces per tip side; pieces past the padded pattern count are not copied (never read)
+    for (int q = tid; q < nk * 2 * 8; q += kThreadsP) {
+      const int i = q >> 4, sd = (q >> 3) & 1, r = q & 7;
+      const DevOp &o = ops[k0 + i];
+      const int kind = sd ? o.r_kind : o.l_kind, id = sd ? o.r_id : o.l_id;
+      if (kind != GEMS_CHILD_TIP || pbase + 16 * r >= c.P) continue;
+      cp_async16(&st.tips[b][i][sd][16 * r], c.tips + (size_t)id * c.P + pbase + 16 * r);
+    }
+  }
+}
+
+// 16-byte moves of a thread's C x 4 values (FP32: one float4 per category; FP64: two double2)
+template <int C>
+__device__ __forceinline__ void ld_cg(const float *src, float (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < C; q++) {
+    const float4 t = __ldcg(reinterpret_cast<const float4 *>(src) + q);
+    v[q][0] = t.x, v[q][1] = t.y, v[q][2] = t.z, v[q][3] = t.w;
+  }
+}
+template <int C>
+__device__ __forceinline__ void ld_cg(const double *src, double (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < 2 * C; q++) {
+    const double2 t = __ldcg(reinterpret_cast<const double2 *>(src) + q);
+    v[q >> 1][2 * (q & 1)] = t.x, v[q >> 1][2 * (q & 1) + 1] = t.y;
+  }
+}
+template <int C>
+__device__ __forceinline__ void st_cs(float *dst, const float (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < C; q++)
+    __stcs(reinterpret_cast<float4 *>(dst) + q, make_float4(v[q][0], v[q][1], v[q][2], v[q][3]));
+}
+template <int C>
+__device__ __forceinline__ void st_cs(double *dst, const double (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < 2 * C; q++)
+    __stcs(reinterpret_cast<double2 *>(dst) + q,
+           make_double2(v[q >> 1][2 * (q & 1)], v[q >> 1][2 * (q & 1) + 1]));
+}
+// shared memory, [piece][thread] (a warp's accesses are 512 contiguous bytes)
+template <int C>
+__device__ __forceinline__ void sm_put(unsigned char *base, const float (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < C; q++)
+    reinterpret_cast<float4 *>(base)[q * kThreadsP + threadIdx.x] =
+        make_float4(v[q][0], v[q][1], v[q][2], v[q][3]);
+}
+template <int C>
+__device__ __forceinline__ void sm_put(unsigned char *base, const double (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < 2 * C; q++)
+    reinterpret_cast<double2 *>(base)[q * kThreadsP + threadIdx.x] =
+        make_double2(v[q >> 1][2 * (q & 1)], v[q >> 1][2 * (q & 1) + 1]);
+}
+template <int C>
+__device__ __forceinline__ void sm_get(const unsigned char *base, float (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < C; q++) {
+    const float4 t = reinterpret_cast<const float4 *>(base)[q * kThreadsP + threadIdx.x];
+    v[q][0] = t.x, v[q][1] = t.y, v[q][2] = t.z, v[q][3] = t.w;
+  }
+}
+template <int C>
+__device__ __forceinline__ void sm_get(const unsigned char *base, double (&v)[C][4]) {
+#pragma unroll
+  for (int q = 0; q < 2 * C; q++) {
+    const double2 t = reinterpret_cast<const double2 *>(base)[q * kThreadsP + threadIdx.x];
+    v[q >> 1][2 * (q & 1)] = t.x, v[q >> 1][2 * (q & 1) + 1] = t.y;
+  }
+}
+
+template <typename R, int C>
+struct StackP {
+  unsigned char *base;
+  int depth;
+  static constexpr int kEntry = 4 * C * (int)sizeof(R);  // value bytes of one thread's entry
+  __device__ __forceinline__ uint16_t *scs() const {
+    return reinterpret_cast<uint16_t *>(base + (size_t)depth * kEntry * kThreadsP);
+  }
+  static size_t bytes(int depth) { return (size_t)depth * kThreadsP * (kEntry + 2 * C); }
+  __device__ __forceinline__ void put(int pos, const R (&v)[C][4], const int (&sc)[C]) const {
+    sm_put<C>(base + (size_t)pos * kEntry * kThreadsP, v);
+#pragma unroll
+    for (int cc = 0; cc < C; cc++)
+      scs()[((size_t)pos * C + cc) * kThreadsP + threadIdx.x] = (uint16_t)sc[cc];
+  }
+  __device__ __forceinline__ void get(int pos, R (&v)[C][4], int (&sc)[C]) const {
+    sm_get<C>(base + (size_t)pos * kEntry * kThreadsP, v);
+#pragma unroll
+    for (int cc = 0; cc < C; cc++) sc[cc] = scs()[((size_t)pos * C + cc) * kThreadsP + threadIdx.x];
+  }
+};
+
+// one child's message for all categories: L from the plan's source, the op's transition applied
+template <typename R, bool SAFE, int C>
+__device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int kind, int id,
+                                      int src, int pos, const StackP<R, C> &stk,
+                                      const R (&fwd)[C][4], const int (&fwd_s)[C],
+                                      const unsigned char *__restrict__ tabS,
+                                      const R *__restrict__ tk, int side, int tipbyte, long p,
+                                      R (&v)[C][4], int (&s)[C]) {
+  using T = Tab4P<R, C>;
+  if (kind == GEMS_CHILD_TIP) {
+    const int st = min(tipbyte, c.unknown);
+#pragma unroll
+    for (int cc = 0; cc < C; cc++) s[cc] = 0;
+    if constexpr (sizeof(R) == 4) {
+      const int mask = st < 4 ? 1 << st : (st < 18 ? st - 3 : 15);
+      const float4 *P4 = reinterpret_cast<const float4 *>(tabS) + side * 4 * C;
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int cc = 0; cc < C; cc++) {
+          const float4 r = P4[x * C + cc];
+          float acc = 0.f;
+          if (mask & 1) acc = acc + r.x;
+          if (mask & 2) acc = acc + r.y;
+          if (mask & 4) acc = acc + r.z;
+          if (mask & 8) acc = acc + r.w;
+          v[cc][x] = acc;
+        }
+    } else {
+      const int blk = 4 * C;
+      const double *row;
+      if (st < 4 || st == c.unknown) {
+        row = reinterpret_cast<const double *>(tabS) + T::kD + side * T::kLeaf +
+              (st < 4 ? st : 4) * blk;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+          for (int cc = 0; cc < C; cc++) v[cc][x] = row[x * C + cc];
+      } else {
+        row = tk + 2 * blk + (size_t)side * (c.unknown + 1) * blk + (size_t)st * blk;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+          for (int cc = 0; cc < C; cc++) v[cc][x] = __ldg(row + x * C + cc);
+      }
+    }
+    return;
+  }
+  R L[C][4];
+  if (src == kSrcFwd) {
+#pragma unroll
+    for (int cc = 0; cc < C; cc++) {
+#pragma unroll
+      for (int x = 0; x < 4; x++) L[cc][x] = fwd[cc][x];
+      s[cc] = fwd_s[cc];
+    }
+  } else if (src == kSrcStack) {
+    stk.get(min(pos, stk.depth - 1), L, s);
+  } else {
+    ld_cg<C>(static_cast<const R *>(c.partials) + (size_t)id * c.slot_elems + (size_t)p * (4 * C),
+             L);
+    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+    if (SAFE) {
+#pragma unroll
+      for (int cc = 0; cc < C; cc++) s[cc] = sc[(size_t)p * C + cc];
+    } else {
+      const int v0 = sc[p];
+#pragma unroll
+      for (int cc = 0; cc < C; cc++) s[cc] = v0;
+    }
+  }
+  if constexpr (sizeof(R) == 4) {
+    const float4 *P4 = reinterpret_cast<const float4 *>(tabS) + side * 4 * C;
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+      for (int cc = 0; cc < C; cc++) {
+        const float4 r = P4[x * C + cc];
+        v[cc][x] = fmaf(r.w, L[cc][3], fmaf(r.z, L[cc][2], fmaf(r.y, L[cc][1], fmaf(r.x, L[cc][0], 0.f))));
+      }
+  } else {
+    const double *d = reinterpret_cast<const double *>(tabS) + side * 4 * C;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int cc = 0; cc < C; cc++) L[cc][i] *= d[i * C + cc];
+#pragma unroll
+    for (int cc = 0; cc < C; cc++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc = fma(E.evec[x * 4 + i], L[cc][i], acc);
+        v[cc][x] = acc;
+      }
+  }
+}
+
+template <typename R, bool SAFE, int C>
+__global__ void __launch_bounds__(kThreadsP)
+    k_traverse4p(DevCtx c, const DevOp *__restrict__ ops, int nops, const R *__restrict__ tab,
+                 size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
+  extern __shared__ __align__(16) unsigned char smem_p[];
+  StageP<R, C> &st = *reinterpret_cast<StageP<R, C> *>(smem_p);
+  const StackP<R, C> stk{smem_p + sizeof(StageP<R, C>), depth};
+  const long pbase = p0 + (long)blockIdx.x * kThreadsP;
+  const long pq = pbase + threadIdx.x;
+  const bool act = pq < p1;
+  const long p = act ? pq : p0;
+  const bool tips_async = (pbase & 15) == 0;
+  R fwd[C][4];
+  int fwd_s[C];
+#pragma unroll
+  for (int cc = 0; cc < C; cc++) {
+    fwd_s[cc] = 0;
+#pragma unroll
+    for (int x = 0; x < 4; x++) fwd[cc][x] = R(0);
+  }
+  R *part = static_cast<R *>(c.partials);
+  stage4p<R, C>(st, 0, c, ops, tab, stride, 0, min(kChunkP, nops), pbase, tips_async);
+  cp_async_commit();
+  for (int k0 = 0; k0 < nops; k0 += kChunkP) {
+    const int b = (k0 / kChunkP) & 1, nk = min(kChunkP, nops - k0);
+    if (k0 + kChunkP < nops)
+      stage4p<R, C>(st, b ^ 1, c, ops, tab, stride, k0 + kChunkP,
+                    min(kChunkP, nops - k0 - kChunkP), pbase, tips_async);
+    cp_async_commit();
+    cp_async_wait1();  // this chunk's copies are done (the next chunk's may still fly)
+    __syncthreads();
+    for (int i = 0; i < nk; i++) {
+      const DevOp &o = st.desc[b][i];
+      const int w = o.pad_;
+      const int lkind = plan_lkind(w), rkind = plan_rkind(w);
+      const bool tiptip = lkind == GEMS_CHILD_TIP && rkind == GEMS_CHILD_TIP;
+      const R *tk = tab + (size_t)(k0 + i) * stride;
+      int tb[2] = {0, 0};
+      if (lkind == GEMS_CHILD_TIP)
+        tb[0] = tips_async ? st.tips[b][i][0][threadIdx.x] : c.tips[(size_t)o.l_id * c.P + p];
+      if (rkind == GEMS_CHILD_TIP)
+        tb[1] = tips_async ? st.tips[b][i][1][threadIdx.x] : c.tips[(size_t)o.r_id * c.P + p];
+      R vl[C][4], vr[C][4];
+      int sl[C], sr[C];
+      msg4p<R, SAFE, C>(c, E, lkind, o.l_id, plan_lsrc(w), plan_lpos(w), stk, fwd, fwd_s,
+                        st.tab[b][i], tk, 0, tb[0], p, vl, sl);
+      msg4p<R, SAFE, C>(c, E, rkind, o.r_id, plan_rsrc(w), plan_rpos(w), stk, fwd, fwd_s,
+                        st.tab[b][i], tk, 1, tb[1], p, vr, sr);
+      R out[C][4];
+      R mx[C];
+#pragma unroll
+      for (int cc = 0; cc < C; cc++) {
+        mx[cc] = R(0);
+        if constexpr (sizeof(R) == 4) {
+#pragma unroll
+          for (int x = 0; x < 4; x++) {
+            out[cc][x] = vl[cc][x] * vr[cc][x];
+            mx[cc] = fmaxf(mx[cc], out[cc][x]);
+          }
+        } else {
+          double tmp[4];
+#pragma unroll
+          for (int x = 0; x < 4; x++) tmp[x] = vl[cc][x] * vr[cc][x];
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            double acc = 0.0;
+#pragma unroll
+            for (int x = 0; x < 4; x++) acc = fma(E.inv[j * 4 + x], tmp[x], acc);
+            out[cc][j] = acc;
+            mx[cc] = fmax(mx[cc], fabs(acc));
+          }
+        }
+      }
+      int so[C];
+      if constexpr (SAFE) {
+#pragma unroll
+        for (int cc = 0; cc < C; cc++) {
+          so[cc] = sl[cc] + sr[cc];
+          bool thr;
+          if constexpr (sizeof(R) == 4) thr = mx[cc] < kScaleThrF;
+          else thr = mx[cc] < kScaleThr;
+          if (!tiptip && thr && c.invar[p] == 0.0) {
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+              if constexpr (sizeof(R) == 4) out[cc][x] *= 18446744073709551616.0f;  // 2^64
+              else out[cc][x] = ldexp(out[cc][x], kScaleExp);
+            }
+            so[cc] += 1;
+          }
+        }
+      } else {
+        R m = mx[0];
+#pragma unroll
+        for (int cc = 1; cc < C; cc++) m = sizeof(R) == 4 ? fmaxf(m, mx[cc]) : fmax(m, mx[cc]);
+        int s0 = sl[0] + sr[0];
+        bool thr;
+        if constexpr (sizeof(R) == 4) thr = m < kScaleThrF;
+        else thr = m < kScaleThr;
+        if (!tiptip && thr && c.invar[p] == 0.0) {
+#pragma unroll
+          for (int cc = 0; cc < C; cc++)
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+              if constexpr (sizeof(R) == 4) out[cc][x] *= 18446744073709551616.0f;  // 2^64
+              else out[cc][x] = ldexp(out[cc][x], kScaleExp);
+            }
+          s0 += 1;
+        }
+#pragma unroll
+        for (int cc = 0; cc < C; cc++) so[cc] = s0;
+      }
+      if (act) {
+        st_cs<C>(part + (size_t)o.dst_slot * c.slot_elems + (size_t)p * (4 * C), out);
+        uint16_t *sc = c.scale + (size_t)o.dst_slot * c.slot_scale;
+        if (SAFE) {
+#pragma unroll
+          for (int cc = 0; cc < C; cc++) sc[(size_t)p * C + cc] = (uint16_t)so[cc];
+        } else {
+          sc[p] = (uint16_t)so[0];
+        }
+      }
+      if (plan_out(w) == kSrcStack) stk.put(min(plan_opos(w), max(depth - 1, 0)), out, so);
+#pragma unroll
+      for (int cc = 0; cc < C; cc++) {
+#pragma unroll
+        for (int x = 0; x < 4; x++) fwd[cc][x] = out[cc][x];
+        fwd_s[cc] = so[cc];
+      }
+    }
+    __syncthreads();  // buffer b is refilled two chunks on
+  }
+}
+
 inline int grid_for(const Session *s, int p0, int p1) {
   const long threads = (long)(p1 - p0) * s->G;
   return (int)((threads + kThreads - 1) / kThreads);
@@ -883,8 +1306,12 @@ inline int grid_for(const Session *s, int p0, int p1) {
 struct Variant4 {
   int pp, blocks;
   const void *fn[2];  // [safe]
-  bool stack;         // plan-driven kernel (k_traverse4s): takes the plan depth, dynamic smem
+  bool stack;         // plan-driven kernel: takes the plan depth, dynamic smem
   size_t (*smem)(int depth);
+  // one thread per pattern (k_traverse4p): kernels and shared memory by category count
+  bool per_pattern = false;
+  const void *fnC[2][4] = {};       // [safe][C = 1, 2, 4, 8]
+  size_t (*smemC[4])(int depth) = {};
 };
 template <int PP, int B>
 Variant4 mix_variant() {
@@ -902,13 +1329,36 @@ Variant4 stack_variant() {
           {(const void *)k_traverse4s<R, false, PP, B>, (const void *)k_traverse4s<R, true, PP, B>},
           true, &Stack4<R, PP>::bytes};
 }
+template <typename R, int C>
+size_t smem4p(int depth) {
+  return sizeof(StageP<R, C>) + StackP<R, C>::bytes(depth);
+}
+template <typename R>
+Variant4 pattern_variant() {
+  Variant4 v{1, 0, {nullptr, nullptr}, true, nullptr};
+  v.per_pattern = true;
+  const void *f[2][4] = {{(const void *)k_traverse4p<R, false, 1>, (const void *)k_traverse4p<R, false, 2>,
+                          (const void *)k_traverse4p<R, false, 4>, (const void *)k_traverse4p<R, false, 8>},
+                         {(const void *)k_traverse4p<R, true, 1>, (const void *)k_traverse4p<R, true, 2>,
+                          (const void *)k_traverse4p<R, true, 4>, (const void *)k_traverse4p<R, true, 8>}};
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 4; b++) v.fnC[a][b] = f[a][b];
+  v.smemC[0] = &smem4p<R, 1>;
+  v.smemC[1] = &smem4p<R, 2>;
+  v.smemC[2] = &smem4p<R, 4>;
+  v.smemC[3] = &smem4p<R, 8>;
+  return v;
+}
+int cat_index(int C) { return C == 1 ? 0 : C == 2 ? 1 : C == 4 ? 2 : C == 8 ? 3 : -1; }
 const Variant4 *variants4(bool mixed, int *n) {
-  static const Variant4 mix[] = {stack_variant<float, 2, 4>(), stack_variant<float, 1, 6>(),
-                                 stack_variant<float, 4, 2>(), mix_variant<2, 5>(),
-                                 mix_variant<2, 6>(), mix_variant<4, 3>(), mix_variant<1, 8>()};
-  static const Variant4 f64[] = {stack_variant<double, 1, 4>(), stack_variant<double, 2, 3>(),
-                                 f64_variant<2, 4>(), f64_variant<3, 3>(), f64_variant<1, 6>()};
-  *n = mixed ? 7 : 5;
+  static const Variant4 mix[] = {pattern_variant<float>(),      stack_variant<float, 2, 4>(),
+                                 stack_variant<float, 1, 6>(),  stack_variant<float, 4, 2>(),
+                                 mix_variant<2, 5>(),           mix_variant<2, 6>(),
+                                 mix_variant<4, 3>(),           mix_variant<1, 8>()};
+  static const Variant4 f64[] = {pattern_variant<double>(),     stack_variant<double, 1, 4>(),
+                                 stack_variant<double, 2, 3>(), f64_variant<2, 4>(),
+                                 f64_variant<3, 3>(),           f64_variant<1, 6>()};
+  *n = mixed ? 8 : 6;
   return mixed ? mix : f64;
 }
 constexpr long long kTuneMinWork = 1ll << 22;  // patterns x ops below which no tuning is done
@@ -927,44 +1377,71 @@ int tuned4(const Session *s, bool mixed) {
   return it == g_tune.end() ? -1 : it->second;
 }
 
-constexpr size_t kMaxDynSmem = 227 * 1024;
+// dynamic shared memory a kernel may take on this device: the opt-in maximum per block less
+// the kernel's static shared memory
+size_t max_dyn_smem(const void *fn, int device) {
+  int optin = 0;
+  cudaFuncAttributes fa{};
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) !=
+          cudaSuccess ||
+      cudaFuncGetAttributes(&fa, fn) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return optin > (int)fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+}
 
 int launch4(Session *s, bool mixed, int v, int nops, int p0, int p1, const EigPack<4> *E) {
   int nv = 0;
   const Variant4 *all = variants4(mixed, &nv);
-  if (all[v].stack && all[v].smem(s->plan_depth) > kMaxDynSmem) {
-    // a plan deeper than this variant's shared memory holds: the first variant without a stack
+  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  const int ci = cat_index(s->desc.ncat);
+  auto kernel = [&](const Variant4 &x) -> const void * {
+    return x.per_pattern ? (ci >= 0 ? x.fnC[safe][ci] : nullptr) : x.fn[safe];
+  };
+  auto smem_of = [&](const Variant4 &x, int depth) -> size_t {
+    return x.per_pattern ? x.smemC[ci](depth) : x.smem(depth);
+  };
+  // a variant that cannot run this session (categories without an instance, a plan deeper than
+  // its shared memory) hands over to the first variant that reads children from global memory
+  auto usable = [&](const Variant4 &x) {
+    if (!x.stack) return true;
+    const void *f = kernel(x);
+    return f && smem_of(x, s->plan_depth) <= max_dyn_smem(f, s->desc.device);
+  };
+  if (!usable(all[v])) {
     v = 0;
     while (v < nv && all[v].stack) v++;
   }
   const Variant4 &var = all[v];
-  const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
-  const long per = (long)(kThreads / s->G) * var.pp;
+  const void *fn = kernel(var);
+  const int threads = var.per_pattern ? kThreadsP : kThreads;
+  const long per = var.per_pattern ? kThreadsP : (long)(kThreads / s->G) * var.pp;
   const int grid = (int)((p1 - p0 + per - 1) / per);
   DevCtx c = s->ctx();
   const DevOp *ops = s->d_ops;
   size_t stride = s->op_stride;
   if (var.stack) {
     int depth = s->plan_depth;
-    const size_t smem = var.smem(depth);
+    const size_t smem = smem_of(var, depth);
     // the limit is a per-kernel attribute shared by every thread of the process: always set to
     // the largest size a plan may need
-    GEMS_CUDA(cudaFuncSetAttribute(var.fn[safe], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)std::min(var.smem(kPlanMaxPos), kMaxDynSmem)));
+    GEMS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)std::min(smem_of(var, kPlanMaxPos),
+                                                 max_dyn_smem(fn, s->desc.device))));
     EigPack<4> e{};
     if (E) e = *E;
-    void *args[] = {&c, &ops, &nops, mixed ? (void *)&s->d_opmats : (void *)&s->d_opmats,
-                    &stride, &e, &p0, &p1, &depth};
-    GEMS_CUDA(cudaLaunchKernel(var.fn[safe], dim3(grid), dim3(kThreads), args, smem, s->stream));
+    void *args[] = {&c, &ops, &nops, (void *)&s->d_opmats, &stride, &e, &p0, &p1, &depth};
+    GEMS_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, smem, s->stream));
   } else if (mixed) {
     const float *tab = reinterpret_cast<const float *>(s->d_opmats);
     void *args[] = {&c, &ops, &nops, &tab, &stride, &p0, &p1};
-    GEMS_CUDA(cudaLaunchKernel(var.fn[safe], dim3(grid), dim3(kThreads), args, 0, s->stream));
+    GEMS_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, 0, s->stream));
   } else {
     const double *tab = s->d_opmats;
     EigPack<4> e = *E;
     void *args[] = {&c, &ops, &nops, &tab, &stride, &e, &p0, &p1};
-    GEMS_CUDA(cudaLaunchKernel(var.fn[safe], dim3(grid), dim3(kThreads), args, 0, s->stream));
+    GEMS_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(threads), args, 0, s->stream));
   }
   s->launches++;
   return GEMS_OK;
@@ -1069,24 +1546,35 @@ int traverse_v2_wave_patterns(const Session *s) {
   const bool mixed = s->desc.precision == GEMS_PREC_MIXED;
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
   const bool four = s->desc.nstates == 4;
-  int pp = 1;
+  int per_block = kThreads / s->G, threads = kThreads;
+  size_t smem = 0;
   const void *fn = nullptr;
   if (four) {
     int nv = 0, v = shape4(s, mixed);
     const Variant4 &var = variants4(mixed, &nv)[v < 0 ? 0 : v];
-    fn = var.fn[safe];
-    pp = var.pp;
+    const int ci = cat_index(s->desc.ncat);
+    if (var.per_pattern && ci >= 0) {
+      fn = var.fnC[safe][ci];
+      smem = var.smemC[ci](s->plan_depth);
+      per_block = threads = kThreadsP;
+    } else if (!var.per_pattern) {
+      fn = var.fn[safe];
+      per_block *= var.pp;
+      if (var.stack) smem = var.smem(s->plan_depth);
+    } else {
+      return 0;
+    }
   } else {
     fn = mixed ? (safe ? (const void *)k_traverse_mix<20, true> : (const void *)k_traverse_mix<20, false>)
                : (safe ? (const void *)k_traverse_f64<20, true> : (const void *)k_traverse_f64<20, false>);
   }
   int nsm = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->desc.device) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0) != cudaSuccess) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  return per_sm * nsm * (kThreads / s->G) * pp;
+  return per_sm * nsm * per_block;
 }
 
 int traverse_v2_shape(const Session *s, int *patterns_per_group, int *blocks_per_sm) {
@@ -1098,6 +1586,17 @@ int traverse_v2_shape(const Session *s, int *patterns_per_group, int *blocks_per
   const Variant4 &var = variants4(mixed, &nv)[v < 0 ? 0 : v];
   *patterns_per_group = var.pp;
   *blocks_per_sm = var.blocks;
+  const int ci = cat_index(s->desc.ncat);
+  if (var.per_pattern && ci >= 0) {
+    // one thread per pattern: the resident blocks follow from the plan's shared memory
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, var.fnC[s->desc.scaling == GEMS_SCALE_SAFE][ci], kThreadsP,
+            var.smemC[ci](s->plan_depth)) == cudaSuccess)
+      *blocks_per_sm = per_sm;
+    else
+      cudaGetLastError();
+  }
   return v < 0 ? 1 : GEMS_OK;
 }
 
