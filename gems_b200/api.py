@@ -144,6 +144,13 @@ class Ingest:
             pass
 
 
+def min_pool_slots(ntaxa):
+    """The fewest partial slots a tree may run in (LM_MEM_SAVE: log2(leafNum) + LH_MIN_CONST,
+    tree/phylotree.cpp:42,1026-1040)."""
+    import math
+    return int(math.log2(ntaxa)) + 1
+
+
 def full_traversal(tree):
     """Ops of a from-scratch traversal with one slot per internal node (slot = node - ntaxa),
     rooted at the branch between leaf 0 and its neighbour, and that branch: (ops, branch)."""
@@ -403,9 +410,15 @@ class PhyloTree:
     @classmethod
     def from_case(cls, tree, model, aln, precision="fp64", scaling="norm", device=0,
                   slots="node", invar=None):
-        """Session + tree for a synthetic case (synth.Tree, synth.Model, synth.Alignment)."""
+        """Session + tree for a synthetic case (synth.Tree, synth.Model, synth.Alignment).
+        slots: "node" (one partial per internal node, LM_PER_NODE), "branch" (one per directed
+        branch), "pool" (LM_MEM_SAVE at its floor, log2(ntaxa) + 1 slots) or a slot count."""
         nint = tree.ntaxa - 2
-        nslots = nint if slots == "node" else 3 * nint
+        if isinstance(slots, int):
+            nslots = slots
+        else:
+            nslots = {"node": nint, "branch": 3 * nint,
+                      "pool": min_pool_slots(tree.ntaxa)}[slots]
         s = Session(tree.ntaxa, aln.npat, model.nstates, model.ncat, nslots, precision,
                     scaling, device)
         s.upload_tips(aln.patterns)

@@ -363,8 +363,9 @@ __global__ void k_prep_ops_mix(DevCtx c, const DevOp *ops, float *tab, size_t st
   __syncthreads();
   float *leaf = tab + (size_t)k * stride_f + (size_t)2 * nnC + (size_t)side * (c.unknown + 1) * c.block;
   const int rows = (c.unknown + 1) * c.block;
+  // stored [s][c][x]: a category's message for state s is n contiguous floats
   for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
-    const int s = idx / c.block, r = idx - s * c.block, x = r / C, cc = r - x * C;
+    const int s = idx / c.block, r = idx - s * c.block, cc = r / n, x = r - cc * n;
     const double *ind = c.tip_real + (size_t)s * n;
     float acc = 0.f;
     for (int y = 0; y < n; y++) acc = fmaf(Pm[(x * C + cc) * n + y], (float)ind[y], acc);
@@ -380,9 +381,9 @@ __device__ __forceinline__ void msg_mix(const DevCtx &c, int kind, int id,
   const int C = c.C;
   if (kind == GEMS_CHILD_TIP) {
     const int st = min((int)c.tips[(size_t)id * c.P + p], c.unknown);
-    const float *lt = leaf + (size_t)st * c.block + gl;
+    const float *lt = leaf + (size_t)st * c.block + gl * N;
 #pragma unroll
-    for (int x = 0; x < N; x++) v[x] = __ldg(lt + x * C);
+    for (int x = 0; x < N; x++) v[x] = __ldg(lt + x);
     s = 0;
   } else {
     const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
@@ -510,9 +511,8 @@ __device__ __forceinline__ void msg_mix4(const DevCtx &c, int kind, int id,
     for (int u = 0; u < PP; u++) st[u] = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
 #pragma unroll
     for (int u = 0; u < PP; u++) {
-      const float *lt = leaf + (size_t)st[u] * c.block + gq;
-#pragma unroll
-      for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
+      const float4 t = __ldg(reinterpret_cast<const float4 *>(leaf + (size_t)st[u] * c.block) + gq);
+      v[u][0] = t.x, v[u][1] = t.y, v[u][2] = t.z, v[u][3] = t.w;
       s[u] = 0;
     }
   } else {
@@ -658,9 +658,8 @@ __device__ __forceinline__ void msg4s(const DevCtx &c, const EigPack<4> &E, int 
 #pragma unroll
       for (int u = 0; u < PP; u++) {
         const int st = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
-        const float *lt = leaf + (size_t)st * c.block + gq;
-#pragma unroll
-        for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
+        const float4 t = __ldg(reinterpret_cast<const float4 *>(leaf + (size_t)st * c.block) + gq);
+        v[u][0] = t.x, v[u][1] = t.y, v[u][2] = t.z, v[u][3] = t.w;
         s[u] = 0;
       }
       return;
@@ -884,12 +883,15 @@ __global__ void __launch_bounds__(kThreads, B)
 constexpr int kThreadsP = 128;  // patterns per CTA
 constexpr int kChunkP = 8;      // ops staged together
 
+// staged op table: the head (mixed: P_c(t) as [side][x][c][y] floats; FP64: the exp factors as
+// [side][i][c] doubles), then per side the leaf rows of the bases A, C, G, T and of the unknown
+// state; the global table holds the head, then a row per state and side (mixed [c][x], FP64
+// [x][c])
 template <typename R, int C>
 struct Tab4P {
-  static constexpr int kP = 2 * 16 * C;    // mixed: P_c(t) floats, [side][x][c][y]
-  static constexpr int kD = 2 * 4 * C;     // FP64: exp factors, [side][i][c]
-  static constexpr int kLeaf = 5 * 4 * C;  // FP64: leaf rows {A, C, G, T, unknown}, [5][x][c]
-  static constexpr int kBytes = sizeof(R) == 4 ? kP * 4 : (kD + 2 * kLeaf) * 8;
+  static constexpr int kH = sizeof(R) == 4 ? 2 * 16 * C : 2 * 4 * C;  // head elements
+  static constexpr int kLeaf = 5 * 4 * C;                             // leaf elements per side
+  static constexpr int kBytes = (kH + 2 * kLeaf) * (int)sizeof(R);
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -946,20 +948,17 @@ __device__ __forceinline__ void stage4p(StageP<R, C> &st, int b, const DevCtx &c
     const int i = q / kPieces, r = q - i * kPieces;
     const R *tk = tab + (size_t)(k0 + i) * stride;
     const char *src;
-    if constexpr (sizeof(R) == 4) {
-      src = reinterpret_cast<const char *>(tk) + 16 * r;
+    const int blk = 4 * C, u1 = c.unknown + 1;
+    const int off = 16 * r;  // byte offset inside the staged table
+    constexpr int hB = T::kH * (int)sizeof(R), rowsB = 16 * C * (int)sizeof(R),
+                  rowB = 4 * C * (int)sizeof(R);
+    if (off < hB) {
+      src = reinterpret_cast<const char *>(tk) + off;
     } else {
-      const int blk = 4 * C, u1 = c.unknown + 1;
-      const int off = 16 * r;  // byte offset inside the staged table
-      constexpr int dB = T::kD * 8, rowsB = 16 * C * 8, rowB = 4 * C * 8;
-      if (off < dB) {
-        src = reinterpret_cast<const char *>(tk) + off;
-      } else {
-        const int o = off - dB, side = o / (rowsB + rowB), w = o - side * (rowsB + rowB);
-        const double *leaf = tk + 2 * blk + (size_t)side * u1 * blk;
-        src = w < rowsB ? reinterpret_cast<const char *>(leaf) + w
-                        : reinterpret_cast<const char *>(leaf + (size_t)c.unknown * blk) + (w - rowsB);
-      }
+      const int o = off - hB, side = o / (rowsB + rowB), w = o - side * (rowsB + rowB);
+      const R *leaf = tk + T::kH + (size_t)side * u1 * blk;
+      src = w < rowsB ? reinterpret_cast<const char *>(leaf) + w
+                      : reinterpret_cast<const char *>(leaf + (size_t)c.unknown * blk) + (w - rowsB);
     }
     cp_async16(st.tab[b][i] + 16 * r, src);
   }
@@ -1046,16 +1045,24 @@ struct StackP {
     return reinterpret_cast<uint16_t *>(base + (size_t)depth * kEntry * kThreadsP);
   }
   static size_t bytes(int depth) { return (size_t)depth * kThreadsP * (kEntry + 2 * C); }
+  // counters: C per entry under SAFE scaling, the first one only under NORM (all are equal)
+  template <bool SAFE>
   __device__ __forceinline__ void put(int pos, const R (&v)[C][4], const int (&sc)[C]) const {
     sm_put<C>(base + (size_t)pos * kEntry * kThreadsP, v);
 #pragma unroll
-    for (int cc = 0; cc < C; cc++)
+    for (int cc = 0; cc < (SAFE ? C : 1); cc++)
       scs()[((size_t)pos * C + cc) * kThreadsP + threadIdx.x] = (uint16_t)sc[cc];
   }
+  template <bool SAFE>
   __device__ __forceinline__ void get(int pos, R (&v)[C][4], int (&sc)[C]) const {
     sm_get<C>(base + (size_t)pos * kEntry * kThreadsP, v);
 #pragma unroll
-    for (int cc = 0; cc < C; cc++) sc[cc] = scs()[((size_t)pos * C + cc) * kThreadsP + threadIdx.x];
+    for (int cc = 0; cc < (SAFE ? C : 1); cc++)
+      sc[cc] = scs()[((size_t)pos * C + cc) * kThreadsP + threadIdx.x];
+    if (!SAFE) {
+#pragma unroll
+      for (int cc = 1; cc < C; cc++) sc[cc] = sc[0];
+    }
   }
 };
 
@@ -1073,25 +1080,36 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
 #pragma unroll
     for (int cc = 0; cc < C; cc++) s[cc] = 0;
     if constexpr (sizeof(R) == 4) {
-      const int mask = st < 4 ? 1 << st : (st < 18 ? st - 3 : 15);
-      const float4 *P4 = reinterpret_cast<const float4 *>(tabS) + side * 4 * C;
-#pragma unroll
-      for (int x = 0; x < 4; x++)
+      if (st < 4 || st == c.unknown) {
+        const float4 *row = reinterpret_cast<const float4 *>(tabS) +
+                            (T::kH + side * T::kLeaf + (st < 4 ? st : 4) * 4 * C) / 4;
 #pragma unroll
         for (int cc = 0; cc < C; cc++) {
-          const float4 r = P4[x * C + cc];
-          float acc = 0.f;
-          if (mask & 1) acc = acc + r.x;
-          if (mask & 2) acc = acc + r.y;
-          if (mask & 4) acc = acc + r.z;
-          if (mask & 8) acc = acc + r.w;
-          v[cc][x] = acc;
+          const float4 t = row[cc];
+          v[cc][0] = t.x, v[cc][1] = t.y, v[cc][2] = t.z, v[cc][3] = t.w;
         }
+      } else {
+        // an ambiguity code: the sum of the P columns of its states, in state order
+        const int mask = st - 3;
+        const float4 *P4 = reinterpret_cast<const float4 *>(tabS) + side * 4 * C;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+          for (int cc = 0; cc < C; cc++) {
+            const float4 r = P4[x * C + cc];
+            float acc = 0.f;
+            if (mask & 1) acc = acc + r.x;
+            if (mask & 2) acc = acc + r.y;
+            if (mask & 4) acc = acc + r.z;
+            if (mask & 8) acc = acc + r.w;
+            v[cc][x] = acc;
+          }
+      }
     } else {
       const int blk = 4 * C;
       const double *row;
       if (st < 4 || st == c.unknown) {
-        row = reinterpret_cast<const double *>(tabS) + T::kD + side * T::kLeaf +
+        row = reinterpret_cast<const double *>(tabS) + T::kH + side * T::kLeaf +
               (st < 4 ? st : 4) * blk;
 #pragma unroll
         for (int x = 0; x < 4; x++)
@@ -1116,7 +1134,7 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
       s[cc] = fwd_s[cc];
     }
   } else if (src == kSrcStack) {
-    stk.get(min(pos, stk.depth - 1), L, s);
+    stk.template get<SAFE>(min(pos, stk.depth - 1), L, s);
   } else {
     ld_cg<C>(static_cast<const R *>(c.partials) + (size_t)id * c.slot_elems + (size_t)p * (4 * C),
              L);
@@ -1158,7 +1176,7 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
 }
 
 template <typename R, bool SAFE, int C>
-__global__ void __launch_bounds__(kThreadsP)
+__global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
     k_traverse4p(DevCtx c, const DevOp *__restrict__ ops, int nops, const R *__restrict__ tab,
                  size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
   extern __shared__ __align__(16) unsigned char smem_p[];
@@ -1278,7 +1296,8 @@ __global__ void __launch_bounds__(kThreadsP)
           sc[p] = (uint16_t)so[0];
         }
       }
-      if (plan_out(w) == kSrcStack) stk.put(min(plan_opos(w), max(depth - 1, 0)), out, so);
+      if (plan_out(w) == kSrcStack)
+        stk.template put<SAFE>(min(plan_opos(w), max(depth - 1, 0)), out, so);
 #pragma unroll
       for (int cc = 0; cc < C; cc++) {
 #pragma unroll

@@ -15,11 +15,19 @@ struct Tree {
   gems_session *s = nullptr;
   int ntaxa = 0, nnode = 0, nedges = 0, nslots = 0;
   bool per_branch = false;  // one slot per directed branch (no re-orientation)
+  // LM_MEM_SAVE (tree/memslot.cpp, tree/phylotree.cpp:1026-1040): fewer slots than internal
+  // nodes; directed branches get a slot when their partial is computed, and a full pool gives
+  // up the unlocked slot whose partial is cheapest to recompute (smallest subtree)
+  bool pool = false;
+  int pool_free = 0;               // slots not handed out yet (MemSlotVector::free_count)
+  std::vector<char> slot_locked;   // per slot (MEM_LOCKED)
+  std::vector<int> sub_size;       // per directed branch: leaves of the subtree it points to
+  int pool_status = GEMS_OK;       // GEMS_ERR_ADMISSION when a traversal found no slot
   std::vector<int> deg, adj, eu, ev;
   std::vector<double> len;
   // directed branch d = u*3+k: u -> adj[u*3+k]; its partial is the subtree at adj[u*3+k]
   std::vector<char> computed;
-  std::vector<int> dslot;      // per_branch: slot of directed branch
+  std::vector<int> dslot;      // per_branch and pool: slot of directed branch (-1: none)
   std::vector<int> node_slot;  // per node: slot of internal node (LM_PER_NODE)
   std::vector<int> owner;      // per slot: directed branch currently holding it, -1 if none
   int cur_u = -1, cur_k = 0;
@@ -49,7 +57,112 @@ struct Tree {
     }
     return sl;
   }
-  int slot_of(int d) const { return per_branch ? dslot[d] : node_slot[adj[d]]; }
+  int slot_of(int d) const { return per_branch || pool ? dslot[d] : node_slot[adj[d]]; }
+
+  // PhyloNode::computeSize (tree/phylonode.cpp:91): leaves below every directed branch
+  int size_below(int u, int k) {
+    const int d = u * 3 + k, v = adj[d];
+    if (sub_size[d] > 0) return sub_size[d];
+    int n = 0;
+    if (leaf(v)) {
+      n = 1;
+    } else {
+      for (int j = 0; j < deg[v]; j++)
+        if (adj[v * 3 + j] != u) n += size_below(v, j);
+    }
+    return sub_size[d] = n;
+  }
+  void compute_sizes() {
+    sub_size.assign(nnode * 3, 0);
+    for (int u = 0; u < nnode; u++)
+      for (int k = 0; k < deg[u]; k++) size_below(u, k);
+  }
+
+  // MemSlotVector::lock / unlock (tree/memslot.cpp:92-121): a partial in use by the traversal
+  // being built keeps its slot
+  bool lock(int d) {
+    if (!pool || leaf(adj[d]) || dslot[d] < 0 || slot_locked[dslot[d]]) return false;
+    slot_locked[dslot[d]] = 1;
+    return true;
+  }
+  void unlock(int d) {
+    if (pool && dslot[d] >= 0) slot_locked[dslot[d]] = 0;
+  }
+  void give_slot(int d, int sl) {
+    if (owner[sl] >= 0 && owner[sl] != d) {
+      computed[owner[sl]] = 0;  // clearPartialLh of the branch that held it
+      dslot[owner[sl]] = -1;
+    }
+    if (dslot[d] >= 0 && dslot[d] != sl) owner[dslot[d]] = -1;  // d's old slot is free again
+    owner[sl] = d;
+    dslot[d] = sl;
+  }
+  // MemSlotVector::allocate (tree/memslot.cpp:138-175): a free slot, else the unlocked slot of
+  // the smallest subtree
+  bool allocate(int d) {
+    if (pool_free < nslots) {
+      give_slot(d, pool_free++);
+      return true;
+    }
+    for (int sl = 0; sl < nslots; sl++)
+      if (!slot_locked[sl] && owner[sl] < 0) {
+        give_slot(d, sl);
+        return true;
+      }
+    int best = -1, best_size = 1 << 30;
+    for (int sl = 0; sl < nslots; sl++) {
+      if (slot_locked[sl] || owner[sl] < 0) continue;
+      if (sub_size[owner[sl]] < best_size) {
+        best = sl;
+        best_size = sub_size[owner[sl]];
+        if (best_size == 2) break;  // the smallest subtree an internal partial can have
+      }
+    }
+    if (best < 0) return false;
+    give_slot(d, best);
+    return true;
+  }
+
+  // computeTraversalInfo with LM_MEM_SAVE (tree/phylotree.cpp:6031-6140): children in
+  // descending subtree size, the partial re-oriented from a back-neighbour's slot when it has
+  // none, else a slot allocated; children locked until their parent's op is listed.  Returns
+  // whether the partial of (dad -> node) was locked.
+  bool collect_pool(int dad, int node) {
+    const int d = dir(dad, node);
+    if (computed[d] || leaf(node)) return lock(d);
+    int kids[2], nk = 0;
+    for (int k = 0; k < deg[node]; k++)
+      if (adj[node * 3 + k] != dad) kids[nk++] = adj[node * 3 + k];
+    if (sub_size[dir(node, kids[0])] < sub_size[dir(node, kids[1])]) std::swap(kids[0], kids[1]);
+    bool lk[2];
+    for (int i = 0; i < 2; i++) lk[i] = collect_pool(node, kids[i]);
+    computed[d] = 1;
+    // reorientPartialLh (:6011): take over the slot of a back-neighbour (an unlocked one)
+    if (dslot[d] < 0) {
+      for (int i = 0; i < 2; i++) {
+        const int back = dir(kids[i], node);
+        if (dslot[back] >= 0 && !slot_locked[dslot[back]]) {
+          give_slot(d, dslot[back]);
+          break;
+        }
+      }
+    }
+    if ((dslot[d] < 0 || slot_locked[dslot[d]]) && !allocate(d)) pool_status = GEMS_ERR_ADMISSION;
+    for (int i = 0; i < 2; i++)
+      if (lk[i]) unlock(dir(node, kids[i]));
+    gems_op op{};
+    op.dst_slot = dslot[d] < 0 ? 0 : dslot[d];
+    auto child = [&](int c, int &kind, int &id, double &l) {
+      l = len[node * 3 + find(node, c)];
+      kind = leaf(c) ? GEMS_CHILD_TIP : GEMS_CHILD_PARTIAL;
+      id = leaf(c) ? c : dslot[dir(node, c)];
+    };
+    child(kids[0], op.left_kind, op.left_id, op.left_len);
+    child(kids[1], op.right_kind, op.right_id, op.right_len);
+    ops.push_back(op);
+    partial_ops++;
+    return lock(d);
+  }
 
   // computeTraversalInfo (tree/phylotree.cpp:6031-6140): postorder list of stale partials
   void collect(int dad, int node) {
@@ -85,8 +198,20 @@ struct Tree {
   gems_branch branch(int &node, int &dad) {
     if (leaf(node)) std::swap(node, dad);
     ops.clear();
-    collect(dad, node);
-    if (!leaf(dad)) collect(node, dad);
+    if (pool) {
+      // the larger side first (phylokernelnew.h:1176-1190); both ends stay locked until the
+      // list is complete
+      pool_status = GEMS_OK;
+      int a = dad, b = node;
+      if (sub_size[dir(dad, node)] < sub_size[dir(node, dad)]) std::swap(a, b);
+      const bool la = collect_pool(a, b);
+      const bool lb = collect_pool(b, a);
+      if (la) unlock(dir(a, b));
+      if (lb) unlock(dir(b, a));
+    } else {
+      collect(dad, node);
+      if (!leaf(dad)) collect(node, dad);
+    }
     gems_branch br{};
     br.dad_slot = slot_of(dir(dad, node));
     if (leaf(dad)) {
@@ -153,6 +278,7 @@ struct Tree {
 
   int lh_branch(int node, int dad, double *lnl, double *pattern_lh) {
     gems_branch br = branch(node, dad);
+    if (pool_status) return pool_status;
     return gems_branch_lnl(s, ops.data(), (int)ops.size(), &br, lnl, pattern_lh);
   }
 
@@ -160,6 +286,7 @@ struct Tree {
     int st;
     if (!theta_computed) {
       gems_branch br = branch(node, dad);
+      if (pool_status) return pool_status;
       st = gems_branch_derv(s, ops.data(), (int)ops.size(), &br, 1, df, ddf, nullptr);
       if (st == GEMS_OK) theta_computed = true;
     } else {
@@ -195,6 +322,7 @@ struct Tree {
     theta_computed = false;
     int n = node2, d = node1;
     gems_branch br = branch(n, d);
+    if (pool_status) return pool_status;
     double optx = cur;
     int nev = 0;
     int st = gems_newton_branch(s, ops.data(), (int)ops.size(), &br, 1, min_bl, max_bl, min_bl,
@@ -260,8 +388,12 @@ struct Tree {
     if (leaf(u) || leaf(v) || find(u, v) < 0 || ku_a < 0 || kv_b < 0 || a == v || b == u)
       return GEMS_ERR_BAD_ARG;
     const int du = u * 3 + ku_a, dv = v * 3 + kv_b;
-    if (per_branch) {
+    if (per_branch || pool) {
       std::swap(dslot[du], dslot[dv]);
+      if (pool) {  // the slots follow their subtrees: their owners are re-pointed
+        if (dslot[du] >= 0) owner[dslot[du]] = du;
+        if (dslot[dv] >= 0) owner[dslot[dv]] = dv;
+      }
     } else {
       // the buffers of a and b stay with their subtrees: re-point their owners
       const bool own_a = !leaf(a) && owner[node_slot[a]] == du;
@@ -290,6 +422,7 @@ struct Tree {
     }
     theta_computed = false;
     cur_u = -1;
+    if (pool) compute_sizes();
     return GEMS_OK;
   }
 
@@ -318,6 +451,7 @@ struct Tree {
     }
     int node = adj[cur_u * 3 + cur_k], dad = cur_u;
     gems_branch br = branch(node, dad);
+    if (pool_status) return pool_status;
     const int st = gems_branch_lnl_from_host(s, states, ptn_freq, ptn_invar, ops.data(),
                                              (int)ops.size(), &br, nchunks, lnl, pattern_lh);
     if (st) std::fill(computed.begin(), computed.end(), 0);
@@ -374,13 +508,19 @@ int gems_tree_create(gems_session *s, int nedges, const int *eu, const int *ev,
     return GEMS_ERR_BAD_ARG;
   }
   const int nslots = desc.nslots;
-  if (nslots < ninternal) {
+  // LM_MEM_SAVE's floor: log2(leafNum) + LH_MIN_CONST slots (tree/phylotree.cpp:42,1026-1040)
+  const int min_slots = (int)std::log2((double)t->ntaxa) + 1;
+  if (nslots < ninternal && nslots < min_slots) {
     delete t;
     return GEMS_ERR_ADMISSION;
   }
   t->nslots = nslots;
   int next = 0;
-  if (nslots >= 3 * ninternal) {
+  if (nslots < ninternal) {
+    t->pool = true;
+    t->slot_locked.assign(nslots, 0);
+    t->compute_sizes();
+  } else if (nslots >= 3 * ninternal) {
     t->per_branch = true;
     for (int u = 0; u < t->nnode; u++)
       for (int k = 0; k < t->deg[u]; k++)

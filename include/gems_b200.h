@@ -286,9 +286,14 @@ int gems_check_barrier_timeout(int device, int *status);
 /* ---- tree mirror (PhyloTree calls on the path) ---- */
 typedef struct gems_tree gems_tree;
 /* Unrooted binary tree: leaves 0..ntaxa-1, internal nodes ntaxa..nedges; each node's
- * neighbour order follows the edge order.  The session must have been created with
- * nslots >= ntaxa-2 (one partial per internal node, LM_PER_NODE) and may have up to
- * 3*(ntaxa-2) (one per directed branch). */
+ * neighbour order follows the edge order.  The session's nslots chooses the memory mode:
+ * ntaxa-2 (one partial per internal node, LM_PER_NODE, tree/phylotree.cpp:905-960);
+ * 3*(ntaxa-2) (one per directed branch); or fewer than ntaxa-2, down to
+ * floor(log2(ntaxa)) + 1 (LM_MEM_SAVE, tree/memslot.cpp:28-229, tree/phylotree.cpp:1026-1040):
+ * a directed branch gets a slot when its partial is computed, a full pool gives up the
+ * unlocked slot of the smallest subtree (that partial is recomputed when next needed), and
+ * children are traversed larger subtree first.  Fewer slots return GEMS_ERR_ADMISSION, as
+ * does a traversal that finds every slot locked.  Results are the same in every mode. */
 int gems_tree_create(gems_session *s, int nedges, const int *eu, const int *ev,
                      const double *len, gems_tree **out);
 int gems_tree_destroy(gems_tree *t);

@@ -39,7 +39,7 @@ def run_pair(tree, model, aln, precision, slots, nreq, safe=False, tc=None, inva
     return out
 
 
-@pytest.mark.parametrize("slots", ["node", "branch"])
+@pytest.mark.parametrize("slots", ["node", "branch", "pool"])
 @pytest.mark.parametrize("n", [4, 20])
 def test_nni5_fp64(gpu, n, slots):
     tree, model, aln = case(n, 24, 3000, 21 + n)
