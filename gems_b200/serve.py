@@ -37,7 +37,7 @@ import types
 import numpy as np
 
 from . import synth
-from .api import GemsError, PhyloTree, Session
+from .api import GemsError, PhyloTree, Session, min_pool_slots
 
 
 @dataclasses.dataclass
@@ -50,11 +50,30 @@ class SessionSpec:
     precision: str
     seed: int
 
-    def footprint(self, npat):
-        nslots = self.ntaxa - 2
+    def footprint(self, npat, nslots=None):
+        """Device bytes of the session with `nslots` partial slots (default: one per internal
+        node, LM_PER_NODE)."""
+        nslots = self.ntaxa - 2 if nslots is None else nslots
         scaling = "safe" if self.nstates == 61 else "norm"
         return Session.footprint(self.ntaxa, npat, self.nstates, self.ncat, nslots,
                                  self.precision, scaling)
+
+    def slot_plan(self, npat, avail, memsave=True):
+        """(nslots, bytes) of the largest session that fits `avail` bytes: one slot per internal
+        node when it fits, else (memsave) the most slots of the LM_MEM_SAVE pool that fit, down
+        to its floor; None when nothing fits."""
+        full = self.footprint(npat)
+        if full <= avail:
+            return None, full
+        if not memsave:
+            return None
+        lo = min_pool_slots(self.ntaxa)
+        base = self.footprint(npat, lo)
+        per = self.footprint(npat, lo + 1) - base
+        if base > avail:
+            return None
+        n = min(self.ntaxa - 3, lo + (avail - base) // max(per, 1))
+        return int(n), base + (int(n) - lo) * per
 
 
 def build_case(spec: SessionSpec):
@@ -70,12 +89,14 @@ def build_case(spec: SessionSpec):
     return tree, model, aln
 
 
-def open_session(spec, case, device=0, tree=None):
-    """The session of a case, on the case's tree or on `tree` (an evicted session's)."""
+def open_session(spec, case, device=0, tree=None, nslots=None):
+    """The session of a case, on the case's tree or on `tree` (an evicted session's), with one
+    partial slot per internal node or `nslots` (an LM_MEM_SAVE pool)."""
     t0, model, aln = case
     return PhyloTree.from_case(tree if tree is not None else t0, model, aln,
                                precision=spec.precision,
-                               scaling="safe" if spec.nstates == 61 else "norm", device=device)
+                               scaling="safe" if spec.nstates == 61 else "norm", device=device,
+                               slots="node" if nslots is None else int(nslots))
 
 
 def saved_tree(gt: PhyloTree, ntaxa: int):
@@ -114,9 +135,14 @@ def run_alone(spec, case, nreq, device=0, opener=open_session):
 
 
 class Server:
-    def __init__(self, device=0, budget_bytes=None, workers=8, evict=True, opener=open_session):
-        """opener(spec, case, device, tree) builds a session's tree object (open_session: a
-        PhyloTree on the GPU); budget_bytes defaults to 85% of the device's free memory."""
+    def __init__(self, device=0, budget_bytes=None, workers=8, evict=True, opener=open_session,
+                 memsave=True):
+        """opener(spec, case, device, tree[, nslots]) builds a session's tree object
+        (open_session: a PhyloTree on the GPU); budget_bytes defaults to 85% of the device's
+        free memory.  With memsave, a session that does not fit with one partial slot per
+        internal node is admitted with the largest LM_MEM_SAVE pool that fits the free budget
+        (its evicted partials are recomputed when needed) before any idle session is evicted;
+        only a session whose smallest pool cannot fit waits for evictions."""
         if budget_bytes is None:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
@@ -126,6 +152,7 @@ class Server:
         self.workers = workers
         self.evict = evict
         self.opener = opener
+        self.memsave = memsave
 
     def run(self, specs, cases, requests, preopen=False):
         """requests: list of (arrival_s, sid) in arrival order, arrival times counted from the
@@ -135,8 +162,14 @@ class Server:
         kept in self.open_ms.  Returns the per-request records and the stream's wall time."""
         lock = threading.Condition()
         npat = {s.sid: cases[s.sid][2].npat for s in specs}
-        fp = {s.sid: s.footprint(npat[s.sid]) for s in specs}
         spec_of = {s.sid: s for s in specs}
+        # bytes a session holds once admitted (its plan), and the least it can be admitted with
+        fp = {s.sid: s.footprint(npat[s.sid]) for s in specs}
+        fp_min = {s.sid: (s.slot_plan(npat[s.sid], 1 << 62, False)[1] if not self.memsave else
+                          s.footprint(npat[s.sid], min_pool_slots(s.ntaxa)))
+                  for s in specs}
+        nslots_of = {}   # sid -> slots of an admitted pool session (absent: one per node)
+        self.pool_admissions = 0
         remaining = collections.Counter(sid for _, sid in requests)
         pending = collections.defaultdict(collections.deque)  # sid -> deque of (arr, idx, seq)
         seq_of = collections.Counter()
@@ -151,13 +184,31 @@ class Server:
         open_fail = collections.Counter()
         last_used = {}   # sid -> end of its last request
         for sid in fp:
-            if fp[sid] > self.budget:
+            if fp_min[sid] > self.budget:
                 state["rejected"].add(sid)
+
+        def plan_locked(sid):
+            """Admission plan of sid in the free budget: sets fp[sid] (and its slots)."""
+            plan = spec_of[sid].slot_plan(npat[sid], self.budget - state["used"], self.memsave)
+            if plan is None:
+                return False
+            n, b = plan
+            fp[sid] = b
+            if n is None:
+                nslots_of.pop(sid, None)
+            else:
+                nslots_of[sid] = n
+                self.pool_admissions += 1
+            return True
 
         def open_one(sid):
             t = time.perf_counter()
             try:
-                gt = self.opener(spec_of[sid], cases[sid], self.device, saved.get(sid))
+                if sid in nslots_of:
+                    gt = self.opener(spec_of[sid], cases[sid], self.device, saved.get(sid),
+                                     nslots=nslots_of[sid])
+                else:
+                    gt = self.opener(spec_of[sid], cases[sid], self.device, saved.get(sid))
                 gt.computeLikelihood()
             except GemsError:
                 return None
@@ -170,7 +221,7 @@ class Server:
             for sid in dict.fromkeys(sid for _, sid in requests):
                 if sid in state["rejected"]:
                     continue
-                if state["used"] + fp[sid] > self.budget:
+                if not plan_locked(sid):
                     break
                 state["used"] += fp[sid]
                 queue.append(sid)
@@ -202,8 +253,14 @@ class Server:
             if not waiting_admit:
                 return None, []
             sid = waiting_admit[0]
-            need = state["used"] + fp[sid] - self.budget
             victims = []
+            if plan_locked(sid):  # fits the free budget, at full size or as a pool
+                need = 0
+            else:  # room for its smallest admissible form, from idle sessions
+                fp[sid] = fp_min[sid]
+                if self.memsave:
+                    nslots_of[sid] = min_pool_slots(spec_of[sid].ntaxa)
+                need = state["used"] + fp[sid] - self.budget
             if need > 0:
                 if not self.evict:
                     return None, []

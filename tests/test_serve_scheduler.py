@@ -14,7 +14,7 @@ from oracle import oracle as orc
 class OracleSession:
     """An oracle tree in the role of a session's tree object (same method names)."""
 
-    def __init__(self, spec, case, device=0, tree=None):
+    def __init__(self, spec, case, device=0, tree=None, nslots=None):
         t0, model, aln = case
         self.t = orc.OracleTree(tree if tree is not None else t0, model, aln,
                                 safe=spec.nstates == 61)
@@ -48,18 +48,50 @@ def test_admission_batching_and_eviction_keep_results():
     # arrivals spread out, so that sessions sit idle with requests still to come
     specs, reqs, cases = stream(5, 40, seed=8, rate=300.0)
     fps = sorted(s.footprint(cases[s.sid][2].npat) for s in specs)
-    srv = serve.Server(budget_bytes=fps[-1] + fps[0], workers=3, opener=OracleSession)
+    srv = serve.Server(budget_bytes=fps[-1] + fps[0], workers=3, opener=OracleSession,
+                       memsave=False)
     records, _ = srv.run(specs, cases, reqs)
     assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
     assert srv.evictions > 0
     same_as_alone(specs, cases, records)
 
 
+def test_memsave_admits_pools_before_evicting():
+    """With LM_MEM_SAVE pools, sessions that do not fit at full size are admitted with fewer
+    slots instead of waiting for evictions; results are unchanged."""
+    specs, reqs, cases = stream(5, 40, seed=8, rate=300.0)
+    fps = sorted(s.footprint(cases[s.sid][2].npat) for s in specs)
+    srv = serve.Server(budget_bytes=fps[-1] + fps[0], workers=3, opener=OracleSession)
+    records, _ = srv.run(specs, cases, reqs)
+    assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
+    assert srv.pool_admissions > 0
+    same_as_alone(specs, cases, records)
+
+
+def test_memsave_admits_a_session_only_its_pool_fits():
+    """A budget below a session's full footprint but above its smallest pool: admitted as a
+    pool (no rejection), results unchanged; below the pool: rejected."""
+    specs, reqs, cases = stream(4, 24, seed=9)
+    fps = {s.sid: s.footprint(cases[s.sid][2].npat) for s in specs}
+    big = max(fps, key=fps.get)
+    sp = specs[big]
+    floor = sp.footprint(cases[big][2].npat, serve.min_pool_slots(sp.ntaxa))
+    assert floor < fps[big]
+    srv = serve.Server(budget_bytes=fps[big] - 1, workers=2, opener=OracleSession)
+    records, _ = srv.run(specs, cases, reqs)
+    assert not any(r.get("rejected") for r in records)
+    assert srv.pool_admissions > 0
+    same_as_alone(specs, cases, records)
+    srv = serve.Server(budget_bytes=floor - 1, workers=2, opener=OracleSession)
+    records, _ = srv.run(specs, cases, reqs)
+    assert all(r.get("rejected") for r, (_, sid) in zip(records, reqs) if sid == big)
+
+
 def test_session_that_cannot_fit_is_rejected():
     specs, reqs, cases = stream(4, 24, seed=9)
     fps = {s.sid: s.footprint(cases[s.sid][2].npat) for s in specs}
     budget = sorted(fps.values())[-1] - 1
-    srv = serve.Server(budget_bytes=budget, workers=2, opener=OracleSession)
+    srv = serve.Server(budget_bytes=budget, workers=2, opener=OracleSession, memsave=False)
     records, _ = srv.run(specs, cases, reqs)
     for r, (_, sid) in zip(records, reqs):
         assert bool(r.get("rejected")) == (fps[sid] > budget)
