@@ -7,10 +7,10 @@ missing, the calls raise.
 """
 from .api import (GemsError, PhyloTree, Session, STATUS, op_array, branch_struct,
                   measure_peaks, check_barrier_timeout, compress_alignment, Ingest, full_traversal,
-                  traverse_batch, branch_lnl_batch,
-                  GEMS_CHILD_PARTIAL, GEMS_CHILD_TIP)
+                  traverse_batch, branch_lnl_batch, set_models_from_rates,
+                  optimize_all_branches_batch, GEMS_CHILD_PARTIAL, GEMS_CHILD_TIP)
 
 __all__ = ["GemsError", "PhyloTree", "Session", "STATUS", "op_array", "branch_struct",
            "measure_peaks", "check_barrier_timeout", "compress_alignment", "Ingest", "full_traversal",
-           "traverse_batch", "branch_lnl_batch",
-           "GEMS_CHILD_PARTIAL", "GEMS_CHILD_TIP"]
+           "traverse_batch", "branch_lnl_batch", "set_models_from_rates",
+           "optimize_all_branches_batch", "GEMS_CHILD_PARTIAL", "GEMS_CHILD_TIP"]

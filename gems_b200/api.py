@@ -176,6 +176,35 @@ def full_traversal(tree):
     return ops, branch_struct(root - nt, GEMS_CHILD_TIP, 0, rlen)
 
 
+def set_models_from_rates(sessions, exch_upper, freq, rates, props):
+    """gems_set_model_from_rates_batch: every session's eigensystem in one launch.  Arguments
+    are per-session sequences (stacked row by row)."""
+    lib = _lib.gems()
+    arr = _session_array(sessions)
+    ex = np.ascontiguousarray(np.stack([_f64(x) for x in exch_upper]))
+    fr = np.ascontiguousarray(np.stack([_f64(x) for x in freq]))
+    rt = np.ascontiguousarray(np.stack([_f64(x) for x in rates]))
+    pr = np.ascontiguousarray(np.stack([_f64(x) for x in props]))
+    _check(lib.gems_set_model_from_rates_batch(arr, len(sessions), _dptr(ex), _dptr(fr),
+                                               _dptr(rt), _dptr(pr)),
+           "gems_set_model_from_rates_batch")
+
+
+def optimize_all_branches_batch(trees, my_iterations=100, tolerance=0.001, maxNRStep=100):
+    """gems_tree_optimize_all_branches_batch: optimizeAllBranches on PhyloTrees of one topology
+    (one per candidate model), their device work overlapped; returns their lnL."""
+    lib = _lib.gems()
+    arr = (c_void_p * len(trees))()
+    for i, t in enumerate(trees):
+        arr[i] = t.handle.value
+    out = np.zeros(len(trees))
+    _check(lib.gems_tree_optimize_all_branches_batch(arr, len(trees), int(my_iterations),
+                                                     c_double(tolerance), int(maxNRStep),
+                                                     _dptr(out)),
+           "gems_tree_optimize_all_branches_batch")
+    return out
+
+
 def _session_array(sessions):
     arr = (c_void_p * len(sessions))()
     for i, s in enumerate(sessions):

@@ -9,6 +9,7 @@
 // inv_evec[i][j] = V[j][i] * sqrt(pi_j), Q = evec diag(eval) inv_evec.
 // The basis differs from tred2/tqli by column order and sign; likelihoods do not depend on it.
 #include <cmath>
+#include <vector>
 
 #include "gems_internal.cuh"
 
@@ -19,8 +20,28 @@ namespace {
 constexpr double kZeroFreq = 1e-10;
 constexpr int kMaxSweeps = 60;
 
+__device__ void jacobi_one(int n, const double *exch_upper, const double *freq_in, double *out,
+                           int *flag);
+
 __global__ void k_jacobi(int n, const double *exch_upper, const double *freq_in, double *out,
                          int *flag) {
+  jacobi_one(n, exch_upper, freq_in, out, flag);
+}
+
+// one candidate model per CTA: exch[i] at exch + i * n(n-1)/2, freq[i] at freq + i * n, the
+// eigensystem into out[i]
+struct EigJob {
+  double *out;
+  int *flag;
+};
+__global__ void k_jacobi_batch(int n, const double *exch, const double *freq,
+                               const EigJob *jobs) {
+  const int i = blockIdx.x, nu = n * (n - 1) / 2;
+  jacobi_one(n, exch + (size_t)i * nu, freq + (size_t)i * n, jobs[i].out, jobs[i].flag);
+}
+
+__device__ void jacobi_one(int n, const double *exch_upper, const double *freq_in, double *out,
+                           int *flag) {
   extern __shared__ double sm[];
   const int ld = kMaxStates + 1;
   double *A = sm;                 // [m][ld]
@@ -179,6 +200,43 @@ int launch_eigen(Session *s, const double *exch_upper, const double *freq) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   cudaFree(d_in);
   if (e != cudaSuccess) return cuda_status(e, "eigen");
+  return GEMS_OK;
+}
+
+// every session's eigensystem in one launch (one CTA each), on the first session's stream
+int launch_eigen_batch(Session *const *ss, int nsess, const double *exch_upper,
+                       const double *freq) {
+  const int n = ss[0]->desc.nstates;
+  const size_t nu = (size_t)n * (n - 1) / 2;
+  for (int i = 0; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
+  cudaStream_t st = ss[0]->stream;
+  const size_t in_bytes = sizeof(double) * nsess * (nu + n);
+  char *d_buf = nullptr;
+  GEMS_CUDA(cudaMalloc(&d_buf, in_bytes + sizeof(EigJob) * nsess));
+  double *d_exch = reinterpret_cast<double *>(d_buf), *d_freq = d_exch + nsess * nu;
+  EigJob *d_jobs = reinterpret_cast<EigJob *>(d_buf + in_bytes);
+  std::vector<EigJob> jobs(nsess);
+  for (int i = 0; i < nsess; i++) jobs[i] = {ss[i]->d_model, ss[i]->d_flag};
+  const size_t smem = sizeof(double) * (2 * kMaxStates * (kMaxStates + 1) + 2 * kMaxStates);
+  cudaError_t e = cudaMemcpyAsync(d_exch, exch_upper, sizeof(double) * nsess * nu,
+                                  cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_freq, freq, sizeof(double) * nsess * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(EigJob) * nsess, cudaMemcpyHostToDevice, st);
+  for (int i = 0; i < nsess && e == cudaSuccess; i++)
+    e = cudaMemsetAsync(ss[i]->d_flag, 0, sizeof(int), st);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_jacobi_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+  if (e == cudaSuccess) {
+    k_jacobi_batch<<<nsess, 128, smem, st>>>(n, d_exch, d_freq, d_jobs);
+    ss[0]->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d_buf);
+  if (e != cudaSuccess) return cuda_status(e, "eigen batch");
   return GEMS_OK;
 }
 

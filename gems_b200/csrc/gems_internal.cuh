@@ -203,7 +203,14 @@ int launch_derv(Session *s, double length, double *df, double *ddf);
 int launch_from_buffer(Session *s, double length, double *lnl);
 int launch_newton(Session *s, double length0, double min_len, double max_len, double xacc,
                   int max_steps, double *opt_len, int *nevals);
+// the same in two halves: enqueue (result copied to pinned host memory), then wait and read
+int launch_newton_async(Session *s, double guess, double min_len, double max_len, double xacc,
+                        int max_steps);
+int newton_result(Session *s, double *opt_len, int *nevals);
 int launch_eigen(Session *s, const double *exch_upper, const double *freq);
+// the same for nsess sessions of one state count in one launch (inputs stacked per session)
+int launch_eigen_batch(Session *const *ss, int nsess, const double *exch_upper,
+                       const double *freq);
 int launch_unpack_partial(Session *s, int slot, double *d_out);
 // mixed precision (kernels_mixed.cu)
 int launch_prep_ops_mixed(Session *s, int nops);

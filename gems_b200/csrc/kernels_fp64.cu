@@ -746,6 +746,19 @@ int launch_from_buffer(Session *s, double length, double *lnl) {
 
 int launch_newton(Session *s, double guess, double min_len, double max_len, double xacc,
                   int max_steps, double *opt_len, int *nevals) {
+  if (int st = launch_newton_async(s, guess, min_len, max_len, xacc, max_steps)) return st;
+  return newton_result(s, opt_len, nevals);
+}
+
+int newton_result(Session *s, double *opt_len, int *nevals) {
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  *opt_len = s->h_result[0];
+  *nevals = (int)s->h_result[1];
+  return (int)s->h_result[2];
+}
+
+int launch_newton_async(Session *s, double guess, double min_len, double max_len, double xacc,
+                        int max_steps) {
   DevCtx c = s->ctx();
   const size_t smem = 3 * sizeof(double) * s->block;
   int dev = s->desc.device, nsm = 0, per_sm = 0;
@@ -778,10 +791,7 @@ int launch_newton(Session *s, double guess, double min_len, double max_len, doub
   if (int st = prof_end(s, 5, ev0)) return st;
   GEMS_CUDA(cudaMemcpyAsync(s->h_result, s->d_result, 3 * sizeof(double), cudaMemcpyDeviceToHost,
                             s->stream));
-  GEMS_CUDA(cudaStreamSynchronize(s->stream));
-  *opt_len = s->h_result[0];
-  *nevals = (int)s->h_result[1];
-  return (int)s->h_result[2];
+  return GEMS_OK;
 }
 
 int check_barrier_timeout(int device, int *status) {

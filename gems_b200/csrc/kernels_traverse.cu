@@ -1396,9 +1396,17 @@ int tuned4(const Session *s, bool mixed) {
   return it == g_tune.end() ? -1 : it->second;
 }
 
-// dynamic shared memory a kernel may take on this device: the opt-in maximum per block less
-// the kernel's static shared memory
-size_t max_dyn_smem(const void *fn, int device) {
+// dynamic shared memory a kernel may take on a device: the opt-in maximum per block less the
+// kernel's static shared memory.  Looked up once per (kernel, device), when the kernel's limit
+// attribute is also raised to it (an attribute of the kernel, shared by every host thread), so
+// that launches make no attribute calls.
+std::mutex g_smem_mu;
+std::map<std::pair<const void *, int>, size_t> g_smem;
+size_t max_dyn_smem(const void *fn, int device, size_t want) {
+  std::lock_guard<std::mutex> g(g_smem_mu);
+  auto key = std::make_pair(fn, device);
+  auto it = g_smem.find(key);
+  if (it != g_smem.end()) return it->second;
   int optin = 0;
   cudaFuncAttributes fa{};
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) !=
@@ -1407,7 +1415,14 @@ size_t max_dyn_smem(const void *fn, int device) {
     cudaGetLastError();
     return 0;
   }
-  return optin > (int)fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  const size_t lim = optin > (int)fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)std::min(want, lim)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  g_smem[key] = std::min(want, lim);
+  return g_smem[key];
 }
 
 int launch4(Session *s, bool mixed, int v, int nops, int p0, int p1, const EigPack<4> *E) {
@@ -1426,7 +1441,8 @@ int launch4(Session *s, bool mixed, int v, int nops, int p0, int p1, const EigPa
   auto usable = [&](const Variant4 &x) {
     if (!x.stack) return true;
     const void *f = kernel(x);
-    return f && smem_of(x, s->plan_depth) <= max_dyn_smem(f, s->desc.device);
+    return f && smem_of(x, s->plan_depth) <=
+                    max_dyn_smem(f, s->desc.device, smem_of(x, kPlanMaxPos));
   };
   if (!usable(all[v])) {
     v = 0;
@@ -1443,11 +1459,6 @@ int launch4(Session *s, bool mixed, int v, int nops, int p0, int p1, const EigPa
   if (var.stack) {
     int depth = s->plan_depth;
     const size_t smem = smem_of(var, depth);
-    // the limit is a per-kernel attribute shared by every thread of the process: always set to
-    // the largest size a plan may need
-    GEMS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)std::min(smem_of(var, kPlanMaxPos),
-                                                 max_dyn_smem(fn, s->desc.device))));
     EigPack<4> e{};
     if (E) e = *E;
     void *args[] = {&c, &ops, &nops, (void *)&s->d_opmats, &stride, &e, &p0, &p1, &depth};

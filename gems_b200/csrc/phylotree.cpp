@@ -312,21 +312,28 @@ struct Tree {
   }
 
   // PhyloTree::optimizeOneBranch (tree/phylotree.cpp:2620-2670) with the Newton loop of
-  // Optimization::minimizeNewton (utils/optimization.cpp:422-499) run on the device.
-  int optimize_one(int node1, int node2, int clear_lh, int max_nr) {
+  // Optimization::minimizeNewton (utils/optimization.cpp:422-499) run on the device, in two
+  // halves: the traversal, theta and Newton loop enqueued on the session's stream, then the
+  // result applied (the divergence check, the new length, clearReversePartialLh).
+  double pending_len = 0;
+  int optimize_begin(int node1, int node2, int max_nr) {
     const int k = find(node1, node2);
     if (k < 0) return GEMS_ERR_BAD_ARG;
     cur_u = node1;
     cur_k = k;
-    const double cur = len[node1 * 3 + k];
+    pending_len = len[node1 * 3 + k];
     theta_computed = false;
     int n = node2, d = node1;
     gems_branch br = branch(n, d);
     if (pool_status) return pool_status;
+    return gems_newton_branch_async(s, ops.data(), (int)ops.size(), &br, 1, min_bl, max_bl,
+                                    min_bl, max_nr);
+  }
+  int optimize_finish(int node1, int node2, int clear_lh) {
+    const double cur = pending_len;
     double optx = cur;
     int nev = 0;
-    int st = gems_newton_branch(s, ops.data(), (int)ops.size(), &br, 1, min_bl, max_bl, min_bl,
-                                max_nr, &optx, &nev);
+    int st = gems_newton_branch_wait(s, &optx, &nev);
     newton_evals = nev;
     if (st != GEMS_OK) return st;
     theta_computed = true;
@@ -342,6 +349,10 @@ struct Tree {
       clear_reverse(node2, node1);
     }
     return GEMS_OK;
+  }
+  int optimize_one(int node1, int node2, int clear_lh, int max_nr) {
+    if (int st = optimize_begin(node1, node2, max_nr)) return st;
+    return optimize_finish(node1, node2, clear_lh);
   }
 
   // PhyloTree::optimizeAllBranches(my_iterations, tolerance, maxNRStep)
@@ -377,6 +388,14 @@ struct Tree {
     }
     *out = tree_lh;
     return GEMS_OK;
+  }
+
+  // the branch order of optimizeAllBranches (computeBestTraversal, tree/phylotree.cpp:2710)
+  void best_traversal(std::vector<int> &n1, std::vector<int> &n2) const {
+    std::vector<int> h(nnode, 0);
+    const int far = far_leaf(0, -1, h);
+    far_leaf(far, -1, h);
+    preorder(far, -1, h, n1, n2);
   }
 
   // PhyloTree::doNNI (tree/phylotree.cpp:4059-4125): exchange subtree a (at u) with subtree b
@@ -462,6 +481,66 @@ struct Tree {
 }  // namespace
 
 struct gems_tree : public Tree {};
+
+namespace {
+
+// optimizeAllBranches on trees of one topology (ModelFinder's candidate models on one tree),
+// each tree exactly as gems_tree_optimize_all_branches runs it, in lock-step over the common
+// branch order: every tree's Newton loop on a branch is enqueued before any result is read,
+// so the candidates' device work overlaps
+int optimize_all_batch(gems_tree *const *ts, int n, int iterations, double tol, int max_nr,
+                       double *out) {
+  std::vector<int> n1, n2;
+  ts[0]->best_traversal(n1, n2);
+  std::vector<double> tree_lh(n, 0.0);
+  std::vector<char> active(n, 1);
+  std::vector<std::vector<double>> saved(n);
+  for (int i = 0; i < n; i++) {
+    if (int st = ts[i]->lh_branch(n2[0], n1[0], &tree_lh[i], nullptr)) return st;
+    saved[i].resize(ts[i]->nedges);
+  }
+  for (int it = 0; it < iterations; it++) {
+    bool any = false;
+    for (int i = 0; i < n; i++) {
+      if (!active[i]) continue;
+      any = true;
+      Tree &t = *ts[i];
+      for (int e = 0; e < t.nedges; e++) saved[i][e] = t.len[t.eu[e] * 3 + t.find(t.eu[e], t.ev[e])];
+    }
+    if (!any) break;
+    for (size_t j = 0; j < n1.size(); j++) {
+      for (int i = 0; i < n; i++)
+        if (active[i])
+          if (int st = ts[i]->optimize_begin(n1[j], n2[j], max_nr)) return st;
+      for (int i = 0; i < n; i++)
+        if (active[i])
+          if (int st = ts[i]->optimize_finish(n1[j], n2[j], 1)) return st;
+    }
+    for (int i = 0; i < n; i++) {
+      if (!active[i]) continue;
+      Tree &t = *ts[i];
+      double new_lh = 0;
+      if (int st = t.from_buffer(&new_lh)) return st;
+      if (new_lh < tree_lh[i] - tol * 0.1) {
+        std::fill(t.computed.begin(), t.computed.end(), 0);
+        t.theta_computed = false;
+        for (int e = 0; e < t.nedges; e++) t.set_len(t.eu[e], t.ev[e], saved[i][e]);
+        if (int st = t.compute_likelihood(&new_lh, nullptr)) return st;
+        tree_lh[i] = new_lh;
+        active[i] = 0;
+      } else if (tree_lh[i] <= new_lh && new_lh <= tree_lh[i] + tol) {
+        tree_lh[i] = new_lh;
+        active[i] = 0;
+      } else {
+        tree_lh[i] = new_lh;
+      }
+    }
+  }
+  for (int i = 0; i < n; i++) out[i] = tree_lh[i];
+  return GEMS_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -613,6 +692,18 @@ int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double toleran
                                     int max_nr_step, double *lnl) {
   if (!t || !lnl || iterations < 1 || max_nr_step < 1) return GEMS_ERR_BAD_ARG;
   return t->optimize_all(iterations, tolerance, max_nr_step, lnl);
+}
+
+int gems_tree_optimize_all_branches_batch(gems_tree *const *trees, int ntrees, int iterations,
+                                          double tolerance, int max_nr_step, double *lnl) {
+  if (!trees || ntrees < 1 || !lnl || iterations < 1 || max_nr_step < 1) return GEMS_ERR_BAD_ARG;
+  for (int i = 0; i < ntrees; i++) {
+    if (!trees[i]) return GEMS_ERR_BAD_ARG;
+    if (trees[i]->adj != trees[0]->adj || trees[i]->deg != trees[0]->deg) return GEMS_ERR_BAD_ARG;
+    for (int j = 0; j < i; j++)
+      if (trees[j] == trees[i] || trees[j]->s == trees[i]->s) return GEMS_ERR_BAD_ARG;
+  }
+  return optimize_all_batch(trees, ntrees, iterations, tolerance, max_nr_step, lnl);
 }
 
 int gems_tree_nni(gems_tree *t, int u, int v, int a, int b) {

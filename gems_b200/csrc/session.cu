@@ -663,6 +663,37 @@ int gems_set_model_from_rates(gems_session *s, const double *exch_upper, const d
   return upload_model(s, es.data(), es.data() + n, es.data() + n + n * n, rates, props);
 }
 
+int gems_set_model_from_rates_batch(gems_session *const *ss, int nsess, const double *exch_upper,
+                                    const double *freq, const double *rates,
+                                    const double *props) {
+  if (!ss || nsess < 1 || nsess > Session::kMaxBatch || !exch_upper || !freq || !rates || !props)
+    return GEMS_ERR_BAD_ARG;
+  for (int i = 0; i < nsess; i++) {
+    if (!ss[i] || ss[i]->desc.device != ss[0]->desc.device ||
+        ss[i]->desc.nstates != ss[0]->desc.nstates || ss[i]->desc.ncat != ss[0]->desc.ncat) {
+      set_error("batched models: sessions must share device, state and category counts");
+      return GEMS_ERR_BAD_ARG;
+    }
+    for (int j = 0; j < i; j++)
+      if (ss[j] == ss[i]) return GEMS_ERR_BAD_ARG;
+  }
+  const int n = ss[0]->desc.nstates, C = ss[0]->desc.ncat;
+  for (int i = 0; i < nsess * C; i++)
+    if (!(rates[i] >= 0) || !(props[i] >= 0)) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(ss[0]->desc.device));
+  std::vector<Session *> v(ss, ss + nsess);
+  if (int st = launch_eigen_batch(v.data(), nsess, exch_upper, freq)) return st;
+  std::vector<double> es((size_t)n + 2 * n * n);
+  for (int i = 0; i < nsess; i++) {
+    GEMS_CUDA(cudaMemcpy(es.data(), ss[i]->d_model, es.size() * sizeof(double),
+                         cudaMemcpyDeviceToHost));
+    if (int st = upload_model(ss[i], es.data(), es.data() + n, es.data() + n + n * n,
+                              rates + (size_t)i * C, props + (size_t)i * C))
+      return st;
+  }
+  return GEMS_OK;
+}
+
 int gems_get_eigensystem(gems_session *s, double *eval, double *evec, double *inv_evec) {
   if (!s || !s->model_set) return GEMS_ERR_STATE;
   const int n = s->desc.nstates;
@@ -923,11 +954,10 @@ int gems_lnl_from_buffer(gems_session *s, double length, double *lnl, double *pa
   return GEMS_OK;
 }
 
-int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
-                       int compute_theta, double min_len, double max_len, double xacc,
-                       int max_steps, double *opt_len, int *nevals) {
-  if (!s || !opt_len || (nops > 0 && !ops) || !(min_len >= 0) || !(max_len >= min_len) ||
-      max_steps < 1)
+int gems_newton_branch_async(gems_session *s, const gems_op *ops, int nops,
+                             const gems_branch *br, int compute_theta, double min_len,
+                             double max_len, double xacc, int max_steps) {
+  if (!s || (nops > 0 && !ops) || !(min_len >= 0) || !(max_len >= min_len) || max_steps < 1)
     return GEMS_ERR_BAD_ARG;
   GEMS_CUDA(cudaSetDevice(s->desc.device));
   int st = check_branch(s, br);
@@ -943,10 +973,26 @@ int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems
     set_error("theta not computed");
     return GEMS_ERR_STATE;
   }
+  return launch_newton_async(s, br->length, min_len, max_len, xacc, max_steps);
+}
+
+int gems_newton_branch_wait(gems_session *s, double *opt_len, int *nevals) {
+  if (!s || !opt_len) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
   int ne = 0;
-  st = launch_newton(s, br->length, min_len, max_len, xacc, max_steps, opt_len, &ne);
+  const int st = newton_result(s, opt_len, &ne);
   if (nevals) *nevals = ne;
   return st;
+}
+
+int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
+                       int compute_theta, double min_len, double max_len, double xacc,
+                       int max_steps, double *opt_len, int *nevals) {
+  if (!opt_len) return GEMS_ERR_BAD_ARG;
+  int st = gems_newton_branch_async(s, ops, nops, br, compute_theta, min_len, max_len, xacc,
+                                    max_steps);
+  if (st) return st;
+  return gems_newton_branch_wait(s, opt_len, nevals);
 }
 
 int gems_get_partial(gems_session *s, int slot, double *partial, uint16_t *scale) {

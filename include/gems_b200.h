@@ -133,6 +133,14 @@ int gems_set_model(gems_session *s, const double *eval, const double *evec,
  * model/modelmarkov.cpp:1389-1630).  exch_upper holds the n(n-1)/2 exchangeabilities. */
 int gems_set_model_from_rates(gems_session *s, const double *exch_upper, const double *freq,
                               const double *rates, const double *props);
+/* gems_set_model_from_rates for nsess sessions of one device, state count and category count
+ * (at most 128) with every eigendecomposition in one launch, one CTA per model: ModelFinder's
+ * candidate models (model/modelfactory.cpp:1263,1367,1558; main/phylotesting.cpp).  Inputs are
+ * stacked per session: exch_upper[nsess][n(n-1)/2], freq[nsess][n], rates[nsess][ncat],
+ * props[nsess][ncat].  No counterpart in the reference (one decomposition per model). */
+int gems_set_model_from_rates_batch(gems_session *const *sessions, int nsess,
+                                    const double *exch_upper, const double *freq,
+                                    const double *rates, const double *props);
 /* Copy back the eigensystem in use (for inspection). */
 int gems_get_eigensystem(gems_session *s, double *eval, double *evec, double *inv_evec);
 
@@ -198,6 +206,15 @@ int gems_lnl_from_buffer(gems_session *s, double length, double *lnl, double *pa
 int gems_newton_branch(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,
                        int compute_theta, double min_len, double max_len, double xacc,
                        int max_steps, double *opt_len, int *nevals);
+/* gems_newton_branch in two halves, so that the Newton loops of many sessions (ModelFinder's
+ * candidate models on one tree) run on their streams at the same time: _async enqueues the
+ * traversal, theta and the device Newton loop and returns; _wait waits for the session's stream
+ * and returns opt_len, nevals and the loop's status.  No counterpart in the reference (it
+ * optimises candidates one after the other). */
+int gems_newton_branch_async(gems_session *s, const gems_op *ops, int nops,
+                             const gems_branch *br, int compute_theta, double min_len,
+                             double max_len, double xacc, int max_steps);
+int gems_newton_branch_wait(gems_session *s, double *opt_len, int *nevals);
 
 /* ---- allocation-free evaluation ---- */
 /* No counterpart in the reference.  lnL at branch length `length` from a theta buffer the
@@ -320,6 +337,15 @@ int gems_tree_optimize_one_branch(gems_tree *t, int node1, int node2, int clear_
 /* optimizeAllBranches(my_iterations, tolerance, maxNRStep) (tree/phylotree.cpp:2724) */
 int gems_tree_optimize_all_branches(gems_tree *t, int iterations, double tolerance,
                                     int max_nr_step, double *lnl);
+/* optimizeAllBranches on ntrees trees of one topology (built from the same edge list, each on
+ * its own session: ModelFinder's candidate models on one tree, model/modelfactory.cpp:1263,1367
+ * and main/phylotesting.cpp), lnl[ntrees].  Each tree runs exactly the sequence of
+ * gems_tree_optimize_all_branches and ends with the same lengths and lnL; the trees move
+ * through the common branch order together and every tree's Newton loop on a branch is
+ * enqueued before any result is read, so their device work overlaps.  No counterpart in the
+ * reference (it optimises one candidate after the other). */
+int gems_tree_optimize_all_branches_batch(gems_tree *const *trees, int ntrees, int iterations,
+                                          double tolerance, int max_nr_step, double *lnl);
 /* PhyloTree::doNNI (tree/phylotree.cpp:4059-4125): swap subtree a (a neighbour of u) with
  * subtree b (a neighbour of v) across the internal branch (u, v); partials and lengths move
  * with their subtrees, the partials looking back across u or v are invalidated.  The edge

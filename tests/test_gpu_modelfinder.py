@@ -1,0 +1,93 @@
+"""ModelFinder's candidate models on one alignment and tree, batched: 16 candidates' rate
+matrices decomposed in one launch (gems_set_model_from_rates_batch) and their branch lengths
+optimised together (gems_tree_optimize_all_branches_batch).  Each candidate must end exactly
+where its own optimizeAllBranches ends (lnL and lengths, bit for bit); on the oracle's
+eigensystems the batch ends within the FP64 bar of the oracle's optimizeAllBranches."""
+import numpy as np
+import pytest
+
+from gems_b200 import PhyloTree, Session, optimize_all_branches_batch, set_models_from_rates, synth
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def candidates(n, k, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(k):
+        alpha = float(rng.uniform(0.3, 1.5))
+        if n == 4:
+            m = synth.dna_gtr(rng, 4, alpha)
+        elif n == 20:
+            m = synth.protein(rng, 4, alpha)
+        else:
+            m = synth.codon_gy(rng, 4, alpha)
+        out.append(m)
+    return out
+
+
+def open_sessions(tree, aln, models, precision, scaling):
+    ss = []
+    for m in models:
+        s = Session(tree.ntaxa, aln.npat, m.nstates, m.ncat, tree.ntaxa - 2, precision, scaling)
+        s.upload_tips(aln.patterns)
+        s.upload_patterns(aln.weights)
+        ss.append(s)
+    set_models_from_rates(ss, [m.exch_upper for m in models], [m.freq for m in models],
+                          [m.rates for m in models], [m.props for m in models])
+    return ss
+
+
+@pytest.mark.parametrize("n,k,precision,scaling", [(4, 16, "fp64", "norm"),
+                                                   (20, 8, "fp64", "norm"),
+                                                   (61, 6, "fp64", "safe"),
+                                                   (4, 16, "mixed", "norm")])
+def test_batched_candidates_match_one_by_one_and_oracle(gpu, n, k, precision, scaling):
+    truth = candidates(n, 1, 71 + n)[0]
+    tree = synth.random_tree(16, 0.12, 72 + n)
+    aln = synth.simulate(tree, truth, {4: 3000, 20: 1500, 61: 600}[n], 73 + n)
+    models = candidates(n, k, 74 + n)
+    # batched: one eigendecomposition launch, the optimisations overlapped
+    ss = open_sessions(tree, aln, models, precision, scaling)
+    trees = [PhyloTree(s, tree.eu, tree.ev, tree.length) for s in ss]
+    lnl_b = optimize_all_branches_batch(trees, 100, 0.001, 100)
+    # one by one, each on its own session with its own decomposition call
+    for i, m in enumerate(models):
+        s = Session(tree.ntaxa, aln.npat, n, m.ncat, tree.ntaxa - 2, precision, scaling)
+        s.upload_tips(aln.patterns)
+        s.upload_patterns(aln.weights)
+        s.set_model_from_rates(m.exch_upper, m.freq, m.rates, m.props)
+        one = PhyloTree(s, tree.eu, tree.ev, tree.length)
+        lnl_1 = one.optimizeAllBranches(100, 0.001, 100)
+        assert lnl_b[i] == lnl_1, (i, lnl_b[i], lnl_1)
+        np.testing.assert_array_equal(trees[i].getBranchLengths(), one.getBranchLengths())
+        one.close()
+        s.close()
+    for t, s in zip(trees, ss):
+        t.close()
+        s.close()
+
+
+@pytest.mark.parametrize("n,k", [(4, 16), (20, 6)])
+def test_batched_optimisation_matches_oracle(gpu, n, k):
+    """Candidates on the oracle's own eigensystems: every batched optimisation ends within the
+    FP64 bar of the oracle's optimizeAllBranches."""
+    truth = candidates(n, 1, 81 + n)[0]
+    tree = synth.random_tree(14, 0.1, 82 + n)
+    aln = synth.simulate(tree, truth, 2000 if n == 4 else 1000, 83 + n)
+    models = []
+    for m in candidates(n, k, 84 + n):
+        ev, v, iv = orc.eigensystem(m.exch_upper, m.freq)
+        models.append(synth.Model(n, m.exch_upper, m.freq, m.rates, m.props, ev, v, iv))
+    trees = [PhyloTree.from_case(tree, m, aln) for m in models]
+    lnl_b = optimize_all_branches_batch(trees, 100, 0.001, 100)
+    for i, m in enumerate(models):
+        ot = orc.OracleTree(tree, m, aln)
+        lo = ot.optimizeAllBranches(100, 0.001, 100)
+        assert abs(lnl_b[i] - lo) <= 1e-9 * abs(lo)
+        np.testing.assert_allclose(trees[i].getBranchLengths(), ot.getBranchLengths(),
+                                   rtol=1e-7, atol=1e-9)
+    for t in trees:
+        t.close()
+        t.session.close()

@@ -46,14 +46,21 @@ def test_admission_by_footprint(gpu):
     records, _ = srv.run(specs, cases, reqs)
     assert all(r is not None and not r.get("rejected") for r in records)
     check_same_as_alone(specs, cases, records)
-    # a budget below the largest footprint rejects exactly the sessions that cannot fit
+    # a budget below the largest footprint rejects exactly the sessions that cannot fit at one
+    # slot per internal node (pools off) ...
     budget = fps[-1] - 1
-    srv = serve.Server(workers=2, budget_bytes=budget)
+    srv = serve.Server(workers=2, budget_bytes=budget, memsave=False)
     records, _ = srv.run(specs, cases, reqs)
     for r, (_, sid) in zip(records, reqs):
         assert r is not None
         assert bool(r.get("rejected")) == (specs[sid].footprint(cases[sid][2].npat) > budget)
     assert any(r.get("rejected") for r in records)
+    # ... and with LM_MEM_SAVE pools that session is served from a pool, with the same results
+    srv = serve.Server(workers=2, budget_bytes=budget)
+    records, _ = srv.run(specs, cases, reqs)
+    assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
+    assert srv.pool_admissions > 0
+    check_same_as_alone(specs, cases, records)
 
 
 def test_eviction_keeps_results(gpu):
