@@ -63,18 +63,19 @@ struct DevCtx {
   size_t slot_scale;       // P * (safe ? C : 1)
 };
 
-// Layout of FP32 partials.  The 20- and 61-state mixed forms store each slot tile-major:
+// Layout of FP32 partials.  The 4-, 20- and 61-state mixed forms store each slot tile-major:
 //   [tile of 128 patterns][chunk = category * K + state / 4][128 rows][4 states]
-// with K = 5 (20 states) or 16 (61 states padded to 64, the pad stored as zeros).  This is
+// with K = 1 (4 states), 5 (20 states) or 16 (61 states padded to 64, the pad stored as zeros).  This is
 // the tensor-core operand layout: one contiguous block per (tile, slot) -- or per (tile, slot,
 // category) for 61 states -- so a tile moves with one bulk copy, and a warp's 32 rows of one
-// chunk are 512 contiguous bytes.  The 4-state form is pattern-major [P][C][n].
+// chunk are 512 contiguous bytes; for 4 states a thread that holds a pattern's C categories
+// stores C float4s, each instruction of a warp a contiguous 512-byte run.
 // mix_off<N>: offset of state 0 of category cc of pattern p within a slot; mix_cs<N>: floats
 // between consecutive 4-state chunks of that row; mix_k<N>: chunks per category (0: not tiled).
 constexpr int kMixTile = 128;
 template <int N>
 __host__ __device__ constexpr int mix_k() {
-  return N == 20 ? 5 : (N == 61 ? 16 : 0);
+  return N == 20 ? 5 : (N == 61 ? 16 : (N == 4 ? 1 : 0));
 }
 template <int N>
 __host__ __device__ inline size_t mix_off(const DevCtx &c, long p, int cc) {

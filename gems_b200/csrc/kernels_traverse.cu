@@ -642,230 +642,6 @@ struct Stack4 {
   static size_t bytes(int depth) { return (size_t)depth * PP * kThreads * (kVal + 2); }
 };
 
-// one child's message: L from the plan's source, then the op's transition applied
-template <typename R, bool SAFE, int PP>
-__device__ __forceinline__ void msg4s(const DevCtx &c, const EigPack<4> &E, int kind, int id,
-                                      int src, int pos, const Stack4<R, PP> &stk,
-                                      const R (&fwd)[PP][4], const int (&fwd_s)[PP],
-                                      const R *__restrict__ tabk, int side, const long (&p)[PP],
-                                      int gq, R (&v)[PP][4], int (&s)[PP]) {
-  const int C = c.C;
-  if constexpr (sizeof(R) == 4) {
-    const size_t nnC = (size_t)16 * C;
-    const float *Pm = tabk + side * nnC;
-    const float *leaf = tabk + 2 * nnC + (size_t)side * (c.unknown + 1) * c.block;
-    if (kind == GEMS_CHILD_TIP) {
-#pragma unroll
-      for (int u = 0; u < PP; u++) {
-        const int st = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
-        const float4 t = __ldg(reinterpret_cast<const float4 *>(leaf + (size_t)st * c.block) + gq);
-        v[u][0] = t.x, v[u][1] = t.y, v[u][2] = t.z, v[u][3] = t.w;
-        s[u] = 0;
-      }
-      return;
-    }
-    float L[PP][4];
-    if (src == kSrcFwd) {
-#pragma unroll
-      for (int u = 0; u < PP; u++) {
-#pragma unroll
-        for (int x = 0; x < 4; x++) L[u][x] = fwd[u][x];
-        s[u] = fwd_s[u];
-      }
-    } else if (src == kSrcStack) {
-#pragma unroll
-      for (int u = 0; u < PP; u++) stk.get(min(pos, stk.depth - 1), u, L[u], s[u]);
-    } else {
-      const float *base = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems;
-      const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
-#pragma unroll
-      for (int u = 0; u < PP; u++) {
-        const float4 t = __ldcg(reinterpret_cast<const float4 *>(base + mix_off<4>(c, p[u], gq)));
-        L[u][0] = t.x, L[u][1] = t.y, L[u][2] = t.z, L[u][3] = t.w;
-      }
-#pragma unroll
-      for (int u = 0; u < PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
-    }
-#pragma unroll
-    for (int x = 0; x < 4; x++) {
-      const float4 r = __ldg(reinterpret_cast<const float4 *>(Pm + ((size_t)x * C + gq) * 4));
-#pragma unroll
-      for (int u = 0; u < PP; u++)
-        v[u][x] = fmaf(r.w, L[u][3], fmaf(r.z, L[u][2], fmaf(r.y, L[u][1], fmaf(r.x, L[u][0], 0.f))));
-    }
-  } else {
-    const int blk = c.block;
-    const double *d = tabk + side * blk;
-    const double *leaf = tabk + 2 * blk + (size_t)side * (c.unknown + 1) * blk;
-    if (kind == GEMS_CHILD_TIP) {
-#pragma unroll
-      for (int u = 0; u < PP; u++) {
-        const int st = min((int)c.tips[(size_t)id * c.P + p[u]], c.unknown);
-        const double *lt = leaf + (size_t)st * blk + gq;
-#pragma unroll
-        for (int x = 0; x < 4; x++) v[u][x] = __ldg(lt + x * C);
-        s[u] = 0;
-      }
-      return;
-    }
-    double L[PP][4];
-    if (src == kSrcFwd) {
-#pragma unroll
-      for (int u = 0; u < PP; u++) {
-#pragma unroll
-        for (int x = 0; x < 4; x++) L[u][x] = fwd[u][x];
-        s[u] = fwd_s[u];
-      }
-    } else if (src == kSrcStack) {
-#pragma unroll
-      for (int u = 0; u < PP; u++) stk.get(min(pos, stk.depth - 1), u, L[u], s[u]);
-    } else {
-      const double *base = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
-      const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
-#pragma unroll
-      for (int u = 0; u < PP; u++) {
-        const double2 *s2 = reinterpret_cast<const double2 *>(base + (size_t)p[u] * blk + gq * 4);
-        const double2 a = __ldcg(s2), b = __ldcg(s2 + 1);
-        L[u][0] = a.x, L[u][1] = a.y, L[u][2] = b.x, L[u][3] = b.y;
-      }
-#pragma unroll
-      for (int u = 0; u < PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const double di = __ldg(d + i * C + gq);
-#pragma unroll
-      for (int u = 0; u < PP; u++) L[u][i] *= di;
-    }
-#pragma unroll
-    for (int u = 0; u < PP; u++)
-#pragma unroll
-      for (int x = 0; x < 4; x++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int i = 0; i < 4; i++) acc = fma(E.evec[x * 4 + i], L[u][i], acc);
-        v[u][x] = acc;
-      }
-  }
-}
-
-template <typename R, bool SAFE, int PP, int B>
-__global__ void __launch_bounds__(kThreads, B)
-    k_traverse4s(DevCtx c, const DevOp *__restrict__ ops, int nops, const R *__restrict__ tab,
-                 size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
-  extern __shared__ __align__(16) unsigned char stk_raw[];
-  const int G = c.G, C = c.C;
-  const int gl = threadIdx.x & (G - 1);
-  const int gq = gl < C ? gl : 0;  // loads of idle lanes stay inside the tables
-  const int per = kThreads / G;
-  const long pb = p0 + (long)blockIdx.x * per * PP + threadIdx.x / G;
-  long p[PP];
-  bool act[PP];
-#pragma unroll
-  for (int u = 0; u < PP; u++) {
-    const long q = pb + (long)u * per;
-    act[u] = q < p1 && gl < C;
-    p[u] = q < p1 ? q : p0;
-  }
-  const Stack4<R, PP> stk{stk_raw, depth};
-  R fwd[PP][4];
-  int fwd_s[PP];
-#pragma unroll
-  for (int u = 0; u < PP; u++) {
-    fwd_s[u] = 0;
-#pragma unroll
-    for (int x = 0; x < 4; x++) fwd[u][x] = R(0);
-  }
-  R *part = static_cast<R *>(c.partials);
-  __shared__ int4 s_ops[kOpChunk];
-  for (int k = 0; k < nops; k++) {
-    if ((k & (kOpChunk - 1)) == 0) {
-      const int nk = min(kOpChunk, nops - k);
-      __syncthreads();  // the previous chunk is no longer read
-      for (int i = threadIdx.x; i < nk; i += blockDim.x) {
-        const DevOp o = ops[k + i];
-        s_ops[i] = make_int4(o.dst_slot, o.l_id, o.r_id, o.pad_);
-      }
-      __syncthreads();
-    }
-    const int4 od = s_ops[k & (kOpChunk - 1)];
-    const int w = od.w;
-    const R *tk = tab + (size_t)k * stride;
-    const int lkind = plan_lkind(w), rkind = plan_rkind(w);
-    const bool tiptip = lkind == GEMS_CHILD_TIP && rkind == GEMS_CHILD_TIP;
-    R vl[PP][4], vr[PP][4];
-    int sl[PP], sr[PP];
-    msg4s<R, SAFE, PP>(c, E, lkind, od.y, plan_lsrc(w), plan_lpos(w), stk, fwd, fwd_s, tk, 0, p,
-                       gq, vl, sl);
-    msg4s<R, SAFE, PP>(c, E, rkind, od.z, plan_rsrc(w), plan_rpos(w), stk, fwd, fwd_s, tk, 1, p,
-                       gq, vr, sr);
-    const int outk = plan_out(w), opos = min(plan_opos(w), max(depth - 1, 0));
-#pragma unroll
-    for (int u = 0; u < PP; u++) {
-      R out[4];
-      R lh_max = R(0);
-      if constexpr (sizeof(R) == 4) {
-#pragma unroll
-        for (int x = 0; x < 4; x++) {
-          out[x] = vl[u][x] * vr[u][x];
-          lh_max = fmaxf(lh_max, out[x]);
-        }
-      } else {
-        double tmp[4];
-#pragma unroll
-        for (int x = 0; x < 4; x++) tmp[x] = vl[u][x] * vr[u][x];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          double acc = 0.0;
-#pragma unroll
-          for (int x = 0; x < 4; x++) acc = fma(E.inv[j * 4 + x], tmp[x], acc);
-          out[j] = acc;
-          lh_max = fmax(lh_max, fabs(acc));
-        }
-      }
-      if (!act[u]) lh_max = R(0);
-      if constexpr (!SAFE) {
-        if constexpr (sizeof(R) == 4) lh_max = group_maxf(lh_max, G);
-        else lh_max = group_max(lh_max, G);
-      }
-      int s_out = sl[u] + sr[u];
-      bool thr;
-      if constexpr (sizeof(R) == 4) thr = lh_max < kScaleThrF;
-      else thr = lh_max < kScaleThr;
-      if (act[u] && !tiptip && thr && c.invar[p[u]] == 0.0) {
-#pragma unroll
-        for (int x = 0; x < 4; x++) {
-          if constexpr (sizeof(R) == 4) out[x] *= 18446744073709551616.0f;  // 2^64
-          else out[x] = ldexp(out[x], kScaleExp);
-        }
-        s_out += 1;
-      }
-      if (act[u]) {
-        if constexpr (sizeof(R) == 4) {
-          __stcs(reinterpret_cast<float4 *>(part + (size_t)od.x * c.slot_elems +
-                                            mix_off<4>(c, p[u], gl)),
-                 make_float4(out[0], out[1], out[2], out[3]));
-        } else {
-          double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)od.x * c.slot_elems +
-                                                    (size_t)p[u] * c.block + gl * 4);
-          __stcs(d2, make_double2(out[0], out[1]));
-          __stcs(d2 + 1, make_double2(out[2], out[3]));
-        }
-        uint16_t *sc = c.scale + (size_t)od.x * c.slot_scale;
-        if (SAFE)
-          sc[(size_t)p[u] * C + gl] = (uint16_t)s_out;
-        else if (gl == 0)
-          sc[p[u]] = (uint16_t)s_out;
-      }
-      if (outk == kSrcStack) stk.put(opos, u, out, s_out);
-#pragma unroll
-      for (int x = 0; x < 4; x++) fwd[u][x] = out[x];
-      fwd_s[u] = s_out;
-    }
-    __syncwarp();
-  }
-}
-
 // ---------------------------------------------------------------------------------------
 // 4 states, one thread per pattern (all C categories in registers), with the traversal plan.
 // Every per-op input a thread needs sits in shared memory before the op starts: the op
@@ -890,7 +666,10 @@ constexpr int kChunkP = 8;      // ops staged together
 template <typename R, int C>
 struct Tab4P {
   static constexpr int kH = sizeof(R) == 4 ? 2 * 16 * C : 2 * 4 * C;  // head elements
-  static constexpr int kLeaf = 5 * 4 * C;                             // leaf elements per side
+  // a staged leaf row: 4C values, FP32 rows padded by 4 floats so that the rows of different
+  // states start in different bank groups (lanes of a warp read the rows of their own states)
+  static constexpr int kRow = sizeof(R) == 4 ? 4 * C + 4 : 4 * C;
+  static constexpr int kLeaf = 5 * kRow;  // leaf elements per side
   static constexpr int kBytes = (kH + 2 * kLeaf) * (int)sizeof(R);
 };
 
@@ -943,24 +722,25 @@ __device__ __forceinline__ void stage4p(StageP<R, C> &st, int b, const DevCtx &c
     cp_async8(reinterpret_cast<char *>(&st.desc[b][i]) + 8 * r,
               reinterpret_cast<const char *>(ops + k0 + i) + 8 * r);
   }
-  constexpr int kPieces = T::kBytes / 16;
+  constexpr int kPieces = (T::kH + 10 * 4 * C) * (int)sizeof(R) / 16;  // pieces copied
   for (int q = tid; q < nk * kPieces; q += kThreadsP) {
     const int i = q / kPieces, r = q - i * kPieces;
     const R *tk = tab + (size_t)(k0 + i) * stride;
-    const char *src;
     const int blk = 4 * C, u1 = c.unknown + 1;
-    const int off = 16 * r;  // byte offset inside the staged table
-    constexpr int hB = T::kH * (int)sizeof(R), rowsB = 16 * C * (int)sizeof(R),
-                  rowB = 4 * C * (int)sizeof(R);
-    if (off < hB) {
-      src = reinterpret_cast<const char *>(tk) + off;
+    constexpr int hP = T::kH * (int)sizeof(R) / 16, rowP = 4 * C * (int)sizeof(R) / 16;
+    const char *src;
+    int dst;  // byte offset inside the staged table
+    if (r < hP) {
+      src = reinterpret_cast<const char *>(tk) + 16 * r;
+      dst = 16 * r;
     } else {
-      const int o = off - hB, side = o / (rowsB + rowB), w = o - side * (rowsB + rowB);
+      const int o = r - hP, side = o / (5 * rowP), rr = o - side * 5 * rowP, row = rr / rowP,
+                pc = rr - row * rowP;
       const R *leaf = tk + T::kH + (size_t)side * u1 * blk;
-      src = w < rowsB ? reinterpret_cast<const char *>(leaf) + w
-                      : reinterpret_cast<const char *>(leaf + (size_t)c.unknown * blk) + (w - rowsB);
+      src = reinterpret_cast<const char *>(leaf + (size_t)(row < 4 ? row : c.unknown) * blk) + 16 * pc;
+      dst = (T::kH + side * T::kLeaf + row * T::kRow) * (int)sizeof(R) + 16 * pc;
     }
-    cp_async16(st.tab[b][i] + 16 * r, src);
+    cp_async16(st.tab[b][i] + dst, src);
   }
   if (tips_async) {
     // 8 pieces per tip side; pieces past the padded pattern count are not copied (never read)
@@ -974,12 +754,21 @@ __device__ __forceinline__ void stage4p(StageP<R, C> &st, int b, const DevCtx &c
   }
 }
 
+// a pattern's category 0 within a slot: FP32 tile-major (mix_off<4>), FP64 pattern-major
+template <typename R>
+__device__ __forceinline__ size_t pat_off(const DevCtx &c, long p) {
+  if constexpr (sizeof(R) == 4) return mix_off<4>(c, p, 0);
+  else return (size_t)p * c.block;
+}
+
 // 16-byte moves of a thread's C x 4 values (FP32: one float4 per category; FP64: two double2)
+// FP32: src points at category 0 of the pattern in the tile-major slot, categories mix_cs<4>()
+// floats apart; FP64: the pattern's C x 4 values are contiguous
 template <int C>
 __device__ __forceinline__ void ld_cg(const float *src, float (&v)[C][4]) {
 #pragma unroll
   for (int q = 0; q < C; q++) {
-    const float4 t = __ldcg(reinterpret_cast<const float4 *>(src) + q);
+    const float4 t = __ldcg(reinterpret_cast<const float4 *>(src + (size_t)q * mix_cs<4>()));
     v[q][0] = t.x, v[q][1] = t.y, v[q][2] = t.z, v[q][3] = t.w;
   }
 }
@@ -995,7 +784,8 @@ template <int C>
 __device__ __forceinline__ void st_cs(float *dst, const float (&v)[C][4]) {
 #pragma unroll
   for (int q = 0; q < C; q++)
-    __stcs(reinterpret_cast<float4 *>(dst) + q, make_float4(v[q][0], v[q][1], v[q][2], v[q][3]));
+    __stcs(reinterpret_cast<float4 *>(dst + (size_t)q * mix_cs<4>()),
+           make_float4(v[q][0], v[q][1], v[q][2], v[q][3]));
 }
 template <int C>
 __device__ __forceinline__ void st_cs(double *dst, const double (&v)[C][4]) {
@@ -1036,15 +826,39 @@ __device__ __forceinline__ void sm_get(const unsigned char *base, double (&v)[C]
   }
 }
 
+// the fields of an op a thread uses, and its tip bytes (0 for a partial child)
+struct OpFetch {
+  int w, l_id, r_id, dst, tb[2];
+};
+__device__ __forceinline__ OpFetch fetch4p(const DevOp &o, const uint8_t (&tips)[2][kThreadsP],
+                                           bool tips_async, const DevCtx &c, long p) {
+  OpFetch f;
+  f.w = o.pad_;
+  f.l_id = o.l_id;
+  f.r_id = o.r_id;
+  f.dst = o.dst_slot;
+  f.tb[0] = f.tb[1] = 0;
+  if (plan_lkind(f.w) == GEMS_CHILD_TIP)
+    f.tb[0] = tips_async ? tips[0][threadIdx.x] : c.tips[(size_t)f.l_id * c.P + p];
+  if (plan_rkind(f.w) == GEMS_CHILD_TIP)
+    f.tb[1] = tips_async ? tips[1][threadIdx.x] : c.tips[(size_t)f.r_id * c.P + p];
+  return f;
+}
+
+// the plan's stack of one thread: positions 0 and 1 in registers (the common ones: positions
+// are handed out lowest first), deeper ones in shared memory
+constexpr int kRegPos = 2;
 template <typename R, int C>
 struct StackP {
   unsigned char *base;
-  int depth;
+  int depth;  // positions held in shared memory (plan depth - kRegPos)
   static constexpr int kEntry = 4 * C * (int)sizeof(R);  // value bytes of one thread's entry
   __device__ __forceinline__ uint16_t *scs() const {
     return reinterpret_cast<uint16_t *>(base + (size_t)depth * kEntry * kThreadsP);
   }
-  static size_t bytes(int depth) { return (size_t)depth * kThreadsP * (kEntry + 2 * C); }
+  static size_t bytes(int plan_depth) {
+    return (size_t)std::max(plan_depth - kRegPos, 0) * kThreadsP * (kEntry + 2 * C);
+  }
   // counters: C per entry under SAFE scaling, the first one only under NORM (all are equal)
   template <bool SAFE>
   __device__ __forceinline__ void put(int pos, const R (&v)[C][4], const int (&sc)[C]) const {
@@ -1071,6 +885,8 @@ template <typename R, bool SAFE, int C>
 __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int kind, int id,
                                       int src, int pos, const StackP<R, C> &stk,
                                       const R (&fwd)[C][4], const int (&fwd_s)[C],
+                                      const R (&r0)[C][4], const int (&r0s)[C],
+                                      const R (&r1)[C][4], const int (&r1s)[C],
                                       const unsigned char *__restrict__ tabS,
                                       const R *__restrict__ tk, int side, int tipbyte, long p,
                                       R (&v)[C][4], int (&s)[C]) {
@@ -1082,7 +898,7 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
     if constexpr (sizeof(R) == 4) {
       if (st < 4 || st == c.unknown) {
         const float4 *row = reinterpret_cast<const float4 *>(tabS) +
-                            (T::kH + side * T::kLeaf + (st < 4 ? st : 4) * 4 * C) / 4;
+                            (T::kH + side * T::kLeaf + (st < 4 ? st : 4) * T::kRow) / 4;
 #pragma unroll
         for (int cc = 0; cc < C; cc++) {
           const float4 t = row[cc];
@@ -1110,7 +926,7 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
       const double *row;
       if (st < 4 || st == c.unknown) {
         row = reinterpret_cast<const double *>(tabS) + T::kH + side * T::kLeaf +
-              (st < 4 ? st : 4) * blk;
+              (st < 4 ? st : 4) * T::kRow;
 #pragma unroll
         for (int x = 0; x < 4; x++)
 #pragma unroll
@@ -1133,10 +949,19 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
       for (int x = 0; x < 4; x++) L[cc][x] = fwd[cc][x];
       s[cc] = fwd_s[cc];
     }
+  } else if (src == kSrcStack && pos < kRegPos) {
+    const R(&rv)[C][4] = pos == 0 ? r0 : r1;
+    const int(&rs)[C] = pos == 0 ? r0s : r1s;
+#pragma unroll
+    for (int cc = 0; cc < C; cc++) {
+#pragma unroll
+      for (int x = 0; x < 4; x++) L[cc][x] = rv[cc][x];
+      s[cc] = rs[cc];
+    }
   } else if (src == kSrcStack) {
-    stk.template get<SAFE>(min(pos, stk.depth - 1), L, s);
+    stk.template get<SAFE>(min(pos - kRegPos, stk.depth - 1), L, s);
   } else {
-    ld_cg<C>(static_cast<const R *>(c.partials) + (size_t)id * c.slot_elems + (size_t)p * (4 * C),
+    ld_cg<C>(static_cast<const R *>(c.partials) + (size_t)id * c.slot_elems + pat_off<R>(c, p),
              L);
     const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
     if (SAFE) {
@@ -1181,7 +1006,15 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
                  size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
   extern __shared__ __align__(16) unsigned char smem_p[];
   StageP<R, C> &st = *reinterpret_cast<StageP<R, C> *>(smem_p);
-  const StackP<R, C> stk{smem_p + sizeof(StageP<R, C>), depth};
+  const StackP<R, C> stk{smem_p + sizeof(StageP<R, C>), max(depth - kRegPos, 0)};
+  R r0[C][4], r1[C][4];
+  int r0s[C], r1s[C];
+#pragma unroll
+  for (int cc = 0; cc < C; cc++) {
+    r0s[cc] = r1s[cc] = 0;
+#pragma unroll
+    for (int x = 0; x < 4; x++) r0[cc][x] = r1[cc][x] = R(0);
+  }
   const long pbase = p0 + (long)blockIdx.x * kThreadsP;
   const long pq = pbase + threadIdx.x;
   const bool act = pq < p1;
@@ -1206,23 +1039,21 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
     cp_async_commit();
     cp_async_wait1();  // this chunk's copies are done (the next chunk's may still fly)
     __syncthreads();
+    // an op's descriptor fields and tip bytes are fetched while the previous op computes, so
+    // that the chain descriptor -> tip byte -> leaf row is off each op's critical path
+    OpFetch cur = fetch4p(st.desc[b][0], st.tips[b][0], tips_async, c, p), nxt{};
     for (int i = 0; i < nk; i++) {
-      const DevOp &o = st.desc[b][i];
-      const int w = o.pad_;
+      if (i + 1 < nk) nxt = fetch4p(st.desc[b][i + 1], st.tips[b][i + 1], tips_async, c, p);
+      const int w = cur.w;
       const int lkind = plan_lkind(w), rkind = plan_rkind(w);
       const bool tiptip = lkind == GEMS_CHILD_TIP && rkind == GEMS_CHILD_TIP;
       const R *tk = tab + (size_t)(k0 + i) * stride;
-      int tb[2] = {0, 0};
-      if (lkind == GEMS_CHILD_TIP)
-        tb[0] = tips_async ? st.tips[b][i][0][threadIdx.x] : c.tips[(size_t)o.l_id * c.P + p];
-      if (rkind == GEMS_CHILD_TIP)
-        tb[1] = tips_async ? st.tips[b][i][1][threadIdx.x] : c.tips[(size_t)o.r_id * c.P + p];
       R vl[C][4], vr[C][4];
       int sl[C], sr[C];
-      msg4p<R, SAFE, C>(c, E, lkind, o.l_id, plan_lsrc(w), plan_lpos(w), stk, fwd, fwd_s,
-                        st.tab[b][i], tk, 0, tb[0], p, vl, sl);
-      msg4p<R, SAFE, C>(c, E, rkind, o.r_id, plan_rsrc(w), plan_rpos(w), stk, fwd, fwd_s,
-                        st.tab[b][i], tk, 1, tb[1], p, vr, sr);
+      msg4p<R, SAFE, C>(c, E, lkind, cur.l_id, plan_lsrc(w), plan_lpos(w), stk, fwd, fwd_s, r0,
+                        r0s, r1, r1s, st.tab[b][i], tk, 0, cur.tb[0], p, vl, sl);
+      msg4p<R, SAFE, C>(c, E, rkind, cur.r_id, plan_rsrc(w), plan_rpos(w), stk, fwd, fwd_s, r0,
+                        r0s, r1, r1s, st.tab[b][i], tk, 1, cur.tb[1], p, vr, sr);
       R out[C][4];
       R mx[C];
 #pragma unroll
@@ -1287,8 +1118,8 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
         for (int cc = 0; cc < C; cc++) so[cc] = s0;
       }
       if (act) {
-        st_cs<C>(part + (size_t)o.dst_slot * c.slot_elems + (size_t)p * (4 * C), out);
-        uint16_t *sc = c.scale + (size_t)o.dst_slot * c.slot_scale;
+        st_cs<C>(part + (size_t)cur.dst * c.slot_elems + pat_off<R>(c, p), out);
+        uint16_t *sc = c.scale + (size_t)cur.dst * c.slot_scale;
         if (SAFE) {
 #pragma unroll
           for (int cc = 0; cc < C; cc++) sc[(size_t)p * C + cc] = (uint16_t)so[cc];
@@ -1296,13 +1127,329 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
           sc[p] = (uint16_t)so[0];
         }
       }
-      if (plan_out(w) == kSrcStack)
-        stk.template put<SAFE>(min(plan_opos(w), max(depth - 1, 0)), out, so);
+      if (plan_out(w) == kSrcStack) {
+        const int op_pos = plan_opos(w);
+        if (op_pos == 0 || op_pos == 1) {
+#pragma unroll
+          for (int cc = 0; cc < C; cc++) {
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+              if (op_pos == 0) r0[cc][x] = out[cc][x];
+              else r1[cc][x] = out[cc][x];
+            }
+            if (op_pos == 0) r0s[cc] = so[cc];
+            else r1s[cc] = so[cc];
+          }
+        } else {
+          stk.template put<SAFE>(min(op_pos - kRegPos, max(stk.depth - 1, 0)), out, so);
+        }
+      }
 #pragma unroll
       for (int cc = 0; cc < C; cc++) {
 #pragma unroll
         for (int x = 0; x < 4; x++) fwd[cc][x] = out[cc][x];
         fwd_s[cc] = so[cc];
+      }
+      cur = nxt;
+    }
+    __syncthreads();  // buffer b is refilled two chunks on
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// 4 states, a lane per category (G lanes a pattern, PP patterns a lane group), with the
+// traversal plan and every per-op input staged in shared memory one chunk of kChunkP ops ahead
+// (as k_traverse4p): op descriptors, op tables (head and the leaf rows of A, C, G, T and the
+// unknown state) and the tip bytes of the CTA's patterns.  Lane c applies its category's
+// transition: FP64 d_c (*) L then evec, FP32 the rows of P_c; the tip message is the lane's part
+// of the staged leaf row (ambiguity codes read the global table).  Same arithmetic and order as
+// k_traverse_f64x / k_traverse_mix4: bit-identical values.
+// ---------------------------------------------------------------------------------------
+struct StageQ {  // byte offsets of the regions of the dynamic shared memory
+  int tab_bytes, npb;  // bytes of one staged op table; patterns of the CTA
+  size_t desc, tab, tips, stack;
+  __host__ __device__ static size_t up16(size_t x) { return (x + 15) & ~(size_t)15; }
+  __host__ __device__ StageQ(bool fp64, int C, int npb_) : npb(npb_) {
+    const int kH = fp64 ? 8 * C : 32 * C, kLeaf = 20 * C;
+    tab_bytes = (kH + 2 * kLeaf) * (fp64 ? 8 : 4);
+    desc = 0;
+    tab = up16(desc + 2 * kChunkP * sizeof(DevOp));
+    tips = up16(tab + (size_t)2 * kChunkP * tab_bytes);
+    stack = up16(tips + (size_t)2 * kChunkP * 2 * npb);
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ void stage4q(unsigned char *sm, const StageQ &L, int b,
+                                        const DevCtx &c, const DevOp *__restrict__ ops,
+                                        const R *__restrict__ tab, size_t stride, int k0, int nk,
+                                        long pbase, bool tips_async) {
+  const int tid = threadIdx.x, nt = blockDim.x, C = c.C, blk = 4 * C, u1 = c.unknown + 1;
+  constexpr int kDescPieces = sizeof(DevOp) / 8;
+  DevOp *desc = reinterpret_cast<DevOp *>(sm + L.desc) + b * kChunkP;
+  for (int q = tid; q < kDescPieces * nk; q += nt) {
+    const int i = q / kDescPieces, r = q - i * kDescPieces;
+    cp_async8(reinterpret_cast<char *>(desc + i) + 8 * r,
+              reinterpret_cast<const char *>(ops + k0 + i) + 8 * r);
+  }
+  const int pieces = L.tab_bytes / 16;
+  const int hB = (sizeof(R) == 4 ? 32 * C : 8 * C) * (int)sizeof(R);
+  const int rowsB = 16 * C * (int)sizeof(R), rowB = 4 * C * (int)sizeof(R);
+  unsigned char *tb = sm + L.tab + (size_t)b * kChunkP * L.tab_bytes;
+  for (int q = tid; q < nk * pieces; q += nt) {
+    const int i = q / pieces, r = q - i * pieces, off = 16 * r;
+    const R *tk = tab + (size_t)(k0 + i) * stride;
+    const char *src;
+    if (off < hB) {
+      src = reinterpret_cast<const char *>(tk) + off;
+    } else {
+      const int o = off - hB, side = o / (rowsB + rowB), w = o - side * (rowsB + rowB);
+      const R *leaf = tk + hB / (int)sizeof(R) + (size_t)side * u1 * blk;
+      src = w < rowsB ? reinterpret_cast<const char *>(leaf) + w
+                      : reinterpret_cast<const char *>(leaf + (size_t)c.unknown * blk) + (w - rowsB);
+    }
+    cp_async16(tb + (size_t)i * L.tab_bytes + off, src);
+  }
+  if (tips_async) {
+    const int per_side = L.npb / 16;
+    uint8_t *tp = sm + L.tips + (size_t)b * kChunkP * 2 * L.npb;
+    for (int q = tid; q < nk * 2 * per_side; q += nt) {
+      const int i = q / (2 * per_side), rem = q - i * 2 * per_side, sd = rem / per_side,
+                r = rem - sd * per_side;
+      const DevOp &o = ops[k0 + i];
+      const int kind = sd ? o.r_kind : o.l_kind, id = sd ? o.r_id : o.l_id;
+      if (kind != GEMS_CHILD_TIP || pbase + 16 * r >= c.P) continue;
+      cp_async16(tp + ((size_t)i * 2 + sd) * L.npb + 16 * r,
+                 c.tips + (size_t)id * c.P + pbase + 16 * r);
+    }
+  }
+}
+
+// a lane's message for one child: L from the plan's source, its category's transition applied
+template <typename R, bool SAFE, int PP>
+__device__ __forceinline__ void msg4q(const DevCtx &c, const EigPack<4> &E, int kind, int id,
+                                      int src, int pos, const Stack4<R, PP> &stk,
+                                      const R (&fwd)[PP][4], const int (&fwd_s)[PP],
+                                      const unsigned char *__restrict__ tabS,
+                                      const R *__restrict__ tk, int side, const int (&tb)[PP],
+                                      const long (&p)[PP], int gq, R (&v)[PP][4], int (&s)[PP]) {
+  const int C = c.C, blk = 4 * C;
+  const int kH = sizeof(R) == 4 ? 32 * C : 8 * C, kLeaf = 20 * C;
+  if (kind == GEMS_CHILD_TIP) {
+#pragma unroll
+    for (int u = 0; u < PP; u++) {
+      const int st = min(tb[u], c.unknown);
+      s[u] = 0;
+      if (st < 4 || st == c.unknown) {
+        const R *row = reinterpret_cast<const R *>(tabS) + kH + side * kLeaf +
+                       (st < 4 ? st : 4) * blk;
+        if constexpr (sizeof(R) == 4) {  // [c][x]
+          const float4 t = reinterpret_cast<const float4 *>(row)[gq];
+          v[u][0] = t.x, v[u][1] = t.y, v[u][2] = t.z, v[u][3] = t.w;
+        } else {  // [x][c]
+#pragma unroll
+          for (int x = 0; x < 4; x++) v[u][x] = row[x * C + gq];
+        }
+      } else {
+        const R *leaf = tk + kH + (size_t)side * (c.unknown + 1) * blk + (size_t)st * blk;
+        if constexpr (sizeof(R) == 4) {
+          const float4 t = __ldg(reinterpret_cast<const float4 *>(leaf) + gq);
+          v[u][0] = t.x, v[u][1] = t.y, v[u][2] = t.z, v[u][3] = t.w;
+        } else {
+#pragma unroll
+          for (int x = 0; x < 4; x++) v[u][x] = __ldg(leaf + x * C + gq);
+        }
+      }
+    }
+    return;
+  }
+  R L[PP][4];
+  if (src == kSrcFwd) {
+#pragma unroll
+    for (int u = 0; u < PP; u++) {
+#pragma unroll
+      for (int x = 0; x < 4; x++) L[u][x] = fwd[u][x];
+      s[u] = fwd_s[u];
+    }
+  } else if (src == kSrcStack) {
+#pragma unroll
+    for (int u = 0; u < PP; u++) stk.get(min(pos, stk.depth - 1), u, L[u], s[u]);
+  } else {
+    const R *base = static_cast<const R *>(c.partials) + (size_t)id * c.slot_elems;
+    const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
+#pragma unroll
+    for (int u = 0; u < PP; u++) {
+      if constexpr (sizeof(R) == 4) {
+        const float4 t = __ldcg(reinterpret_cast<const float4 *>(base + mix_off<4>(c, p[u], gq)));
+        L[u][0] = t.x, L[u][1] = t.y, L[u][2] = t.z, L[u][3] = t.w;
+      } else {
+        const double2 *s2 = reinterpret_cast<const double2 *>(base + (size_t)p[u] * blk + gq * 4);
+        const double2 a = __ldcg(s2), b2 = __ldcg(s2 + 1);
+        L[u][0] = a.x, L[u][1] = a.y, L[u][2] = b2.x, L[u][3] = b2.y;
+      }
+      s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
+    }
+  }
+  if constexpr (sizeof(R) == 4) {
+    const float4 *P4 = reinterpret_cast<const float4 *>(tabS) + side * 4 * C;
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const float4 r = P4[x * C + gq];
+#pragma unroll
+      for (int u = 0; u < PP; u++)
+        v[u][x] = fmaf(r.w, L[u][3], fmaf(r.z, L[u][2], fmaf(r.y, L[u][1], fmaf(r.x, L[u][0], 0.f))));
+    }
+  } else {
+    const double *d = reinterpret_cast<const double *>(tabS) + side * 4 * C;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const double di = d[i * C + gq];
+#pragma unroll
+      for (int u = 0; u < PP; u++) L[u][i] *= di;
+    }
+#pragma unroll
+    for (int u = 0; u < PP; u++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc = fma(E.evec[x * 4 + i], L[u][i], acc);
+        v[u][x] = acc;
+      }
+  }
+}
+
+template <typename R, bool SAFE, int PP, int B>
+__global__ void __launch_bounds__(kThreads, B)
+    k_traverse4q(DevCtx c, const DevOp *__restrict__ ops, int nops, const R *__restrict__ tab,
+                 size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
+  extern __shared__ __align__(16) unsigned char smem_q[];
+  const int G = c.G, C = c.C;
+  const int gl = threadIdx.x & (G - 1);
+  const int gq = gl < C ? gl : 0;  // loads of idle lanes stay inside the tables
+  const int per = kThreads / G;
+  const StageQ L(sizeof(R) == 8, C, per * PP);
+  const long pbase = p0 + (long)blockIdx.x * per * PP;
+  const bool tips_async = (pbase & 15) == 0;
+  long p[PP];
+  bool act[PP];
+  int toff[PP];  // the pattern's byte in the staged tip rows
+#pragma unroll
+  for (int u = 0; u < PP; u++) {
+    toff[u] = u * per + threadIdx.x / G;
+    const long q = pbase + toff[u];
+    act[u] = q < p1 && gl < C;
+    p[u] = q < p1 ? q : p0;
+  }
+  const Stack4<R, PP> stk{smem_q + L.stack, depth};
+  R fwd[PP][4];
+  int fwd_s[PP];
+#pragma unroll
+  for (int u = 0; u < PP; u++) {
+    fwd_s[u] = 0;
+#pragma unroll
+    for (int x = 0; x < 4; x++) fwd[u][x] = R(0);
+  }
+  R *part = static_cast<R *>(c.partials);
+  stage4q<R>(smem_q, L, 0, c, ops, tab, stride, 0, min(kChunkP, nops), pbase, tips_async);
+  cp_async_commit();
+  for (int k0 = 0; k0 < nops; k0 += kChunkP) {
+    const int b = (k0 / kChunkP) & 1, nk = min(kChunkP, nops - k0);
+    if (k0 + kChunkP < nops)
+      stage4q<R>(smem_q, L, b ^ 1, c, ops, tab, stride, k0 + kChunkP,
+                 min(kChunkP, nops - k0 - kChunkP), pbase, tips_async);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const DevOp *desc = reinterpret_cast<const DevOp *>(smem_q + L.desc) + b * kChunkP;
+    const unsigned char *tabs = smem_q + L.tab + (size_t)b * kChunkP * L.tab_bytes;
+    const uint8_t *tips = smem_q + L.tips + (size_t)b * kChunkP * 2 * L.npb;
+    for (int i = 0; i < nk; i++) {
+      const DevOp &o = desc[i];
+      const int w = o.pad_;
+      const int lkind = plan_lkind(w), rkind = plan_rkind(w);
+      const bool tiptip = lkind == GEMS_CHILD_TIP && rkind == GEMS_CHILD_TIP;
+      const R *tk = tab + (size_t)(k0 + i) * stride;
+      const unsigned char *tabS = tabs + (size_t)i * L.tab_bytes;
+      int tbl[PP], tbr[PP];
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+        tbl[u] = tbr[u] = 0;
+        if (lkind == GEMS_CHILD_TIP)
+          tbl[u] = tips_async ? tips[(size_t)(2 * i) * L.npb + toff[u]]
+                              : c.tips[(size_t)o.l_id * c.P + p[u]];
+        if (rkind == GEMS_CHILD_TIP)
+          tbr[u] = tips_async ? tips[(size_t)(2 * i + 1) * L.npb + toff[u]]
+                              : c.tips[(size_t)o.r_id * c.P + p[u]];
+      }
+      R vl[PP][4], vr[PP][4];
+      int sl[PP], sr[PP];
+      msg4q<R, SAFE, PP>(c, E, lkind, o.l_id, plan_lsrc(w), plan_lpos(w), stk, fwd, fwd_s, tabS,
+                         tk, 0, tbl, p, gq, vl, sl);
+      msg4q<R, SAFE, PP>(c, E, rkind, o.r_id, plan_rsrc(w), plan_rpos(w), stk, fwd, fwd_s, tabS,
+                         tk, 1, tbr, p, gq, vr, sr);
+      const int outk = plan_out(w), opos = min(plan_opos(w), max(depth - 1, 0));
+#pragma unroll
+      for (int u = 0; u < PP; u++) {
+        R out[4];
+        R lh_max = R(0);
+        if constexpr (sizeof(R) == 4) {
+#pragma unroll
+          for (int x = 0; x < 4; x++) {
+            out[x] = vl[u][x] * vr[u][x];
+            lh_max = fmaxf(lh_max, out[x]);
+          }
+        } else {
+          double tmp[4];
+#pragma unroll
+          for (int x = 0; x < 4; x++) tmp[x] = vl[u][x] * vr[u][x];
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            double acc = 0.0;
+#pragma unroll
+            for (int x = 0; x < 4; x++) acc = fma(E.inv[j * 4 + x], tmp[x], acc);
+            out[j] = acc;
+            lh_max = fmax(lh_max, fabs(acc));
+          }
+        }
+        if (!act[u]) lh_max = R(0);
+        if constexpr (!SAFE) {
+          if constexpr (sizeof(R) == 4) lh_max = group_maxf(lh_max, G);
+          else lh_max = group_max(lh_max, G);
+        }
+        int s_out = sl[u] + sr[u];
+        bool thr;
+        if constexpr (sizeof(R) == 4) thr = lh_max < kScaleThrF;
+        else thr = lh_max < kScaleThr;
+        if (act[u] && !tiptip && thr && c.invar[p[u]] == 0.0) {
+#pragma unroll
+          for (int x = 0; x < 4; x++) {
+            if constexpr (sizeof(R) == 4) out[x] *= 18446744073709551616.0f;  // 2^64
+            else out[x] = ldexp(out[x], kScaleExp);
+          }
+          s_out += 1;
+        }
+        if (act[u]) {
+          if constexpr (sizeof(R) == 4) {
+            __stcs(reinterpret_cast<float4 *>(part + (size_t)o.dst_slot * c.slot_elems +
+                                              mix_off<4>(c, p[u], gl)),
+                   make_float4(out[0], out[1], out[2], out[3]));
+          } else {
+            double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)o.dst_slot * c.slot_elems +
+                                                      (size_t)p[u] * c.block + gl * 4);
+            __stcs(d2, make_double2(out[0], out[1]));
+            __stcs(d2 + 1, make_double2(out[2], out[3]));
+          }
+          uint16_t *sc = c.scale + (size_t)o.dst_slot * c.slot_scale;
+          if (SAFE)
+            sc[(size_t)p[u] * C + gl] = (uint16_t)s_out;
+          else if (gl == 0)
+            sc[p[u]] = (uint16_t)s_out;
+        }
+        if (outk == kSrcStack) stk.put(opos, u, out, s_out);
+#pragma unroll
+        for (int x = 0; x < 4; x++) fwd[u][x] = out[x];
+        fwd_s[u] = s_out;
       }
     }
     __syncthreads();  // buffer b is refilled two chunks on
@@ -1326,7 +1473,7 @@ struct Variant4 {
   int pp, blocks;
   const void *fn[2];  // [safe]
   bool stack;         // plan-driven kernel: takes the plan depth, dynamic smem
-  size_t (*smem)(int depth);
+  size_t (*smem)(int depth, int C, int G);
   // one thread per pattern (k_traverse4p): kernels and shared memory by category count
   bool per_pattern = false;
   const void *fnC[2][4] = {};       // [safe][C = 1, 2, 4, 8]
@@ -1342,11 +1489,15 @@ Variant4 f64_variant() {
   return {PP, B, {(const void *)k_traverse_f64x<false, PP, B>, (const void *)k_traverse_f64x<true, PP, B>},
           false, nullptr};
 }
+template <typename R, int PP>
+size_t smem4q(int depth, int C, int G) {
+  return StageQ(sizeof(R) == 8, C, kThreads / G * PP).stack + Stack4<R, PP>::bytes(depth);
+}
 template <typename R, int PP, int B>
-Variant4 stack_variant() {
+Variant4 staged_variant() {
   return {PP, B,
-          {(const void *)k_traverse4s<R, false, PP, B>, (const void *)k_traverse4s<R, true, PP, B>},
-          true, &Stack4<R, PP>::bytes};
+          {(const void *)k_traverse4q<R, false, PP, B>, (const void *)k_traverse4q<R, true, PP, B>},
+          true, &smem4q<R, PP>};
 }
 template <typename R, int C>
 size_t smem4p(int depth) {
@@ -1370,14 +1521,14 @@ Variant4 pattern_variant() {
 }
 int cat_index(int C) { return C == 1 ? 0 : C == 2 ? 1 : C == 4 ? 2 : C == 8 ? 3 : -1; }
 const Variant4 *variants4(bool mixed, int *n) {
-  static const Variant4 mix[] = {pattern_variant<float>(),      stack_variant<float, 2, 4>(),
-                                 stack_variant<float, 1, 6>(),  stack_variant<float, 4, 2>(),
-                                 mix_variant<2, 5>(),           mix_variant<2, 6>(),
-                                 mix_variant<4, 3>(),           mix_variant<1, 8>()};
-  static const Variant4 f64[] = {pattern_variant<double>(),     stack_variant<double, 1, 4>(),
-                                 stack_variant<double, 2, 3>(), f64_variant<2, 4>(),
-                                 f64_variant<3, 3>(),           f64_variant<1, 6>()};
-  *n = mixed ? 8 : 6;
+  static const Variant4 mix[] = {pattern_variant<float>(),        staged_variant<float, 2, 4>(),
+                                 staged_variant<float, 1, 6>(),   mix_variant<2, 5>(),
+                                 mix_variant<2, 6>(),             mix_variant<4, 3>(),
+                                 mix_variant<1, 8>()};
+  static const Variant4 f64[] = {staged_variant<double, 1, 4>(),  staged_variant<double, 2, 3>(),
+                                 pattern_variant<double>(),       f64_variant<2, 4>(),
+                                 f64_variant<3, 3>(),             f64_variant<1, 6>()};
+  *n = mixed ? 7 : 6;
   return mixed ? mix : f64;
 }
 constexpr long long kTuneMinWork = 1ll << 22;  // patterns x ops below which no tuning is done
@@ -1434,7 +1585,7 @@ int launch4(Session *s, bool mixed, int v, int nops, int p0, int p1, const EigPa
     return x.per_pattern ? (ci >= 0 ? x.fnC[safe][ci] : nullptr) : x.fn[safe];
   };
   auto smem_of = [&](const Variant4 &x, int depth) -> size_t {
-    return x.per_pattern ? x.smemC[ci](depth) : x.smem(depth);
+    return x.per_pattern ? x.smemC[ci](depth) : x.smem(depth, s->desc.ncat, s->G);
   };
   // a variant that cannot run this session (categories without an instance, a plan deeper than
   // its shared memory) hands over to the first variant that reads children from global memory
@@ -1590,7 +1741,7 @@ int traverse_v2_wave_patterns(const Session *s) {
     } else if (!var.per_pattern) {
       fn = var.fn[safe];
       per_block *= var.pp;
-      if (var.stack) smem = var.smem(s->plan_depth);
+      if (var.stack) smem = var.smem(s->plan_depth, s->desc.ncat, s->G);
     } else {
       return 0;
     }

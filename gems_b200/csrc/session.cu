@@ -124,9 +124,10 @@ static Sizes compute_sizes(const gems_session_desc &d) {
   const size_t elem = d.precision == GEMS_PREC_MIXED ? sizeof(float) : sizeof(double);
   // 20- and 61-state mixed partials are tile-major in 128-pattern tiles (the tensor-core
   // layout; 61 states padded to 64)
-  z.tiled = (d.nstates == 20 || d.nstates == 61) && d.precision == GEMS_PREC_MIXED;
+  z.tiled = (d.nstates == 4 || d.nstates == 20 || d.nstates == 61) &&
+            d.precision == GEMS_PREC_MIXED;
   z.slot_elems = z.tiled ? (P + kMixTile - 1) / kMixTile * kMixTile * d.ncat *
-                               (d.nstates == 20 ? 20 : 64)
+                               (d.nstates == 61 ? 64 : d.nstates)
                          : P * blk;
   z.partial_bytes = (size_t)d.nslots * z.slot_elems * elem;
   z.scale_bytes = (size_t)d.nslots * P * (d.scaling == GEMS_SCALE_SAFE ? d.ncat : 1) * 2;
@@ -1016,7 +1017,8 @@ int gems_get_partial(gems_session *s, int slot, double *partial, uint16_t *scale
         for (int cc = 0; cc < s->desc.ncat; cc++) {
           for (int x = 0; x < nst; x++) {
             const size_t o =
-                !s->tiled ? (size_t)p * blk + (size_t)cc * nst + x
+                !s->tiled   ? (size_t)p * blk + (size_t)cc * nst + x
+                : nst == 4  ? mix_off<4>(c, p, cc) + x
                 : nst == 20 ? mix_off<20>(c, p, cc) + (size_t)(x / 4) * mix_cs<20>() + x % 4
                             : mix_off<61>(c, p, cc) + (size_t)(x / 4) * mix_cs<61>() + x % 4;
             partial[(size_t)p * blk + (size_t)cc * nst + x] = tmp[o];

@@ -29,11 +29,11 @@ def computed_partials(gt, tree):
     return out
 
 
-# shapes: the plan-driven kernels first (one thread per pattern, then FP64: 2, mixed: 3 with a
-# lane per category), then the kernels that read
-# every child from global memory
+# shapes: the plan-driven kernels with staged inputs first (mixed: one thread per pattern, then
+# two with a lane per category; FP64: two with a lane per category, then one thread per
+# pattern), then the kernels that read every child and table from global memory
 @pytest.mark.parametrize("scaling", ["norm", "safe"])
-@pytest.mark.parametrize("precision,nshapes", [("fp64", 6), ("mixed", 8)])
+@pytest.mark.parametrize("precision,nshapes", [("fp64", 6), ("mixed", 7)])
 def test_every_shape_gives_the_same_values(gpu, precision, nshapes, scaling):
     tree, model, aln = case(11, 40, 5001)
     ref = None

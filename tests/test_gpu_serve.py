@@ -69,7 +69,7 @@ def test_eviction_keeps_results(gpu):
     results stay bit-identical to running it alone."""
     specs, reqs, cases = workload(nsess=6, nreq=40, seed=6)
     fps = sorted(s.footprint(cases[s.sid][2].npat) for s in specs)
-    srv = serve.Server(workers=3, budget_bytes=fps[-1] + fps[0])
+    srv = serve.Server(workers=3, budget_bytes=fps[-1] + fps[0], memsave=False)
     records, _ = srv.run(specs, cases, reqs)
     assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
     assert srv.evictions > 0
