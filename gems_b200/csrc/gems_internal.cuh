@@ -92,6 +92,54 @@ __host__ __device__ constexpr int mix_cs() {
   return mix_k<N>() > 0 ? kMixTile * 4 : 4;
 }
 
+// Layout of FP64 partials: pattern-major [P][C][n], except 4 states, tile-major like the mixed
+// forms so that stores coalesce:
+//   [tile of 128 patterns][category][half h: states 2h, 2h + 1][128 rows][2 doubles]
+// (a lane's or thread's 16-byte store of one half, and a warp's store of a category half is one
+// contiguous run).  f64_off: offset of a (pattern, category) row's states x, x + 1 (x even).
+constexpr int kF64Half = kMixTile * 2;  // doubles between the two halves of a row
+template <int N>
+__host__ __device__ inline size_t f64_off(const DevCtx &c, long p, int cc, int x = 0) {
+  if constexpr (N == 4) {
+    return (size_t)(p / kMixTile) * ((size_t)c.C * 2 * kF64Half) +
+           (size_t)(2 * cc + (x >> 1)) * kF64Half + (size_t)(p % kMixTile) * 2 + (x & 1);
+  } else {
+    return (size_t)p * c.block + (size_t)cc * N + x;
+  }
+}
+
+#ifdef __CUDACC__
+// a (pattern, category) row of an FP64 partial slot, in 16-byte pieces (N even) or doubles
+template <int N>
+__device__ __forceinline__ void load_row(const double *__restrict__ slot, const DevCtx &c, long p,
+                                         int cc, double (&v)[N]) {
+  if constexpr (N % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < N; i += 2) {
+      const double2 t = __ldcg(reinterpret_cast<const double2 *>(slot + f64_off<N>(c, p, cc, i)));
+      v[i] = t.x, v[i + 1] = t.y;
+    }
+  } else {
+    const double *src = slot + f64_off<N>(c, p, cc);
+#pragma unroll
+    for (int i = 0; i < N; i++) v[i] = __ldcg(src + i);
+  }
+}
+template <int N>
+__device__ __forceinline__ void store_row(double *__restrict__ slot, const DevCtx &c, long p,
+                                          int cc, const double (&v)[N]) {
+  if constexpr (N % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < N; i += 2)
+      *reinterpret_cast<double2 *>(slot + f64_off<N>(c, p, cc, i)) = make_double2(v[i], v[i + 1]);
+  } else {
+    double *dst = slot + f64_off<N>(c, p, cc);
+#pragma unroll
+    for (int i = 0; i < N; i++) dst[i] = v[i];
+  }
+}
+#endif
+
 // one session of a batched tensor-core launch (sessions that share the op list: the same tree
 // and lengths, e.g. candidate models on one alignment)
 struct TcJob {
@@ -212,7 +260,6 @@ int launch_eigen(Session *s, const double *exch_upper, const double *freq);
 // the same for nsess sessions of one state count in one launch (inputs stacked per session)
 int launch_eigen_batch(Session *const *ss, int nsess, const double *exch_upper,
                        const double *freq);
-int launch_unpack_partial(Session *s, int slot, double *d_out);
 // mixed precision (kernels_mixed.cu)
 int launch_prep_ops_mixed(Session *s, int nops);
 int launch_traverse_mixed(Session *s, int nops, int p0, int p1);

@@ -138,10 +138,9 @@ __device__ __forceinline__ void child_msg(const DevCtx &c, int kind, int id, con
     for (int x = 0; x < N; x++) v[x] = __ldg(lt + x);
     s = 0;
   } else {
-    const double *src = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems +
-                        (size_t)p * c.block + gl * N;
+    const double *slot = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
     double L[N];
-    load_vec<N>(src, L);
+    load_row<N>(slot, c, p, gl, L);
     const double *e = E + (size_t)gl * N * N;
 #pragma unroll
     for (int x = 0; x < N; x++) {
@@ -204,7 +203,7 @@ __global__ void __launch_bounds__(kThreads) k_traverse(DevCtx c, const DevOp *__
         for (int j = 0; j < N; j++) out[j] = ldexp(out[j], kScaleExp);
         s_out += 1;
       }
-      store_vec<N>(part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * c.block + gl * N, out);
+      store_row<N>(part + (size_t)op.dst_slot * c.slot_elems, c, p, gl, out);
       uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
       if (SAFE)
         sc[(size_t)p * C + gl] = (uint16_t)s_out;
@@ -247,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_branch_lnl(DevCtx c, gems_branch b
   int ssum = 0;
   if (act) {
     double dad[N];
-    load_vec<N>(part + (size_t)br.dad_slot * c.slot_elems + (size_t)p * c.block + gl * N, dad);
+    load_row<N>(part + (size_t)br.dad_slot * c.slot_elems, c, p, gl, dad);
     const uint16_t *sd = c.scale + (size_t)br.dad_slot * c.slot_scale;
     ssum = SAFE ? sd[(size_t)p * c.C + gl] : sd[p];
     if (br.node_kind == GEMS_CHILD_TIP) {
@@ -257,7 +256,7 @@ __global__ void __launch_bounds__(kThreads) k_branch_lnl(DevCtx c, gems_branch b
       for (int i = 0; i < N; i++) lh_cat = fma(__ldg(nt + i), dad[i], lh_cat);
     } else {
       double nd[N];
-      load_vec<N>(part + (size_t)br.node_id * c.slot_elems + (size_t)p * c.block + gl * N, nd);
+      load_row<N>(part + (size_t)br.node_id * c.slot_elems, c, p, gl, nd);
       const double *val = bt + gl * N;
 #pragma unroll
       for (int i = 0; i < N; i++) lh_cat = fma(__ldg(val + i) * nd[i], dad[i], lh_cat);
@@ -323,7 +322,7 @@ __global__ void __launch_bounds__(kThreads) k_theta(DevCtx c, gems_branch br) {
   int ssum = 0;
   if (act) {
     double dad[N];
-    load_vec<N>(part + (size_t)br.dad_slot * c.slot_elems + (size_t)p * c.block + gl * N, dad);
+    load_row<N>(part + (size_t)br.dad_slot * c.slot_elems, c, p, gl, dad);
     const uint16_t *sd = c.scale + (size_t)br.dad_slot * c.slot_scale;
     ssum = SAFE ? sd[(size_t)p * c.C + gl] : sd[p];
     if (br.node_kind == GEMS_CHILD_TIP) {
@@ -333,7 +332,7 @@ __global__ void __launch_bounds__(kThreads) k_theta(DevCtx c, gems_branch br) {
       for (int i = 0; i < N; i++) th[i] = __ldg(tp + i) * dad[i];
     } else {
       double nd[N];
-      load_vec<N>(part + (size_t)br.node_id * c.slot_elems + (size_t)p * c.block + gl * N, nd);
+      load_row<N>(part + (size_t)br.node_id * c.slot_elems, c, p, gl, nd);
 #pragma unroll
       for (int i = 0; i < N; i++) th[i] = nd[i] * dad[i];
       const uint16_t *sn = c.scale + (size_t)br.node_id * c.slot_scale;
@@ -612,11 +611,6 @@ __global__ void __launch_bounds__(kThreads) k_newton(DevCtx c, double guess, dou
 }
 
 // unpack a FP64 slot (identity copy; layout is already pattern-major)
-__global__ void k_copy_slot(const double *src, double *dst, size_t n) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    dst[i] = src[i];
-}
 
 inline int grid_for(const Session *s) {
   const long groups = s->P;
@@ -816,12 +810,5 @@ int check_barrier_timeout(int device, int *status) {
   return GEMS_OK;
 }
 
-int launch_unpack_partial(Session *s, int slot, double *d_out) {
-  const double *src = static_cast<const double *>(s->d_partials) + (size_t)slot * s->P * s->block;
-  k_copy_slot<<<256, 256, 0, s->stream>>>(src, d_out, (size_t)s->P * s->block);
-  s->launches++;
-  GEMS_CUDA(cudaGetLastError());
-  return GEMS_OK;
-}
 
 }  // namespace gems

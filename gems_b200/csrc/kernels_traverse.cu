@@ -115,21 +115,8 @@ __device__ __forceinline__ void msg_f64(const DevCtx &c, const EigPack<N> &E, in
     for (int x = 0; x < N; x++) v[x] = __ldg(lt + x * C);
     s = 0;
   } else {
-    const double *src = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems +
-                        (size_t)p * c.block + gl * N;
     double L[N];
-    if constexpr (N % 2 == 0) {
-      const double2 *s2 = reinterpret_cast<const double2 *>(src);
-#pragma unroll
-      for (int i = 0; i < N / 2; i++) {
-        const double2 t = __ldcg(s2 + i);
-        L[2 * i] = t.x;
-        L[2 * i + 1] = t.y;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < N; i++) L[i] = __ldcg(src + i);
-    }
+    load_row<N>(static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems, c, p, gl, L);
 #pragma unroll
     for (int i = 0; i < N; i++) L[i] *= __ldg(d + i * C + gl);
 #pragma unroll
@@ -192,15 +179,7 @@ __global__ void __launch_bounds__(kThreads) k_traverse_f64(DevCtx c, const DevOp
         for (int j = 0; j < N; j++) out[j] = ldexp(out[j], kScaleExp);
         s_out += 1;
       }
-      double *dst = part + (size_t)op.dst_slot * c.slot_elems + (size_t)p * blk + gl * N;
-      if constexpr (N % 2 == 0) {
-        double2 *d2 = reinterpret_cast<double2 *>(dst);
-#pragma unroll
-        for (int i = 0; i < N / 2; i++) d2[i] = make_double2(out[2 * i], out[2 * i + 1]);
-      } else {
-#pragma unroll
-        for (int i = 0; i < N; i++) dst[i] = out[i];
-      }
+      store_row<N>(part + (size_t)op.dst_slot * c.slot_elems, c, p, gl, out);
       uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
       if (SAFE)
         sc[(size_t)p * C + gl] = (uint16_t)s_out;
@@ -238,14 +217,7 @@ __device__ __forceinline__ void msg_f64_4(const DevCtx &c, const EigPack<4> &E, 
     const double *base = static_cast<const double *>(c.partials) + (size_t)id * c.slot_elems;
     double L[PP][4];
 #pragma unroll
-    for (int u = 0; u < PP; u++) {
-      const double2 *s2 = reinterpret_cast<const double2 *>(base + (size_t)p[u] * c.block + gq * 4);
-      const double2 a = __ldcg(s2), b = __ldcg(s2 + 1);
-      L[u][0] = a.x;
-      L[u][1] = a.y;
-      L[u][2] = b.x;
-      L[u][3] = b.y;
-    }
+    for (int u = 0; u < PP; u++) load_row<4>(base, c, p[u], gq, L[u]);
     const uint16_t *sc = c.scale + (size_t)id * c.slot_scale;
 #pragma unroll
     for (int u = 0; u < PP; u++) s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
@@ -320,10 +292,7 @@ __global__ void __launch_bounds__(kThreads, B)
           for (int j = 0; j < 4; j++) out[j] = ldexp(out[j], kScaleExp);
           s_out += 1;
         }
-        double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)op.dst_slot * c.slot_elems +
-                                                  (size_t)p[u] * blk + gl * 4);
-        d2[0] = make_double2(out[0], out[1]);
-        d2[1] = make_double2(out[2], out[3]);
+        store_row<4>(part + (size_t)op.dst_slot * c.slot_elems, c, p[u], gl, out);
         uint16_t *sc = c.scale + (size_t)op.dst_slot * c.slot_scale;
         if (SAFE)
           sc[(size_t)p[u] * C + gl] = (uint16_t)s_out;
@@ -758,12 +727,12 @@ __device__ __forceinline__ void stage4p(StageP<R, C> &st, int b, const DevCtx &c
 template <typename R>
 __device__ __forceinline__ size_t pat_off(const DevCtx &c, long p) {
   if constexpr (sizeof(R) == 4) return mix_off<4>(c, p, 0);
-  else return (size_t)p * c.block;
+  else return f64_off<4>(c, p, 0, 0);
 }
 
 // 16-byte moves of a thread's C x 4 values (FP32: one float4 per category; FP64: two double2)
-// FP32: src points at category 0 of the pattern in the tile-major slot, categories mix_cs<4>()
-// floats apart; FP64: the pattern's C x 4 values are contiguous
+// src points at category 0 of the pattern in the tile-major slot: FP32 categories mix_cs<4>()
+// floats apart; FP64 (f64_off) in halves kF64Half doubles apart, a category two halves
 template <int C>
 __device__ __forceinline__ void ld_cg(const float *src, float (&v)[C][4]) {
 #pragma unroll
@@ -775,8 +744,8 @@ __device__ __forceinline__ void ld_cg(const float *src, float (&v)[C][4]) {
 template <int C>
 __device__ __forceinline__ void ld_cg(const double *src, double (&v)[C][4]) {
 #pragma unroll
-  for (int q = 0; q < 2 * C; q++) {
-    const double2 t = __ldcg(reinterpret_cast<const double2 *>(src) + q);
+  for (int q = 0; q < 2 * C; q++) {  // piece q: category q / 2, half q % 2 (f64_off)
+    const double2 t = __ldcg(reinterpret_cast<const double2 *>(src + (size_t)q * kF64Half));
     v[q >> 1][2 * (q & 1)] = t.x, v[q >> 1][2 * (q & 1) + 1] = t.y;
   }
 }
@@ -791,7 +760,7 @@ template <int C>
 __device__ __forceinline__ void st_cs(double *dst, const double (&v)[C][4]) {
 #pragma unroll
   for (int q = 0; q < 2 * C; q++)
-    __stcs(reinterpret_cast<double2 *>(dst) + q,
+    __stcs(reinterpret_cast<double2 *>(dst + (size_t)q * kF64Half),
            make_double2(v[q >> 1][2 * (q & 1)], v[q >> 1][2 * (q & 1) + 1]));
 }
 // shared memory, [piece][thread] (a warp's accesses are 512 contiguous bytes)
@@ -845,19 +814,23 @@ __device__ __forceinline__ OpFetch fetch4p(const DevOp &o, const uint8_t (&tips)
   return f;
 }
 
-// the plan's stack of one thread: positions 0 and 1 in registers (the common ones: positions
-// are handed out lowest first), deeper ones in shared memory
-constexpr int kRegPos = 2;
+// the plan's stack of one thread: FP32 positions 0 and 1 in registers (the common ones:
+// positions are handed out lowest first), deeper ones in shared memory; FP64 all in shared
+// memory (its registers already limit the resident blocks)
+template <typename R>
+__host__ __device__ constexpr int reg_pos() {
+  return sizeof(R) == 4 ? 2 : 0;
+}
 template <typename R, int C>
 struct StackP {
   unsigned char *base;
-  int depth;  // positions held in shared memory (plan depth - kRegPos)
+  int depth;  // positions held in shared memory (plan depth - reg_pos<R>())
   static constexpr int kEntry = 4 * C * (int)sizeof(R);  // value bytes of one thread's entry
   __device__ __forceinline__ uint16_t *scs() const {
     return reinterpret_cast<uint16_t *>(base + (size_t)depth * kEntry * kThreadsP);
   }
   static size_t bytes(int plan_depth) {
-    return (size_t)std::max(plan_depth - kRegPos, 0) * kThreadsP * (kEntry + 2 * C);
+    return (size_t)std::max(plan_depth - reg_pos<R>(), 0) * kThreadsP * (kEntry + 2 * C);
   }
   // counters: C per entry under SAFE scaling, the first one only under NORM (all are equal)
   template <bool SAFE>
@@ -949,7 +922,7 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
       for (int x = 0; x < 4; x++) L[cc][x] = fwd[cc][x];
       s[cc] = fwd_s[cc];
     }
-  } else if (src == kSrcStack && pos < kRegPos) {
+  } else if (src == kSrcStack && pos < reg_pos<R>()) {
     const R(&rv)[C][4] = pos == 0 ? r0 : r1;
     const int(&rs)[C] = pos == 0 ? r0s : r1s;
 #pragma unroll
@@ -959,7 +932,7 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
       s[cc] = rs[cc];
     }
   } else if (src == kSrcStack) {
-    stk.template get<SAFE>(min(pos - kRegPos, stk.depth - 1), L, s);
+    stk.template get<SAFE>(min(pos - reg_pos<R>(), stk.depth - 1), L, s);
   } else {
     ld_cg<C>(static_cast<const R *>(c.partials) + (size_t)id * c.slot_elems + pat_off<R>(c, p),
              L);
@@ -1006,7 +979,7 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
                  size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
   extern __shared__ __align__(16) unsigned char smem_p[];
   StageP<R, C> &st = *reinterpret_cast<StageP<R, C> *>(smem_p);
-  const StackP<R, C> stk{smem_p + sizeof(StageP<R, C>), max(depth - kRegPos, 0)};
+  const StackP<R, C> stk{smem_p + sizeof(StageP<R, C>), max(depth - reg_pos<R>(), 0)};
   R r0[C][4], r1[C][4];
   int r0s[C], r1s[C];
 #pragma unroll
@@ -1129,7 +1102,7 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
       }
       if (plan_out(w) == kSrcStack) {
         const int op_pos = plan_opos(w);
-        if (op_pos == 0 || op_pos == 1) {
+        if (op_pos < reg_pos<R>()) {
 #pragma unroll
           for (int cc = 0; cc < C; cc++) {
 #pragma unroll
@@ -1141,7 +1114,7 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
             else r1s[cc] = so[cc];
           }
         } else {
-          stk.template put<SAFE>(min(op_pos - kRegPos, max(stk.depth - 1, 0)), out, so);
+          stk.template put<SAFE>(min(op_pos - reg_pos<R>(), max(stk.depth - 1, 0)), out, so);
         }
       }
 #pragma unroll
@@ -1283,9 +1256,7 @@ __device__ __forceinline__ void msg4q(const DevCtx &c, const EigPack<4> &E, int 
         const float4 t = __ldcg(reinterpret_cast<const float4 *>(base + mix_off<4>(c, p[u], gq)));
         L[u][0] = t.x, L[u][1] = t.y, L[u][2] = t.z, L[u][3] = t.w;
       } else {
-        const double2 *s2 = reinterpret_cast<const double2 *>(base + (size_t)p[u] * blk + gq * 4);
-        const double2 a = __ldcg(s2), b2 = __ldcg(s2 + 1);
-        L[u][0] = a.x, L[u][1] = a.y, L[u][2] = b2.x, L[u][3] = b2.y;
+        load_row<4>(base, c, p[u], gq, L[u]);
       }
       s[u] = SAFE ? sc[(size_t)p[u] * C + gq] : sc[p[u]];
     }
@@ -1435,10 +1406,11 @@ __global__ void __launch_bounds__(kThreads, B)
                                               mix_off<4>(c, p[u], gl)),
                    make_float4(out[0], out[1], out[2], out[3]));
           } else {
-            double2 *d2 = reinterpret_cast<double2 *>(part + (size_t)o.dst_slot * c.slot_elems +
-                                                      (size_t)p[u] * c.block + gl * 4);
-            __stcs(d2, make_double2(out[0], out[1]));
-            __stcs(d2 + 1, make_double2(out[2], out[3]));
+            double *slot = part + (size_t)o.dst_slot * c.slot_elems;
+            __stcs(reinterpret_cast<double2 *>(slot + f64_off<4>(c, p[u], gl, 0)),
+                   make_double2(out[0], out[1]));
+            __stcs(reinterpret_cast<double2 *>(slot + f64_off<4>(c, p[u], gl, 2)),
+                   make_double2(out[2], out[3]));
           }
           uint16_t *sc = c.scale + (size_t)o.dst_slot * c.slot_scale;
           if (SAFE)
@@ -1525,8 +1497,8 @@ const Variant4 *variants4(bool mixed, int *n) {
                                  staged_variant<float, 1, 6>(),   mix_variant<2, 5>(),
                                  mix_variant<2, 6>(),             mix_variant<4, 3>(),
                                  mix_variant<1, 8>()};
-  static const Variant4 f64[] = {staged_variant<double, 1, 4>(),  staged_variant<double, 2, 3>(),
-                                 pattern_variant<double>(),       f64_variant<2, 4>(),
+  static const Variant4 f64[] = {pattern_variant<double>(),       staged_variant<double, 1, 4>(),
+                                 staged_variant<double, 2, 3>(),  f64_variant<2, 4>(),
                                  f64_variant<3, 3>(),             f64_variant<1, 6>()};
   *n = mixed ? 7 : 6;
   return mixed ? mix : f64;

@@ -128,7 +128,8 @@ static Sizes compute_sizes(const gems_session_desc &d) {
             d.precision == GEMS_PREC_MIXED;
   z.slot_elems = z.tiled ? (P + kMixTile - 1) / kMixTile * kMixTile * d.ncat *
                                (d.nstates == 61 ? 64 : d.nstates)
-                         : P * blk;
+                         : d.nstates == 4 ? (P + kMixTile - 1) / kMixTile * kMixTile * blk
+                                          : P * blk;  // FP64 4 states: tile-major (f64_off)
   z.partial_bytes = (size_t)d.nslots * z.slot_elems * elem;
   z.scale_bytes = (size_t)d.nslots * P * (d.scaling == GEMS_SCALE_SAFE ? d.ncat : 1) * 2;
   // theta + scale_all, pattern_lh, df_frac, ddf_term
@@ -1001,10 +1002,21 @@ int gems_get_partial(gems_session *s, int slot, double *partial, uint16_t *scale
   GEMS_CUDA(cudaSetDevice(s->desc.device));
   const size_t blk = s->block, n = (size_t)s->desc.nptn * blk;
   if (partial) {
-    if (s->desc.precision == GEMS_PREC_FP64) {
-      const double *src = static_cast<const double *>(s->d_partials) + (size_t)slot * s->P * blk;
+    if (s->desc.precision == GEMS_PREC_FP64 && s->desc.nstates != 4) {
+      const double *src = static_cast<const double *>(s->d_partials) + (size_t)slot * s->slot_elems;
       GEMS_CUDA(cudaMemcpyAsync(partial, src, n * sizeof(double), cudaMemcpyDeviceToHost,
                                 s->stream));
+    } else if (s->desc.precision == GEMS_PREC_FP64) {  // 4 states: tile-major rows
+      std::vector<double> tmp(s->slot_elems);
+      const double *src = static_cast<const double *>(s->d_partials) + (size_t)slot * s->slot_elems;
+      GEMS_CUDA(cudaMemcpyAsync(tmp.data(), src, s->slot_elems * sizeof(double),
+                                cudaMemcpyDeviceToHost, s->stream));
+      GEMS_CUDA(cudaStreamSynchronize(s->stream));
+      const DevCtx c = s->ctx();
+      for (long p = 0; p < s->desc.nptn; p++)
+        for (int cc = 0; cc < s->desc.ncat; cc++)
+          for (int x = 0; x < 4; x++)
+            partial[(size_t)p * blk + (size_t)cc * 4 + x] = tmp[f64_off<4>(c, p, cc, x)];
     } else {
       std::vector<float> tmp(s->slot_elems);
       const float *src = static_cast<const float *>(s->d_partials) + (size_t)slot * s->slot_elems;
