@@ -139,6 +139,9 @@ def compact_line(line):
                           "capacity_req_s": _r(sv["capacity_req_s"]),
                           "p50_ms": _r(sv["latency_ms"]["p50"]),
                           "p99_ms": _r(sv["latency_ms"]["p99"]), "load": sv["load"]}
+        if "at_half_capacity" in sv:
+            h = sv["at_half_capacity"]
+            out["serving"]["p99_ms_at_0.5"] = _r(h["latency_ms"]["p99"])
     if "ingest" in line:
         g = line["ingest"]
         out["ingest"] = {"device_ms": _r(g["device_path_ms"]), "host_ms": _r(g["host_path_ms"]),
@@ -643,10 +646,13 @@ def serving_block(local, nsess=48, nreq=800, load=0.7, taxa=(8, 256), sites=(500
     per request.  Two passes over the same stream, sessions opened before each: every request
     queued at once gives the capacity; Poisson arrivals at `load` x capacity give the request
     latency.  Session open times (create, upload, first full lnL) are reported apart."""
+    import torch
     from gems_b200 import serve
     kw = dict(seed=5, taxa=taxa, sites=sites)
     specs, reqs = serve.make_stream(nsess, nreq, 1.0, **kw)
     cases = {sp.sid: serve.build_case(sp) for sp in specs}
+    torch.cuda.empty_cache()
+    free_gb = torch.cuda.mem_get_info(local)[0] / 1e9
     srv = serve.Server(device=local, workers=16)
     records, wall = srv.run(specs, cases, [(0.0, sid) for _, sid in reqs], preopen=True)
     cap = serve.summarize(records, wall, specs, cases)
@@ -655,13 +661,23 @@ def serving_block(local, nsess=48, nreq=800, load=0.7, taxa=(8, 256), sites=(500
     _, reqs = serve.make_stream(nsess, nreq, rate, **kw)
     records, wall = srv.run(specs, cases, reqs, preopen=True)
     out = serve.summarize(records, wall, specs, cases)
+    # the same stream at half the capacity (per-session order serialises a session's requests,
+    # so the open-loop capacity is below the closed-loop one)
+    _, reqs = serve.make_stream(nsess, nreq, 0.5 * cap["throughput_req_s"], **kw)
+    rec5, wall5 = srv.run(specs, cases, reqs, preopen=True)
+    half = serve.summarize(rec5, wall5, specs, cases)
+    out["at_half_capacity"] = {"offered_rate_req_s": 0.5 * cap["throughput_req_s"],
+                               "throughput_req_s": half["throughput_req_s"],
+                               "latency_ms": half["latency_ms"], "failed": half["failed"]}
     out.update({"capacity_req_s": cap["throughput_req_s"], "capacity_failed": cap["failed"],
                 "capacity_rejected": cap["rejected"], "capacity_wall_s": cap["wall_s"],
                 "offered_rate_req_s": rate, "load": load,
                 "session_open_ms": {"p50": float(np.percentile(opened, 50)),
                                     "p99": float(np.percentile(opened, 99)),
                                     "max": float(opened.max())},
-                "sessions": nsess, "workers": 16,
+                "sessions": nsess, "workers": 16, "free_gb_at_start": free_gb,
+                "budget_gb": srv.budget / 1e9, "pool_admissions": srv.pool_admissions,
+                "evictions": srv.evictions,
                 "stream": f"seeded; taxa {taxa[0]}-{taxa[1]}, sites {sites[0]:,}-{sites[1]:,} "
                           "(log-uniform), states {4,20,61}, categories {1,4,8}, fp64/mixed; "
                           "request = NNI + Newton on the 5 branches around it + lnL; latency at "

@@ -383,6 +383,10 @@ class Session:
         cores."""
         _check(self.lib.gems_session_set_option(self.handle, 1, int(on)), "set_option")
 
+    def set_newton_share(self, k):
+        """The device Newton kernel takes at most 1/k of the GPU (GEMS_OPT_NEWTON_SHARE)."""
+        _check(self.lib.gems_session_set_option(self.handle, 4, int(k)), "set_option")
+
     def set_autotune(self, on=True, force_shape=None):
         """Tune the 4-state traversal's launch shape on its first large traversal (default), or
         force shape k of the kernel's list (comparisons)."""

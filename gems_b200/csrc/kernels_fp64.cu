@@ -21,6 +21,7 @@
 #include <cooperative_groups.h>
 
 #include <climits>
+#include <algorithm>
 #include <cmath>
 #include <string>
 
@@ -765,7 +766,7 @@ int launch_newton_async(Session *s, double guess, double min_len, double max_len
     return GEMS_ERR_CUDA;
   }
   long want = grid_for(s);
-  long maxg = (long)nsm * per_sm;
+  long maxg = std::max(1L, (long)nsm * per_sm / s->newton_share);
   int grid = (int)(want < maxg ? want : maxg);
   if (grid < 1) grid = 1;
   if (2 * 2 * grid > s->nred) {

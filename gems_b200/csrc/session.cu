@@ -549,6 +549,10 @@ int gems_session_set_option(gems_session *s, int option, int value) {
     case GEMS_OPT_TILED_FP64:
       s->g61_enabled = value != 0;
       return GEMS_OK;
+    case GEMS_OPT_NEWTON_SHARE:
+      if (value < 1 || value > 64) return GEMS_ERR_BAD_ARG;
+      s->newton_share = value;
+      return GEMS_OK;
     case GEMS_OPT_AUTOTUNE:
       if (value < 0) return GEMS_ERR_BAD_ARG;
       s->autotune = value == 1;

@@ -93,10 +93,14 @@ def open_session(spec, case, device=0, tree=None, nslots=None):
     """The session of a case, on the case's tree or on `tree` (an evicted session's), with one
     partial slot per internal node or `nslots` (an LM_MEM_SAVE pool)."""
     t0, model, aln = case
-    return PhyloTree.from_case(tree if tree is not None else t0, model, aln,
-                               precision=spec.precision,
-                               scaling="safe" if spec.nstates == 61 else "norm", device=device,
-                               slots="node" if nslots is None else int(nslots))
+    gt = PhyloTree.from_case(tree if tree is not None else t0, model, aln,
+                             precision=spec.precision,
+                             scaling="safe" if spec.nstates == 61 else "norm", device=device,
+                             slots="node" if nslots is None else int(nslots))
+    # many sessions share the GPU: a Newton loop takes at most a quarter of it, so that it runs
+    # beside the others' work instead of waiting for the whole device
+    gt.session.set_newton_share(4)
+    return gt
 
 
 def saved_tree(gt: PhyloTree, ntaxa: int):

@@ -103,7 +103,12 @@ int gems_session_stream(gems_session *s, void **stream);
  * GEMS_OPT_TILED_FP64 (default 1): the FP64 61-state traversal (1 to 8 categories) runs as
  * register-tiled GEMMs over 128-row tiles; 0 selects the per-row kernel (same values, bit for
  * bit). */
-enum { GEMS_OPT_TENSOR_CORES = 1, GEMS_OPT_TILED_FP64 = 2, GEMS_OPT_AUTOTUNE = 3 };
+enum { GEMS_OPT_TENSOR_CORES = 1, GEMS_OPT_TILED_FP64 = 2, GEMS_OPT_AUTOTUNE = 3,
+       GEMS_OPT_NEWTON_SHARE = 4 };
+/* GEMS_OPT_NEWTON_SHARE (default 1): the device Newton loop (gems_newton_branch) is one
+ * cooperative kernel whose blocks are all resident at once; with value k it takes at most 1/k
+ * of the GPU's resident blocks, so that it runs beside other sessions' work instead of waiting
+ * for the whole GPU (a server with many sessions sets k > 1).  Results do not change. */
 /* GEMS_OPT_AUTOTUNE (default 1): the first traversal of a 4-state session class (precision,
  * scaling, categories, pattern count to the power of two) with at least 2^22 pattern-updates
  * times every launch shape of the traversal kernel (patterns per lane group x blocks per SM; all
