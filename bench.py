@@ -707,6 +707,9 @@ def main():
                     help="pattern chunks of the overlapped tip upload in the e2e measurement")
     ap.add_argument("--no-tc", action="store_true",
                     help="20-state mixed traversal on CUDA cores instead of tcgen05")
+    ap.add_argument("--traversal-shape", type=int, default=None,
+                    help="force shape k of the 4-state traversal's list instead of tuning "
+                         "(profiling runs: the captured kernel is then known in advance)")
     args = ap.parse_args()
     if args.sites is None:
         args.sites = NSITES if args.config == "dna512" else 100_000
@@ -750,6 +753,8 @@ def main():
             gt = PhyloTree.from_case(tree, model, aln, precision=prec, device=local)
             if args.no_tc:
                 gt.session.set_tensor_cores(False)
+            if args.traversal_shape is not None:
+                gt.session.set_autotune(False, force_shape=args.traversal_shape)
             stream = torch.cuda.ExternalStream(gt.session.stream_handle(), device=local)
             ms, lnl, kms, launches = time_lnl(gt, args.steps, args.warmup, stream, dist, lnl_buf)
             s_bytes = 8 if prec == "fp64" else 4

@@ -292,7 +292,8 @@ bool tc61_supported(const Session *s);
 int launch_prep_ops_tc61(Session *s, int nops);
 // p0 a multiple of 128, p1 a multiple of 128 or P
 int launch_traverse_tc61(Session *s, int nops, int p0, int p1);
-int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, int p1);
+int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, int p1,
+                               bool with_tables);
 // FP64 61-state traversal as register-tiled GEMMs, C in {1, 2, 4, 8} (kernels_g61.cu)
 size_t g61_op_doubles(int ncat, int unknown);
 bool g61_supported(const Session *s);

@@ -55,37 +55,79 @@ constexpr int kAhi61 = 128;
 // K = source state y), floats per op
 __host__ __device__ constexpr size_t op_floats61(int C) { return (size_t)2 * C * (kBSide / 4); }
 
-__global__ void k_prep_ops_tc61(DevCtx c, const DevOp *ops, float *tab, size_t stride_f) {
-  // exp terms [C][n], then evec and inv_evec [n][n]: every product below reads shared memory
+// The op tables of a job's op k and side (blockIdx.x, blockIdx.y; job blockIdx.z of `jobs`, or
+// `one` when jobs is null).  P_c(t) = evec . diag(exp(eval * rate_c * t)) . inv_evec in FP64,
+// clamped at 0, then split into TF32 hi and lo images.  Register-tiled: a thread owns the 4 x 4
+// block of target states 4xq..4xq+3 by source states 4j..4j+3 (one float4 of every image row
+// it writes), so each term of the sum costs 9 shared-memory reads for 16 FMAs; the sum over i
+// runs in index order with the same fma(evec * exp, inv_evec, acc) steps as a scalar loop.
+// Shared memory: exp terms [C][n]; evec as [64][n] (rows 61..63 zero); inv_evec as
+// [n][4 e][16 j] = inv_evec[i][4j + e] (columns 61..63 zero), so that the 16 lanes of a
+// half-warp read 16 consecutive doubles.
+constexpr int kPrepThreads = 256;  // 16 row quads x 16 column quads
+__host__ __device__ constexpr size_t prep61_smem_doubles(int C) {
+  return (size_t)C * kN + (size_t)kNP * kN + (size_t)kN * kNP;
+}
+__global__ void __launch_bounds__(kPrepThreads)
+    k_prep_ops_tc61(const __grid_constant__ TcJob one, const TcJob *__restrict__ jobs,
+                    size_t stride_f) {
   extern __shared__ double ex[];
+  const TcJob &job = jobs ? jobs[blockIdx.z] : one;
+  const DevCtx &c = job.c;
   const int k = blockIdx.x, side = blockIdx.y;
-  const DevOp op = ops[k];
+  const DevOp op = job.ops[k];
   const double len = side ? op.r_len : op.l_len;
   const int C = c.C, n = kN;
-  double *ev = ex + C * n, *iv = ev + n * n;
+  double *ev = ex + C * n, *iv = ev + kNP * n;
   for (int idx = threadIdx.x; idx < C * n; idx += blockDim.x) {
     const int cc = idx / n, i = idx - cc * n;
     ex[idx] = exp(c.eval[i] * (c.rates[cc] * len));
   }
-  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-    ev[idx] = c.evec[idx];
-    iv[idx] = c.inv_evec[idx];
+  for (int idx = threadIdx.x; idx < kNP * n; idx += blockDim.x) {
+    const int x = idx / n;
+    ev[idx] = x < n ? c.evec[idx] : 0.0;
+    const int i = idx / kNP, r = idx - i * kNP, e = r >> 4, j = r & 15, y = 4 * j + e;
+    iv[idx] = y < n ? c.inv_evec[i * n + y] : 0.0;
   }
   __syncthreads();
-  float *img = tab + (size_t)k * stride_f + (size_t)side * C * (kBSide / 4);
+  // the job's own table, written here and read by its traversal
+  float *img = const_cast<float *>(job.tab) + (size_t)k * stride_f + (size_t)side * C * (kBSide / 4);
   const int per = kBImg / 4;  // floats of one image
-  for (int idx = threadIdx.x; idx < C * per; idx += blockDim.x) {
-    const int cc = idx / per, r = idx - cc * per;
-    const int chunk = r / (kNP * 4), rr = r - chunk * kNP * 4, x = rr / 4, y = chunk * 4 + (rr & 3);
-    float v = 0.f;
-    if (x < n && y < n) {
-      double acc = 0.0;
-      for (int i = 0; i < n; i++) acc = fma(ev[x * n + i] * ex[cc * n + i], iv[i * n + y], acc);
-      v = (float)fmax(acc, 0.0);
+  const int j = threadIdx.x & 15, xq = threadIdx.x >> 4;
+  for (int cc = 0; cc < C; cc++) {
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) acc[r][e] = 0.0;
+    const double *exc = ex + cc * n;
+    for (int i = 0; i < n; i++) {
+      const double xi = exc[i];
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) a[r] = ev[(4 * xq + r) * n + i] * xi;
+#pragma unroll
+      for (int e = 0; e < 4; e++) b[e] = iv[i * kNP + e * 16 + j];
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[r][e] = fma(a[r], b[e], acc[r][e]);
     }
-    const float hi = tf32_rna(v);
-    img[(size_t)cc * 2 * per + r] = hi;
-    img[(size_t)cc * 2 * per + per + r] = tf32_rna(v - hi);
+    // image element (row x, K index y) at chunk y / 4, row x, lane y % 4
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int x = 4 * xq + r;
+      float v[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++)
+        v[e] = (x < n && 4 * j + e < n) ? (float)fmax(acc[r][e], 0.0) : 0.f;
+      const float4 hi = make_float4(tf32_rna(v[0]), tf32_rna(v[1]), tf32_rna(v[2]), tf32_rna(v[3]));
+      const float4 lo = make_float4(tf32_rna(v[0] - hi.x), tf32_rna(v[1] - hi.y),
+                                    tf32_rna(v[2] - hi.z), tf32_rna(v[3] - hi.w));
+      const size_t o = (size_t)cc * 2 * per + ((size_t)j * kNP + x) * 4;
+      *reinterpret_cast<float4 *>(img + o) = hi;
+      *reinterpret_cast<float4 *>(img + o + per) = lo;
+    }
   }
 }
 
@@ -403,24 +445,32 @@ bool tc61_supported(const Session *s) {
          s->desc.scaling == GEMS_SCALE_SAFE && s->tc_enabled && s->tiled;
 }
 
-int launch_prep_ops_tc61(Session *s, int nops) {
-  if (nops <= 0) return GEMS_OK;
-  DevCtx c = s->ctx();
-  const size_t smem = sizeof(double) * ((size_t)s->desc.ncat * kN + 2 * kN * kN);
+// op tables of `njobs` sessions that share one op list and category count, one launch on s0's
+// stream: jobs on the device (njobs > 1) or the single job `one`
+static int prep61(Session *s0, const TcJob &one, const TcJob *jobs, int njobs, int nops) {
+  const size_t smem = sizeof(double) * prep61_smem_doubles(s0->desc.ncat);
   // the limit is a per-kernel attribute shared by every thread of the process: always set to
   // the largest size (kMaxCat categories)
   GEMS_CUDA(cudaFuncSetAttribute(k_prep_ops_tc61, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(double) * ((size_t)kMaxCat * kN + 2 * kN * kN))));
-  k_prep_ops_tc61<<<dim3(nops, 2), 256, smem, s->stream>>>(
-      c, s->d_ops, reinterpret_cast<float *>(s->d_opmats), s->op_stride_tc);
-  s->launches++;
+                                 (int)(sizeof(double) * prep61_smem_doubles(kMaxCat))));
+  k_prep_ops_tc61<<<dim3(nops, 2, njobs), kPrepThreads, smem, s0->stream>>>(one, jobs,
+                                                                            s0->op_stride_tc);
+  s0->launches++;
   GEMS_CUDA(cudaGetLastError());
   return GEMS_OK;
 }
 
+int launch_prep_ops_tc61(Session *s, int nops) {
+  if (nops <= 0) return GEMS_OK;
+  const TcJob one{s->ctx(), s->d_ops, reinterpret_cast<const float *>(s->d_opmats)};
+  return prep61(s, one, nullptr, 1, nops);
+}
+
 // one launch over the tiles of every session in `ss` (all with the same op list, pattern
-// count, categories and device), on the stream of ss[0]
-int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, int p1) {
+// count, categories and device), on the stream of ss[0]; with_tables: the sessions' op tables
+// are built first, by one launch over every (session, op, side)
+int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, int p1,
+                               bool with_tables) {
   if (nops <= 0 || nsess <= 0 || p1 <= p0) return GEMS_OK;
   Session *s0 = ss[0];
   if (p0 % kTile != 0 || (p1 % kTile != 0 && p1 != s0->P)) {
@@ -442,6 +492,8 @@ int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, 
   std::memcpy(s0->h_jobs, jobs.data(), sizeof(TcJob) * nsess);
   GEMS_CUDA(cudaMemcpyAsync(s0->d_jobs, s0->h_jobs, sizeof(TcJob) * nsess,
                             cudaMemcpyHostToDevice, s0->stream));
+  if (with_tables)
+    if (int st = prep61(s0, jobs[0], nsess > 1 ? s0->d_jobs : nullptr, nsess, nops)) return st;
   const size_t smem = tc61_smem();
   GEMS_CUDA(cudaFuncSetAttribute(k_traverse_tc61, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
@@ -467,7 +519,7 @@ int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, 
 
 int launch_traverse_tc61(Session *s, int nops, int p0, int p1) {
   Session *one[1] = {s};
-  return launch_traverse_tc61_batch(one, 1, nops, p0, p1);
+  return launch_traverse_tc61_batch(one, 1, nops, p0, p1, false);
 }
 
 }  // namespace gems

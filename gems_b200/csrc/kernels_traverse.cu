@@ -615,8 +615,8 @@ struct Stack4 {
 // 4 states, one thread per pattern (all C categories in registers), with the traversal plan.
 // Every per-op input a thread needs sits in shared memory before the op starts: the op
 // descriptors, the op tables and the tip bytes of the CTA's 128 patterns are copied with
-// cp.async one chunk of kChunkP ops ahead (double-buffered), and children produced in the
-// launch come from registers (forwarded) or the per-thread stack.  Per op a warp then does
+// cp.async one chunk of ops ahead (double-buffered; chunk_p<R>() ops), and children produced in
+// the launch come from registers (forwarded) or the per-thread stack.  Per op a warp then does
 // shared-memory reads, FMAs and one coalesced 32 x (C*4 values) store: no load on its critical
 // path.  Mixed form: the tip messages are taken from the staged P_c(t) (a tip's value for
 // state set S is the sum of the P columns in S, added in state order as the table of
@@ -626,7 +626,12 @@ struct Stack4 {
 // k_traverse_f64x.
 // ---------------------------------------------------------------------------------------
 constexpr int kThreadsP = 128;  // patterns per CTA
-constexpr int kChunkP = 8;      // ops staged together
+constexpr int kChunkP = 8;      // ops staged together (lane-per-category kernel)
+// ops staged together by the one-thread-per-pattern kernel: 8 for FP32; 4 for FP64, whose
+// tables are twice the size and whose stack lives in shared memory, so that three CTAs fit an
+// SM (the plan depth of a 512-taxon tree is 3: 68 KB a CTA)
+template <typename R>
+__host__ __device__ constexpr int chunk_p() { return sizeof(R) == 4 ? 8 : 4; }
 
 // staged op table: the head (mixed: P_c(t) as [side][x][c][y] floats; FP64: the exp factors as
 // [side][i][c] doubles), then per side the leaf rows of the bases A, C, G, T and of the unknown
@@ -635,9 +640,10 @@ constexpr int kChunkP = 8;      // ops staged together
 template <typename R, int C>
 struct Tab4P {
   static constexpr int kH = sizeof(R) == 4 ? 2 * 16 * C : 2 * 4 * C;  // head elements
-  // a staged leaf row: 4C values, FP32 rows padded by 4 floats so that the rows of different
-  // states start in different bank groups (lanes of a warp read the rows of their own states)
-  static constexpr int kRow = sizeof(R) == 4 ? 4 * C + 4 : 4 * C;
+  // a staged leaf row: 4C values padded by 16 bytes (4 floats, 2 doubles) so that the rows of
+  // different states start in different bank groups (lanes of a warp read the rows of their
+  // own states; unpadded rows are a multiple of 128 bytes apart and collide)
+  static constexpr int kRow = sizeof(R) == 4 ? 4 * C + 4 : 4 * C + 2;
   static constexpr int kLeaf = 5 * kRow;  // leaf elements per side
   static constexpr int kBytes = (kH + 2 * kLeaf) * (int)sizeof(R);
 };
@@ -664,9 +670,9 @@ __device__ __forceinline__ void cp_async_wait1() {
 
 template <typename R, int C>
 struct StageP {
-  DevOp desc[2][kChunkP];
-  alignas(16) unsigned char tab[2][kChunkP][Tab4P<R, C>::kBytes];
-  alignas(16) uint8_t tips[2][kChunkP][2][kThreadsP];
+  DevOp desc[2][chunk_p<R>()];
+  alignas(16) unsigned char tab[2][chunk_p<R>()][Tab4P<R, C>::kBytes];
+  alignas(16) uint8_t tips[2][chunk_p<R>()][2][kThreadsP];
 };
 // every 16-byte copy target inside StageP, and the stack placed after it, stay 16-byte aligned
 static_assert(Tab4P<float, 1>::kBytes % 16 == 0 && Tab4P<double, 1>::kBytes % 16 == 0 &&
@@ -974,7 +980,7 @@ __device__ __forceinline__ void msg4p(const DevCtx &c, const EigPack<4> &E, int 
 }
 
 template <typename R, bool SAFE, int C>
-__global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 3)
     k_traverse4p(DevCtx c, const DevOp *__restrict__ ops, int nops, const R *__restrict__ tab,
                  size_t stride, const EigPack<4> E, int p0, int p1, int depth) {
   extern __shared__ __align__(16) unsigned char smem_p[];
@@ -1002,13 +1008,14 @@ __global__ void __launch_bounds__(kThreadsP, sizeof(R) == 4 ? 4 : 2)
     for (int x = 0; x < 4; x++) fwd[cc][x] = R(0);
   }
   R *part = static_cast<R *>(c.partials);
-  stage4p<R, C>(st, 0, c, ops, tab, stride, 0, min(kChunkP, nops), pbase, tips_async);
+  constexpr int kCh = chunk_p<R>();
+  stage4p<R, C>(st, 0, c, ops, tab, stride, 0, min(kCh, nops), pbase, tips_async);
   cp_async_commit();
-  for (int k0 = 0; k0 < nops; k0 += kChunkP) {
-    const int b = (k0 / kChunkP) & 1, nk = min(kChunkP, nops - k0);
-    if (k0 + kChunkP < nops)
-      stage4p<R, C>(st, b ^ 1, c, ops, tab, stride, k0 + kChunkP,
-                    min(kChunkP, nops - k0 - kChunkP), pbase, tips_async);
+  for (int k0 = 0; k0 < nops; k0 += kCh) {
+    const int b = (k0 / kCh) & 1, nk = min(kCh, nops - k0);
+    if (k0 + kCh < nops)
+      stage4p<R, C>(st, b ^ 1, c, ops, tab, stride, k0 + kCh, min(kCh, nops - k0 - kCh), pbase,
+                    tips_async);
     cp_async_commit();
     cp_async_wait1();  // this chunk's copies are done (the next chunk's may still fly)
     __syncthreads();

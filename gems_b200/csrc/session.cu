@@ -779,14 +779,13 @@ int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, 
     for (int i = 0; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
     return GEMS_OK;
   }
-  for (int i = 0; i < nsess; i++) {
+  for (int i = 0; i < nsess; i++)
     if (int st = upload_ops(ss[i], ops, nops)) return st;
-    if (int st = launch_prep_ops_tc61(ss[i], nops)) return st;
-  }
-  // the batched launch runs on the first session's stream after every session's tables
+  // the batched launches (every session's op tables, then the traversal) run on the first
+  // session's stream after every session's op list is on the device
   for (int i = 1; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
   std::vector<Session *> v(ss, ss + nsess);
-  if (int st = launch_traverse_tc61_batch(v.data(), nsess, nops, 0, s0->P)) return st;
+  if (int st = launch_traverse_tc61_batch(v.data(), nsess, nops, 0, s0->P, true)) return st;
   for (int i = 0; i < nsess; i++) invalidate_theta(ss[i], ops, nops);
   return GEMS_OK;
 }
