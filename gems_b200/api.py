@@ -558,6 +558,13 @@ class PhyloTree:
         _check(self.lib.gems_tree_get_edges(self.handle, _dptr(self.eu), _dptr(self.ev)),
                "get_edges")
 
+    def doSPR(self, node, dad, node2, dad2):
+        """Prune the subtree at node from the internal node dad and regraft dad into the branch
+        (node2, dad2) (gems_tree_spr: assessSPRMove's move, tree/phylotree.cpp:4822)."""
+        _check(self.lib.gems_tree_spr(self.handle, node, dad, node2, dad2), "doSPR")
+        _check(self.lib.gems_tree_get_edges(self.handle, _dptr(self.eu), _dptr(self.ev)),
+               "get_edges")
+
     def neighbors(self, u):
         """Nodes adjacent to u, in edge order."""
         i = np.nonzero((self.eu == u) | (self.ev == u))[0]

@@ -522,10 +522,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       }
       s_out[1] = s_out[0];
     }
-    // The output rows are stored as hi + lo of their split (so that a later split of the stored
-    // value gives the same operands), straight into the tile-major slot: for one chunk a warp
-    // writes 32 consecutive rows, 512 contiguous bytes.  When the next op consumes this output
-    // the split rows also go into its operand buffers.
+    // The output rows are stored as computed, straight into the tile-major slot: for one chunk
+    // a warp writes 32 consecutive rows, 512 contiguous bytes.  When the next op consumes this
+    // output, the split of the same values goes into its operand buffers: exactly what a later
+    // copy of the stored rows splits into, so a forwarded and a copied child give the same bits.
     float *dtile = static_cast<float *>(c.partials) + (size_t)cur.dst_slot * c.slot_elems +
                    (size_t)tile * (5 * C * kAChunk / 4);
     float *fl = nxt_fwd == 1 ? Alo[1] : Alo[0];
@@ -540,16 +540,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         for (int i = 0; i < kN / 4; i++) {
           const float4 v = make_float4(out[j][4 * i] * f[j], out[j][4 * i + 1] * f[j],
                                        out[j][4 * i + 2] * f[j], out[j][4 * i + 3] * f[j]);
-          float4 l;
-          split4(v, h[i], l);
           const int idx = (cc * 5 + i) * kTile + row;
-          const float4 stored = join4(h[i], l);
-          reinterpret_cast<float4 *>(dtile)[idx] = stored;
+          reinterpret_cast<float4 *>(dtile)[idx] = v;
           if (nxt_fwd >= 0) {
-            // forward the split of the stored value, which is what a copy of this row splits
-            // into: when lo rounded to exactly half a TF32 ulp of hi, that split moves the ulp
-            // from lo to hi (same sum, other products)
-            split4(stored, h[i], l);
+            float4 l;
+            split4(v, h[i], l);
             reinterpret_cast<float4 *>(fl)[idx] = l;
           }
         }

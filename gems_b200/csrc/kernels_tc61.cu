@@ -17,7 +17,8 @@
 //   -> the next step's operand tiles start copying (landing buffers free)
 //   -> MMAs (issued by an elected lane), wait -> the next step's B images start copying
 //   -> epilogue: tcgen05.ld of the accumulators, products, SAFE rescaling by 2^64 with uint16
-//      counters, coalesced stores of the rows (stored as hi + lo of their split)
+//      counters, coalesced stores of the rows (as computed; every consumer splits the stored
+//      values the same way)
 // The step after the last category of an op may need that op's output of the same category
 // (one category: C = 1); that copy is issued after the epilogue's stores instead.
 //
@@ -406,9 +407,7 @@ __global__ void __launch_bounds__(kThreads61, 1)
         if (x + 3 >= kN) w.w = 0.f;
         if (x >= kN) w.x = 0.f;
       }
-      float4 h, l;
-      split4(w, h, l);
-      reinterpret_cast<float4 *>(dst)[(8 * half + i) * kTile + row] = join4(h, l);
+      reinterpret_cast<float4 *>(dst)[(8 * half + i) * kTile + row] = w;
     }
     if (act && half == 0)
       c.scale[(size_t)cur.op.dst_slot * c.slot_scale + (size_t)p * C + cur.cat] = (uint16_t)s_out;

@@ -445,6 +445,107 @@ struct Tree {
     return GEMS_OK;
   }
 
+  // the nodes of the subtree at v (away from u)
+  void mark(int v, int u, std::vector<char> &m) const {
+    m[v] = 1;
+    for (int k = 0; k < deg[v]; k++)
+      if (adj[v * 3 + k] != u) mark(adj[v * 3 + k], v, m);
+  }
+  // every partial whose subtree holds node x (the directed branches pointing at x)
+  void clear_toward(int x) {
+    for (int k = 0; k < deg[x]; k++) {
+      const int c = adj[x * 3 + k];
+      computed[dir(c, x)] = 0;
+      clear_reverse(c, x);
+    }
+  }
+
+  // SPR with the geometry of assessSPRMove (tree/phylotree.cpp:4822-4880): the subtree at
+  // `node` is pruned from internal `dad`, whose other neighbours s1 < s2 (by node id; the
+  // reference takes them in its neighbour order) are joined by one branch of their summed
+  // length, and dad is inserted into the branch (node2, dad2): its entry that pointed at s1 now
+  // points at dad2, the one that pointed at s2 at node2, each half the branch's length.  Edges:
+  // (dad, s1) -> (s1, s2), (dad, s2) -> (dad, dad2), (node2, dad2) -> (dad, node2).
+  // Partials: the four neighbour entries whose subtree moves unchanged keep theirs (slot and
+  // validity: (s1->s2) takes (dad->s2)'s, (s2->s1) (dad->s1)'s, (dad->dad2) (node2->dad2)'s,
+  // (dad->node2) (dad2->node2)'s), the two new entries pointing at dad take the slots of the
+  // two old ones (one slot per directed branch and pool modes), and every partial whose subtree
+  // holds dad before or after the move is invalidated, which also covers any of the four whose
+  // subtree did change (a regraft next to s1 or s2).
+  int spr(int node, int dad, int node2, int dad2) {
+    auto bad = [&](int x) { return x < 0 || x >= nnode; };
+    if (bad(node) || bad(dad) || bad(node2) || bad(dad2)) return GEMS_ERR_BAD_ARG;
+    const int kn = find(dad, node);
+    if (leaf(dad) || kn < 0 || find(node2, dad2) < 0 || node2 == dad || dad2 == dad)
+      return GEMS_ERR_BAD_ARG;
+    std::vector<char> in_s(nnode, 0);
+    mark(node, dad, in_s);
+    if (in_s[node2] || in_s[dad2]) return GEMS_ERR_BAD_ARG;
+    int ks[2], nk = 0;
+    for (int k = 0; k < 3; k++)
+      if (k != kn) ks[nk++] = k;
+    if (adj[dad * 3 + ks[0]] > adj[dad * 3 + ks[1]]) std::swap(ks[0], ks[1]);
+    const int s1 = adj[dad * 3 + ks[0]], s2 = adj[dad * 3 + ks[1]];
+    const int ia = dad * 3 + ks[0], ib = dad * 3 + ks[1];
+    const int ic = dir(s1, dad), id = dir(s2, dad);
+    const int ie = dir(node2, dad2), iff = dir(dad2, node2);
+    const double l1 = len[ia], l2 = len[ib], l = len[ie];
+    clear_toward(dad);
+    // contents: idx[i] takes src[i]'s (validity, and its slot in per-branch and pool modes)
+    const int idx[6] = {ic, id, ia, ib, ie, iff}, src[6] = {ib, ia, ie, iff, ic, id};
+    char cm[6];
+    int ds[6];
+    for (int i = 0; i < 6; i++) {
+      cm[i] = computed[src[i]];
+      ds[i] = dslot.empty() ? -1 : dslot[src[i]];
+    }
+    // LM_PER_NODE: a node's buffer owned by a moved entry follows it (the first four moves keep
+    // their target node); dad's buffer was owned by an entry that now points elsewhere or by one
+    // just invalidated, so it is released.  Every new owner is decided on the old owners.
+    std::vector<std::pair<int, int>> reown;  // (slot, new owner)
+    if (!per_branch && !pool) {
+      for (int i = 0; i < 4; i++) {
+        const int v = adj[src[i]];
+        if (!leaf(v) && owner[node_slot[v]] == src[i]) reown.push_back({node_slot[v], idx[i]});
+      }
+      reown.push_back({node_slot[dad], -1});
+    }
+    adj[ic] = s2;
+    adj[id] = s1;
+    len[ic] = len[id] = l1 + l2;
+    adj[ia] = dad2;
+    adj[ib] = node2;
+    adj[ie] = dad;
+    adj[iff] = dad;
+    len[ia] = len[ib] = len[ie] = len[iff] = l / 2;
+    for (int i = 0; i < 6; i++) computed[idx[i]] = cm[i];
+    if (per_branch || pool) {
+      for (int i = 0; i < 6; i++) dslot[idx[i]] = ds[i];
+      for (int i = 0; i < 6; i++)
+        if (ds[i] >= 0) owner[ds[i]] = idx[i];
+    } else {
+      for (const auto &r : reown) owner[r.first] = r.second;
+    }
+    clear_toward(dad);
+    int e_s1 = -1, e_s2 = -1, e_r = -1;
+    for (int e = 0; e < nedges; e++) {
+      const int a = eu[e], b = ev[e];
+      if ((a == dad && b == s1) || (a == s1 && b == dad)) e_s1 = e;
+      else if ((a == dad && b == s2) || (a == s2 && b == dad)) e_s2 = e;
+      else if ((a == node2 && b == dad2) || (a == dad2 && b == node2)) e_r = e;
+    }
+    eu[e_s1] = s1;
+    ev[e_s1] = s2;
+    eu[e_s2] = dad;
+    ev[e_s2] = dad2;
+    eu[e_r] = dad;
+    ev[e_r] = node2;
+    theta_computed = false;
+    cur_u = -1;
+    if (pool) compute_sizes();
+    return GEMS_OK;
+  }
+
   // PhyloTree::computeLikelihood (tree/phylotree.cpp:1258-1295)
   int compute_likelihood(double *lnl, double *pattern_lh) {
     if (cur_u < 0) {
@@ -711,6 +812,11 @@ int gems_tree_nni(gems_tree *t, int u, int v, int a, int b) {
       a >= t->nnode || b >= t->nnode)
     return GEMS_ERR_BAD_ARG;
   return t->nni(u, v, a, b);
+}
+
+int gems_tree_spr(gems_tree *t, int node, int dad, int node2, int dad2) {
+  if (!t) return GEMS_ERR_BAD_ARG;
+  return t->spr(node, dad, node2, dad2);
 }
 
 int gems_tree_get_edges(gems_tree *t, int *eu, int *ev) {

@@ -127,13 +127,6 @@ __device__ __forceinline__ void split4(float4 v, float4 &h, float4 &l) {
   l = make_float4(tf32_rna(v.x - h.x), tf32_rna(v.y - h.y), tf32_rna(v.z - h.z),
                   tf32_rna(v.w - h.w));
 }
-// the value a row is stored as: hi + lo of its split (exact in FP32).  A later split of the
-// stored value gives the same sum, and the same hi and lo except when lo rounded to exactly
-// half a TF32 ulp of hi with the sign of hi: then the ulp moves from lo to hi.  Split the
-// stored value again wherever it must match a copy of it.
-__device__ __forceinline__ float4 join4(float4 h, float4 l) {
-  return make_float4(h.x + l.x, h.y + l.y, h.z + l.z, h.w + l.w);
-}
 
 }  // namespace tc
 }  // namespace gems

@@ -1,11 +1,15 @@
 """Serving loop: many tree-search sessions resident in HBM, requests batched continuously.
 
 A session is one alignment + model + tree kept on the GPU (its partials, scale counters,
-theta and tip bytes).  A request is a local tree move as tree search issues them: an NNI on an
-internal branch (tree/phylotree.cpp:4059 doNNI), then Newton optimisation of the five branches
-around it (the central one and its four neighbours, as the NNI-5 evaluation of
-getBestNNIForBran does, tree/phylotree.cpp:4176), then the tree log-likelihood.  Only the
-partials on the affected paths are recomputed.
+theta and tip bytes).  A request is a local tree move as tree search issues them, then the
+tree log-likelihood:
+  * an NNI on an internal branch (tree/phylotree.cpp:4059 doNNI), then Newton optimisation of
+    the five branches around it (the central one and its four neighbours, as the NNI-5
+    evaluation of getBestNNIForBran does, tree/phylotree.cpp:4176);
+  * or an SPR: a subtree pruned and regrafted within a radius (tree/phylotree.cpp:4822
+    assessSPRMove's move), then Newton on the four branches swapSPR optimises
+    (tree/phylotree.cpp:4764-4768).
+Only the partials on the affected paths are recomputed.
 
 Scheduling:
   * admission by HBM footprint: a session is created on the GPU when its footprint
@@ -126,13 +130,72 @@ def nni5(gt: PhyloTree, ntaxa: int, rng: np.random.Generator):
     return gt.computeLikelihoodFromBuffer(), len(branches)
 
 
+SPR_RADIUS = 3      # regraft branches at most this many branches from the pruned joint
+SPR_SHARE = 0.3     # share of requests that are SPR moves (the rest are NNI)
+
+
+def spr_regraft_branches(gt, node, dad, radius=SPR_RADIUS):
+    """Branches (x, y) the subtree at node (pruned from dad) can be regrafted into: those of the
+    remaining tree within `radius` branches of the joint that pruning leaves (dad's two other
+    neighbours s1, s2, joined), the joint itself excluded (regrafting there is no move).  The
+    search walks outwards from s1 and s2, as swapSPR does up to its radius
+    (tree/phylotree.cpp:4694-4820)."""
+    s1, s2 = sorted(x for x in gt.neighbors(dad) if x != node)
+    out, frontier, seen = [], [(s1, dad), (s2, dad)], {dad, s1, s2}
+    for _ in range(radius):
+        nxt = []
+        for x, back in frontier:
+            for y in gt.neighbors(x):
+                if y == back or y == dad or y in (s1, s2) and x in (s1, s2):
+                    continue
+                out.append((y, x))
+                if y not in seen:
+                    seen.add(y)
+                    nxt.append((y, x))
+        frontier = nxt
+    return s1, s2, out
+
+
+def spr4(gt, ntaxa: int, rng: np.random.Generator, radius=SPR_RADIUS):
+    """One SPR request: a random subtree pruned from a random internal node and regrafted into
+    a branch within `radius` (assessSPRMove's move, tree/phylotree.cpp:4822-4880), Newton on the
+    four branches swapSPR optimises after a move (the pruned subtree's branch, the two halves
+    of the regraft branch and the joined branch, tree/phylotree.cpp:4764-4768), then the lnL
+    from the buffers.  Returns (lnL, branches optimised)."""
+    edges = list(zip(gt.eu.tolist(), gt.ev.tolist()))
+    for _ in range(64):
+        u, v = edges[int(rng.integers(len(edges)))]
+        node, dad = (u, v) if rng.integers(2) else (v, u)
+        if dad < ntaxa:
+            continue
+        s1, s2, cand = spr_regraft_branches(gt, node, dad, radius)
+        if cand:
+            break
+    else:
+        return nni5(gt, ntaxa, rng)
+    node2, dad2 = cand[int(rng.integers(len(cand)))]
+    gt.doSPR(node, dad, node2, dad2)
+    branches = [(node, dad), (dad2, dad), (node2, dad), (s1, s2)]
+    for p, q in branches:
+        gt.optimizeOneBranch(p, q)
+    return gt.computeLikelihoodFromBuffer(), len(branches)
+
+
+def tree_move(gt, ntaxa: int, rng: np.random.Generator):
+    """One serving request: an SPR (share SPR_SHARE) or an NNI, drawn from the request's own
+    seeded generator, so a session's results do not depend on scheduling."""
+    if rng.random() < SPR_SHARE:
+        return spr4(gt, ntaxa, rng)
+    return nni5(gt, ntaxa, rng)
+
+
 def run_alone(spec, case, nreq, device=0, opener=open_session):
     """The session's requests in order, nothing else on the GPU."""
     gt = opener(spec, case, device)
     gt.computeLikelihood()
     out = []
     for k in range(nreq):
-        out.append(nni5(gt, spec.ntaxa, np.random.default_rng((spec.seed, k)))[0])
+        out.append(tree_move(gt, spec.ntaxa, np.random.default_rng((spec.seed, k)))[0])
     gt.close()
     gt.session.close()
     return out
@@ -359,8 +422,8 @@ class Server:
                 gt = open_sess[sid]
                 ts = time.perf_counter() - t0
                 try:
-                    lnl, nbr = nni5(gt, spec_of[sid].ntaxa,
-                                    np.random.default_rng((spec_of[sid].seed, seq)))
+                    lnl, nbr = tree_move(gt, spec_of[sid].ntaxa,
+                                         np.random.default_rng((spec_of[sid].seed, seq)))
                     err = None
                 except GemsError as e:  # the request fails; the server carries on
                     lnl, nbr, err = None, 0, str(e)

@@ -356,7 +356,19 @@ int gems_tree_optimize_all_branches_batch(gems_tree *const *trees, int ntrees, i
  * with their subtrees, the partials looking back across u or v are invalidated.  The edge
  * list reported by gems_tree_get_edges changes accordingly. */
 int gems_tree_nni(gems_tree *t, int u, int v, int a, int b);
-/* current edge list (same order as at creation; endpoints change with NNIs) */
+/* The SPR move of PhyloTree::assessSPRMove (tree/phylotree.cpp:4822-4880): the subtree at node
+ * is pruned from the internal node dad, whose two other neighbours s1 < s2 (by node id) are
+ * joined by one branch of their summed length, and dad is inserted into the branch
+ * (node2, dad2) -- which must lie outside the pruned subtree and not touch dad -- with half the
+ * branch's length on each side.  Edges reported by gems_tree_get_edges: (dad, s1) becomes
+ * (s1, s2), (dad, s2) becomes (dad, dad2), (node2, dad2) becomes (dad, node2).  Partials whose
+ * subtree is unchanged stay valid; every partial whose subtree holds dad before or after the
+ * move is recomputed by the next evaluation.  The reference's SPR search (swapSPR) applies the
+ * same move and then optimises the branches (node, dad), (dad2, dad), (node2, dad), (s1, s2)
+ * with optimizeOneBranch (tree/phylotree.cpp:4764-4768).  GEMS_ERR_BAD_ARG for a move that
+ * does not satisfy the conditions (the tree is unchanged). */
+int gems_tree_spr(gems_tree *t, int node, int dad, int node2, int dad2);
+/* current edge list (same order as at creation; endpoints change with NNI and SPR moves) */
 int gems_tree_get_edges(gems_tree *t, int *eu, int *ev);
 /* PhyloTree::computeFuncDerv (tree/phylotree.cpp:2555): set the length of branch
  * (node1, node2) to value without invalidating partials and return f = -dlnL/dt,

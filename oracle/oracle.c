@@ -1145,6 +1145,98 @@ int orc_nni(orc_tree *t, int u, int v, int a, int b) {
     return 0;
 }
 
+/* marks the nodes of the subtree at v (away from u) */
+static void mark_subtree(const orc_tree *t, int v, int u, unsigned char *m) {
+    m[v] = 1;
+    for (int k = 0; k < t->deg[v]; k++)
+        if (t->adj[v * 3 + k] != u) mark_subtree(t, t->adj[v * 3 + k], v, m);
+}
+
+/* clears every partial whose subtree holds node x (the directed branches pointing at x) */
+static void clear_toward(orc_tree *t, int x) {
+    for (int k = 0; k < t->deg[x]; k++) {
+        int c = t->adj[x * 3 + k];
+        t->computed[c * 3 + find_nei(t, c, x)] = 0;
+        clear_reverse(t, c, x);
+    }
+}
+
+/* SPR move with the geometry of assessSPRMove (tree/phylotree.cpp:4822-4880): the subtree at
+ * `node` is pruned from `dad` (internal), whose two other neighbours s1 < s2 (by node id; the
+ * reference takes them in its neighbour order) are joined by one branch of their summed length;
+ * dad is then inserted into the branch (node2, dad2), its entry that pointed at s1 taking dad2
+ * and the one that pointed at s2 node2, each half the branch's length.  Edges: (dad, s1) becomes (s1, s2), (dad, s2) becomes (dad, dad2),
+ * (node2, dad2) becomes (dad, node2).  The four neighbour entries that keep their subtree keep
+ * their partials ((s1->s2) takes (dad->s2)'s, (s2->s1) (dad->s1)'s, (dad->dad2) (node2->dad2)'s,
+ * (dad->node2) (dad2->node2)'s); every partial whose subtree holds dad before or after the move
+ * is cleared, which also covers any of the four whose subtree did change. */
+int orc_spr(orc_tree *t, int node, int dad, int node2, int dad2) {
+    if (node < 0 || dad < 0 || node2 < 0 || dad2 < 0 || node >= t->nnode || dad >= t->nnode ||
+        node2 >= t->nnode || dad2 >= t->nnode)
+        return -1;
+    int kn = find_nei(t, dad, node);
+    if (is_leaf(t, dad) || kn < 0 || find_nei(t, node2, dad2) < 0 || node2 == dad || dad2 == dad)
+        return -1;
+    unsigned char *in_s = calloc((size_t)t->nnode, 1);
+    mark_subtree(t, node, dad, in_s);
+    int bad = in_s[node2] || in_s[dad2];
+    free(in_s);
+    if (bad) return -1;
+    int ks[2], nk = 0;
+    for (int k = 0; k < 3; k++)
+        if (k != kn) ks[nk++] = k;
+    if (t->adj[dad * 3 + ks[0]] > t->adj[dad * 3 + ks[1]]) {
+        int tk = ks[0];
+        ks[0] = ks[1];
+        ks[1] = tk;
+    }
+    int s1 = t->adj[dad * 3 + ks[0]], s2 = t->adj[dad * 3 + ks[1]];
+    int ia = dad * 3 + ks[0], ib = dad * 3 + ks[1];
+    int ic = s1 * 3 + find_nei(t, s1, dad), id = s2 * 3 + find_nei(t, s2, dad);
+    int ie = node2 * 3 + find_nei(t, node2, dad2), iff = dad2 * 3 + find_nei(t, dad2, node2);
+    double l1 = t->len[ia], l2 = t->len[ib], l = t->len[ie];
+    clear_toward(t, dad);
+    int idx[6] = {ic, id, ia, ib, ie, iff}, src[6] = {ib, ia, ie, iff, ic, id};
+    double *pl[6];
+    uint16_t *sc[6];
+    unsigned char cm[6];
+    for (int i = 0; i < 6; i++) {
+        pl[i] = t->plh[src[i]];
+        sc[i] = t->scl[src[i]];
+        cm[i] = t->computed[src[i]];
+    }
+    t->adj[ic] = s2;
+    t->adj[id] = s1;
+    t->len[ic] = t->len[id] = l1 + l2;
+    t->adj[ia] = dad2;
+    t->adj[ib] = node2;
+    t->adj[ie] = dad;
+    t->adj[iff] = dad;
+    t->len[ia] = t->len[ib] = t->len[ie] = t->len[iff] = l / 2;
+    for (int i = 0; i < 6; i++) {
+        t->plh[idx[i]] = pl[i];
+        t->scl[idx[i]] = sc[i];
+        t->computed[idx[i]] = cm[i];
+    }
+    clear_toward(t, dad);
+    int e_s1 = -1, e_s2 = -1, e_r = -1;
+    for (int e = 0; e < t->nedges; e++) {
+        int a = t->eu[e], b = t->ev[e];
+        if ((a == dad && b == s1) || (a == s1 && b == dad)) e_s1 = e;
+        else if ((a == dad && b == s2) || (a == s2 && b == dad)) e_s2 = e;
+        else if ((a == node2 && b == dad2) || (a == dad2 && b == node2)) e_r = e;
+    }
+    t->eu[e_s1] = s1;
+    t->ev[e_s1] = s2;
+    t->eu[e_s2] = dad;
+    t->ev[e_s2] = dad2;
+    t->eu[e_r] = dad;
+    t->ev[e_r] = node2;
+    t->theta_computed = 0;
+    t->cur_u = -1;
+    return 0;
+}
+
 void orc_compute_func_derv(orc_tree *t, int node1, int node2, double value, int new_branch,
                            double *f, double *df) {
     t->cur_u = node1;

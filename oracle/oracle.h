@@ -75,6 +75,9 @@ void orc_compute_likelihood_derv(orc_tree *t, int node, int dad, double *df, dou
 double orc_compute_likelihood_from_buffer(orc_tree *t);
 /* phylotree.cpp:4059 doNNI: swap subtree a (at u) with subtree b (at v) across branch (u, v) */
 int orc_nni(orc_tree *t, int u, int v, int a, int b);
+/* phylotree.cpp:4822 assessSPRMove's move: prune the subtree at node from dad, regraft dad into
+ * the branch (node2, dad2) (halves of its length; dad's other branches joined, lengths summed) */
+int orc_spr(orc_tree *t, int node, int dad, int node2, int dad2);
 /* phylotree.cpp:2555 computeFuncDerv on branch (node1, node2) at length value: f = -dlnL/dt,
  * df = -d2lnL/dt2, theta rebuilt first when new_branch != 0 */
 void orc_compute_func_derv(orc_tree *t, int node1, int node2, double value, int new_branch,

@@ -139,6 +139,22 @@ class OracleTree:
             elif {x, y} == {v, b}:
                 self.eu[i], self.ev[i] = u, b
 
+    def doSPR(self, node, dad, node2, dad2):
+        """Prune the subtree at node from dad and regraft dad into the branch (node2, dad2)."""
+        others = sorted(x for x in self.neighbors(dad) if x != node)
+        assert len(others) == 2 and node in self.neighbors(dad), "dad must be internal"
+        s1, s2 = others
+        assert self.L.orc_spr(self.h, node, dad, node2, dad2) == 0
+        # edges: (dad, s1) -> (s1, s2), (dad, s2) -> (dad, dad2), (node2, dad2) -> (dad, node2)
+        for i in range(len(self.eu)):
+            e = {int(self.eu[i]), int(self.ev[i])}
+            if e == {dad, s1}:
+                self.eu[i], self.ev[i] = s1, s2
+            elif e == {dad, s2}:
+                self.eu[i], self.ev[i] = dad, dad2
+            elif e == {node2, dad2}:
+                self.eu[i], self.ev[i] = dad, node2
+
     def neighbors(self, u):
         return [int(b) if a == u else int(a) for a, b in zip(self.eu, self.ev) if u in (a, b)]
 

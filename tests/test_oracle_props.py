@@ -95,3 +95,70 @@ def test_nni_changes_topology_and_back():
     assert a in ot.neighbors(u) and b in ot.neighbors(v)
     l2 = ot.computeLikelihood()
     assert abs(l2 - l0) <= 1e-9 * abs(l0)
+
+
+def _fresh_lnl(ot, tree, model, aln):
+    fresh = orc.OracleTree(synth.Tree(tree.ntaxa, ot.eu.copy(), ot.ev.copy(),
+                                      ot.getBranchLengths()), model, aln)
+    return fresh.computeLikelihood()
+
+
+@pytest.mark.parametrize("n", [4, 20])
+def test_spr_incremental_equals_fresh_tree(n):
+    """doSPR + the four-branch optimisation keeps the partial buffers consistent: the lnL read
+    from the buffers equals a from-scratch lnL of a new tree with the resulting topology."""
+    from gems_b200.serve import spr4
+    tree, model, aln = small_case(n, ntaxa=14)
+    ot = orc.OracleTree(tree, model, aln)
+    ot.computeLikelihood()
+    for k in range(6):
+        lnl, nbr = spr4(ot, tree.ntaxa, np.random.default_rng((9, k)))
+        assert nbr == 4
+        ref = _fresh_lnl(ot, tree, model, aln)
+        assert abs(lnl - ref) <= 1e-9 * abs(ref), (k, lnl, ref)
+
+
+def test_spr_every_regraft_of_one_prune():
+    """Every regraft branch within the radius of one pruned subtree, the moves next to the
+    joint (dad2 or node2 a former neighbour of dad) included: after each move the lnL computed
+    on the moved tree's buffers equals a fresh tree's, the edge list holds a binary tree with
+    the same leaves, and the joined branch has the summed length."""
+    from gems_b200.serve import spr_regraft_branches
+    tree, model, aln = small_case(4, ntaxa=12)
+    base = orc.OracleTree(tree, model, aln)
+    u, v = next((int(a), int(b)) for a, b in zip(tree.eu, tree.ev)
+                if a >= tree.ntaxa and b >= tree.ntaxa)
+    node, dad = u, v
+    s1, s2, cand = spr_regraft_branches(base, node, dad, radius=10)
+    assert any(s1 in c or s2 in c for c in cand)
+    for node2, dad2 in cand:
+        ot = orc.OracleTree(tree, model, aln)
+        ot.computeLikelihood()
+        l1 = ot.getBranchLength(dad, s1)
+        l2 = ot.getBranchLength(dad, s2)
+        l = ot.getBranchLength(node2, dad2)
+        ot.doSPR(node, dad, node2, dad2)
+        assert sorted(ot.neighbors(dad)) == sorted([node, node2, dad2])
+        assert s2 in ot.neighbors(s1)
+        assert ot.getBranchLength(s1, s2) == l1 + l2
+        assert ot.getBranchLength(dad, node2) == l / 2 == ot.getBranchLength(dad, dad2)
+        deg = np.bincount(np.concatenate([ot.eu, ot.ev]))
+        assert np.all(deg[: tree.ntaxa] == 1) and np.all(deg[tree.ntaxa:] == 3)
+        got = ot.computeLikelihood()
+        ref = _fresh_lnl(ot, tree, model, aln)
+        assert abs(got - ref) <= 1e-10 * abs(ref), (node2, dad2, got, ref)
+
+
+def test_spr_refuses_bad_moves():
+    tree, model, aln = small_case(4, ntaxa=10)
+    ot = orc.OracleTree(tree, model, aln)
+    u, v = next((int(a), int(b)) for a, b in zip(tree.eu, tree.ev)
+                if a >= tree.ntaxa and b >= tree.ntaxa)
+    inside = [x for x in ot.neighbors(u) if x != v][0]   # a branch inside the pruned subtree
+    with pytest.raises(AssertionError):
+        ot.doSPR(u, v, inside, u)
+    with pytest.raises(AssertionError):                  # a branch at dad itself
+        ot.doSPR(u, v, [x for x in ot.neighbors(v) if x != u][0], v)
+    leaf = next(x for x in range(tree.ntaxa))
+    with pytest.raises(AssertionError):                  # dad must be internal
+        ot.doSPR(ot.neighbors(leaf)[0], leaf, u, v)
