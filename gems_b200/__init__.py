@@ -8,9 +8,11 @@ missing, the calls raise.
 from .api import (GemsError, PhyloTree, Session, STATUS, op_array, branch_struct,
                   measure_peaks, check_barrier_timeout, compress_alignment, Ingest, full_traversal,
                   traverse_batch, branch_lnl_batch, set_models_from_rates,
-                  optimize_all_branches_batch, GEMS_CHILD_PARTIAL, GEMS_CHILD_TIP)
+                  optimize_all_branches_batch, compute_likelihood_batch, evaluate_rates_batch,
+                  GEMS_CHILD_PARTIAL, GEMS_CHILD_TIP)
 
 __all__ = ["GemsError", "PhyloTree", "Session", "STATUS", "op_array", "branch_struct",
            "measure_peaks", "check_barrier_timeout", "compress_alignment", "Ingest", "full_traversal",
            "traverse_batch", "branch_lnl_batch", "set_models_from_rates",
-           "optimize_all_branches_batch", "GEMS_CHILD_PARTIAL", "GEMS_CHILD_TIP"]
+           "optimize_all_branches_batch", "compute_likelihood_batch", "evaluate_rates_batch",
+           "GEMS_CHILD_PARTIAL", "GEMS_CHILD_TIP"]

@@ -205,6 +205,32 @@ def optimize_all_branches_batch(trees, my_iterations=100, tolerance=0.001, maxNR
     return out
 
 
+def compute_likelihood_batch(trees):
+    """gems_tree_compute_likelihood_batch: computeLikelihood of PhyloTrees on sessions that share
+    the alignment's shape (one per candidate model), evaluated together; returns their lnL."""
+    lib = _lib.gems()
+    arr = (c_void_p * len(trees))()
+    for i, t in enumerate(trees):
+        arr[i] = t.handle.value
+    out = np.zeros(len(trees))
+    _check(lib.gems_tree_compute_likelihood_batch(arr, len(trees), _dptr(out)),
+           "gems_tree_compute_likelihood_batch")
+    return out
+
+
+def evaluate_rates_batch(trees, rates, props=None):
+    """Every candidate at new category rates (a new Gamma shape: RateGamma::computeFunction,
+    model/rategamma.cpp:178-186, once per candidate): gems_set_rates on each tree's session,
+    every partial cleared, then one batched evaluation.  rates[i] (and props[i], default equal
+    proportions) are tree i's; returns their lnL."""
+    for i, t in enumerate(trees):
+        r = _f64(rates[i])
+        p = np.full(len(r), 1.0 / len(r)) if props is None else _f64(props[i])
+        t.session.set_rates(r, p)
+        t.clearAllPartialLH()
+    return compute_likelihood_batch(trees)
+
+
 def _session_array(sessions):
     arr = (c_void_p * len(sessions))()
     for i, s in enumerate(sessions):
@@ -377,6 +403,12 @@ class Session:
         _check(self.lib.gems_reweighted_derv(self.handle, _dptr(df), _dptr(ddf)),
                "gems_reweighted_derv")
         return df, ddf
+
+    def set_rates(self, rates, props):
+        """New category rates and proportions, eigensystem kept (gems_set_rates); partials
+        computed before are stale."""
+        r, p = _f64(rates), _f64(props)
+        _check(self.lib.gems_set_rates(self.handle, _dptr(r), _dptr(p)), "gems_set_rates")
 
     def set_tensor_cores(self, on=True):
         """20-state mixed traversal on tcgen05 split-TF32 products (default) or FP32 CUDA

@@ -807,6 +807,31 @@ int gems_tree_optimize_all_branches_batch(gems_tree *const *trees, int ntrees, i
   return optimize_all_batch(trees, ntrees, iterations, tolerance, max_nr_step, lnl);
 }
 
+int gems_tree_compute_likelihood_batch(gems_tree *const *trees, int ntrees, double *lnl) {
+  if (!trees || ntrees <= 0 || !lnl) return GEMS_ERR_BAD_ARG;
+  std::vector<gems_session *> ss(ntrees);
+  std::vector<gems_branch> br(ntrees);
+  std::vector<const gems_op *> ops(ntrees);
+  std::vector<int> nops(ntrees);
+  for (int i = 0; i < ntrees; i++) {
+    gems_tree *t = trees[i];
+    if (!t) return GEMS_ERR_BAD_ARG;
+    // the branch computeLikelihood evaluates (compute_likelihood)
+    if (t->cur_u < 0) {
+      std::vector<int> h(t->nnode, 0);
+      t->cur_u = t->far_leaf(0, -1, h);
+      t->cur_k = 0;
+    }
+    int node = t->adj[t->cur_u * 3 + t->cur_k], dad = t->cur_u;
+    br[i] = t->branch(node, dad);
+    if (t->pool_status) return t->pool_status;
+    ss[i] = t->s;
+    ops[i] = t->ops.data();
+    nops[i] = (int)t->ops.size();
+  }
+  return gems_branch_lnl_batch_ops(ss.data(), ntrees, ops.data(), nops.data(), br.data(), lnl);
+}
+
 int gems_tree_nni(gems_tree *t, int u, int v, int a, int b) {
   if (!t || u < 0 || v < 0 || a < 0 || b < 0 || u >= t->nnode || v >= t->nnode ||
       a >= t->nnode || b >= t->nnode)

@@ -654,6 +654,27 @@ int gems_set_model(gems_session *s, const double *eval, const double *evec,
   return upload_model(s, eval, evec, inv_evec, rates, props);
 }
 
+int gems_set_rates(gems_session *s, const double *rates, const double *props) {
+  if (!s || !rates || !props) return GEMS_ERR_BAD_ARG;
+  if (!s->model_set) {
+    set_error("model not set");
+    return GEMS_ERR_STATE;
+  }
+  const int n = s->desc.nstates, C = s->desc.ncat;
+  for (int c = 0; c < C; c++)
+    if (!(rates[c] >= 0) || !(props[c] >= 0)) return GEMS_ERR_BAD_ARG;
+  GEMS_CUDA(cudaSetDevice(s->desc.device));
+  // the model block is [eval n][evec n*n][inv_evec n*n][rates C][props C][tip tables]: only the
+  // rates and proportions change (the tip tables depend on inv_evec alone)
+  std::vector<double> rp(rates, rates + C);
+  rp.insert(rp.end(), props, props + C);
+  GEMS_CUDA(cudaMemcpyAsync(s->d_model + n + 2 * (size_t)n * n, rp.data(), rp.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, s->stream));
+  GEMS_CUDA(cudaStreamSynchronize(s->stream));
+  s->theta_valid = false;
+  return GEMS_OK;
+}
+
 int gems_set_model_from_rates(gems_session *s, const double *exch_upper, const double *freq,
                               const double *rates, const double *props) {
   if (!s || !exch_upper || !freq || !rates || !props) return GEMS_ERR_BAD_ARG;
@@ -747,9 +768,13 @@ int gems_compute_partial(gems_session *s, const gems_op *op, int ptn_lower, int 
   return GEMS_OK;
 }
 
-int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, int nops) {
-  if (!ss || nsess <= 0 || nsess > Session::kMaxBatch || (nops > 0 && !ops))
-    return GEMS_ERR_BAD_ARG;
+// every session's own op list (ops[i], nops[i]); sessions must share device, pattern count,
+// states, categories and slots.  All tcgen05 61-state sessions with lists of one length: one
+// launch for every session's op tables and one traversal launch over every (session, tile);
+// otherwise one traversal per session, each on its own stream (their work overlaps).
+static int traverse_batch_lists(gems_session *const *ss, int nsess, const gems_op *const *ops,
+                                const int *nops) {
+  if (!ss || !ops || !nops || nsess <= 0 || nsess > Session::kMaxBatch) return GEMS_ERR_BAD_ARG;
   Session *s0 = ss[0];
   if (!s0) return GEMS_ERR_BAD_ARG;
   bool tc = true;
@@ -761,6 +786,7 @@ int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, 
       set_error("batched sessions must share device, patterns, states, categories and slots");
       return GEMS_ERR_BAD_ARG;
     }
+    if (nops[i] < 0 || (nops[i] > 0 && !ops[i])) return GEMS_ERR_BAD_ARG;
     if (!s->model_set || !s->tips_ok) {
       set_error(!s->model_set ? "model not set" : "tip states invalid (last upload was rejected)");
       return GEMS_ERR_STATE;
@@ -770,47 +796,65 @@ int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, 
         set_error("a session appears twice in the batch");
         return GEMS_ERR_BAD_ARG;
       }
-    tc = tc && tc61_supported(s);
+    tc = tc && tc61_supported(s) && nops[i] == nops[0];
   }
   GEMS_CUDA(cudaSetDevice(s0->desc.device));
-  if (!tc) {  // no batched kernel for this form: one traversal per session, on its own stream
+  if (!tc || nops[0] == 0) {
     for (int i = 0; i < nsess; i++)
-      if (int st = run_ops(ss[i], ops, nops)) return st;
+      if (int st = run_ops(ss[i], ops[i], nops[i])) return st;
     for (int i = 0; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
     return GEMS_OK;
   }
   for (int i = 0; i < nsess; i++)
-    if (int st = upload_ops(ss[i], ops, nops)) return st;
+    if (int st = upload_ops(ss[i], ops[i], nops[i])) return st;
   // the batched launches (every session's op tables, then the traversal) run on the first
   // session's stream after every session's op list is on the device
   for (int i = 1; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
   std::vector<Session *> v(ss, ss + nsess);
-  if (int st = launch_traverse_tc61_batch(v.data(), nsess, nops, 0, s0->P, true)) return st;
-  for (int i = 0; i < nsess; i++) invalidate_theta(ss[i], ops, nops);
+  if (int st = launch_traverse_tc61_batch(v.data(), nsess, nops[0], 0, s0->P, true)) return st;
+  for (int i = 0; i < nsess; i++) invalidate_theta(ss[i], ops[i], nops[i]);
   return GEMS_OK;
 }
 
-int gems_branch_lnl_batch(gems_session *const *ss, int nsess, const gems_op *ops, int nops,
-                          const gems_branch *br, double *lnl) {
-  if (!lnl) return GEMS_ERR_BAD_ARG;
-  if (int st = gems_traverse_batch(ss, nsess, ops, nops)) return st;
+int gems_traverse_batch(gems_session *const *ss, int nsess, const gems_op *ops, int nops) {
+  if (!ss || nsess <= 0 || nsess > Session::kMaxBatch || (nops > 0 && !ops))
+    return GEMS_ERR_BAD_ARG;
+  std::vector<const gems_op *> o(nsess, ops);
+  std::vector<int> n(nsess, nops);
+  return traverse_batch_lists(ss, nsess, o.data(), n.data());
+}
+
+int gems_branch_lnl_batch_ops(gems_session *const *ss, int nsess, const gems_op *const *ops,
+                              const int *nops, const gems_branch *br, double *lnl) {
+  if (!lnl || !br) return GEMS_ERR_BAD_ARG;
+  for (int i = 0; i < nsess && ss; i++)
+    if (ss[i])
+      if (int st = check_branch(ss[i], &br[i])) return st;
+  if (int st = traverse_batch_lists(ss, nsess, ops, nops)) return st;
   bool mixed = true;
   for (int i = 0; i < nsess; i++) mixed = mixed && ss[i]->desc.precision == GEMS_PREC_MIXED;
   if (!mixed) {
     for (int i = 0; i < nsess; i++)
-      if (int st = gems_branch_lnl(ss[i], nullptr, 0, br, &lnl[i], nullptr)) return st;
+      if (int st = gems_branch_lnl(ss[i], nullptr, 0, &br[i], &lnl[i], nullptr)) return st;
     return GEMS_OK;
   }
   // every session's branch terms enqueued on its own stream first, then the results read
-  for (int i = 0; i < nsess; i++) {
-    if (int st = check_branch(ss[i], br)) return st;
-    if (int st = enqueue_theta_mixed(ss[i], br, true, false)) return st;
-  }
+  for (int i = 0; i < nsess; i++)
+    if (int st = enqueue_theta_mixed(ss[i], &br[i], true, false)) return st;
   for (int i = 0; i < nsess; i++) {
     GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
     lnl[i] = theta_mixed_lnl(ss[i]);
   }
   return GEMS_OK;
+}
+
+int gems_branch_lnl_batch(gems_session *const *ss, int nsess, const gems_op *ops, int nops,
+                          const gems_branch *br, double *lnl) {
+  if (!ss || !lnl || !br || nsess <= 0 || nsess > Session::kMaxBatch) return GEMS_ERR_BAD_ARG;
+  std::vector<const gems_op *> o(nsess, ops);
+  std::vector<int> n(nsess, nops);
+  std::vector<gems_branch> b(nsess, *br);
+  return gems_branch_lnl_batch_ops(ss, nsess, o.data(), n.data(), b.data(), lnl);
 }
 
 int gems_branch_lnl(gems_session *s, const gems_op *ops, int nops, const gems_branch *br,

@@ -146,6 +146,12 @@ int gems_set_model_from_rates(gems_session *s, const double *exch_upper, const d
 int gems_set_model_from_rates_batch(gems_session *const *sessions, int nsess,
                                     const double *exch_upper, const double *freq,
                                     const double *rates, const double *props);
+/* New category rates and proportions (rates[ncat], props[ncat]) with the eigensystem kept: what
+ * a new Gamma shape or FreeRate parameters change (RateGamma::computeFunction sets the shape,
+ * recomputes the rates and clears every partial, model/rategamma.cpp:178-186).  The rates come
+ * from the caller, as with gems_set_model.  Partials computed before are stale: clear them in
+ * the caller's tree (gems_tree_clear_all_partial_lh) before the next evaluation. */
+int gems_set_rates(gems_session *s, const double *rates, const double *props);
 /* Copy back the eigensystem in use (for inspection). */
 int gems_get_eigensystem(gems_session *s, double *eval, double *evec, double *inv_evec);
 
@@ -179,6 +185,12 @@ int gems_traverse_batch(gems_session *const *sessions, int nsess, const gems_op 
 /* gems_traverse_batch, then the branch lnL of each session (lnl[nsess]). */
 int gems_branch_lnl_batch(gems_session *const *sessions, int nsess, const gems_op *ops, int nops,
                           const gems_branch *br, double *lnl);
+/* As gems_branch_lnl_batch with each session's own op list (ops[i], nops[i]) and branch
+ * (br[i]): candidates on one tree whose branch lengths differ.  The 61-state mixed form batches
+ * when every list has the same length; every session's branch terms are enqueued before any
+ * result is read. */
+int gems_branch_lnl_batch_ops(gems_session *const *sessions, int nsess, const gems_op *const *ops,
+                              const int *nops, const gems_branch *br, double *lnl);
 /* Branch log-likelihood (computeLikelihoodBranchSIMD, tree/phylokernelnew.h:2658-3275),
  * after running ops (may be 0).  pattern_lh[nptn] optional (log-likelihood per pattern
  * including the scaling correction). */
@@ -356,6 +368,13 @@ int gems_tree_optimize_all_branches_batch(gems_tree *const *trees, int ntrees, i
  * with their subtrees, the partials looking back across u or v are invalidated.  The edge
  * list reported by gems_tree_get_edges changes accordingly. */
 int gems_tree_nni(gems_tree *t, int u, int v, int a, int b);
+/* PhyloTree::computeLikelihood of ntrees trees (one per session, sessions as required by
+ * gems_branch_lnl_batch_ops) evaluated together: each tree's stale partials and its branch,
+ * then one batched evaluation (lnl[ntrees]).  With gems_set_rates and
+ * gems_tree_clear_all_partial_lh it re-evaluates every ModelFinder candidate at a new Gamma
+ * shape at once (RateGamma::computeFunction, model/rategamma.cpp:178-186, once per candidate in
+ * the reference). */
+int gems_tree_compute_likelihood_batch(gems_tree *const *trees, int ntrees, double *lnl);
 /* The SPR move of PhyloTree::assessSPRMove (tree/phylotree.cpp:4822-4880): the subtree at node
  * is pruned from the internal node dad, whose two other neighbours s1 < s2 (by node id) are
  * joined by one branch of their summed length, and dad is inserted into the branch

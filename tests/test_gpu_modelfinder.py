@@ -91,3 +91,49 @@ def test_batched_optimisation_matches_oracle(gpu, n, k):
     for t in trees:
         t.close()
         t.session.close()
+
+
+@pytest.mark.parametrize("n,k,precision,scaling", [(4, 12, "fp64", "norm"),
+                                                   (4, 12, "mixed", "norm"),
+                                                   (20, 6, "mixed", "norm"),
+                                                   (61, 8, "mixed", "safe"),
+                                                   (61, 4, "fp64", "safe")])
+def test_gamma_shapes_batched_match_one_by_one_and_oracle(gpu, n, k, precision, scaling):
+    """Every candidate re-evaluated at a new Gamma shape in one batched call (new rates, all
+    partials cleared, lnL): equal bit for bit to each candidate's own computeLikelihood after
+    the same change, and to the oracle at the form's bar.  The candidates' trees carry
+    different branch lengths (each was optimised on its own), so every session evaluates its
+    own op list."""
+    from gems_b200 import evaluate_rates_batch
+    truth = candidates(n, 1, 91 + n)[0]
+    tree = synth.random_tree(14, 0.1, 92 + n)
+    aln = synth.simulate(tree, truth, {4: 2000, 20: 1000, 61: 500}[n], 93 + n)
+    models = candidates(n, k, 94 + n)
+    rng = np.random.default_rng(95 + n)
+    trees = [PhyloTree.from_case(tree, m, aln, precision=precision, scaling=scaling)
+             for m in models]
+    for t in trees:  # each candidate with its own lengths
+        for e in rng.choice(tree.nedges, 3, replace=False):
+            t.setLength(int(tree.eu[e]), int(tree.ev[e]), float(rng.uniform(0.01, 0.3)))
+        t.computeLikelihood()
+    alphas = rng.uniform(0.2, 2.0, k)
+    rates = [synth.gamma_rates(a, models[i].ncat) for i, a in enumerate(alphas)]
+    lnl_b = evaluate_rates_batch(trees, rates)
+    bar = 1e-9 if precision == "fp64" else 1e-6
+    for i, m in enumerate(models):
+        one = PhyloTree.from_case(tree, m, aln, precision=precision, scaling=scaling)
+        for (u, v), x in zip(zip(tree.eu, tree.ev), trees[i].getBranchLengths()):
+            one.setLength(int(u), int(v), float(x))
+        one.session.set_rates(rates[i], np.full(m.ncat, 1.0 / m.ncat))
+        one.clearAllPartialLH()
+        assert one.computeLikelihood() == lnl_b[i]
+        one.close()
+        one.session.close()
+        mm = synth.Model(n, m.exch_upper, m.freq, rates[i], m.props, m.eval, m.evec, m.inv_evec)
+        ot = orc.OracleTree(synth.Tree(tree.ntaxa, tree.eu, tree.ev, trees[i].getBranchLengths()),
+                            mm, aln, safe=scaling == "safe")
+        lo = ot.computeLikelihood()
+        assert abs(lnl_b[i] - lo) <= bar * abs(lo), (i, lnl_b[i], lo)
+    for t in trees:
+        t.close()
+        t.session.close()
