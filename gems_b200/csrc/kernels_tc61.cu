@@ -52,9 +52,17 @@ constexpr uint32_t kIdesc61 = idesc_tf32(kNP);
 constexpr int kTmemCols61 = 256;          // D[side] at side*64, A_hi[side] at 128 + side*64
 constexpr int kAhi61 = 128;
 
-// op tables: B images [side][C][hi, lo][16 K chunks][64 rows][4] (row = target state x,
-// K = source state y), floats per op
+// op tables: per side and category a 32 KB region.  An internal child's: the B images
+// [hi, lo][16 K chunks][64 rows][4] (row = target state x, K = source state y).  A tip child's:
+// its tip table [62 state codes][64 target states + 4 padding] -- row s < 61 is column s of P_c(t), the
+// message of a tip in state s; row 61 the row sums, the message of the unknown state (every
+// code >= 61) -- so a tip side needs neither MMAs nor B images.  Floats per op:
 __host__ __device__ constexpr size_t op_floats61(int C) { return (size_t)2 * C * (kBSide / 4); }
+constexpr int kTipRows61 = kN + 1;  // 61 states + unknown
+// a tip table row: 64 target states padded by 4 floats, so that the rows of different state
+// codes (the lanes of a warp read their own patterns' rows) start in different bank groups
+constexpr int kTipRow61 = kNP + 4;
+constexpr uint32_t kTipBytes61 = kTipRows61 * kTipRow61 * 4;  // 16,864 bytes
 
 // The op tables of a job's op k and side (blockIdx.x, blockIdx.y; job blockIdx.z of `jobs`, or
 // `one` when jobs is null).  P_c(t) = evec . diag(exp(eval * rate_c * t)) . inv_evec in FP64,
@@ -64,7 +72,9 @@ __host__ __device__ constexpr size_t op_floats61(int C) { return (size_t)2 * C *
 // runs in index order with the same fma(evec * exp, inv_evec, acc) steps as a scalar loop.
 // Shared memory: exp terms [C][n]; evec as [64][n] (rows 61..63 zero); inv_evec as
 // [n][4 e][16 j] = inv_evec[i][4j + e] (columns 61..63 zero), so that the 16 lanes of a
-// half-warp read 16 consecutive doubles.
+// half-warp read 16 consecutive doubles.  A tip side's unknown-state row sums are reduced over
+// the 16 lanes of a half-warp (the threads of one row quad) by a fixed shuffle tree: the same
+// bits in every launch.
 constexpr int kPrepThreads = 256;  // 16 row quads x 16 column quads
 __host__ __device__ constexpr size_t prep61_smem_doubles(int C) {
   return (size_t)C * kN + (size_t)kNP * kN + (size_t)kN * kNP;
@@ -95,6 +105,7 @@ __global__ void __launch_bounds__(kPrepThreads)
   float *img = const_cast<float *>(job.tab) + (size_t)k * stride_f + (size_t)side * C * (kBSide / 4);
   const int per = kBImg / 4;  // floats of one image
   const int j = threadIdx.x & 15, xq = threadIdx.x >> 4;
+  const bool tip = (side ? op.r_kind : op.l_kind) == GEMS_CHILD_TIP;
   for (int cc = 0; cc < C; cc++) {
     double acc[4][4];
 #pragma unroll
@@ -113,6 +124,34 @@ __global__ void __launch_bounds__(kPrepThreads)
       for (int r = 0; r < 4; r++)
 #pragma unroll
         for (int e = 0; e < 4; e++) acc[r][e] = fma(a[r], b[e], acc[r][e]);
+    }
+    if (tip) {
+      // tip table: row s = column s of P_c (target states x consecutive), then the row sums
+      float *tt = img + (size_t)cc * 2 * per;
+      double rs[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int y = 4 * j + e;
+        float v[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const int x = 4 * xq + r;
+          const double a = (x < n && y < n) ? fmax(acc[r][e], 0.0) : 0.0;
+          rs[r] += a;
+          v[r] = (float)a;
+        }
+        if (y < n)
+          *reinterpret_cast<float4 *>(tt + (size_t)y * kTipRow61 + 4 * xq) =
+              make_float4(v[0], v[1], v[2], v[3]);
+      }
+#pragma unroll
+      for (int o = 8; o >= 1; o >>= 1)
+#pragma unroll
+        for (int r = 0; r < 4; r++) rs[r] += __shfl_xor_sync(0xffffffffu, rs[r], o);
+      if (j == 0)
+        *reinterpret_cast<float4 *>(tt + (size_t)n * kTipRow61 + 4 * xq) =
+            make_float4((float)rs[0], (float)rs[1], (float)rs[2], (float)rs[3]);
+      continue;
     }
     // image element (row x, K index y) at chunk y / 4, row x, lane y % 4
 #pragma unroll
@@ -210,13 +249,17 @@ __device__ __forceinline__ void issue_late(const DevCtx &c, const Step &st, int 
     bulk_g2s(s ? sL1 : sL0, src, kATile, bar);
   }
 }
-// B images (hi and lo, both sides) of step `st`
-__device__ __forceinline__ void issue_b(const float *tab_op, int C, int cat, unsigned char *Bbase,
-                                        uint32_t bar) {
-  mbar_expect_tx(bar, 2 * kBSide);
+// the tables of step (op, cat): per side the B images (hi and lo) of an internal child or the
+// tip table of a tip child
+__device__ __forceinline__ void issue_b(const float *tab_op, int C, int cat, const DevOp &op,
+                                        unsigned char *Bbase, uint32_t bar) {
+  uint32_t bytes[2];
+  for (int s = 0; s < 2; s++)
+    bytes[s] = (s ? op.r_kind : op.l_kind) == GEMS_CHILD_PARTIAL ? (uint32_t)kBSide : kTipBytes61;
+  mbar_expect_tx(bar, bytes[0] + bytes[1]);
   for (int s = 0; s < 2; s++)
     bulk_g2s(sptr(Bbase + (size_t)s * kBSide),
-             tab_op + ((size_t)s * C + cat) * (kBSide / 4), kBSide, bar);
+             tab_op + ((size_t)s * C + cat) * (kBSide / 4), bytes[s], bar);
 }
 
 __global__ void __launch_bounds__(kThreads61, 1)
@@ -267,7 +310,7 @@ __global__ void __launch_bounds__(kThreads61, 1)
   Step cur{ops[0], 0};
   if (warp == 0 && elect_one()) {
     issue_land(c, cur, -1, sL0, sL1, tile, bar_land);
-    issue_b(tab, C, 0, Bbase, bar_b);
+    issue_b(tab, C, 0, cur.op, Bbase, bar_b);
   }
   land_pending = b_pending = true;
   int st_l = 0, st_r = 0;  // tip state codes of the current op
@@ -305,31 +348,33 @@ __global__ void __launch_bounds__(kThreads61, 1)
     land_pending = b_pending = false;
     ph_land ^= 1;
     ph_b ^= 1;
-    // operand rows: hi -> TMEM, lo -> shared memory; tips as one-hot rows
+    // operand rows of internal children: hi -> TMEM, lo -> shared memory.  A tip child's
+    // message is its tip table's row: copied into the side's lo buffer (which its side does not
+    // use), so that the next step's tables can overwrite the table region during the epilogue
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-      float h[32];
-      if (s ? inR : inL) {
-        const float4 *a4 = reinterpret_cast<const float4 *>(land + (size_t)s * kATile);
-        float4 *l4 = reinterpret_cast<float4 *>(alo + (size_t)s * kATile);
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const int ch = 8 * half + i;
-          float4 hv, lv;
-          split4(a4[ch * kTile + row], hv, lv);
-          l4[ch * kTile + row] = lv;
-          h[4 * i] = hv.x;
-          h[4 * i + 1] = hv.y;
-          h[4 * i + 2] = hv.z;
-          h[4 * i + 3] = hv.w;
-        }
-      } else {
+      float4 *l4 = reinterpret_cast<float4 *>(alo + (size_t)s * kATile);
+      if (!(s ? inR : inL)) {
         const int st = s ? st_r : st_l;
+        const float4 *tr = reinterpret_cast<const float4 *>(
+                               Bbase + (size_t)s * kBSide + (size_t)(st < kN ? st : kN) * kTipRow61 * 4) +
+                           8 * half;
 #pragma unroll
-        for (int i = 0; i < 32; i++) {
-          const int x = 32 * half + i;
-          h[i] = (x < kN && (st == x || st >= kN)) ? 1.f : 0.f;
-        }
+        for (int i = 0; i < 8; i++) l4[(8 * half + i) * kTile + row] = tr[i];
+        continue;
+      }
+      float h[32];
+      const float4 *a4 = reinterpret_cast<const float4 *>(land + (size_t)s * kATile);
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const int ch = 8 * half + i;
+        float4 hv, lv;
+        split4(a4[ch * kTile + row], hv, lv);
+        l4[ch * kTile + row] = lv;
+        h[4 * i] = hv.x;
+        h[4 * i + 1] = hv.y;
+        h[4 * i + 2] = hv.z;
+        h[4 * i + 3] = hv.w;
       }
       tmem_st32(tmem + lane_off + (uint32_t)(kAhi61 + s * kNP + 32 * half), h);
     }
@@ -338,12 +383,13 @@ __global__ void __launch_bounds__(kThreads61, 1)
     fence_before();
     __syncthreads();
     fence_after();
+    const bool any_in = inL || inR;
     if (warp == 0 && elect_one()) {
       // the landing buffers have been read: the next step's tiles come in
       if (has_next) issue_land(c, nxt, late, sL0, sL1, tile, bar_land);
 #pragma unroll
       for (int s = 0; s < 2; s++) {
-        const bool in = s ? inR : inL;
+        if (!(s ? inR : inL)) continue;
         const uint32_t dtm = tmem + (uint32_t)(s * kNP);
         const uint32_t atm = tmem + (uint32_t)(kAhi61 + s * kNP);
 #pragma unroll
@@ -353,38 +399,58 @@ __global__ void __launch_bounds__(kThreads61, 1)
           const uint64_t bh = dB[s] + kb, bl = dB[s] + kb + (uint64_t)(kBImg >> 4);
           mma_ts(dtm, atm + 8 * ks, bh, kIdesc61, ks > 0 ? 1u : 0u);
           mma_ts(dtm, atm + 8 * ks, bl, kIdesc61, 1u);
-          if (in) mma_ss(dtm, dLo[s] + ko, bh, kIdesc61, 1u);
+          mma_ss(dtm, dLo[s] + ko, bh, kIdesc61, 1u);
         }
       }
-      mma_commit(bar_mma);
+      if (any_in) mma_commit(bar_mma);
     }
     land_pending = has_next;
-    mma_pending = true;
-    if (__syncthreads_or(!mbar_wait(bar_mma, ph_mma))) {
-      ok = false;
-      if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
-      break;
+    if (any_in) {
+      mma_pending = true;
+      if (__syncthreads_or(!mbar_wait(bar_mma, ph_mma))) {
+        ok = false;
+        if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+        break;
+      }
+      mma_pending = false;
+      ph_mma ^= 1;
+      fence_after();
     }
-    mma_pending = false;
-    ph_mma ^= 1;
-    fence_after();
-    // B images of this step are no longer read: the next step's come in under the epilogue
+    // the tables of this step are no longer read (the MMAs are done, the tip rows copied out):
+    // the next step's come in under the epilogue
     if (has_next) {
       if (warp == 0 && elect_one())
-        issue_b(tab + (size_t)(cur.cat + 1 < C ? k : k + 1) * stride_f, C, nxt.cat, Bbase, bar_b);
+        issue_b(tab + (size_t)(cur.cat + 1 < C ? k : k + 1) * stride_f, C, nxt.cat, nxt.op,
+                Bbase, bar_b);
       b_pending = true;
     }
     // ---- epilogue: products, SAFE rescaling of this category, stores
-    uint32_t rl[32], rr[32];
-    tmem_ld32(tmem + lane_off + (uint32_t)(0 * kNP + 32 * half), rl);
-    tmem_ld32(tmem + lane_off + (uint32_t)(1 * kNP + 32 * half), rr);
-    tmem_ld32_wait(rl);
-    tmem_ld32_wait(rr);
+    // messages: an internal child's from its accumulator, a tip's from its table row
+    uint32_t rm[2][32];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (s ? inR : inL) tmem_ld32(tmem + lane_off + (uint32_t)(s * kNP + 32 * half), rm[s]);
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      if (s ? inR : inL) {
+        tmem_ld32_wait(rm[s]);
+      } else {
+        const float4 *tr = reinterpret_cast<const float4 *>(alo + (size_t)s * kATile);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const float4 q = tr[(8 * half + i) * kTile + row];
+          rm[s][4 * i] = __float_as_uint(q.x);
+          rm[s][4 * i + 1] = __float_as_uint(q.y);
+          rm[s][4 * i + 2] = __float_as_uint(q.z);
+          rm[s][4 * i + 3] = __float_as_uint(q.w);
+        }
+      }
+    }
     float v[32];
     float mx = 0.f;
 #pragma unroll
     for (int i = 0; i < 32; i++) {
-      v[i] = fmaxf(__uint_as_float(rl[i]), 0.f) * fmaxf(__uint_as_float(rr[i]), 0.f);
+      v[i] = fmaxf(__uint_as_float(rm[0][i]), 0.f) * fmaxf(__uint_as_float(rm[1][i]), 0.f);
       mx = fmaxf(mx, v[i]);
     }
     ctl->rowmax[half][row] = mx;
