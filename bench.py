@@ -642,10 +642,11 @@ def ingest_block(aln, local, reps=3):
 
 def serving_block(local, nsess=48, nreq=800, load=0.7, taxa=(8, 256), sites=(500, 50_000)):
     """The serving loop on a seeded stream: sessions of 8-256 taxa and 500-50,000 sites
-    (log-uniform), 4/20/61 states, 1/4/8 categories, FP64/mixed; NNI + 5-branch Newton + lnL
-    per request.  Two passes over the same stream, sessions opened before each: every request
-    queued at once gives the capacity; Poisson arrivals at `load` x capacity give the request
-    latency.  Session open times (create, upload, first full lnL) are reported apart."""
+    (log-uniform), 4/20/61 states, 1/4/8 categories, FP64/mixed; per request an NNI with Newton
+    on the 5 branches around it, or (30%) an SPR with Newton on 4 branches, then the lnL.  Passes
+    over the same stream, sessions opened before each: every request queued at once gives the
+    capacity; Poisson arrivals at `load` and at half of the capacity give the request latency.
+    Session open times (create, upload, first full lnL) are reported apart."""
     import torch
     from gems_b200 import serve
     kw = dict(seed=5, taxa=taxa, sites=sites)
@@ -654,6 +655,9 @@ def serving_block(local, nsess=48, nreq=800, load=0.7, taxa=(8, 256), sites=(500
     torch.cuda.empty_cache()
     free_gb = torch.cuda.mem_get_info(local)[0] / 1e9
     srv = serve.Server(device=local, workers=16)
+    # untimed warm-up over the first quarter of the stream: a running server has loaded its
+    # kernels and tuned its launch shapes before the requests measured here arrive
+    srv.run(specs, cases, [(0.0, sid) for _, sid in reqs[: max(1, nreq // 4)]], preopen=True)
     records, wall = srv.run(specs, cases, [(0.0, sid) for _, sid in reqs], preopen=True)
     cap = serve.summarize(records, wall, specs, cases)
     opened = np.array(srv.open_ms)
@@ -680,7 +684,8 @@ def serving_block(local, nsess=48, nreq=800, load=0.7, taxa=(8, 256), sites=(500
                 "evictions": srv.evictions,
                 "stream": f"seeded; taxa {taxa[0]}-{taxa[1]}, sites {sites[0]:,}-{sites[1]:,} "
                           "(log-uniform), states {4,20,61}, categories {1,4,8}, fp64/mixed; "
-                          "request = NNI + Newton on the 5 branches around it + lnL; latency at "
+                          "request = NNI + Newton on the 5 branches around it, or (30%) SPR "
+                          "within radius 3 + Newton on 4 branches, then lnL; latency at "
                           "Poisson arrivals; sessions that fit the HBM budget opened first, the "
                           "others admitted as memory frees"})
     return out

@@ -13,9 +13,12 @@ Only the partials on the affected paths are recomputed.
 
 Scheduling:
   * admission by HBM footprint: a session is created on the GPU when its footprint
-    (gems_session_footprint) fits the remaining budget; it is released after its last
-    request, which admits the next waiting ones.  When the session at the head of the
-    admission queue does not fit, idle sessions (no request running or queued) are evicted,
+    (gems_session_footprint) fits the remaining budget.  A session whose last request has
+    finished stays resident until admission needs its memory or the stream ends: freeing
+    device memory synchronises the whole GPU, so closing it at once stalls every other
+    session's requests.  Admission plans with that memory as free and releases finished
+    sessions first.  When the session at the head of the admission queue still does not fit,
+    idle sessions (no request running or queued) are evicted,
     least recently used first: the evolved tree (topology and branch lengths) is kept on the
     host and the session is rebuilt from it at its next request -- partials are a function of
     the tree, so its results are the same as if it had stayed;
@@ -134,41 +137,50 @@ SPR_RADIUS = 3      # regraft branches at most this many branches from the prune
 SPR_SHARE = 0.3     # share of requests that are SPR moves (the rest are NNI)
 
 
-def spr_regraft_branches(gt, node, dad, radius=SPR_RADIUS):
+def _adjacency(gt):
+    """Every node's neighbours in edge order (the order gt.neighbors returns them in), built in
+    one pass over the edge list."""
+    adj = collections.defaultdict(list)
+    for a, b in zip(gt.eu.tolist(), gt.ev.tolist()):
+        adj[a].append(b)
+        adj[b].append(a)
+    return adj
+
+
+def spr_regraft_branches(gt, node, dad, radius=SPR_RADIUS, adj=None):
     """Branches (x, y) the subtree at node (pruned from dad) can be regrafted into: those of the
     remaining tree within `radius` branches of the joint that pruning leaves (dad's two other
     neighbours s1, s2, joined), the joint itself excluded (regrafting there is no move).  The
     search walks outwards from s1 and s2, as swapSPR does up to its radius
     (tree/phylotree.cpp:4694-4820)."""
-    s1, s2 = sorted(x for x in gt.neighbors(dad) if x != node)
-    out, frontier, seen = [], [(s1, dad), (s2, dad)], {dad, s1, s2}
+    adj = _adjacency(gt) if adj is None else adj
+    s1, s2 = sorted(x for x in adj[dad] if x != node)
+    out, frontier = [], [(s1, dad), (s2, dad)]
     for _ in range(radius):
         nxt = []
         for x, back in frontier:
-            for y in gt.neighbors(x):
-                if y == back or y == dad or y in (s1, s2) and x in (s1, s2):
+            for y in adj[x]:
+                if y == back or y == dad:
                     continue
                 out.append((y, x))
-                if y not in seen:
-                    seen.add(y)
-                    nxt.append((y, x))
+                nxt.append((y, x))
         frontier = nxt
     return s1, s2, out
 
 
 def spr4(gt, ntaxa: int, rng: np.random.Generator, radius=SPR_RADIUS):
-    """One SPR request: a random subtree pruned from a random internal node and regrafted into
-    a branch within `radius` (assessSPRMove's move, tree/phylotree.cpp:4822-4880), Newton on the
-    four branches swapSPR optimises after a move (the pruned subtree's branch, the two halves
-    of the regraft branch and the joined branch, tree/phylotree.cpp:4764-4768), then the lnL
-    from the buffers.  Returns (lnL, branches optimised)."""
-    edges = list(zip(gt.eu.tolist(), gt.ev.tolist()))
-    for _ in range(64):
-        u, v = edges[int(rng.integers(len(edges)))]
-        node, dad = (u, v) if rng.integers(2) else (v, u)
-        if dad < ntaxa:
-            continue
-        s1, s2, cand = spr_regraft_branches(gt, node, dad, radius)
+    """One SPR request: the subtree at a random neighbour of a random internal node pruned and
+    regrafted into a branch within `radius` (assessSPRMove's move,
+    tree/phylotree.cpp:4822-4880), Newton on the four branches swapSPR optimises after a move
+    (the pruned subtree's branch, the two halves of the regraft branch and the joined branch,
+    tree/phylotree.cpp:4764-4768), then the lnL from the buffers.  Returns (lnL, branches
+    optimised)."""
+    adj = _adjacency(gt)
+    internal = sorted(u for u, nb in adj.items() if len(nb) == 3)
+    for _ in range(16):
+        dad = internal[int(rng.integers(len(internal)))]
+        node = adj[dad][int(rng.integers(3))]
+        s1, s2, cand = spr_regraft_branches(gt, node, dad, radius, adj)
         if cand:
             break
     else:
@@ -248,15 +260,21 @@ class Server:
         self.open_ms = []
         self.evictions = 0
         saved = {}       # sid -> tree of an evicted session
+        # sessions whose last request has finished: they stay resident until admission needs
+        # their memory or the stream ends -- freeing device memory synchronises the whole GPU,
+        # so closing them while other sessions' requests run would stall those requests
+        finished = set()
         open_fail = collections.Counter()
         last_used = {}   # sid -> end of its last request
         for sid in fp:
             if fp_min[sid] > self.budget:
                 state["rejected"].add(sid)
 
-        def plan_locked(sid):
-            """Admission plan of sid in the free budget: sets fp[sid] (and its slots)."""
-            plan = spec_of[sid].slot_plan(npat[sid], self.budget - state["used"], self.memsave)
+        def plan_locked(sid, extra=0):
+            """Admission plan of sid in the free budget (plus `extra` bytes about to be released):
+            sets fp[sid] (and its slots)."""
+            plan = spec_of[sid].slot_plan(npat[sid], self.budget - state["used"] + extra,
+                                          self.memsave)
             if plan is None:
                 return False
             n, b = plan
@@ -321,20 +339,25 @@ class Server:
                 return None, []
             sid = waiting_admit[0]
             victims = []
-            if plan_locked(sid):  # fits the free budget, at full size or as a pool
-                need = 0
+            # finished sessions hold memory nobody needs: plan as if it were free
+            releasable = sum(fp[s] for s, g in open_sess.items()
+                             if s in finished and not isinstance(g, str))
+            if plan_locked(sid, releasable):  # fits, at full size or as a pool
+                need = state["used"] + fp[sid] - self.budget
             else:  # room for its smallest admissible form, from idle sessions
                 fp[sid] = fp_min[sid]
                 if self.memsave:
                     nslots_of[sid] = min_pool_slots(spec_of[sid].ntaxa)
                 need = state["used"] + fp[sid] - self.budget
             if need > 0:
-                if not self.evict:
-                    return None, []
-                idle = sorted((last_used.get(s, 0.0), s) for s, g in open_sess.items()
-                              if not isinstance(g, str) and s not in busy and not pending[s])
+                # finished sessions first, then (with eviction) idle ones least recently used
+                # first
+                idle = sorted((s not in finished, last_used.get(s, 0.0), s)
+                              for s, g in open_sess.items()
+                              if not isinstance(g, str) and s not in busy and not pending[s]
+                              and (self.evict or s in finished))
                 freed = 0
-                for _, s in idle:
+                for _, _, s in idle:
                     if freed >= need:
                         break
                     victims.append((s, open_sess.pop(s)))
@@ -344,6 +367,8 @@ class Server:
                         open_sess[s] = g
                     return None, []
                 for s, g in victims:  # their memory counts as used until they are closed
+                    if s in finished:
+                        continue
                     saved[s] = saved_tree(g, spec_of[s].ntaxa)  # before any reopen can read it
                     self.evictions += 1
             waiting_admit.popleft()
@@ -439,10 +464,7 @@ class Server:
                     state["done"] += 1
                     remaining[sid] -= 1
                     if remaining[sid] == 0:
-                        gt.close()
-                        gt.session.close()
-                        open_sess[sid] = "closed"
-                        state["used"] -= fp[sid]
+                        finished.add(sid)
                     lock.notify_all()
 
         threads = [threading.Thread(target=worker) for _ in range(self.workers)]
@@ -453,7 +475,12 @@ class Server:
         disp.join()
         for th in threads:
             th.join()
-        return records, time.perf_counter() - t0
+        wall = time.perf_counter() - t0
+        for s, g in open_sess.items():  # the stream is over: release every session
+            if not isinstance(g, str):
+                g.close()
+                g.session.close()
+        return records, wall
 
 
 def make_stream(nsessions, nrequests, rate, seed, taxa=(8, 1024), sites=(500, 500_000),
