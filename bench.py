@@ -835,18 +835,21 @@ def main():
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
-    # the floor the upload sets: a plain copy of the same host bytes (pinned) to the device
+    # the floor the upload sets: a plain copy of the same host bytes (pinned) to the device, on
+    # a stream torch owns (the pinned allocator records the streams its buffers were copied on,
+    # and the session's stream is destroyed when the session closes)
     dev_pat = torch.empty(aln.patterns.shape, dtype=torch.uint8, device=f"cuda:{local}")
     dev_w = torch.empty(aln.weights.shape, dtype=torch.float64, device=f"cuda:{local}")
-    with torch.cuda.stream(stream):
+    cs = torch.cuda.Stream(device=local)
+    with torch.cuda.stream(cs):
         for _ in range(2):
             dev_pat.copy_(pin_pat, non_blocking=True)
             dev_w.copy_(pin_w, non_blocking=True)
-        e2.record(stream)
+        e2.record(cs)
         for _ in range(args.steps):
             dev_pat.copy_(pin_pat, non_blocking=True)
             dev_w.copy_(pin_w, non_blocking=True)
-        e3.record(stream)
+        e3.record(cs)
     torch.cuda.synchronize()
     ms_h2d = e2.elapsed_time(e3) / args.steps
     del dev_pat, dev_w

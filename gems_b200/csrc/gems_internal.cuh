@@ -191,6 +191,7 @@ struct Session {
   // per pattern chunk and a pinned word for the tip check, created on first use
   static constexpr int kMaxChunks = 64;
   cudaStream_t copy_stream = nullptr;
+  cudaStream_t check_stream = nullptr;  // tip-byte checks of the chunks the copy stream brought
   cudaEvent_t start_ev = nullptr;
   cudaEvent_t chunk_ev[kMaxChunks] = {};
   unsigned int *h_tipmax = nullptr;

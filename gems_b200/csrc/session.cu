@@ -201,6 +201,10 @@ static void free_session(Session *s) {
     cudaStreamSynchronize(s->copy_stream);
     cudaStreamDestroy(s->copy_stream);
   }
+  if (s->check_stream) {
+    cudaStreamSynchronize(s->check_stream);
+    cudaStreamDestroy(s->check_stream);
+  }
   if (s->start_ev) cudaEventDestroy(s->start_ev);
   for (cudaEvent_t e : s->chunk_ev)
     if (e) cudaEventDestroy(e);
@@ -903,17 +907,22 @@ int gems_branch_lnl_from_host(gems_session *s, const uint8_t *states, const doub
   }
   if (!s->copy_stream)
     GEMS_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+  if (!s->check_stream)
+    GEMS_CUDA(cudaStreamCreateWithFlags(&s->check_stream, cudaStreamNonBlocking));
   if (!s->start_ev) GEMS_CUDA(cudaEventCreateWithFlags(&s->start_ev, cudaEventDisableTiming));
   for (cudaEvent_t &e : s->chunk_ev)
     if (!e) GEMS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   if (!s->h_tipmax) GEMS_CUDA(cudaHostAlloc((void **)&s->h_tipmax, sizeof(unsigned int), 0));
   const int n = s->desc.nptn, ntaxa = s->desc.ntaxa;
   unsigned int *d_max = reinterpret_cast<unsigned int *>(s->d_flag) + 8;
-  cudaStream_t cs = s->copy_stream;
+  // the copy stream carries only the copies, back to back; each chunk's tip-byte check runs on
+  // the check stream once the chunk has arrived, beside the next copy
+  cudaStream_t cs = s->copy_stream, ks = s->check_stream;
   // nothing queued on the session stream may still read the old tips, weights or +I terms
   GEMS_CUDA(cudaEventRecord(s->start_ev, s->stream));
   GEMS_CUDA(cudaStreamWaitEvent(cs, s->start_ev, 0));
-  GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), cs));
+  GEMS_CUDA(cudaStreamWaitEvent(ks, s->start_ev, 0));
+  GEMS_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), ks));
   // +I terms first (the traversal's scaling rule reads them); the weights, which only the branch
   // terms read, go up after the last tip chunk
   if (ptn_invar)
@@ -937,18 +946,20 @@ int gems_branch_lnl_from_host(gems_session *s, const uint8_t *states, const doub
     if (w > 0)
       GEMS_CUDA(cudaMemcpy2DAsync(s->d_tips + p0, s->P, states + p0, n, w, ntaxa,
                                   cudaMemcpyHostToDevice, cs));
+    GEMS_CUDA(cudaEventRecord(s->chunk_ev[c], cs));
+    GEMS_CUDA(cudaStreamWaitEvent(ks, s->chunk_ev[c], 0));
     const long long words = (long long)(p1 - p0) / 16 * ntaxa;
     const int grid = (int)std::min<long long>(148 * 8, (words + 255) / 256);
-    k_tips_max<<<grid, 256, 0, cs>>>(s->d_tips, s->P, n, ntaxa, p0, p1, d_max);
+    k_tips_max<<<grid, 256, 0, ks>>>(s->d_tips, s->P, n, ntaxa, p0, p1, d_max);
     s->launches++;
     GEMS_CUDA(cudaGetLastError());
-    GEMS_CUDA(cudaEventRecord(s->chunk_ev[c], cs));
     GEMS_CUDA(cudaStreamWaitEvent(s->stream, s->chunk_ev[c], 0));
     if ((st = launch_traverse_v2(s, nops, p0, p1))) return st;
   }
   GEMS_CUDA(cudaMemcpyAsync(s->d_freq, ptn_freq, n * sizeof(double), cudaMemcpyHostToDevice, cs));
-  GEMS_CUDA(cudaMemcpyAsync(s->h_tipmax, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost, cs));
+  GEMS_CUDA(cudaMemcpyAsync(s->h_tipmax, d_max, sizeof(unsigned int), cudaMemcpyDeviceToHost, ks));
   GEMS_CUDA(cudaStreamSynchronize(cs));
+  GEMS_CUDA(cudaStreamSynchronize(ks));
   if ((int)*s->h_tipmax > s->unknown) {
     s->tips_ok = false;
     GEMS_CUDA(cudaStreamSynchronize(s->stream));
