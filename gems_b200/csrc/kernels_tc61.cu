@@ -6,24 +6,28 @@
 // For a tile of 128 patterns each child product is D[128 x 64] = A[128 x 64] . B^T (61 states
 // padded to 64 in K and N; the padding rows of B are zero), issued as tcgen05.mma kind::tf32
 // M=128 N=64 K=8, FP32 accuracy from split TF32 (A.B ~ A_hi.B_hi + A_hi.B_lo + A_lo.B_hi).
-// A tip child is a one-hot (or all-ones for the unknown state) operand row, exact in TF32, so it
-// needs only the first two products and no table.
+// A tip child needs no product: its message is a row of the op's tip table (column s of
+// P_c(t) for a tip in state s, the row sums for the unknown state), which the table copy brings
+// in place of that side's B images.
 //
 // The work of one op is done category by category ("steps"): one category of a child tile is
 // 16 chunks x 2 KB = 32 KB, contiguous in the tile-major layout (mix_off<61>), brought by one
 // cp.async.bulk.  Per step (one CTA per SM, 256 threads, 2 per pattern row):
-//   wait(operand tiles, B images of this step)
-//   -> split: hi -> TMEM operand columns (tcgen05.st), lo -> shared memory; one-hot rows of tips
+//   wait(operand tiles, tables of this step)
+//   -> split of internal children: hi -> TMEM operand columns (tcgen05.st), lo -> shared
+//      memory; a tip child's table row is copied into its side's (unused) lo buffer
 //   -> the next step's operand tiles start copying (landing buffers free)
-//   -> MMAs (issued by an elected lane), wait -> the next step's B images start copying
+//   -> MMAs of internal children (issued by an elected lane), wait -> the next step's tables
+//      start copying
 //   -> epilogue: tcgen05.ld of the accumulators, products, SAFE rescaling by 2^64 with uint16
 //      counters, coalesced stores of the rows (as computed; every consumer splits the stored
 //      values the same way)
 // The step after the last category of an op may need that op's output of the same category
 // (one category: C = 1); that copy is issued after the epilogue's stores instead.
 //
-// The kernel takes an array of jobs (sessions that share one tree and op list: ModelFinder's
-// candidate models on one alignment), grid (tiles, jobs), so many small sessions fill the GPU
+// The kernel takes an array of jobs (sessions that share one tree: ModelFinder's candidate
+// models on one alignment; each job has its own op list), grid (tiles, jobs), so many small
+// sessions fill the GPU
 // in one launch.  Every mbarrier wait is bounded; on expiry the CTA records GEMS_ERR_TIMEOUT,
 // waits (bounded) for its copies in flight, frees its TMEM and returns.
 #include <cstring>
