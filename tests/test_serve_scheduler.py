@@ -96,3 +96,59 @@ def test_session_that_cannot_fit_is_rejected():
     for r, (_, sid) in zip(records, reqs):
         assert bool(r.get("rejected")) == (fps[sid] > budget)
     same_as_alone(specs, cases, [r for r in records if not r.get("rejected")])
+
+
+class CountingSession(OracleSession):
+    """OracleSession that records when it was closed and whether requests were still running."""
+    log = []
+
+    def __init__(self, spec, case, device=0, tree=None, nslots=None):
+        super().__init__(spec, case, device, tree, nslots)
+        self.sid = spec.sid
+        self.session = types.SimpleNamespace(close=lambda: None)
+
+    def close(self):
+        CountingSession.log.append(self.sid)
+
+
+def test_finished_sessions_stay_resident_until_the_stream_ends():
+    """With room for every session, none is closed while the stream runs (closing frees device
+    memory, which synchronises the GPU): every close comes after the last request."""
+    specs, reqs, cases = stream(5, 30, seed=12, rate=2000.0)
+    CountingSession.log = []
+    srv = serve.Server(budget_bytes=1 << 60, workers=3, opener=CountingSession)
+    done_before = []
+    orig = serve.tree_move
+
+    def move(gt, ntaxa, rng):
+        done_before.append(len(CountingSession.log))
+        return orig(gt, ntaxa, rng)
+
+    serve.tree_move = move
+    try:
+        records, _ = srv.run(specs, cases, reqs)
+    finally:
+        serve.tree_move = orig
+    assert all(r is not None and not r.get("error") for r in records)
+    assert max(done_before) == 0            # nothing was closed while requests ran
+    assert sorted(CountingSession.log) == sorted({sid for _, sid in reqs})
+    assert srv.evictions == 0
+    same_as_alone(specs, cases, records)
+
+
+def test_finished_sessions_released_before_idle_ones_are_evicted():
+    """A budget for about two sessions: finished sessions make room first, so fewer idle
+    sessions (with requests still to come) are evicted than sessions are admitted late; results
+    are unchanged."""
+    specs, reqs, cases = stream(6, 36, seed=13, rate=400.0)
+    fps = sorted(s.footprint(cases[s.sid][2].npat) for s in specs)
+    CountingSession.log = []
+    srv = serve.Server(budget_bytes=fps[-1] + fps[-2], workers=2, opener=CountingSession,
+                       memsave=False)
+    records, _ = srv.run(specs, cases, reqs)
+    assert all(r is not None and not r.get("rejected") and not r.get("error") for r in records)
+    same_as_alone(specs, cases, records)
+    # every close of a session with requests still to come is an eviction; the others were
+    # finished sessions released for room or at the end
+    assert len(CountingSession.log) >= len({sid for _, sid in reqs})
+    assert srv.evictions == len(CountingSession.log) - len({sid for _, sid in reqs})
