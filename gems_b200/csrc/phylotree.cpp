@@ -829,7 +829,14 @@ int gems_tree_compute_likelihood_batch(gems_tree *const *trees, int ntrees, doub
     ops[i] = t->ops.data();
     nops[i] = (int)t->ops.size();
   }
-  return gems_branch_lnl_batch_ops(ss.data(), ntrees, ops.data(), nops.data(), br.data(), lnl);
+  const int st =
+      gems_branch_lnl_batch_ops(ss.data(), ntrees, ops.data(), nops.data(), br.data(), lnl);
+  if (st) {
+    // the op lists marked their partials computed, but nothing (or not all of it) ran: every
+    // tree recomputes from scratch at its next evaluation
+    for (int i = 0; i < ntrees; i++) std::fill(trees[i]->computed.begin(), trees[i]->computed.end(), 0);
+  }
+  return st;
 }
 
 int gems_tree_nni(gems_tree *t, int u, int v, int a, int b) {

@@ -137,3 +137,35 @@ def test_gamma_shapes_batched_match_one_by_one_and_oracle(gpu, n, k, precision, 
     for t in trees:
         t.close()
         t.session.close()
+
+
+def test_rate_and_batch_error_paths(gpu):
+    """gems_set_rates before any model is a state error; a negative rate is refused; a batch of
+    sessions of different shapes is refused before anything runs."""
+    from gems_b200 import GemsError, compute_likelihood_batch
+    m4 = candidates(4, 1, 5)[0]
+    tree = synth.random_tree(10, 0.1, 6)
+    aln = synth.simulate(tree, m4, 300, 7)
+    s = Session(tree.ntaxa, aln.npat, 4, m4.ncat, tree.ntaxa - 2, "fp64", "norm")
+    with pytest.raises(GemsError) as e:
+        s.set_rates(m4.rates, m4.props)
+    assert e.value.status == 7  # GEMS_ERR_STATE
+    s.close()
+    a = PhyloTree.from_case(tree, m4, aln)
+    with pytest.raises(GemsError) as e:
+        a.session.set_rates(-m4.rates, m4.props)
+    assert e.value.status == 5  # GEMS_ERR_BAD_ARG
+    m20 = candidates(20, 1, 8)[0]
+    aln20 = synth.simulate(tree, m20, 300, 9)
+    b = PhyloTree.from_case(tree, m20, aln20)
+    with pytest.raises(GemsError) as e:
+        compute_likelihood_batch([a, b])
+    assert e.value.status == 5
+    # the refused batch left no partial marked computed that was not: each tree still gives
+    # its own lnL
+    la = compute_likelihood_batch([a])[0]
+    a.clearAllPartialLH()
+    assert a.computeLikelihood() == la
+    for t in (a, b):
+        t.close()
+        t.session.close()
