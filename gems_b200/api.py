@@ -476,13 +476,15 @@ class PhyloTree:
     def from_case(cls, tree, model, aln, precision="fp64", scaling="norm", device=0,
                   slots="node", invar=None):
         """Session + tree for a synthetic case (synth.Tree, synth.Model, synth.Alignment).
-        slots: "node" (one partial per internal node, LM_PER_NODE), "branch" (one per directed
-        branch), "pool" (LM_MEM_SAVE at its floor, log2(ntaxa) + 1 slots) or a slot count."""
+        slots: "node" (one partial per internal node, LM_PER_NODE), "node+spare" (the same
+        with two spare slots for evaluateNNI, the reference's nni_partial_lh), "branch" (one
+        per directed branch), "pool" (LM_MEM_SAVE at its floor, log2(ntaxa) + 1 slots) or a
+        slot count."""
         nint = tree.ntaxa - 2
         if isinstance(slots, int):
             nslots = slots
         else:
-            nslots = {"node": nint, "branch": 3 * nint,
+            nslots = {"node": nint, "node+spare": nint + 2, "branch": 3 * nint,
                       "pool": min_pool_slots(tree.ntaxa)}[slots]
         s = Session(tree.ntaxa, aln.npat, model.nstates, model.ncat, nslots, precision,
                     scaling, device)
@@ -583,6 +585,18 @@ class PhyloTree:
         if len(i) == 0:
             raise KeyError((u, v))
         return float(self.getBranchLengths()[i[0]])
+
+    def evaluateNNI(self, u, v, maxNRStep=10):
+        """getBestNNIForBran's evaluation of the internal branch (u, v), the tree unchanged
+        (gems_tree_nni_evaluate): [(a, b, lnl, lengths[5])] for the two NNIs, lengths =
+        central, u's outer two, v's outer two."""
+        moves = np.zeros(4, np.int32)
+        lnl = np.zeros(2)
+        lens = np.zeros(10)
+        _check(self.lib.gems_tree_nni_evaluate(self.handle, u, v, int(maxNRStep), _dptr(moves),
+                                               _dptr(lnl), _dptr(lens)), "evaluateNNI")
+        return [(int(moves[2 * c]), int(moves[2 * c + 1]), float(lnl[c]), lens[5 * c:5 * c + 5])
+                for c in range(2)]
 
     def doNNI(self, u, v, a, b):
         """Swap subtree a (at u) with subtree b (at v) across the internal branch (u, v)."""

@@ -3,6 +3,7 @@
 // device session owns every buffer.  Each method names the reference member it restates
 // (paths relative to the IQ-TREE 3 source tree).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -36,6 +37,7 @@ struct Tree {
   long long partial_ops = 0;
   int newton_evals = 0;
   std::vector<gems_op> ops;
+  std::vector<char> *track = nullptr;  // when set: the slots every traversal writes
 
   int find(int u, int v) const {
     for (int k = 0; k < deg[u]; k++)
@@ -212,6 +214,8 @@ struct Tree {
       collect(dad, node);
       if (!leaf(dad)) collect(node, dad);
     }
+    if (track)
+      for (const gems_op &o : ops) (*track)[o.dst_slot] = 1;
     gems_branch br{};
     br.dad_slot = slot_of(dir(dad, node));
     if (leaf(dad)) {
@@ -546,6 +550,99 @@ struct Tree {
     return GEMS_OK;
   }
 
+  // PhyloTree::getBestNNIForBran's evaluation (tree/phylotree.cpp:4176-4420, NNI-5 with one
+  // evaluation round): both NNIs of the internal branch (u, v) -- u's neighbour a (the smaller
+  // of its two other neighbours) swapped with each of v's other neighbours b (in id order) --
+  // each evaluated by Newton on u's two outer branches, the central one and v's two outer ones
+  // (outer branches in id order; the reference takes its neighbour order), the partial looking
+  // back across each branch cleared before it is optimised, then the lnL from the buffers; the
+  // swap is undone after each, and the lengths travel with the subtrees from the first move to
+  // the second, as in the reference.  The tree is left as it was: its host state is restored,
+  // and a partial held in a slot the evaluation wrote is recomputed when next needed.  With one
+  // slot per internal node and two spare slots (nslots = internal nodes + 2), u's and v's
+  // partials are computed in the spares (the reference's nni_partial_lh), so the tree's own
+  // partials survive.  moves[2][2] = (a, b); lnl[2]; lens[2][5] = central, u's outer, v's outer.
+  int nni_evaluate(int u, int v, int max_nr, int *moves, double *lnl, double *lens) {
+    if (leaf(u) || leaf(v) || find(u, v) < 0) return GEMS_ERR_BAD_ARG;
+    auto others = [&](int x, int y) {
+      std::array<int, 2> o{};
+      int n = 0;
+      for (int k = 0; k < 3; k++)
+        if (adj[x * 3 + k] != y) o[n++] = adj[x * 3 + k];
+      if (o[0] > o[1]) std::swap(o[0], o[1]);
+      return o;
+    };
+    const auto s_adj = adj, s_eu = eu, s_ev = ev, s_dslot = dslot, s_node = node_slot,
+               s_owner = owner, s_sub = sub_size;
+    const auto s_len = len;
+    const auto s_comp = computed;
+    const auto s_lock = slot_locked;
+    const int s_free = pool_free, s_cur_u = cur_u, s_cur_k = cur_k;
+    std::vector<char> written(nslots, 0);
+    track = &written;
+    const int ninternal = nnode - ntaxa;
+    const bool spare = !per_branch && !pool && nslots >= ninternal + 2;
+    if (spare) {  // u's and v's partials go to the two spare slots
+      node_slot[u] = nslots - 2;
+      node_slot[v] = nslots - 1;
+      owner[nslots - 2] = owner[nslots - 1] = -1;
+      for (int x = 0; x < nnode; x++)
+        for (int k = 0; k < deg[x]; k++)
+          if (adj[x * 3 + k] == u || adj[x * 3 + k] == v) computed[x * 3 + k] = 0;
+    }
+    const int a = others(u, v)[0];
+    const auto bs = others(v, u);
+    int st = GEMS_OK;
+    for (int cnt = 0; cnt < 2 && st == GEMS_OK; cnt++) {
+      const int b = bs[cnt];
+      moves[2 * cnt] = a;
+      moves[2 * cnt + 1] = b;
+      if ((st = nni(u, v, a, b))) break;
+      double *L = lens + 5 * cnt;
+      int i = 1;
+      for (int x : others(u, v)) {
+        computed[dir(x, u)] = 0;
+        if ((st = optimize_one(u, x, 0, max_nr))) break;
+        L[i++] = len[u * 3 + find(u, x)];
+      }
+      if (st) break;
+      computed[dir(v, u)] = 0;
+      if ((st = optimize_one(u, v, 0, max_nr))) break;
+      L[0] = len[u * 3 + find(u, v)];
+      for (int y : others(v, u)) {
+        computed[dir(y, v)] = 0;
+        if ((st = optimize_one(v, y, 0, max_nr))) break;
+        L[i++] = len[v * 3 + find(v, y)];
+      }
+      if (st) break;
+      computed[dir(u, v)] = 0;
+      if ((st = from_buffer(&lnl[cnt]))) break;
+      st = nni(u, v, b, a);
+    }
+    track = nullptr;
+    adj = s_adj;
+    eu = s_eu;
+    ev = s_ev;
+    dslot = s_dslot;
+    node_slot = s_node;
+    owner = s_owner;
+    sub_size = s_sub;
+    len = s_len;
+    computed = s_comp;
+    slot_locked = s_lock;
+    pool_free = s_free;
+    cur_u = s_cur_u;
+    cur_k = s_cur_k;
+    theta_computed = false;  // the session's theta now belongs to the evaluation
+    // a partial of the tree held in a slot the evaluation wrote is stale
+    for (int d = 0; d < (int)computed.size(); d++) {
+      if (!computed[d] || leaf(adj[d])) continue;
+      const int sl = slot_of(d);
+      if (sl < 0 || written[sl]) computed[d] = 0;
+    }
+    return st;
+  }
+
   // PhyloTree::computeLikelihood (tree/phylotree.cpp:1258-1295)
   int compute_likelihood(double *lnl, double *pattern_lh) {
     if (cur_u < 0) {
@@ -844,6 +941,14 @@ int gems_tree_nni(gems_tree *t, int u, int v, int a, int b) {
       a >= t->nnode || b >= t->nnode)
     return GEMS_ERR_BAD_ARG;
   return t->nni(u, v, a, b);
+}
+
+int gems_tree_nni_evaluate(gems_tree *t, int u, int v, int max_nr_step, int *moves,
+                           double *lnl, double *lens) {
+  if (!t || !moves || !lnl || !lens || u < 0 || v < 0 || u >= t->nnode || v >= t->nnode ||
+      max_nr_step < 1)
+    return GEMS_ERR_BAD_ARG;
+  return t->nni_evaluate(u, v, max_nr_step, moves, lnl, lens);
 }
 
 int gems_tree_spr(gems_tree *t, int node, int dad, int node2, int dad2) {

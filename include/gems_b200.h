@@ -375,6 +375,21 @@ int gems_tree_nni(gems_tree *t, int u, int v, int a, int b);
  * shape at once (RateGamma::computeFunction, model/rategamma.cpp:178-186, once per candidate in
  * the reference). */
 int gems_tree_compute_likelihood_batch(gems_tree *const *trees, int ntrees, double *lnl);
+/* PhyloTree::getBestNNIForBran's evaluation (tree/phylotree.cpp:4176-4420, NNI-5, one
+ * evaluation round) on the internal branch (u, v), leaving the tree unchanged: the two NNIs --
+ * u's neighbour a (the smaller of u's other two) swapped with each of v's other neighbours b,
+ * in id order -- each swapped in, its five branches optimised by Newton (max_nr_step steps;
+ * the reference's NNI_MAX_NR_STEP is 10) in the order u's outer two, the central one, v's
+ * outer two (outer ones in id order; the reference uses its neighbour order), the partial
+ * looking back across each branch cleared before it is optimised, the lnL read from the
+ * buffers, and swapped back.  As in the reference the optimised lengths carry over from the
+ * first move to the second.  Out: moves[2][2] = (a, b), lnl[2], lens[2][5] = central, u's
+ * outer, v's outer.  Apply the better one with gems_tree_nni and gems_tree_set_length.  With
+ * one slot per internal node and two spare slots (nslots = internal nodes + 2) the evaluation
+ * computes in the spares and every partial of the tree stays valid; otherwise the partials
+ * whose slots it used are recomputed when next needed. */
+int gems_tree_nni_evaluate(gems_tree *t, int u, int v, int max_nr_step, int *moves, double *lnl,
+                           double *lens);
 /* The SPR move of PhyloTree::assessSPRMove (tree/phylotree.cpp:4822-4880): the subtree at node
  * is pruned from the internal node dad, whose two other neighbours s1 < s2 (by node id) are
  * joined by one branch of their summed length, and dad is inserted into the branch

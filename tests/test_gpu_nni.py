@@ -69,3 +69,98 @@ def test_nni5_mixed(gpu, n, tc):
     for lg, lo, bg, bo in run_pair(tree, model, aln, "mixed", "node", 6, tc=tc):
         assert abs(lg - lo) <= 1e-6 * abs(lo), (lg, lo)
         np.testing.assert_allclose(bg, bo, rtol=2e-4, atol=1e-7)
+
+
+def oracle_evaluate_nni(ot, u, v, max_nr=10):
+    """getBestNNIForBran's NNI-5 evaluation done by hand on the oracle, in the canonical order
+    gems_tree_nni_evaluate uses (u's smaller other neighbour a against each of v's other
+    neighbours b in id order; u's outer branches, the central one, v's outer branches, outer
+    ones in id order); the lengths carry over from the first move to the second and are put
+    back at the end."""
+    saved = ot.getBranchLengths().copy()
+    eu, ev = ot.eu.copy(), ot.ev.copy()
+    a = min(x for x in ot.neighbors(u) if x != v)
+    out = []
+    for b in sorted(y for y in ot.neighbors(v) if y != u):
+        ot.doNNI(u, v, a, b)
+        lens = [0.0] * 5
+        i = 1
+        for x in sorted(x for x in ot.neighbors(u) if x != v):
+            ot.optimizeOneBranch(u, x, True, max_nr)
+            lens[i] = ot.getBranchLength(u, x)
+            i += 1
+        ot.optimizeOneBranch(u, v, True, max_nr)
+        lens[0] = ot.getBranchLength(u, v)
+        for y in sorted(y for y in ot.neighbors(v) if y != u):
+            ot.optimizeOneBranch(v, y, True, max_nr)
+            lens[i] = ot.getBranchLength(v, y)
+            i += 1
+        out.append((a, b, ot.computeLikelihoodFromBuffer(), np.array(lens)))
+        ot.doNNI(u, v, b, a)
+    np.testing.assert_array_equal(ot.eu, eu)
+    for (x, y), ln in zip(zip(ot.eu.tolist(), ot.ev.tolist()), saved):
+        ot.setLength(x, y, float(ln))
+    return out
+
+
+@pytest.mark.parametrize("slots", ["node", "node+spare", "branch", "pool"])
+def test_evaluate_nni_matches_oracle_and_leaves_tree(gpu, slots):
+    """gems_tree_nni_evaluate on several internal branches: both moves' lnL and five lengths as
+    the oracle doing the same sequence; the tree (edges, lengths, lnL) unchanged after."""
+    tree, model, aln = case(4, 20, 2500, 91)
+    ot = orc.OracleTree(tree, model, aln)
+    gt = PhyloTree.from_case(tree, model, aln, precision="fp64", slots=slots)
+    l0 = gt.computeLikelihood()
+    ot.computeLikelihood()
+    internal = [(int(a), int(b)) for a, b in zip(tree.eu, tree.ev)
+                if a >= tree.ntaxa and b >= tree.ntaxa][:4]
+    for u, v in internal:
+        got = gt.evaluateNNI(u, v)
+        ref = oracle_evaluate_nni(ot, u, v)
+        for (ga, gb, gl, gL), (ra, rb, rl, rL) in zip(got, ref):
+            assert (ga, gb) == (ra, rb)
+            assert abs(gl - rl) <= 1e-9 * abs(rl), (u, v, gl, rl)
+            np.testing.assert_allclose(gL, rL, rtol=1e-7, atol=1e-10)
+        np.testing.assert_array_equal(gt.eu, tree.eu)
+        np.testing.assert_array_equal(gt.getBranchLengths(), tree.length)
+        assert gt.computeLikelihood() == l0
+    gt.close()
+    gt.session.close()
+
+
+def test_evaluate_nni_with_spare_slots_keeps_the_partials(gpu):
+    """With two spare slots the evaluation computes in them: the tree's partials stay valid, so
+    the next lnL at the same branch recomputes nothing; without spares the central partials
+    are recomputed."""
+    tree, model, aln = case(4, 24, 2000, 93)
+    u, v = next((int(a), int(b)) for a, b in zip(tree.eu, tree.ev)
+                if a >= tree.ntaxa and b >= tree.ntaxa)
+    res = {}
+    for slots in ("node+spare", "node"):
+        gt = PhyloTree.from_case(tree, model, aln, precision="fp64", slots=slots)
+        l0 = gt.computeLikelihoodBranch(u, v)
+        gt.evaluateNNI(u, v)
+        before = gt.stats()[0]
+        assert gt.computeLikelihoodBranch(u, v) == l0
+        res[slots] = gt.stats()[0] - before
+        gt.close()
+        gt.session.close()
+    assert res["node+spare"] == 0
+    assert res["node"] > 0
+
+
+def test_evaluate_nni_mixed(gpu):
+    tree, model, aln = case(20, 16, 1500, 95)
+    ot = orc.OracleTree(tree, model, aln)
+    gt = PhyloTree.from_case(tree, model, aln, precision="mixed", slots="node+spare")
+    gt.computeLikelihood()
+    ot.computeLikelihood()
+    u, v = next((int(a), int(b)) for a, b in zip(tree.eu, tree.ev)
+                if a >= tree.ntaxa and b >= tree.ntaxa)
+    for (ga, gb, gl, gL), (ra, rb, rl, rL) in zip(gt.evaluateNNI(u, v),
+                                                  oracle_evaluate_nni(ot, u, v)):
+        assert (ga, gb) == (ra, rb)
+        assert abs(gl - rl) <= 1e-6 * abs(rl)
+        np.testing.assert_allclose(gL, rL, rtol=2e-4, atol=1e-7)
+    gt.close()
+    gt.session.close()
