@@ -415,6 +415,11 @@ class Session:
         cores."""
         _check(self.lib.gems_session_set_option(self.handle, 1, int(on)), "set_option")
 
+    def set_tc20_halves(self, on=True):
+        """20-state tcgen05 traversal at two CTAs per SM in half-steps (GEMS_OPT_TC20_HALVES);
+        same values bit for bit."""
+        _check(self.lib.gems_session_set_option(self.handle, 5, int(on)), "set_option")
+
     def set_newton_share(self, k):
         """The device Newton kernel takes at most 1/k of the GPU (GEMS_OPT_NEWTON_SHARE)."""
         _check(self.lib.gems_session_set_option(self.handle, 4, int(k)), "set_option")

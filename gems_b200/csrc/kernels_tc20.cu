@@ -581,6 +581,362 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
                  : "memory");
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Two CTAs per SM, in half-steps (GEMS_OPT_TC20_HALVES).  A CTA of 128 threads (one per
+// pattern row) runs its tile's op list two categories at a time: per half-step a side's operand
+// tile is 10 chunks (20 KB), its B images 12 KB, and the CTA needs 113 KB of shared memory and
+// 256 TMEM columns, so two CTAs share an SM and one's copy, MMA and barrier waits are covered by
+// the other's work.  No child is forwarded: every internal child is copied from the slot
+// (usually from L2), the copy of the op that just wrote it issued after its stores.  NORM
+// scaling spans every category of a row: the first half-step's rows are stored as computed and,
+// when the row needs scaling (rare), re-read and scaled after the last half-step; SAFE scaling
+// is per category.  Values are those of the one-CTA kernel bit for bit (same products, same
+// split, same summation order); only the schedule differs.
+// ---------------------------------------------------------------------------------------
+constexpr int kThreadsH = kTile;                       // one thread per pattern row
+constexpr int kHalfChunks = 10;                        // chunks of two categories
+constexpr int kLandH = (kHalfChunks + 1) * kAChunk;    // + a chunk that stays zero: 22 KB
+constexpr int kBSideH = 2 * 2 * kBImg;                 // two categories' hi and lo: 12 KB
+constexpr int kTmemColsH = 256;
+constexpr int kAhiColH = 128;                          // A_hi[side][j] at 128 + (2 side + j) 24
+
+struct TcSharedH {
+  uint64_t bar_land, bar_tab, bar_mma;
+  uint32_t tmem_base;
+};
+size_t tc_smem_h() { return 4 * (size_t)kLandH + 2 * (size_t)kBSideH + sizeof(TcSharedH) + 64; }
+
+// categories of half-step h (2 or, for the last half of an odd C, 1)
+__device__ __forceinline__ int half_cats(int C, int h) { return min(2, C - 2 * h); }
+
+// the child tiles of half-step h of op `o` (all but `late`) into the landing buffers; the
+// barrier expects every child's bytes, `late`'s included (its copy is issued by issue_late_h)
+__device__ __forceinline__ void issue_land_h(const DevCtx &c, const DevOp &o, int h, int late,
+                                             uint32_t sL0, uint32_t sL1, int tile, uint32_t bar) {
+  const uint32_t bytes = (uint32_t)half_cats(c.C, h) * 5 * kAChunk;
+  uint32_t total = 0;
+  for (int s = 0; s < 2; s++)
+    if ((s ? o.r_kind : o.l_kind) == GEMS_CHILD_PARTIAL) total += bytes;
+  mbar_expect_tx(bar, total);
+  for (int s = 0; s < 2; s++) {
+    const int kind = s ? o.r_kind : o.l_kind, id = s ? o.r_id : o.l_id;
+    if (kind != GEMS_CHILD_PARTIAL || id == late) continue;
+    const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
+                       (size_t)tile * (5 * c.C * kAChunk / 4) + (size_t)10 * h * (kAChunk / 4);
+    bulk_g2s(s ? sL1 : sL0, src, bytes, bar);
+  }
+}
+__device__ __forceinline__ void issue_late_h(const DevCtx &c, const DevOp &o, int h, int late,
+                                             uint32_t sL0, uint32_t sL1, int tile, uint32_t bar) {
+  const uint32_t bytes = (uint32_t)half_cats(c.C, h) * 5 * kAChunk;
+  for (int s = 0; s < 2; s++) {
+    const int kind = s ? o.r_kind : o.l_kind, id = s ? o.r_id : o.l_id;
+    if (kind != GEMS_CHILD_PARTIAL || id != late) continue;
+    const float *src = static_cast<const float *>(c.partials) + (size_t)id * c.slot_elems +
+                       (size_t)tile * (5 * c.C * kAChunk / 4) + (size_t)10 * h * (kAChunk / 4);
+    bulk_g2s(s ? sL1 : sL0, src, bytes, bar);
+  }
+}
+// the tables of half-step h of op `o`, per side: an internal child's B images of the half's
+// categories, a tip child's whole tip table
+__device__ __forceinline__ void issue_tab_h(const DevCtx &c, const DevOp &o, const float *tk,
+                                            int h, unsigned char *Bbase, uint32_t bar) {
+  const int C = c.C, nc = half_cats(C, h);
+  uint32_t bytes[2];
+  for (int s = 0; s < 2; s++)
+    bytes[s] = (s ? o.r_kind : o.l_kind) == GEMS_CHILD_PARTIAL
+                   ? (uint32_t)nc * 2 * kBImg
+                   : (uint32_t)(c.unknown + 1) * tip_row_floats(C) * 4;
+  mbar_expect_tx(bar, bytes[0] + bytes[1]);
+  const size_t imgf = kBImg / 4;
+  for (int s = 0; s < 2; s++) {
+    const bool in = (s ? o.r_kind : o.l_kind) == GEMS_CHILD_PARTIAL;
+    const float *src = in ? tk + ((size_t)(s * C + 2 * h) * 2) * imgf
+                          : tk + (size_t)2 * C * 2 * imgf +
+                                (size_t)s * (c.unknown + 1) * tip_row_floats(C);
+    bulk_g2s(sptr(Bbase + (size_t)s * kBSideH), src, bytes[s], bar);
+  }
+}
+
+template <bool SAFE>
+__global__ void __launch_bounds__(kThreadsH, 2)
+    k_traverse_tc20h(DevCtx c, const DevOp *__restrict__ ops, int nops,
+                     const float *__restrict__ tab, size_t stride_f, int *flag, int tile0) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *land[2] = {smem_raw, smem_raw + kLandH};
+  unsigned char *alo[2] = {smem_raw + 2 * kLandH, smem_raw + 3 * kLandH};
+  unsigned char *Bbase = smem_raw + 4 * kLandH;
+  TcSharedH *ctl = reinterpret_cast<TcSharedH *>(Bbase + 2 * kBSideH);
+  const int t = threadIdx.x, warp = t >> 5, row = t;
+  const int C = c.C, H = (C + 1) / 2, nsteps = nops * H;
+  const int tile = tile0 + blockIdx.x;
+  const long p = (long)tile * kTile + row;
+  const bool act = p < c.P;
+  const uint32_t bar_land = sptr(&ctl->bar_land), bar_tab = sptr(&ctl->bar_tab),
+                 bar_mma = sptr(&ctl->bar_mma);
+  if (t == 0) {
+    mbar_init(bar_land, 1);
+    mbar_init(bar_tab, 1);
+    mbar_init(bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // every landing and lo buffer starts at zero: chunks a half-step does not fill (the K padding
+  // chunk, and the second category's chunks of a one-category half) hold finite values
+  for (int i = t; i < 4 * kLandH / 16; i += kThreadsH)
+    reinterpret_cast<float4 *>(smem_raw)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (warp == 0) tmem_alloc(sptr(&ctl->tmem_base), kTmemColsH);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = ctl->tmem_base;
+  const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+  const uint32_t sL[2] = {sptr(land[0]), sptr(land[1])};
+  const uint64_t dLo[2] = {sdesc(sptr(alo[0]), kAChunk, 128), sdesc(sptr(alo[1]), kAChunk, 128)};
+  const uint64_t dB[2] = {sdesc(sptr(Bbase), kNP * 16, 128),
+                          sdesc(sptr(Bbase + kBSideH), kNP * 16, 128)};
+  const bool inv0 = act ? c.invar[p] == 0.0 : false;
+  float *part = static_cast<float *>(c.partials);
+  uint32_t ph_land = 0, ph_tab = 0, ph_mma = 0;
+  bool ok = true, land_pending = false, tab_pending = false, mma_pending = false;
+
+  DevOp cur = ops[0];
+  if (warp == 0 && elect_one()) {
+    issue_land_h(c, cur, 0, -1, sL[0], sL[1], tile, bar_land);
+    issue_tab_h(c, cur, tab, 0, Bbase, bar_tab);
+  }
+  land_pending = tab_pending = true;
+  int st_l = 0, st_r = 0;  // tip state codes of the current op
+  if (act) {
+    if (cur.l_kind == GEMS_CHILD_TIP) st_l = min((int)c.tips[(size_t)cur.l_id * c.P + p], c.unknown);
+    if (cur.r_kind == GEMS_CHILD_TIP) st_r = min((int)c.tips[(size_t)cur.r_id * c.P + p], c.unknown);
+  }
+  float mx_prev = 0.f;  // NORM: the row maximum over the op's earlier half-steps
+
+  for (int step = 0; step < nsteps && ok; step++) {
+    const int k = step / H, h = step - k * H, nc = half_cats(C, h);
+    const bool last_half = h == H - 1;
+    const bool inL = cur.l_kind == GEMS_CHILD_PARTIAL, inR = cur.r_kind == GEMS_CHILD_PARTIAL;
+    const bool tiptip = !inL && !inR;
+    const bool has_next = step + 1 < nsteps;
+    DevOp nxt = cur;
+    int nh = h + 1;
+    if (last_half) {
+      nh = 0;
+      if (has_next) nxt = ops[k + 1];
+    }
+    // the next op's child that this op writes is copied after this op's last stores
+    const int late = (has_next && last_half) ? cur.dst_slot : -1;
+    // children's counters of this half-step's categories (NORM: per pattern)
+    int scl[2] = {0, 0}, scr[2] = {0, 0};
+    if (act) {
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        if (j >= nc) continue;
+        const size_t o = SAFE ? (size_t)p * C + 2 * h + j : (size_t)p;
+        if (inL) scl[j] = c.scale[(size_t)cur.l_id * c.slot_scale + o];
+        if (inR) scr[j] = c.scale[(size_t)cur.r_id * c.slot_scale + o];
+      }
+    }
+    if (__syncthreads_or(!mbar_wait(bar_land, ph_land) || !mbar_wait(bar_tab, ph_tab))) {
+      ok = false;
+      if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+      break;
+    }
+    land_pending = tab_pending = false;
+    ph_land ^= 1;
+    ph_tab ^= 1;
+    // internal children: hi -> TMEM, lo -> shared memory; tip children: the row's tip-table
+    // entries of the half's categories into the side's lo buffer (which it does not use)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      float4 *l4 = reinterpret_cast<float4 *>(alo[s]);
+      if (!(s ? inR : inL)) {
+        const int stc = s ? st_r : st_l;
+        const float4 *lt = reinterpret_cast<const float4 *>(
+            Bbase + (size_t)s * kBSideH + (size_t)stc * tip_row_floats(C) * 4);
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          if (j >= nc) continue;
+#pragma unroll
+          for (int i = 0; i < 5; i++) l4[(j * 5 + i) * kTile + row] = lt[(2 * h + j) * 5 + i];
+        }
+        continue;
+      }
+      const float4 *a4 = reinterpret_cast<const float4 *>(land[s]);
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        if (j >= nc) continue;
+        float4 hv[5];
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+          float4 lv;
+          split4(a4[(j * 5 + i) * kTile + row], hv[i], lv);
+          l4[(j * 5 + i) * kTile + row] = lv;
+        }
+        tmem_st_row(tmem + lane_off + (uint32_t)(kAhiColH + (2 * s + j) * kKP), hv);
+      }
+    }
+    tmem_st_wait();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0 && elect_one()) {
+      // the landing buffers have been read: the next half-step's tiles come in
+      if (has_next) issue_land_h(c, nxt, nh, late, sL[0], sL[1], tile, bar_land);
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        if (!(s ? inR : inL)) continue;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          if (j >= nc) continue;
+          const uint32_t dtm = tmem + (uint32_t)((2 * s + j) * kNP);
+          const uint32_t atm = tmem + (uint32_t)(kAhiColH + (2 * s + j) * kKP);
+          const uint64_t bh = dB[s] + (uint64_t)((j * 2 * kBImg) >> 4);
+          const uint64_t bl = bh + (uint64_t)(kBImg >> 4);
+#pragma unroll
+          for (int ks = 0; ks < kKP / 8; ks++) {
+            const uint64_t ko = (uint64_t)(((j * 5 + 2 * ks) * kAChunk) >> 4);
+            const uint64_t kb = (uint64_t)((2 * ks * kNP * 16) >> 4);
+            mma_tf32_ta(dtm, atm + 8 * ks, bh + kb, ks > 0 ? 1u : 0u);
+            mma_tf32_ta(dtm, atm + 8 * ks, bl + kb, 1u);
+            mma_tf32(dtm, dLo[s] + ko, bh + kb, 1u);
+          }
+        }
+      }
+      if (!tiptip) mma_commit(bar_mma);
+    }
+    land_pending = has_next;
+    if (!tiptip) {
+      mma_pending = true;
+      if (__syncthreads_or(!mbar_wait(bar_mma, ph_mma))) {
+        ok = false;
+        if (t == 0) atomicExch(flag, GEMS_ERR_TIMEOUT);
+        break;
+      }
+      mma_pending = false;
+      ph_mma ^= 1;
+      tc_fence_after();
+    }
+    // the tables of this half-step are no longer read (MMAs done, tip rows copied out)
+    if (has_next) {
+      if (warp == 0 && elect_one())
+        issue_tab_h(c, nxt, tab + (size_t)(last_half ? k + 1 : k) * stride_f, nh, Bbase, bar_tab);
+      tab_pending = true;
+    }
+    // ---- epilogue: messages, products, scaling, stores
+    float out[2][kN];
+    float mx[2] = {0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      if (j >= nc) continue;
+      float m[2][kN];
+      uint32_t r[2][20];
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+        if (s ? inR : inL) tmem_ld20(tmem + lane_off + (uint32_t)((2 * s + j) * kNP), r[s]);
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        if (s ? inR : inL) {
+          tmem_ld_wait(r[s]);
+#pragma unroll
+          for (int x = 0; x < kN; x++) m[s][x] = __uint_as_float(r[s][x]);
+        } else {
+          const float4 *l4 = reinterpret_cast<const float4 *>(alo[s]);
+#pragma unroll
+          for (int i = 0; i < 5; i++) {
+            const float4 v = l4[(j * 5 + i) * kTile + row];
+            m[s][4 * i] = v.x;
+            m[s][4 * i + 1] = v.y;
+            m[s][4 * i + 2] = v.z;
+            m[s][4 * i + 3] = v.w;
+          }
+        }
+      }
+#pragma unroll
+      for (int x = 0; x < kN; x++) {
+        const float v = fmaxf(m[0][x], 0.f) * fmaxf(m[1][x], 0.f);
+        out[j][x] = v;
+        mx[j] = fmaxf(mx[j], v);
+      }
+    }
+    float f[2] = {1.f, 1.f};
+    bool up_all = false;  // NORM: the row is scaled (decided at the op's last half-step)
+    if (SAFE) {
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+        if (j < nc && !tiptip && mx[j] < kScaleThrF && inv0) f[j] = 18446744073709551616.0f;
+    } else {
+      const float m = fmaxf(mx_prev, fmaxf(mx[0], mx[1]));
+      if (last_half) {
+        up_all = !tiptip && m < kScaleThrF && inv0;
+        if (up_all) f[0] = f[1] = 18446744073709551616.0f;  // 2^64
+        mx_prev = 0.f;
+      } else {
+        mx_prev = m;
+      }
+    }
+    float *dtile = part + (size_t)cur.dst_slot * c.slot_elems + (size_t)tile * (5 * C * kAChunk / 4);
+    uint16_t *sd = c.scale + (size_t)cur.dst_slot * c.slot_scale;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      if (j >= nc) continue;
+      const int cc = 2 * h + j;
+#pragma unroll
+      for (int i = 0; i < kN / 4; i++) {
+        const float4 v = make_float4(out[j][4 * i] * f[j], out[j][4 * i + 1] * f[j],
+                                     out[j][4 * i + 2] * f[j], out[j][4 * i + 3] * f[j]);
+        reinterpret_cast<float4 *>(dtile)[(cc * 5 + i) * kTile + row] = v;
+      }
+      if (SAFE && act)
+        sd[(size_t)p * C + cc] =
+            (uint16_t)(scl[j] + scr[j] + (f[j] != 1.f ? 1 : 0));
+    }
+    if (!SAFE && last_half) {
+      if (up_all) {  // the earlier half-steps' rows of this op, stored unscaled: scale them
+        for (int cc = 0; cc < 2 * h; cc++)
+#pragma unroll
+          for (int i = 0; i < kN / 4; i++) {
+            float4 *q = reinterpret_cast<float4 *>(dtile) + (cc * 5 + i) * kTile + row;
+            float4 v = *q;
+            v.x *= 18446744073709551616.0f;
+            v.y *= 18446744073709551616.0f;
+            v.z *= 18446744073709551616.0f;
+            v.w *= 18446744073709551616.0f;
+            *q = v;
+          }
+      }
+      if (act) sd[p] = (uint16_t)(scl[0] + scr[0] + (up_all ? 1 : 0));
+    }
+    // later steps bulk-copy these rows from global memory (through the async proxy)
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (late >= 0 && warp == 0 && elect_one())
+      issue_late_h(c, nxt, nh, late, sL[0], sL[1], tile, bar_land);
+    if (has_next && last_half) {  // the next op: its tip state codes
+      st_l = st_r = 0;
+      if (act) {
+        if (nxt.l_kind == GEMS_CHILD_TIP)
+          st_l = min((int)c.tips[(size_t)nxt.l_id * c.P + p], c.unknown);
+        if (nxt.r_kind == GEMS_CHILD_TIP)
+          st_r = min((int)c.tips[(size_t)nxt.r_id * c.P + p], c.unknown);
+      }
+    }
+    cur = nxt;
+  }
+  if (!ok && t == 0) {
+    if (land_pending) mbar_wait(bar_land, ph_land);
+    if (tab_pending) mbar_wait(bar_tab, ph_tab);
+    if (mma_pending) mbar_wait(bar_mma, ph_mma);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTmemColsH);
+}
+
 }  // namespace
 
 size_t tc20_op_floats(int ncat, int unknown) {
@@ -614,8 +970,35 @@ int launch_traverse_tc20(Session *s, int nops, int p0, int p1) {
     return GEMS_ERR_BAD_ARG;
   }
   DevCtx c = s->ctx();
-  const size_t smem = tc_smem(s->desc.ncat);
   const bool safe = s->desc.scaling == GEMS_SCALE_SAFE;
+  if (s->tc20_halves) {  // two CTAs per SM in half-steps
+    void *fh = safe ? (void *)k_traverse_tc20h<true> : (void *)k_traverse_tc20h<false>;
+    GEMS_CUDA(cudaFuncSetAttribute(fh, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_h()));
+    GEMS_CUDA(cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
+    const int tile0 = p0 / kTile;
+    const int grid = (p1 + kTile - 1) / kTile - tile0;
+    cudaEvent_t ev0;
+    if (int st = prof_begin(s, 0, &ev0)) return st;
+    const float *tab = reinterpret_cast<const float *>(s->d_opmats);
+    if (safe)
+      k_traverse_tc20h<true><<<grid, kThreadsH, tc_smem_h(), s->stream>>>(
+          c, s->d_ops, nops, tab, s->op_stride_tc, s->d_flag, tile0);
+    else
+      k_traverse_tc20h<false><<<grid, kThreadsH, tc_smem_h(), s->stream>>>(
+          c, s->d_ops, nops, tab, s->op_stride_tc, s->d_flag, tile0);
+    s->launches++;
+    GEMS_CUDA(cudaGetLastError());
+    if (int st = prof_end(s, 0, ev0)) return st;
+    int flag = 0;
+    GEMS_CUDA(cudaMemcpyAsync(&flag, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    GEMS_CUDA(cudaStreamSynchronize(s->stream));
+    if (flag) {
+      set_error("tensor-core traversal: bounded wait expired");
+      return GEMS_ERR_TIMEOUT;
+    }
+    return GEMS_OK;
+  }
+  const size_t smem = tc_smem(s->desc.ncat);
   void *fn = safe ? (void *)k_traverse_tc20<true> : (void *)k_traverse_tc20<false>;
   // the limit is a property of the kernel, shared by every session and host thread: set it to
   // the largest size any session needs (4 categories), so that a concurrent setting for another

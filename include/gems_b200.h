@@ -104,7 +104,11 @@ int gems_session_stream(gems_session *s, void **stream);
  * register-tiled GEMMs over 128-row tiles; 0 selects the per-row kernel (same values, bit for
  * bit). */
 enum { GEMS_OPT_TENSOR_CORES = 1, GEMS_OPT_TILED_FP64 = 2, GEMS_OPT_AUTOTUNE = 3,
-       GEMS_OPT_NEWTON_SHARE = 4 };
+       GEMS_OPT_NEWTON_SHARE = 4, GEMS_OPT_TC20_HALVES = 5 };
+/* GEMS_OPT_TC20_HALVES (default 0): the tcgen05 20-state traversal runs two CTAs per SM, each
+ * taking its tile two categories at a time with every internal child copied back from the
+ * slot (no forwarding), instead of one CTA per SM with all categories at once; the values are
+ * the same bits either way. */
 /* GEMS_OPT_NEWTON_SHARE (default 1): the device Newton loop (gems_newton_branch) is one
  * cooperative kernel whose blocks are all resident at once; with value k it takes at most 1/k
  * of the GPU's resident blocks, so that it runs beside other sessions' work instead of waiting
