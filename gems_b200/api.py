@@ -420,6 +420,12 @@ class Session:
         same values bit for bit."""
         _check(self.lib.gems_session_set_option(self.handle, 5, int(on)), "set_option")
 
+    def set_tc61_roles(self, on=True):
+        """61-state tcgen05 traversal with split / MMA / epilogue warp roles on consecutive steps
+        (GEMS_OPT_TC61_ROLES, default) or every warp running the parts in turn; same values bit
+        for bit."""
+        _check(self.lib.gems_session_set_option(self.handle, 6, int(on)), "set_option")
+
     def set_newton_share(self, k):
         """The device Newton kernel takes at most 1/k of the GPU (GEMS_OPT_NEWTON_SHARE)."""
         _check(self.lib.gems_session_set_option(self.handle, 4, int(k)), "set_option")

@@ -209,6 +209,7 @@ struct Session {
   int force_shape = -1;  // >= 0: that launch shape, no tuning (comparisons)
   int newton_share = 1;  // the Newton kernel takes at most 1/newton_share of the GPU
   bool tc20_halves = false;  // 20-state tcgen05 traversal at two CTAs per SM, in half-steps
+  bool tc61_roles = true;    // 61-state tcgen05 traversal with split / MMA / epilogue warp roles
   size_t op_stride_tc = 0;
   // FP32 partials stored tile-major (20- and 61-state mixed forms); elements per slot
   bool tiled = false;

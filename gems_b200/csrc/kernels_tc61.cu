@@ -505,6 +505,413 @@ __global__ void __launch_bounds__(kThreads61, 1)
 
 size_t tc61_smem() { return 4 * (size_t)kATile + 2 * (size_t)kBSide + sizeof(Tc61Shared) + 64; }
 
+// ---------------------------------------------------------------------------------------
+// Warp-role form: the parts of a step run in different warps, on different steps at once, so
+// that the split of step s+1, the MMAs of step s and the epilogue of step s-1 overlap (the form
+// above runs them one after the other in every warp, and the tensor pipe idles through the split
+// and the epilogue).
+//   warps 0-3, split: one thread per pattern row.  Waits for the operand tiles of step s in
+//     landing buffer s&1 and splits each internal child's row: hi -> TMEM A_hi[s&1][side], lo
+//     written back in place (the landing buffer is then the lo operand of the MMAs).
+//   warps 4-7, epilogue: one thread per pattern row.  Waits for the MMAs of step s, reads
+//     D[s&1] and frees it; a tip child's message is its tip table row, read from global memory
+//     (L1-cached: the rows of one table are shared by the patterns of a tile); products, SAFE
+//     rescaling, stores; then publishes the number of steps whose rows are stored.
+//   warp 8, copies: the operand tiles of step s into landing buffer s&1, once the MMAs of step
+//     s-2 are done with it and every step that wrote one of those children has published its
+//     stores; the B images of internal sides, in step order, into a ring of three 32 KB slots.
+//   warp 9, MMAs: step s into D[s&1] once its split is done, its B images have landed and the
+//     epilogue of step s-2 has read D[s&1]; a commit per side frees its ring slot, a commit per
+//     step signals the epilogue and the copies.
+// TMEM: D[b][side] at columns b*128 + side*64, A_hi[b][side] at 256 + b*128 + side*64 (512).
+// Shared memory: landing buffers [2][2 sides][32 KB] and the ring [3][32 KB]: 224 KB.  The
+// products, the split and the summation order are those of the form above: the same bits.
+// Every wait is bounded and also gives up once another role has failed (err); on failure the
+// copy and MMA warps wait (bounded) for what they have in flight before TMEM is freed.
+// ---------------------------------------------------------------------------------------
+constexpr int kWsThreads = 320;
+constexpr int kWsSlots = 3;
+constexpr int kWsTmemCols = 512;
+constexpr int kWsAhi = 256;
+
+struct Ws61Shared {
+  uint64_t full_land[2], split_done[2], mma_done[2], epi_done[2];
+  uint64_t full_slot[kWsSlots], slot_free[kWsSlots];
+  uint64_t drain;  // MMAs in flight when a role failed
+  uint32_t tmem_base;
+  int n_stored;  // steps whose rows are stored and fenced for the async proxy
+  int err;       // set by the first role whose wait expired
+};
+
+__device__ __forceinline__ bool ws_wait(uint32_t bar, uint32_t parity, const int *err) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*(const volatile int *)err) return false;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void ws_fail(int *err, int *flag) {
+  *(volatile int *)err = 1;
+  atomicExch(flag, GEMS_ERR_TIMEOUT);
+}
+__device__ __forceinline__ int ld_acquire_s(const int *p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(sptr(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_s(int *p, int v) {
+  asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(sptr(p)), "r"(v) : "memory");
+}
+// OR of `pred` over the 128 threads of the epilogue warps (named barrier 1)
+__device__ __forceinline__ bool epi_sync_or(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred)
+      : "memory");
+  return r != 0;
+}
+
+// (op, category) of consecutive steps
+struct StepIt {
+  int k, cat;
+  DevOp op;
+};
+__device__ __forceinline__ void step_next(StepIt &it, const DevOp *ops, int nops, int C) {
+  if (++it.cat == C) {
+    it.cat = 0;
+    if (++it.k < nops) it.op = ops[it.k];
+  }
+}
+
+__global__ void __launch_bounds__(kWsThreads, 1)
+    k_traverse_tc61ws(const TcJob *__restrict__ jobs, int nops, size_t stride_f, int *flag,
+                      int tile0) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ TcJob sj;
+  unsigned char *land = smem_raw;               // [buffer][side][32 KB]
+  unsigned char *ring = smem_raw + 4 * kATile;  // [slot][hi 16 KB, lo 16 KB]
+  Ws61Shared *ctl = reinterpret_cast<Ws61Shared *>(ring + kWsSlots * kBSide);
+  const int t = threadIdx.x, warp = t >> 5;
+  if (t == 0) {
+    sj = jobs[blockIdx.y];
+    for (int b = 0; b < 2; b++) {
+      mbar_init(sptr(&ctl->full_land[b]), 1);
+      mbar_init(sptr(&ctl->split_done[b]), kTile);
+      mbar_init(sptr(&ctl->mma_done[b]), 1);
+      mbar_init(sptr(&ctl->epi_done[b]), kTile);
+    }
+    for (int q = 0; q < kWsSlots; q++) {
+      mbar_init(sptr(&ctl->full_slot[q]), 1);
+      mbar_init(sptr(&ctl->slot_free[q]), 1);
+    }
+    mbar_init(sptr(&ctl->drain), 1);
+    ctl->n_stored = 0;
+    ctl->err = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(sptr(&ctl->tmem_base), kWsTmemCols);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const DevCtx &c = sj.c;
+  const DevOp *ops = sj.ops;
+  const float *tab = sj.tab;
+  const int C = c.C;
+  const int tile = tile0 + blockIdx.x;
+  const uint32_t tmem = ctl->tmem_base;
+  const int nsteps = nops * C;
+  int *err = &ctl->err;
+
+  if (warp < 4) {
+    // ---- split
+    const int row = t;
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    StepIt it{0, 0, ops[0]};
+    for (int s = 0; s < nsteps; s++) {
+      const int b = s & 1;
+      const bool inL = it.op.l_kind == GEMS_CHILD_PARTIAL, inR = it.op.r_kind == GEMS_CHILD_PARTIAL;
+      if (__any_sync(0xffffffffu, !ws_wait(sptr(&ctl->full_land[b]), (s >> 1) & 1, err))) {
+        ws_fail(err, flag);
+        break;
+      }
+      fence_after();
+#pragma unroll
+      for (int side = 0; side < 2; side++) {
+        if (!(side ? inR : inL)) continue;
+        float4 *a4 = reinterpret_cast<float4 *>(land + (size_t)(2 * b + side) * kATile);
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+          float h[32];
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            const int ch = 8 * hh + i;
+            float4 hv, lv;
+            split4(a4[ch * kTile + row], hv, lv);
+            a4[ch * kTile + row] = lv;
+            h[4 * i] = hv.x;
+            h[4 * i + 1] = hv.y;
+            h[4 * i + 2] = hv.z;
+            h[4 * i + 3] = hv.w;
+          }
+          tmem_st32(tmem + lane_off + (uint32_t)(kWsAhi + b * 128 + side * kNP + 32 * hh), h);
+        }
+      }
+      tmem_st_wait();
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      fence_before();
+      mbar_arrive(sptr(&ctl->split_done[b]));
+      step_next(it, ops, nops, C);
+    }
+  } else if (warp < 8) {
+    // ---- epilogue
+    const int row = t - 4 * 32;
+    const uint32_t lane_off = (uint32_t)((warp - 4) * 32) << 16;
+    const long p = (long)tile * kTile + row;
+    const bool act = p < c.P;
+    const bool inv0 = act ? c.invar[p] == 0.0 : false;
+    float *part = static_cast<float *>(c.partials);
+    StepIt it{0, 0, ops[0]};
+    int st_l = 0, st_r = 0;
+    for (int s = 0; s < nsteps; s++) {
+      const int b = s & 1;
+      const DevOp op = it.op;
+      const bool inL = op.l_kind == GEMS_CHILD_PARTIAL, inR = op.r_kind == GEMS_CHILD_PARTIAL;
+      if (it.cat == 0 && act) {  // tip state codes of a new op
+        st_l = inL ? 0 : c.tips[(size_t)op.l_id * c.P + p];
+        st_r = inR ? 0 : c.tips[(size_t)op.r_id * c.P + p];
+      }
+      int scl = 0, scr = 0;
+      if (act) {
+        if (inL) scl = c.scale[(size_t)op.l_id * c.slot_scale + (size_t)p * C + it.cat];
+        if (inR) scr = c.scale[(size_t)op.r_id * c.slot_scale + (size_t)p * C + it.cat];
+      }
+      const float *tk = tab + (size_t)it.k * stride_f;
+      const float4 *tip4[2];
+#pragma unroll
+      for (int side = 0; side < 2; side++) {
+        const int st = side ? st_r : st_l;
+        tip4[side] = reinterpret_cast<const float4 *>(
+            tk + ((size_t)side * C + it.cat) * (kBSide / 4) + (size_t)(st < kN ? st : kN) * kTipRow61);
+      }
+      const bool bad = __any_sync(0xffffffffu, !ws_wait(sptr(&ctl->mma_done[b]), (s >> 1) & 1, err));
+      if (!bad) {
+        fence_after();
+        float v[64];
+        float mx = 0.f;
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+          uint32_t rm[2][32];
+#pragma unroll
+          for (int side = 0; side < 2; side++)
+            if (side ? inR : inL)
+              tmem_ld32(tmem + lane_off + (uint32_t)(b * 128 + side * kNP + 32 * hh), rm[side]);
+#pragma unroll
+          for (int side = 0; side < 2; side++) {
+            if (side ? inR : inL) {
+              tmem_ld32_wait(rm[side]);
+            } else {
+#pragma unroll
+              for (int i = 0; i < 8; i++) {
+                const float4 q = __ldg(tip4[side] + 8 * hh + i);
+                rm[side][4 * i] = __float_as_uint(q.x);
+                rm[side][4 * i + 1] = __float_as_uint(q.y);
+                rm[side][4 * i + 2] = __float_as_uint(q.z);
+                rm[side][4 * i + 3] = __float_as_uint(q.w);
+              }
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 32; i++) {
+            const float w = fmaxf(__uint_as_float(rm[0][i]), 0.f) * fmaxf(__uint_as_float(rm[1][i]), 0.f);
+            v[32 * hh + i] = w;
+            mx = fmaxf(mx, w);
+          }
+        }
+        // D[b] has been read: the MMAs of step s+2 may overwrite it
+        fence_before();
+        mbar_arrive(sptr(&ctl->epi_done[b]));
+        int s_out = scl + scr;
+        float f = 1.f;
+        if ((inL || inR) && mx < kScaleThrF && inv0) {
+          f = 18446744073709551616.0f;  // 2^64
+          s_out += 1;
+        }
+        float4 *dst = reinterpret_cast<float4 *>(part + (size_t)op.dst_slot * c.slot_elems +
+                                                 mix_off<61>(c, (long)tile * kTile, it.cat));
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int x = 4 * i;
+          float4 w = make_float4(v[4 * i] * f, v[4 * i + 1] * f, v[4 * i + 2] * f, v[4 * i + 3] * f);
+          if (x + 3 >= kN) {  // padding states stored as zeros
+            if (x + 1 >= kN) w.y = 0.f;
+            if (x + 2 >= kN) w.z = 0.f;
+            if (x + 3 >= kN) w.w = 0.f;
+            if (x >= kN) w.x = 0.f;
+          }
+          dst[i * kTile + row] = w;
+        }
+        if (act)
+          c.scale[(size_t)op.dst_slot * c.slot_scale + (size_t)p * C + it.cat] = (uint16_t)s_out;
+        // later steps bulk-copy these rows from global memory
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+      }
+      if (epi_sync_or(bad)) {
+        ws_fail(err, flag);
+        break;
+      }
+      if (row == 0) st_release_s(&ctl->n_stored, s + 1);
+      step_next(it, ops, nops, C);
+    }
+  } else if (warp == 8) {
+    // ---- copies
+    if (elect_one()) {
+      float *part = static_cast<float *>(c.partials);
+      StepIt it{0, 0, ops[0]};
+      int d1 = -1, d2 = -1, d3 = -1;  // destination slots of the three previous ops
+      int nimg = 0;
+      bool ok = true;
+      bool land_armed[2] = {false, false}, slot_armed[kWsSlots] = {false, false, false};
+      uint32_t land_par[2] = {0, 0}, slot_par[kWsSlots] = {0, 0, 0};
+      for (int s = 0; s < nsteps && ok; s++) {
+        const int b = s & 1, u = s >> 1;
+        const DevOp &op = it.op;
+        const bool in[2] = {op.l_kind == GEMS_CHILD_PARTIAL, op.r_kind == GEMS_CHILD_PARTIAL};
+        const int id[2] = {op.l_id, op.r_id};
+        // landing buffer b: the MMAs of step s-2 have read it
+        if (u >= 1 && !ws_wait(sptr(&ctl->mma_done[b]), (u - 1) & 1, err)) {
+          ok = false;
+          break;
+        }
+        // the children's rows of this category: stored by the step that wrote them (an op at
+        // most three back is waited for exactly, older ones by the step four ops back)
+        int need = 0;
+        for (int side = 0; side < 2; side++) {
+          if (!in[side]) continue;
+          const int back = id[side] == d1 ? 1 : (id[side] == d2 ? 2 : (id[side] == d3 ? 3 : 4));
+          need = max(need, s - back * C + 1);
+        }
+        if (need > 0) {
+          const long long t0 = clock64();
+          while (ld_acquire_s(&ctl->n_stored) < need) {
+            if (*(volatile int *)err || clock64() - t0 > kWaitCycles) {
+              ok = false;
+              break;
+            }
+          }
+          if (!ok) break;
+        }
+        const uint32_t fl = sptr(&ctl->full_land[b]);
+        mbar_expect_tx(fl, (uint32_t)((in[0] ? kATile : 0) + (in[1] ? kATile : 0)));
+        land_armed[b] = true;
+        land_par[b] = u & 1;
+        for (int side = 0; side < 2; side++)
+          if (in[side])
+            bulk_g2s(sptr(land + (size_t)(2 * b + side) * kATile),
+                     part + (size_t)id[side] * c.slot_elems + mix_off<61>(c, (long)tile * kTile, it.cat),
+                     kATile, fl);
+        // B images of the internal sides, in ring order
+        for (int side = 0; side < 2 && ok; side++) {
+          if (!in[side]) continue;
+          const int q = nimg % kWsSlots, uu = nimg / kWsSlots;
+          if (uu >= 1 && !ws_wait(sptr(&ctl->slot_free[q]), (uu - 1) & 1, err)) {
+            ok = false;
+            break;
+          }
+          const uint32_t fs = sptr(&ctl->full_slot[q]);
+          mbar_expect_tx(fs, (uint32_t)kBSide);
+          slot_armed[q] = true;
+          slot_par[q] = uu & 1;
+          bulk_g2s(sptr(ring + (size_t)q * kBSide),
+                   tab + (size_t)it.k * stride_f + ((size_t)side * C + it.cat) * (kBSide / 4),
+                   kBSide, fs);
+          nimg++;
+        }
+        if (it.cat + 1 == C) {
+          d3 = d2;
+          d2 = d1;
+          d1 = op.dst_slot;
+        }
+        step_next(it, ops, nops, C);
+      }
+      if (!ok) {
+        ws_fail(err, flag);
+        // the copies issued must land before the CTA's shared memory is released
+        for (int b = 0; b < 2; b++)
+          if (land_armed[b]) mbar_wait(sptr(&ctl->full_land[b]), land_par[b]);
+        for (int q = 0; q < kWsSlots; q++)
+          if (slot_armed[q]) mbar_wait(sptr(&ctl->full_slot[q]), slot_par[q]);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---- MMAs
+    if (elect_one()) {
+      StepIt it{0, 0, ops[0]};
+      int nimg = 0;
+      bool ok = true;
+      bool slot_used[kWsSlots] = {false, false, false};
+      uint32_t slot_par[kWsSlots] = {0, 0, 0};
+      for (int s = 0; s < nsteps && ok; s++) {
+        const int b = s & 1, u = s >> 1;
+        const bool in[2] = {it.op.l_kind == GEMS_CHILD_PARTIAL, it.op.r_kind == GEMS_CHILD_PARTIAL};
+        if (!ws_wait(sptr(&ctl->split_done[b]), u & 1, err) ||
+            (u >= 1 && !ws_wait(sptr(&ctl->epi_done[b]), (u - 1) & 1, err))) {
+          ok = false;
+          break;
+        }
+        fence_after();
+        for (int side = 0; side < 2; side++) {
+          if (!in[side]) continue;
+          const int q = nimg % kWsSlots, uu = nimg / kWsSlots;
+          if (!ws_wait(sptr(&ctl->full_slot[q]), uu & 1, err)) {
+            ok = false;
+            break;
+          }
+          const uint32_t dtm = tmem + (uint32_t)(b * 128 + side * kNP);
+          const uint32_t atm = tmem + (uint32_t)(kWsAhi + b * 128 + side * kNP);
+          const uint64_t dB = sdesc(sptr(ring + (size_t)q * kBSide), kNP * 16, 128);
+          const uint64_t dLo = sdesc(sptr(land + (size_t)(2 * b + side) * kATile), kAChunk, 128);
+#pragma unroll
+          for (int ks = 0; ks < kNP / 8; ks++) {
+            const uint64_t kb = (uint64_t)((2 * ks * kNP * 16) >> 4);
+            const uint64_t ko = (uint64_t)((2 * ks * kAChunk) >> 4);
+            const uint64_t bh = dB + kb, bl = dB + kb + (uint64_t)(kBImg >> 4);
+            mma_ts(dtm, atm + 8 * ks, bh, kIdesc61, ks > 0 ? 1u : 0u);
+            mma_ts(dtm, atm + 8 * ks, bl, kIdesc61, 1u);
+            mma_ss(dtm, dLo + ko, bh, kIdesc61, 1u);
+          }
+          mma_commit(sptr(&ctl->slot_free[q]));
+          slot_used[q] = true;
+          slot_par[q] = uu & 1;
+          nimg++;
+        }
+        if (!ok) break;
+        mma_commit(sptr(&ctl->mma_done[b]));
+        step_next(it, ops, nops, C);
+      }
+      if (!ok) ws_fail(err, flag);
+      // every MMA has completed (and every commit has arrived) before TMEM and shared memory
+      // are released
+      for (int q = 0; q < kWsSlots; q++)
+        if (slot_used[q]) mbar_wait(sptr(&ctl->slot_free[q]), slot_par[q]);
+      mma_commit(sptr(&ctl->drain));
+      mbar_wait(sptr(&ctl->drain), 0);
+    }
+    __syncwarp();
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kWsTmemCols);
+}
+
+size_t tc61ws_smem() { return 4 * (size_t)kATile + kWsSlots * (size_t)kBSide + sizeof(Ws61Shared) + 64; }
+
 }  // namespace
 
 size_t tc61_op_floats(int ncat) { return op_floats61(ncat); }
@@ -563,16 +970,25 @@ int launch_traverse_tc61_batch(Session *const *ss, int nsess, int nops, int p0, 
                             cudaMemcpyHostToDevice, s0->stream));
   if (with_tables)
     if (int st = prep61(s0, jobs[0], nsess > 1 ? s0->d_jobs : nullptr, nsess, nops)) return st;
-  const size_t smem = tc61_smem();
-  GEMS_CUDA(cudaFuncSetAttribute(k_traverse_tc61, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+  const bool roles = s0->tc61_roles;
+  const size_t smem = roles ? tc61ws_smem() : tc61_smem();
+  if (roles)
+    GEMS_CUDA(cudaFuncSetAttribute(k_traverse_tc61ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  else
+    GEMS_CUDA(cudaFuncSetAttribute(k_traverse_tc61, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
   GEMS_CUDA(cudaMemsetAsync(s0->d_flag, 0, sizeof(int), s0->stream));
   const int tile0 = p0 / kTile;
   const dim3 grid((p1 + kTile - 1) / kTile - tile0, nsess);
   cudaEvent_t ev0;
   if (int st = prof_begin(s0, 0, &ev0)) return st;
-  k_traverse_tc61<<<grid, kThreads61, smem, s0->stream>>>(
-      reinterpret_cast<const TcJob *>(s0->d_jobs), nops, s0->op_stride_tc, s0->d_flag, tile0);
+  if (roles)
+    k_traverse_tc61ws<<<grid, kWsThreads, smem, s0->stream>>>(
+        reinterpret_cast<const TcJob *>(s0->d_jobs), nops, s0->op_stride_tc, s0->d_flag, tile0);
+  else
+    k_traverse_tc61<<<grid, kThreads61, smem, s0->stream>>>(
+        reinterpret_cast<const TcJob *>(s0->d_jobs), nops, s0->op_stride_tc, s0->d_flag, tile0);
   s0->launches++;
   GEMS_CUDA(cudaGetLastError());
   if (int st = prof_end(s0, 0, ev0)) return st;

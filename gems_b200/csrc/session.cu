@@ -560,6 +560,9 @@ int gems_session_set_option(gems_session *s, int option, int value) {
     case GEMS_OPT_TC20_HALVES:
       s->tc20_halves = value != 0;
       return GEMS_OK;
+    case GEMS_OPT_TC61_ROLES:
+      s->tc61_roles = value != 0;
+      return GEMS_OK;
     case GEMS_OPT_AUTOTUNE:
       if (value < 0) return GEMS_ERR_BAD_ARG;
       s->autotune = value == 1;

@@ -32,6 +32,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 // false when the phase did not complete within the clock budget
 __device__ inline bool mbar_wait(uint32_t bar, uint32_t parity) {
   const long long t0 = clock64();

@@ -104,7 +104,11 @@ int gems_session_stream(gems_session *s, void **stream);
  * register-tiled GEMMs over 128-row tiles; 0 selects the per-row kernel (same values, bit for
  * bit). */
 enum { GEMS_OPT_TENSOR_CORES = 1, GEMS_OPT_TILED_FP64 = 2, GEMS_OPT_AUTOTUNE = 3,
-       GEMS_OPT_NEWTON_SHARE = 4, GEMS_OPT_TC20_HALVES = 5 };
+       GEMS_OPT_NEWTON_SHARE = 4, GEMS_OPT_TC20_HALVES = 5, GEMS_OPT_TC61_ROLES = 6 };
+/* GEMS_OPT_TC61_ROLES (default 1): the tcgen05 61-state traversal gives the parts of a step to
+ * different warps (operand split, MMA issue, epilogue, copies) working on consecutive steps at
+ * once, with double-buffered accumulators; 0 selects the form in which every warp runs the
+ * parts one after the other.  The values are the same bits either way. */
 /* GEMS_OPT_TC20_HALVES (default 0): the tcgen05 20-state traversal runs two CTAs per SM, each
  * taking its tile two categories at a time with every internal child copied back from the
  * slot (no forwarding), instead of one CTA per SM with all categories at once; the values are
