@@ -530,7 +530,7 @@ size_t tc61_smem() { return 4 * (size_t)kATile + 2 * (size_t)kBSide + sizeof(Tc6
 // copy and MMA warps wait (bounded) for what they have in flight before TMEM is freed.
 // ---------------------------------------------------------------------------------------
 constexpr int kWsThreads = 320;
-constexpr int kWsSlots = 3;
+constexpr int kWsSlots = 2;
 constexpr int kWsTmemCols = 512;
 constexpr int kWsAhi = 256;
 
@@ -596,7 +596,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   __shared__ TcJob sj;
   unsigned char *land = smem_raw;               // [buffer][side][32 KB]
   unsigned char *ring = smem_raw + 4 * kATile;  // [slot][hi 16 KB, lo 16 KB]
-  Ws61Shared *ctl = reinterpret_cast<Ws61Shared *>(ring + kWsSlots * kBSide);
+  unsigned char *stage = ring + kWsSlots * kBSide;  // output rows of one step (epilogue)
+  Ws61Shared *ctl = reinterpret_cast<Ws61Shared *>(stage + kATile);
   const int t = threadIdx.x, warp = t >> 5;
   if (t == 0) {
     sj = jobs[blockIdx.y];
@@ -700,9 +701,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
             tk + ((size_t)side * C + it.cat) * (kBSide / 4) + (size_t)(st < kN ? st : kN) * kTipRow61);
       }
       const bool bad = __any_sync(0xffffffffu, !ws_wait(sptr(&ctl->mma_done[b]), (s >> 1) & 1, err));
+      float v[64];
+      float f = 1.f;
       if (!bad) {
         fence_after();
-        float v[64];
         float mx = 0.f;
 #pragma unroll
         for (int hh = 0; hh < 2; hh++) {
@@ -737,37 +739,58 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         fence_before();
         mbar_arrive(sptr(&ctl->epi_done[b]));
         int s_out = scl + scr;
-        float f = 1.f;
         if ((inL || inR) && mx < kScaleThrF && inv0) {
           f = 18446744073709551616.0f;  // 2^64
           s_out += 1;
         }
-        float4 *dst = reinterpret_cast<float4 *>(part + (size_t)op.dst_slot * c.slot_elems +
-                                                 mix_off<61>(c, (long)tile * kTile, it.cat));
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-          const int x = 4 * i;
-          float4 w = make_float4(v[4 * i] * f, v[4 * i + 1] * f, v[4 * i + 2] * f, v[4 * i + 3] * f);
-          if (x + 3 >= kN) {  // padding states stored as zeros
-            if (x + 1 >= kN) w.y = 0.f;
-            if (x + 2 >= kN) w.z = 0.f;
-            if (x + 3 >= kN) w.w = 0.f;
-            if (x >= kN) w.x = 0.f;
-          }
-          dst[i * kTile + row] = w;
-        }
         if (act)
           c.scale[(size_t)op.dst_slot * c.slot_scale + (size_t)p * C + it.cat] = (uint16_t)s_out;
-        // later steps bulk-copy these rows from global memory
-        asm volatile("fence.proxy.async.global;" ::: "memory");
       }
+      // every thread agrees on a failure; the previous step's bulk store has read the staging
+      // buffer (its issuing thread waited for that before arriving)
       if (epi_sync_or(bad)) {
+        if (row == 0) bulk_wait<0>();
         ws_fail(err, flag);
         break;
       }
-      if (row == 0) st_release_s(&ctl->n_stored, s + 1);
+      // the rows go out through the staging buffer and one bulk store, which keeps the global
+      // stores out of the epilogue's way; the next steps' copies read them through the same
+      // (async) proxy
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        const int x = 4 * i;
+        float4 w = make_float4(v[4 * i] * f, v[4 * i + 1] * f, v[4 * i + 2] * f, v[4 * i + 3] * f);
+        if (x + 3 >= kN) {  // padding states stored as zeros
+          if (x + 1 >= kN) w.y = 0.f;
+          if (x + 2 >= kN) w.z = 0.f;
+          if (x + 3 >= kN) w.w = 0.f;
+          if (x >= kN) w.x = 0.f;
+        }
+        reinterpret_cast<float4 *>(stage)[i * kTile + row] = w;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (row == 0) {
+        bulk_s2g(part + (size_t)op.dst_slot * c.slot_elems + mix_off<61>(c, (long)tile * kTile, it.cat),
+                 sptr(stage), kATile);
+        bulk_commit();
+        // publish the steps whose rows are in global memory: those before this one (a child is
+        // read C steps after it was written, so this step's rows are not awaited yet), and this
+        // one too when an op has a single category (the next step may read it)
+        if (C == 1) {
+          bulk_wait<0>();
+          asm volatile("fence.proxy.async.global;" ::: "memory");
+          st_release_s(&ctl->n_stored, s + 1);
+        } else {
+          bulk_wait<1>();
+          asm volatile("fence.proxy.async.global;" ::: "memory");
+          st_release_s(&ctl->n_stored, s);
+          bulk_wait_read<0>();
+        }
+      }
       step_next(it, ops, nops, C);
     }
+    if (row == 0) bulk_wait<0>();
   } else if (warp == 8) {
     // ---- copies
     if (elect_one()) {
@@ -776,8 +799,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       int d1 = -1, d2 = -1, d3 = -1;  // destination slots of the three previous ops
       int nimg = 0;
       bool ok = true;
-      bool land_armed[2] = {false, false}, slot_armed[kWsSlots] = {false, false, false};
-      uint32_t land_par[2] = {0, 0}, slot_par[kWsSlots] = {0, 0, 0};
+      bool land_armed[2] = {false, false}, slot_armed[kWsSlots] = {};
+      uint32_t land_par[2] = {0, 0}, slot_par[kWsSlots] = {};
       for (int s = 0; s < nsteps && ok; s++) {
         const int b = s & 1, u = s >> 1;
         const DevOp &op = it.op;
@@ -855,8 +878,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       StepIt it{0, 0, ops[0]};
       int nimg = 0;
       bool ok = true;
-      bool slot_used[kWsSlots] = {false, false, false};
-      uint32_t slot_par[kWsSlots] = {0, 0, 0};
+      bool slot_used[kWsSlots] = {};
+      uint32_t slot_par[kWsSlots] = {};
       for (int s = 0; s < nsteps && ok; s++) {
         const int b = s & 1, u = s >> 1;
         const bool in[2] = {it.op.l_kind == GEMS_CHILD_PARTIAL, it.op.r_kind == GEMS_CHILD_PARTIAL};
@@ -910,7 +933,9 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   if (warp == 0) tmem_dealloc(tmem, kWsTmemCols);
 }
 
-size_t tc61ws_smem() { return 4 * (size_t)kATile + kWsSlots * (size_t)kBSide + sizeof(Ws61Shared) + 64; }
+size_t tc61ws_smem() {
+  return 5 * (size_t)kATile + kWsSlots * (size_t)kBSide + sizeof(Ws61Shared) + 64;
+}
 
 }  // namespace
 
