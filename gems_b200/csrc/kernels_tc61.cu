@@ -513,23 +513,30 @@ size_t tc61_smem() { return 4 * (size_t)kATile + 2 * (size_t)kBSide + sizeof(Tc6
 //   warps 0-3, split: one thread per pattern row.  Waits for the operand tiles of step s in
 //     landing buffer s&1 and splits each internal child's row: hi -> TMEM A_hi[s&1][side], lo
 //     written back in place (the landing buffer is then the lo operand of the MMAs).
-//   warps 4-7, epilogue: one thread per pattern row.  Waits for the MMAs of step s, reads
-//     D[s&1] and frees it; a tip child's message is its tip table row, read from global memory
-//     (L1-cached: the rows of one table are shared by the patterns of a tile); products, SAFE
-//     rescaling, stores; then publishes the number of steps whose rows are stored.
-//   warp 8, copies: the operand tiles of step s into landing buffer s&1, once the MMAs of step
-//     s-2 are done with it and every step that wrote one of those children has published its
-//     stores; the B images of internal sides, in step order, into a ring of three 32 KB slots.
-//   warp 9, MMAs: step s into D[s&1] once its split is done, its B images have landed and the
+//   warps 4-11, epilogue: two threads per pattern row, 32 states each (warps w and w+4 share
+//     TMEM lane quadrant w%4).  A tip child's message is its tip table row, read from global
+//     memory (L1-cached: the rows of one table are shared by the patterns of a tile) before the
+//     wait; waits for the MMAs of step s, reads D[s&1] and frees it; products, the row maximum
+//     over both halves (exchanged in shared memory), SAFE rescaling.  The rows go into a 32 KB
+//     staging buffer and out with one bulk store, so that no per-thread global store sits in the
+//     SM's memory path beside the copies and MMAs; once a step's bulk group has completed, the
+//     number of steps stored is published.  The epilogue is the longest part of a step, so it
+//     has the most warps.
+//   warp 12, copies: the operand tiles of step s into landing buffer s&1, once the MMAs of
+//     step s-2 are done with it and every step that wrote one of those children has published
+//     its stores; the B images of internal sides, in step order, into a ring of two 32 KB slots.
+//   warp 13, MMAs: step s into D[s&1] once its split is done, its B images have landed and the
 //     epilogue of step s-2 has read D[s&1]; a commit per side frees its ring slot, a commit per
 //     step signals the epilogue and the copies.
 // TMEM: D[b][side] at columns b*128 + side*64, A_hi[b][side] at 256 + b*128 + side*64 (512).
-// Shared memory: landing buffers [2][2 sides][32 KB] and the ring [3][32 KB]: 224 KB.  The
-// products, the split and the summation order are those of the form above: the same bits.
+// Shared memory: landing buffers [2][2 sides][32 KB], the ring [2][32 KB] and the staging
+// buffer: 224 KB.  The products, the split and the summation order are those of the form
+// above: the same bits.
 // Every wait is bounded and also gives up once another role has failed (err); on failure the
 // copy and MMA warps wait (bounded) for what they have in flight before TMEM is freed.
 // ---------------------------------------------------------------------------------------
-constexpr int kWsThreads = 320;
+constexpr int kWsThreads = 448;
+constexpr int kWsEpi = 256;  // epilogue threads
 constexpr int kWsSlots = 2;
 constexpr int kWsTmemCols = 512;
 constexpr int kWsAhi = 256;
@@ -541,6 +548,7 @@ struct Ws61Shared {
   uint32_t tmem_base;
   int n_stored;  // steps whose rows are stored and fenced for the async proxy
   int err;       // set by the first role whose wait expired
+  float rowmax[2][kTile];  // epilogue: each half's row maximum
 };
 
 __device__ __forceinline__ bool ws_wait(uint32_t bar, uint32_t parity, const int *err) {
@@ -563,13 +571,13 @@ __device__ __forceinline__ int ld_acquire_s(const int *p) {
 __device__ __forceinline__ void st_release_s(int *p, int v) {
   asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(sptr(p)), "r"(v) : "memory");
 }
-// OR of `pred` over the 128 threads of the epilogue warps (named barrier 1)
+// OR of `pred` over the 256 threads of the epilogue warps (named barrier 1)
 __device__ __forceinline__ bool epi_sync_or(bool pred) {
   uint32_t r;
   asm volatile(
       "{\n\t.reg .pred p, q;\n\t"
       "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, 128, p;\n\t"
+      "bar.red.or.pred q, 1, 256, p;\n\t"
       "selp.u32 %0, 1, 0, q;\n\t}\n"
       : "=r"(r)
       : "r"((uint32_t)pred)
@@ -605,7 +613,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       mbar_init(sptr(&ctl->full_land[b]), 1);
       mbar_init(sptr(&ctl->split_done[b]), kTile);
       mbar_init(sptr(&ctl->mma_done[b]), 1);
-      mbar_init(sptr(&ctl->epi_done[b]), kTile);
+      mbar_init(sptr(&ctl->epi_done[b]), kWsEpi);
     }
     for (int q = 0; q < kWsSlots; q++) {
       mbar_init(sptr(&ctl->full_slot[q]), 1);
@@ -669,10 +677,13 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       mbar_arrive(sptr(&ctl->split_done[b]));
       step_next(it, ops, nops, C);
     }
-  } else if (warp < 8) {
+  } else if (warp < 12) {
     // ---- epilogue
-    const int row = t - 4 * 32;
-    const uint32_t lane_off = (uint32_t)((warp - 4) * 32) << 16;
+    const int ew = warp - 4;
+    const int row = ((ew & 3) << 5) | (t & 31);
+    const int half = ew >> 2;  // states [32 half, 32 half + 32)
+    const uint32_t lane_off = (uint32_t)((ew & 3) * 32) << 16;
+    const bool lead = t == 4 * 32;  // issues the bulk stores and publishes
     const long p = (long)tile * kTile + row;
     const bool act = p < c.P;
     const bool inv0 = act ? c.invar[p] == 0.0 : false;
@@ -692,73 +703,70 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         if (inL) scl = c.scale[(size_t)op.l_id * c.slot_scale + (size_t)p * C + it.cat];
         if (inR) scr = c.scale[(size_t)op.r_id * c.slot_scale + (size_t)p * C + it.cat];
       }
+      // messages: a tip child's from its table row (loaded before the wait), an internal
+      // child's from its accumulator
+      uint32_t rm[2][32];
       const float *tk = tab + (size_t)it.k * stride_f;
-      const float4 *tip4[2];
 #pragma unroll
       for (int side = 0; side < 2; side++) {
+        if (side ? inR : inL) continue;
         const int st = side ? st_r : st_l;
-        tip4[side] = reinterpret_cast<const float4 *>(
-            tk + ((size_t)side * C + it.cat) * (kBSide / 4) + (size_t)(st < kN ? st : kN) * kTipRow61);
+        const float4 *tr = reinterpret_cast<const float4 *>(
+                               tk + ((size_t)side * C + it.cat) * (kBSide / 4) +
+                               (size_t)(st < kN ? st : kN) * kTipRow61) + 8 * half;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const float4 q = __ldg(tr + i);
+          rm[side][4 * i] = __float_as_uint(q.x);
+          rm[side][4 * i + 1] = __float_as_uint(q.y);
+          rm[side][4 * i + 2] = __float_as_uint(q.z);
+          rm[side][4 * i + 3] = __float_as_uint(q.w);
+        }
       }
       const bool bad = __any_sync(0xffffffffu, !ws_wait(sptr(&ctl->mma_done[b]), (s >> 1) & 1, err));
-      float v[64];
-      float f = 1.f;
+      float v[32];
       if (!bad) {
         fence_after();
-        float mx = 0.f;
 #pragma unroll
-        for (int hh = 0; hh < 2; hh++) {
-          uint32_t rm[2][32];
+        for (int side = 0; side < 2; side++)
+          if (side ? inR : inL)
+            tmem_ld32(tmem + lane_off + (uint32_t)(b * 128 + side * kNP + 32 * half), rm[side]);
 #pragma unroll
-          for (int side = 0; side < 2; side++)
-            if (side ? inR : inL)
-              tmem_ld32(tmem + lane_off + (uint32_t)(b * 128 + side * kNP + 32 * hh), rm[side]);
-#pragma unroll
-          for (int side = 0; side < 2; side++) {
-            if (side ? inR : inL) {
-              tmem_ld32_wait(rm[side]);
-            } else {
-#pragma unroll
-              for (int i = 0; i < 8; i++) {
-                const float4 q = __ldg(tip4[side] + 8 * hh + i);
-                rm[side][4 * i] = __float_as_uint(q.x);
-                rm[side][4 * i + 1] = __float_as_uint(q.y);
-                rm[side][4 * i + 2] = __float_as_uint(q.z);
-                rm[side][4 * i + 3] = __float_as_uint(q.w);
-              }
-            }
-          }
-#pragma unroll
-          for (int i = 0; i < 32; i++) {
-            const float w = fmaxf(__uint_as_float(rm[0][i]), 0.f) * fmaxf(__uint_as_float(rm[1][i]), 0.f);
-            v[32 * hh + i] = w;
-            mx = fmaxf(mx, w);
-          }
-        }
+        for (int side = 0; side < 2; side++)
+          if (side ? inR : inL) tmem_ld32_wait(rm[side]);
         // D[b] has been read: the MMAs of step s+2 may overwrite it
         fence_before();
         mbar_arrive(sptr(&ctl->epi_done[b]));
-        int s_out = scl + scr;
-        if ((inL || inR) && mx < kScaleThrF && inv0) {
-          f = 18446744073709551616.0f;  // 2^64
-          s_out += 1;
+        float mx = 0.f;
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+          v[i] = fmaxf(__uint_as_float(rm[0][i]), 0.f) * fmaxf(__uint_as_float(rm[1][i]), 0.f);
+          mx = fmaxf(mx, v[i]);
         }
-        if (act)
-          c.scale[(size_t)op.dst_slot * c.slot_scale + (size_t)p * C + it.cat] = (uint16_t)s_out;
+        ctl->rowmax[half][row] = mx;
       }
-      // every thread agrees on a failure; the previous step's bulk store has read the staging
-      // buffer (its issuing thread waited for that before arriving)
+      // every thread agrees on a failure; both halves' maxima are in place; the previous step's
+      // bulk store has read the staging buffer (its issuing thread waited for that first)
       if (epi_sync_or(bad)) {
-        if (row == 0) bulk_wait<0>();
+        if (lead) bulk_wait<0>();
         ws_fail(err, flag);
         break;
       }
+      const float m = fmaxf(ctl->rowmax[0][row], ctl->rowmax[1][row]);
+      int s_out = scl + scr;
+      float f = 1.f;
+      if ((inL || inR) && m < kScaleThrF && inv0) {
+        f = 18446744073709551616.0f;  // 2^64
+        s_out += 1;
+      }
+      if (act && half == 0)
+        c.scale[(size_t)op.dst_slot * c.slot_scale + (size_t)p * C + it.cat] = (uint16_t)s_out;
       // the rows go out through the staging buffer and one bulk store, which keeps the global
       // stores out of the epilogue's way; the next steps' copies read them through the same
       // (async) proxy
 #pragma unroll
-      for (int i = 0; i < 16; i++) {
-        const int x = 4 * i;
+      for (int i = 0; i < 8; i++) {
+        const int x = 32 * half + 4 * i;
         float4 w = make_float4(v[4 * i] * f, v[4 * i + 1] * f, v[4 * i + 2] * f, v[4 * i + 3] * f);
         if (x + 3 >= kN) {  // padding states stored as zeros
           if (x + 1 >= kN) w.y = 0.f;
@@ -766,11 +774,12 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           if (x + 3 >= kN) w.w = 0.f;
           if (x >= kN) w.x = 0.f;
         }
-        reinterpret_cast<float4 *>(stage)[i * kTile + row] = w;
+        reinterpret_cast<float4 *>(stage)[(8 * half + i) * kTile + row] = w;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("bar.sync 1, 128;" ::: "memory");
-      if (row == 0) {
+      // the rows are staged; also orders this step's reads of rowmax before the next writes
+      asm volatile("bar.sync 2, 256;" ::: "memory");
+      if (lead) {
         bulk_s2g(part + (size_t)op.dst_slot * c.slot_elems + mix_off<61>(c, (long)tile * kTile, it.cat),
                  sptr(stage), kATile);
         bulk_commit();
@@ -790,8 +799,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       }
       step_next(it, ops, nops, C);
     }
-    if (row == 0) bulk_wait<0>();
-  } else if (warp == 8) {
+    if (lead) bulk_wait<0>();
+  } else if (warp == 12) {
     // ---- copies
     if (elect_one()) {
       float *part = static_cast<float *>(c.partials);
