@@ -518,10 +518,12 @@ size_t tc61_smem() { return 4 * (size_t)kATile + 2 * (size_t)kBSide + sizeof(Tc6
 //     memory (L1-cached: the rows of one table are shared by the patterns of a tile) before the
 //     wait; waits for the MMAs of step s, reads D[s&1] and frees it; products, the row maximum
 //     over both halves (exchanged in shared memory), SAFE rescaling.  The rows go into a 32 KB
-//     staging buffer and out with one bulk store, so that no per-thread global store sits in the
-//     SM's memory path beside the copies and MMAs; once a step's bulk group has completed, the
-//     number of steps stored is published.  The epilogue is the longest part of a step, so it
-//     has the most warps.
+//     staging buffer, so that no per-thread global store sits in the SM's memory path beside
+//     the copies and MMAs.  The epilogue is the longest part of a step, so it has the most
+//     warps.
+//   warp 14, stores: one bulk store of the staged rows per step; once it has read the staging
+//     buffer the epilogue may fill it again, and once it has completed the number of steps
+//     stored is published.
 //   warp 12, copies: the operand tiles of step s into landing buffer s&1, once the MMAs of
 //     step s-2 are done with it and every step that wrote one of those children has published
 //     its stores; the B images of internal sides, in step order, into a ring of two 32 KB slots.
@@ -530,12 +532,12 @@ size_t tc61_smem() { return 4 * (size_t)kATile + 2 * (size_t)kBSide + sizeof(Tc6
 //     step signals the epilogue and the copies.
 // TMEM: D[b][side] at columns b*128 + side*64, A_hi[b][side] at 256 + b*128 + side*64 (512).
 // Shared memory: landing buffers [2][2 sides][32 KB], the ring [2][32 KB] and the staging
-// buffer: 224 KB.  The products, the split and the summation order are those of the form
-// above: the same bits.
-// Every wait is bounded and also gives up once another role has failed (err); on failure the
-// copy and MMA warps wait (bounded) for what they have in flight before TMEM is freed.
+// buffer: 224 KB; 480 threads.  The products, the split and the summation order are those of
+// the form above: the same bits.  Every wait is bounded and also gives up once another role has
+// failed (err); on failure the copy, MMA and store warps wait (bounded) for what they have in
+// flight before TMEM and shared memory are released.
 // ---------------------------------------------------------------------------------------
-constexpr int kWsThreads = 448;
+constexpr int kWsThreads = 480;
 constexpr int kWsEpi = 256;  // epilogue threads
 constexpr int kWsSlots = 2;
 constexpr int kWsTmemCols = 512;
@@ -545,6 +547,7 @@ struct Ws61Shared {
   uint64_t full_land[2], split_done[2], mma_done[2], epi_done[2];
   uint64_t full_slot[kWsSlots], slot_free[kWsSlots];
   uint64_t drain;  // MMAs in flight when a role failed
+  uint64_t staged, stage_free;  // the staging buffer holds a step's rows / has been read
   uint32_t tmem_base;
   int n_stored;  // steps whose rows are stored and fenced for the async proxy
   int err;       // set by the first role whose wait expired
@@ -578,6 +581,19 @@ __device__ __forceinline__ bool epi_sync_or(bool pred) {
       "{\n\t.reg .pred p, q;\n\t"
       "setp.ne.u32 p, %1, 0;\n\t"
       "bar.red.or.pred q, 1, 256, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred)
+      : "memory");
+  return r != 0;
+}
+// the same on named barrier 2
+__device__ __forceinline__ bool epi_sync_or2(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 2, 256, p;\n\t"
       "selp.u32 %0, 1, 0, q;\n\t}\n"
       : "=r"(r)
       : "r"((uint32_t)pred)
@@ -620,6 +636,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       mbar_init(sptr(&ctl->slot_free[q]), 1);
     }
     mbar_init(sptr(&ctl->drain), 1);
+    mbar_init(sptr(&ctl->staged), 1);
+    mbar_init(sptr(&ctl->stage_free), 1);
     ctl->n_stored = 0;
     ctl->err = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -683,11 +701,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     const int row = ((ew & 3) << 5) | (t & 31);
     const int half = ew >> 2;  // states [32 half, 32 half + 32)
     const uint32_t lane_off = (uint32_t)((ew & 3) * 32) << 16;
-    const bool lead = t == 4 * 32;  // issues the bulk stores and publishes
+    const bool lead = t == 4 * 32;  // signals the store warp
     const long p = (long)tile * kTile + row;
     const bool act = p < c.P;
     const bool inv0 = act ? c.invar[p] == 0.0 : false;
-    float *part = static_cast<float *>(c.partials);
     StepIt it{0, 0, ops[0]};
     int st_l = 0, st_r = 0;
     for (int s = 0; s < nsteps; s++) {
@@ -745,10 +762,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         }
         ctl->rowmax[half][row] = mx;
       }
-      // every thread agrees on a failure; both halves' maxima are in place; the previous step's
-      // bulk store has read the staging buffer (its issuing thread waited for that first)
+      // every thread agrees on a failure; both halves' maxima are in place
       if (epi_sync_or(bad)) {
-        if (lead) bulk_wait<0>();
         ws_fail(err, flag);
         break;
       }
@@ -761,11 +776,13 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       }
       if (act && half == 0)
         c.scale[(size_t)op.dst_slot * c.slot_scale + (size_t)p * C + it.cat] = (uint16_t)s_out;
-      // the rows go out through the staging buffer and one bulk store, which keeps the global
-      // stores out of the epilogue's way; the next steps' copies read them through the same
-      // (async) proxy
+      // the rows go out through the staging buffer and one bulk store (issued by the store
+      // warp), which keeps the global stores out of the epilogue's way; the next steps' copies
+      // read them through the same (async) proxy.  The previous step's store has read the
+      // staging buffer first.
+      const bool stale = s > 0 && __any_sync(0xffffffffu, !ws_wait(sptr(&ctl->stage_free), (s - 1) & 1, err));
 #pragma unroll
-      for (int i = 0; i < 8; i++) {
+      for (int i = 0; i < 8 && !stale; i++) {
         const int x = 32 * half + 4 * i;
         float4 w = make_float4(v[4 * i] * f, v[4 * i + 1] * f, v[4 * i + 2] * f, v[4 * i + 3] * f);
         if (x + 3 >= kN) {  // padding states stored as zeros
@@ -777,29 +794,40 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         reinterpret_cast<float4 *>(stage)[(8 * half + i) * kTile + row] = w;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      // the rows are staged; also orders this step's reads of rowmax before the next writes
-      asm volatile("bar.sync 2, 256;" ::: "memory");
-      if (lead) {
-        bulk_s2g(part + (size_t)op.dst_slot * c.slot_elems + mix_off<61>(c, (long)tile * kTile, it.cat),
-                 sptr(stage), kATile);
-        bulk_commit();
-        // publish the steps whose rows are in global memory: those before this one (a child is
-        // read C steps after it was written, so this step's rows are not awaited yet), and this
-        // one too when an op has a single category (the next step may read it)
-        if (C == 1) {
-          bulk_wait<0>();
-          asm volatile("fence.proxy.async.global;" ::: "memory");
-          st_release_s(&ctl->n_stored, s + 1);
-        } else {
-          bulk_wait<1>();
-          asm volatile("fence.proxy.async.global;" ::: "memory");
-          st_release_s(&ctl->n_stored, s);
-          bulk_wait_read<0>();
-        }
+      // the rows are staged (or a wait failed); also orders this step's reads of rowmax before
+      // the next step's writes
+      if (epi_sync_or2(stale)) {
+        ws_fail(err, flag);
+        break;
       }
+      if (lead) mbar_arrive(sptr(&ctl->staged));
       step_next(it, ops, nops, C);
     }
-    if (lead) bulk_wait<0>();
+  } else if (warp == 14) {
+    // ---- bulk stores of the staged rows, and the count of steps stored
+    if (elect_one()) {
+      float *part = static_cast<float *>(c.partials);
+      StepIt it{0, 0, ops[0]};
+      for (int s = 0; s < nsteps; s++) {
+        if (!ws_wait(sptr(&ctl->staged), s & 1, err)) {
+          ws_fail(err, flag);
+          break;
+        }
+        bulk_s2g(part + (size_t)it.op.dst_slot * c.slot_elems + mix_off<61>(c, (long)tile * kTile, it.cat),
+                 sptr(stage), kATile);
+        bulk_commit();
+        bulk_wait_read<0>();
+        mbar_arrive(sptr(&ctl->stage_free));
+        // the rows are in global memory: publish the step (this warp has nothing else to do
+        // until the next step is staged)
+        bulk_wait<0>();
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        st_release_s(&ctl->n_stored, s + 1);
+        step_next(it, ops, nops, C);
+      }
+      bulk_wait<0>();
+    }
+    __syncwarp();
   } else if (warp == 12) {
     // ---- copies
     if (elect_one()) {
@@ -881,7 +909,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       }
     }
     __syncwarp();
-  } else {
+  } else if (warp == 13) {
     // ---- MMAs
     if (elect_one()) {
       StepIt it{0, 0, ops[0]};
