@@ -66,8 +66,12 @@ def test_admission_by_footprint(gpu):
 def test_eviction_keeps_results(gpu):
     """A budget that holds the largest session and little more: idle sessions are evicted while
     they still have requests to come, rebuilt from their saved trees, and every session's
-    results stay bit-identical to running it alone."""
-    specs, reqs, cases = workload(nsess=6, nreq=40, seed=6)
+    results stay bit-identical to running it alone.  The requests come round-robin over the
+    sessions, 50 ms apart (longer than a request takes), so a session is idle between its
+    requests while another one waits for room: eviction is needed whatever the sessions' speed."""
+    specs, _, cases = workload(nsess=6, nreq=40, seed=6)
+    sids = [s.sid for s in specs]
+    reqs = [((r * len(sids) + i) * 0.05, sid) for r in range(3) for i, sid in enumerate(sids)]
     fps = sorted(s.footprint(cases[s.sid][2].npat) for s in specs)
     srv = serve.Server(workers=3, budget_bytes=fps[-1] + fps[0], memsave=False)
     records, _ = srv.run(specs, cases, reqs)
