@@ -554,53 +554,10 @@ struct Ws61Shared {
   float rowmax[2][kTile];  // epilogue: each half's row maximum
 };
 
-__device__ __forceinline__ bool ws_wait(uint32_t bar, uint32_t parity, const int *err) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (*(const volatile int *)err) return false;
-    if (clock64() - t0 > kWaitCycles) return false;
-  }
-  return true;
-}
 __device__ __forceinline__ void ws_fail(int *err, int *flag) {
   *(volatile int *)err = 1;
   atomicExch(flag, GEMS_ERR_TIMEOUT);
 }
-__device__ __forceinline__ int ld_acquire_s(const int *p) {
-  int v;
-  asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(sptr(p)) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_s(int *p, int v) {
-  asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(sptr(p)), "r"(v) : "memory");
-}
-// OR of `pred` over the 256 threads of the epilogue warps (named barrier 1)
-__device__ __forceinline__ bool epi_sync_or(bool pred) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, 256, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}\n"
-      : "=r"(r)
-      : "r"((uint32_t)pred)
-      : "memory");
-  return r != 0;
-}
-// the same on named barrier 2
-__device__ __forceinline__ bool epi_sync_or2(bool pred) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 2, 256, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}\n"
-      : "=r"(r)
-      : "r"((uint32_t)pred)
-      : "memory");
-  return r != 0;
-}
-
 // (op, category) of consecutive steps
 struct StepIt {
   int k, cat;
@@ -763,7 +720,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         ctl->rowmax[half][row] = mx;
       }
       // every thread agrees on a failure; both halves' maxima are in place
-      if (epi_sync_or(bad)) {
+      if (bar_or<1, kWsEpi>(bad)) {
         ws_fail(err, flag);
         break;
       }
@@ -796,7 +753,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       // the rows are staged (or a wait failed); also orders this step's reads of rowmax before
       // the next step's writes
-      if (epi_sync_or2(stale)) {
+      if (bar_or<2, kWsEpi>(stale)) {
         ws_fail(err, flag);
         break;
       }
@@ -856,15 +813,9 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           const int back = id[side] == d1 ? 1 : (id[side] == d2 ? 2 : (id[side] == d3 ? 3 : 4));
           need = max(need, s - back * C + 1);
         }
-        if (need > 0) {
-          const long long t0 = clock64();
-          while (ld_acquire_s(&ctl->n_stored) < need) {
-            if (*(volatile int *)err || clock64() - t0 > kWaitCycles) {
-              ok = false;
-              break;
-            }
-          }
-          if (!ok) break;
+        if (need > 0 && !wait_count(&ctl->n_stored, need, err)) {
+          ok = false;
+          break;
         }
         const uint32_t fl = sptr(&ctl->full_land[b]);
         mbar_expect_tx(fl, (uint32_t)((in[0] ? kATile : 0) + (in[1] ? kATile : 0)));

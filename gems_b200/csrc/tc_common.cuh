@@ -42,6 +42,49 @@ __device__ inline bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (clock64() - t0 > kWaitCycles) return false;
   return true;
 }
+// a bounded wait that also gives up once another part of the CTA has failed (*err set)
+__device__ __forceinline__ bool ws_wait(uint32_t bar, uint32_t parity, const int *err) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*(const volatile int *)err) return false;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+  return true;
+}
+// a counter in shared memory published by one thread (release) and polled by others (acquire)
+__device__ __forceinline__ int ld_acquire_s(const int *p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(sptr(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_s(int *p, int v) {
+  asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(sptr(p)), "r"(v) : "memory");
+}
+// bounded wait until the counter reaches `need` (false on expiry or once *err is set)
+__device__ __forceinline__ bool wait_count(const int *cnt, int need, const int *err) {
+  const long long t0 = clock64();
+  while (ld_acquire_s(cnt) < need)
+    if (*(const volatile int *)err || clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+// OR of `pred` over the NT threads that use named barrier BAR (all of them wait for all)
+template <int BAR, int NT>
+__device__ __forceinline__ bool bar_or(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "n"(BAR), "n"(NT)
+      : "memory");
+  return r != 0;
+}
+template <int BAR, int NT>
+__device__ __forceinline__ void bar_sync() {
+  asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(NT) : "memory");
+}
 // contiguous global -> shared copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
                                          uint32_t bar) {
