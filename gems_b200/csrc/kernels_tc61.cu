@@ -551,7 +551,7 @@ struct Ws61Shared {
   uint32_t tmem_base;
   int n_stored;  // steps whose rows are stored and fenced for the async proxy
   int err;       // set by the first role whose wait expired
-  float rowmax[2][kTile];  // epilogue: each half's row maximum
+  float rowmax[2][2][kTile];  // epilogue: each half's row maximum, by step parity
 };
 
 __device__ __forceinline__ void ws_fail(int *err, int *flag) {
@@ -574,14 +574,12 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     k_traverse_tc61ws(const TcJob *__restrict__ jobs, int nops, size_t stride_f, int *flag,
                       int tile0) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ TcJob sj;
   unsigned char *land = smem_raw;               // [buffer][side][32 KB]
   unsigned char *ring = smem_raw + 4 * kATile;  // [slot][hi 16 KB, lo 16 KB]
   unsigned char *stage = ring + kWsSlots * kBSide;  // output rows of one step (epilogue)
   Ws61Shared *ctl = reinterpret_cast<Ws61Shared *>(stage + kATile);
   const int t = threadIdx.x, warp = t >> 5;
   if (t == 0) {
-    sj = jobs[blockIdx.y];
     for (int b = 0; b < 2; b++) {
       mbar_init(sptr(&ctl->full_land[b]), 1);
       mbar_init(sptr(&ctl->split_done[b]), kTile);
@@ -593,7 +591,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       mbar_init(sptr(&ctl->slot_free[q]), 1);
     }
     mbar_init(sptr(&ctl->drain), 1);
-    mbar_init(sptr(&ctl->staged), 1);
+    mbar_init(sptr(&ctl->staged), kWsEpi);
     mbar_init(sptr(&ctl->stage_free), 1);
     ctl->n_stored = 0;
     ctl->err = 0;
@@ -603,9 +601,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   fence_before();
   __syncthreads();
   fence_after();
-  const DevCtx &c = sj.c;
-  const DevOp *ops = sj.ops;
-  const float *tab = sj.tab;
+  const TcJob &job = jobs[blockIdx.y];  // read in place: the shared memory is all in use
+  const DevCtx &c = job.c;
+  const DevOp *ops = job.ops;
+  const float *tab = job.tab;
   const int C = c.C;
   const int tile = tile0 + blockIdx.x;
   const uint32_t tmem = ctl->tmem_base;
@@ -658,12 +657,12 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     const int row = ((ew & 3) << 5) | (t & 31);
     const int half = ew >> 2;  // states [32 half, 32 half + 32)
     const uint32_t lane_off = (uint32_t)((ew & 3) * 32) << 16;
-    const bool lead = t == 4 * 32;  // signals the store warp
     const long p = (long)tile * kTile + row;
     const bool act = p < c.P;
     const bool inv0 = act ? c.invar[p] == 0.0 : false;
     StepIt it{0, 0, ops[0]};
     int st_l = 0, st_r = 0;
+    bool stale_prev = false;  // the previous step's staging wait failed
     for (int s = 0; s < nsteps; s++) {
       const int b = s & 1;
       const DevOp op = it.op;
@@ -717,14 +716,14 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           v[i] = fmaxf(__uint_as_float(rm[0][i]), 0.f) * fmaxf(__uint_as_float(rm[1][i]), 0.f);
           mx = fmaxf(mx, v[i]);
         }
-        ctl->rowmax[half][row] = mx;
+        ctl->rowmax[b][half][row] = mx;
       }
       // every thread agrees on a failure; both halves' maxima are in place
-      if (bar_or<1, kWsEpi>(bad)) {
+      if (bar_or<1, kWsEpi>(bad || stale_prev)) {
         ws_fail(err, flag);
         break;
       }
-      const float m = fmaxf(ctl->rowmax[0][row], ctl->rowmax[1][row]);
+      const float m = fmaxf(ctl->rowmax[b][0][row], ctl->rowmax[b][1][row]);
       int s_out = scl + scr;
       float f = 1.f;
       if ((inL || inR) && m < kScaleThrF && inv0) {
@@ -738,6 +737,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       // read them through the same (async) proxy.  The previous step's store has read the
       // staging buffer first.
       const bool stale = s > 0 && __any_sync(0xffffffffu, !ws_wait(sptr(&ctl->stage_free), (s - 1) & 1, err));
+      if (stale) ws_fail(err, flag);
 #pragma unroll
       for (int i = 0; i < 8 && !stale; i++) {
         const int x = 32 * half + 4 * i;
@@ -751,13 +751,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         reinterpret_cast<float4 *>(stage)[(8 * half + i) * kTile + row] = w;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      // the rows are staged (or a wait failed); also orders this step's reads of rowmax before
-      // the next step's writes
-      if (bar_or<2, kWsEpi>(stale)) {
-        ws_fail(err, flag);
-        break;
-      }
-      if (lead) mbar_arrive(sptr(&ctl->staged));
+      // this thread's rows are staged: the store warp waits for all of them (a failed wait is
+      // agreed on at the next step's barrier)
+      mbar_arrive(sptr(&ctl->staged));
+      stale_prev = stale;
       step_next(it, ops, nops, C);
     }
   } else if (warp == 14) {
