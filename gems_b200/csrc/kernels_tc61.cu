@@ -70,16 +70,16 @@ constexpr uint32_t kTipBytes61 = kTipRows61 * kTipRow61 * 4;  // 16,864 bytes
 
 // The op tables of a job's op k and side (blockIdx.x, blockIdx.y; job blockIdx.z of `jobs`, or
 // `one` when jobs is null).  P_c(t) = evec . diag(exp(eval * rate_c * t)) . inv_evec in FP64,
-// clamped at 0, then split into TF32 hi and lo images.  Register-tiled: a thread owns the 4 x 4
-// block of target states 4xq..4xq+3 by source states 4j..4j+3 (one float4 of every image row
-// it writes), so each term of the sum costs 9 shared-memory reads for 16 FMAs; the sum over i
-// runs in index order with the same fma(evec * exp, inv_evec, acc) steps as a scalar loop.
-// Shared memory: exp terms [C][n]; evec as [64][n] (rows 61..63 zero); inv_evec as
-// [n][4 e][16 j] = inv_evec[i][4j + e] (columns 61..63 zero), so that the 16 lanes of a
-// half-warp read 16 consecutive doubles.  A tip side's unknown-state row sums are reduced over
-// the 16 lanes of a half-warp (the threads of one row quad) by a fixed shuffle tree: the same
-// bits in every launch.
-constexpr int kPrepThreads = 256;  // 16 row quads x 16 column quads
+// clamped at 0, then split into TF32 hi and lo images.  Register-tiled: a thread owns target
+// states 4xq..4xq+3 by the source-state quads jo and jo + 8 (4 x 8 outputs; float4s of the
+// image rows it writes), so each term of the sum costs 13 shared-memory reads for 32 FMAs; the
+// sum over i runs in index order with the same fma(evec * exp, inv_evec, acc) steps as a scalar
+// loop.  Shared memory: exp terms [C][n]; evec as [64][n] (rows 61..63 zero); inv_evec as
+// [n][4 e][16 j] = inv_evec[i][4j + e] (columns 61..63 zero), so that the 8 lanes of a row quad
+// read 8 consecutive doubles.  A tip side's unknown-state row sums add the quads j and j + 8 in
+// the thread, then the 8 lanes of the row quad by a fixed shuffle tree: the same bits in every
+// launch.
+constexpr int kPrepThreads = 128;  // 16 row quads x 8 pairs of column quads
 __host__ __device__ constexpr size_t prep61_smem_doubles(int C) {
   return (size_t)C * kN + (size_t)kNP * kN + (size_t)kN * kNP;
 }
@@ -108,69 +108,89 @@ __global__ void __launch_bounds__(kPrepThreads)
   // the job's own table, written here and read by its traversal
   float *img = const_cast<float *>(job.tab) + (size_t)k * stride_f + (size_t)side * C * (kBSide / 4);
   const int per = kBImg / 4;  // floats of one image
-  const int j = threadIdx.x & 15, xq = threadIdx.x >> 4;
+  // thread: row quad xq (rows 4xq..4xq+3) and the column quads jo and jo + 8
+  const int jo = threadIdx.x & 7, xq = threadIdx.x >> 3;
   const bool tip = (side ? op.r_kind : op.l_kind) == GEMS_CHILD_TIP;
   for (int cc = 0; cc < C; cc++) {
-    double acc[4][4];
+    double acc[4][2][4];  // [row][column quad jo, jo + 8][column in quad]
 #pragma unroll
     for (int r = 0; r < 4; r++)
 #pragma unroll
-      for (int e = 0; e < 4; e++) acc[r][e] = 0.0;
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[r][h][e] = 0.0;
     const double *exc = ex + cc * n;
     for (int i = 0; i < n; i++) {
       const double xi = exc[i];
-      double a[4], b[4];
+      double a[4], b[2][4];
 #pragma unroll
       for (int r = 0; r < 4; r++) a[r] = ev[(4 * xq + r) * n + i] * xi;
 #pragma unroll
-      for (int e = 0; e < 4; e++) b[e] = iv[i * kNP + e * 16 + j];
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) b[h][e] = iv[i * kNP + e * 16 + jo + 8 * h];
 #pragma unroll
       for (int r = 0; r < 4; r++)
 #pragma unroll
-        for (int e = 0; e < 4; e++) acc[r][e] = fma(a[r], b[e], acc[r][e]);
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+          for (int e = 0; e < 4; e++) acc[r][h][e] = fma(a[r], b[h][e], acc[r][h][e]);
     }
     if (tip) {
       // tip table: row s = column s of P_c (target states x consecutive), then the row sums
       float *tt = img + (size_t)cc * 2 * per;
-      double rs[4] = {0.0, 0.0, 0.0, 0.0};
+      double rs[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int y = 4 * j + e;
-        float v[4];
+      for (int h = 0; h < 2; h++) {
+        const int j = jo + 8 * h;
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-          const int x = 4 * xq + r;
-          const double a = (x < n && y < n) ? fmax(acc[r][e], 0.0) : 0.0;
-          rs[r] += a;
-          v[r] = (float)a;
+        for (int e = 0; e < 4; e++) {
+          const int y = 4 * j + e;
+          float v[4];
+#pragma unroll
+          for (int r = 0; r < 4; r++) {
+            const int x = 4 * xq + r;
+            const double a = (x < n && y < n) ? fmax(acc[r][h][e], 0.0) : 0.0;
+            rs[h][r] += a;
+            v[r] = (float)a;
+          }
+          if (y < n)
+            *reinterpret_cast<float4 *>(tt + (size_t)y * kTipRow61 + 4 * xq) =
+                make_float4(v[0], v[1], v[2], v[3]);
         }
-        if (y < n)
-          *reinterpret_cast<float4 *>(tt + (size_t)y * kTipRow61 + 4 * xq) =
-              make_float4(v[0], v[1], v[2], v[3]);
       }
+      // the sums of the 16 column quads by a fixed tree: quads j and j + 8 first (in this
+      // thread), then across the 8 lanes of the row quad
+      double t4[4];
 #pragma unroll
-      for (int o = 8; o >= 1; o >>= 1)
+      for (int r = 0; r < 4; r++) t4[r] = rs[0][r] + rs[1][r];
 #pragma unroll
-        for (int r = 0; r < 4; r++) rs[r] += __shfl_xor_sync(0xffffffffu, rs[r], o);
-      if (j == 0)
+      for (int o = 4; o >= 1; o >>= 1)
+#pragma unroll
+        for (int r = 0; r < 4; r++) t4[r] += __shfl_xor_sync(0xffffffffu, t4[r], o);
+      if (jo == 0)
         *reinterpret_cast<float4 *>(tt + (size_t)n * kTipRow61 + 4 * xq) =
-            make_float4((float)rs[0], (float)rs[1], (float)rs[2], (float)rs[3]);
+            make_float4((float)t4[0], (float)t4[1], (float)t4[2], (float)t4[3]);
       continue;
     }
     // image element (row x, K index y) at chunk y / 4, row x, lane y % 4
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       const int x = 4 * xq + r;
-      float v[4];
 #pragma unroll
-      for (int e = 0; e < 4; e++)
-        v[e] = (x < n && 4 * j + e < n) ? (float)fmax(acc[r][e], 0.0) : 0.f;
-      const float4 hi = make_float4(tf32_rna(v[0]), tf32_rna(v[1]), tf32_rna(v[2]), tf32_rna(v[3]));
-      const float4 lo = make_float4(tf32_rna(v[0] - hi.x), tf32_rna(v[1] - hi.y),
-                                    tf32_rna(v[2] - hi.z), tf32_rna(v[3] - hi.w));
-      const size_t o = (size_t)cc * 2 * per + ((size_t)j * kNP + x) * 4;
-      *reinterpret_cast<float4 *>(img + o) = hi;
-      *reinterpret_cast<float4 *>(img + o + per) = lo;
+      for (int h = 0; h < 2; h++) {
+        const int j = jo + 8 * h;
+        float v[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          v[e] = (x < n && 4 * j + e < n) ? (float)fmax(acc[r][h][e], 0.0) : 0.f;
+        const float4 hi = make_float4(tf32_rna(v[0]), tf32_rna(v[1]), tf32_rna(v[2]), tf32_rna(v[3]));
+        const float4 lo = make_float4(tf32_rna(v[0] - hi.x), tf32_rna(v[1] - hi.y),
+                                      tf32_rna(v[2] - hi.z), tf32_rna(v[3] - hi.w));
+        const size_t o = (size_t)cc * 2 * per + ((size_t)j * kNP + x) * 4;
+        *reinterpret_cast<float4 *>(img + o) = hi;
+        *reinterpret_cast<float4 *>(img + o + per) = lo;
+      }
     }
   }
 }
