@@ -79,11 +79,12 @@ constexpr uint32_t kTipBytes61 = kTipRows61 * kTipRow61 * 4;  // 16,864 bytes
 // read 8 consecutive doubles.  A tip side's unknown-state row sums add the quads j and j + 8 in
 // the thread, then the 8 lanes of the row quad by a fixed shuffle tree: the same bits in every
 // launch.
-constexpr int kPrepThreads = 128;  // 16 row quads x 8 pairs of column quads
+// two halves of 128 threads (16 row quads x 8 pairs of column quads) take alternate categories
+constexpr int kPrepThreads = 256;
 __host__ __device__ constexpr size_t prep61_smem_doubles(int C) {
   return (size_t)C * kN + (size_t)kNP * kN + (size_t)kN * kNP;
 }
-__global__ void __launch_bounds__(kPrepThreads)
+__global__ void __launch_bounds__(kPrepThreads, 2)
     k_prep_ops_tc61(const __grid_constant__ TcJob one, const TcJob *__restrict__ jobs,
                     size_t stride_f) {
   extern __shared__ double ex[];
@@ -108,10 +109,12 @@ __global__ void __launch_bounds__(kPrepThreads)
   // the job's own table, written here and read by its traversal
   float *img = const_cast<float *>(job.tab) + (size_t)k * stride_f + (size_t)side * C * (kBSide / 4);
   const int per = kBImg / 4;  // floats of one image
-  // thread: row quad xq (rows 4xq..4xq+3) and the column quads jo and jo + 8
-  const int jo = threadIdx.x & 7, xq = threadIdx.x >> 3;
+  // thread: row quad xq (rows 4xq..4xq+3) and the column quads jo and jo + 8, in the half of
+  // the block that takes categories sub, sub + 2, ...
+  const int lt = threadIdx.x & 127, sub = threadIdx.x >> 7;
+  const int jo = lt & 7, xq = lt >> 3;
   const bool tip = (side ? op.r_kind : op.l_kind) == GEMS_CHILD_TIP;
-  for (int cc = 0; cc < C; cc++) {
+  for (int cc = sub; cc < C; cc += 2) {
     double acc[4][2][4];  // [row][column quad jo, jo + 8][column in quad]
 #pragma unroll
     for (int r = 0; r < 4; r++)
