@@ -815,8 +815,25 @@ static int traverse_batch_lists(gems_session *const *ss, int nsess, const gems_o
     for (int i = 0; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
     return GEMS_OK;
   }
-  for (int i = 0; i < nsess; i++)
-    if (int st = upload_ops(ss[i], ops[i], nops[i])) return st;
+  // one op list shared by every session (candidate models on one tree): validated and planned
+  // once, the plan copied to each session
+  bool shared = true;
+  for (int i = 1; i < nsess; i++)
+    shared = shared && ops[i] == ops[0] && ss[i]->desc.ntaxa == s0->desc.ntaxa &&
+             ss[i]->nops_max == s0->nops_max;
+  if (int st = upload_ops(s0, ops[0], nops[0])) return st;
+  for (int i = 1; i < nsess; i++) {
+    Session *s = ss[i];
+    if (!shared) {
+      if (int st = upload_ops(s, ops[i], nops[i])) return st;
+      continue;
+    }
+    GEMS_CUDA(cudaStreamSynchronize(s->stream));  // no kernel still reads its op table
+    std::memcpy(s->h_ops, s0->h_ops, sizeof(DevOp) * nops[0]);
+    s->plan_depth = s0->plan_depth;
+    GEMS_CUDA(cudaMemcpyAsync(s->d_ops, s->h_ops, sizeof(DevOp) * nops[0], cudaMemcpyHostToDevice,
+                              s->stream));
+  }
   // the batched launches (every session's op tables, then the traversal) run on the first
   // session's stream after every session's op list is on the device
   for (int i = 1; i < nsess; i++) GEMS_CUDA(cudaStreamSynchronize(ss[i]->stream));
